@@ -1,0 +1,195 @@
+/* lbx.h -- C ABI of the B200 lattice Boltzmann hot path (liblbx.so, sm_100a).
+ *
+ * This is the boundary a new single-GPU platform of the reference (OpenLB 1.8r1,
+ * src/core/platform) binds.  Every entry point names the reference interface it replaces
+ * (paths relative to the reference project).  Conventions:
+ *   - every function returns LBX_OK (0) or a negative lbx_status; lbx_last_error() gives a
+ *     thread-local message.  Nothing throws across the ABI.  The reference's CUDA platform
+ *     turns a failed call into std::runtime_error (gpu/cuda/device.hh:48-53); the C++ host
+ *     layer above this ABI does the same.
+ *   - device memory is owned by the lattice handle; host buffers are caller-owned and only
+ *     used during the call.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream); all
+ *     device work of a call is ordered on it.  One host thread drives one handle at a time;
+ *     calls on different handles are independent.
+ *   - no CPU fallback: without a usable sm_100 device lbx_lattice_create fails with
+ *     LBX_ERR_NO_DEVICE.
+ *
+ * Populations are exchanged in the reference convention: the stored value is f_i - w_i
+ * (src/dynamics/lbm.h:57-63, 296), descriptor ordering of src/descriptor/definition/common.h,
+ * host arrays laid out [q][core cells] with cell = (x * ny + y) * nz + z (z fastest, as
+ * BlockStructure orders cells, src/core/blockStructure.h:71).
+ */
+#ifndef LBX_H
+#define LBX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBX_ABI_VERSION 1
+
+typedef enum {
+  LBX_OK = 0,
+  LBX_ERR_INVALID = -1,     /* bad argument */
+  LBX_ERR_NO_DEVICE = -2,   /* no CUDA device of compute capability 10.x */
+  LBX_ERR_CUDA = -3,        /* a CUDA runtime call failed */
+  LBX_ERR_UNSUPPORTED = -4, /* combination not provided (reference: std::domain_error) */
+  LBX_ERR_OUT_OF_MEMORY = -5,
+  LBX_ERR_STATE = -6        /* call not valid in the handle's current state */
+} lbx_status;
+
+/* Velocity sets (src/descriptor/definition/common.h:76-109, 152-193, 345-400). */
+typedef enum { LBX_D2Q9 = 9, LBX_D3Q19 = 19, LBX_D3Q27 = 27 } lbx_descriptor;
+
+/* Population storage.  F16DEV / BF16DEV hold f_i - w_i in binary16 / bfloat16 with the
+ * collision in float registers; reductions are FP64 in every form. */
+typedef enum { LBX_F64 = 0, LBX_F32 = 1, LBX_F16DEV = 2, LBX_BF16DEV = 3 } lbx_storage;
+
+/* Bulk dynamics of a lattice (one per lattice; the per-cell map below selects it, plain
+ * bounce-back or no dynamics per cell). */
+typedef enum {
+  LBX_BGK = 1,                   /* BGKdynamics            dynamics/dynamics.h:89-99 */
+  LBX_TRT = 2,                   /* TRTdynamics            dynamics/dynamics.h:529-536 */
+  LBX_SMAGORINSKY_BGK = 3,       /* SmagorinskyBGKdynamics smagorinskyBGKdynamics.h:39-44 */
+  LBX_FORCED_BGK = 4,            /* ForcedBGKdynamics      dynamics/dynamics.h:223-230 */
+  LBX_SMAGORINSKY_FORCED_BGK = 5 /* SmagorinskyForcedBGKdynamics smagorinskyBGKdynamics.h:67-73 */
+} lbx_dynamics;
+
+/* Per-cell dynamics ids (the role of BlockDynamicsMap, core/blockDynamicsMap.h:264-416). */
+typedef enum {
+  LBX_CELL_NONE = 0,        /* NoDynamics (dynamics.h:51-63) */
+  LBX_CELL_BULK = 1,        /* the lattice's bulk dynamics */
+  LBX_CELL_BOUNCE_BACK = 2  /* BounceBack = collision::Revert (collision.h:465-484) */
+} lbx_cell_dynamics;
+
+/* Parameters of the bulk dynamics (the ParametersD fields OMEGA, TRT::MAGIC,
+ * LES::SMAGORINSKY and the FORCE field, here uniform over the lattice). */
+typedef struct {
+  double omega;        /* descriptors::OMEGA */
+  double magic;        /* collision::TRT::MAGIC (collision.h:382) */
+  double smagorinsky;  /* collision::LES::SMAGORINSKY (collisionLES.h:69) */
+  double force[3];     /* descriptors::FORCE, acceleration in lattice units */
+} lbx_params;
+
+typedef struct {
+  int32_t q, d;
+  int32_t core[3];       /* nx, ny, nz (nz = 1 in 2D) */
+  int32_t padded[3];     /* core + 2 * pad in each spatial direction (pad = 1; 2D: nz' = 1) */
+  int32_t pad;
+  int32_t periodic[3];
+  int32_t storage;
+  int64_t n_cells;       /* padded cell count = length of each population column */
+  int64_t n_core;        /* core cell count */
+  int64_t column_stride; /* elements between the starts of consecutive population columns */
+  int64_t bytes;         /* device bytes held by the handle */
+  int64_t n_links;       /* halfway bounce-back links */
+} lbx_info;
+
+typedef struct lbx_lattice_s* lbx_lattice;
+
+/* Thread-local message of the last failing call on this thread. */
+const char* lbx_last_error(void);
+int lbx_abi_version(void);
+/* Number of usable devices (compute capability 10.x); 0 without a GPU. */
+int lbx_device_count(void);
+
+/* Create a block lattice of `core` cells (ConcreteBlockLattice ctor, core/blockLattice.h:462;
+ * population storage ImplementationOf<AbstractCyclicColumn>, gpu/cuda/column.h:100-171).
+ * periodic[3] flags make the block periodic along that axis (CuboidDecomposition::
+ * setPeriodicity, geometry/cuboidDecomposition.hh:182 plus the PostCollide overlap copy,
+ * core/superLattice.hh:150-155).  Populations start at 0 (= rest equilibrium at rho = 1). */
+int lbx_lattice_create(int32_t q, const int32_t core[3], const int32_t periodic[3],
+                       int32_t storage, int32_t device, lbx_lattice* out);
+int lbx_lattice_destroy(lbx_lattice lattice);
+int lbx_get_info(lbx_lattice lattice, lbx_info* info);
+
+/* Select the bulk dynamics and its parameters (BlockDynamicsMap::set + setParameter,
+ * core/blockLattice.h:559-576; ConcreteParametersD H2D, gpu/cuda/context.hh:412-467). */
+int lbx_set_dynamics(lbx_lattice lattice, int32_t dynamics, const lbx_params* params);
+
+/* Per-cell dynamics ids for the core cells ([core cells], lbx_cell_dynamics); NULL resets
+ * to "bulk everywhere" (defineDynamics over a material, core/blockLattice.hh:274-286). */
+int lbx_set_cell_dynamics(lbx_lattice lattice, const uint8_t* ids);
+
+/* Halfway bounce-back links: BouzidiVelocityPostProcessor with q = 1/2
+ * (boundary/setBouzidiBoundary.h:129-162), applied after streaming.  Link l acts on core
+ * cell cells[l] (x_b) and direction dirs[l] (x_b + c_k is the solid neighbour); wall[l] is
+ * c_k . u_wall (BOUZIDI_VELOCITY, setBouzidiBoundary.h:386-410), NULL for resting walls.
+ * Replaces any previous link set.  n = 0 removes them. */
+int lbx_set_bouzidi_links(lbx_lattice lattice, int64_t n, const int64_t* cells,
+                          const int32_t* dirs, const double* wall);
+
+/* Host-side setter: derive the links from a material map exactly as setBouzidiBoundary
+ * (q = 1/2 fallback, setBouzidiBoundary.h:236-330) and setBouzidiVelocity (:386-410) do:
+ * for every cell whose material is in solid[0..n_solid) and every direction, a neighbour of
+ * material `fluid` gets a link; wall_velocity[j*3 + a] is the wall velocity of solid[j]
+ * (NULL: resting).  Runs on the host; needs no device work beyond the upload. */
+int lbx_set_bouzidi_from_materials(lbx_lattice lattice, const int32_t* material,
+                                   int32_t fluid, int32_t n_solid, const int32_t* solid,
+                                   const double* wall_velocity);
+/* The same derivation without a lattice (for host tools and tests); returns the link count
+ * through n_out and fills the arrays when they are not NULL (capacity `cap`). */
+int lbx_build_bouzidi_links(int32_t q, const int32_t core[3], const int32_t periodic[3],
+                            const int32_t* material, int32_t fluid, int32_t n_solid,
+                            const int32_t* solid, const double* wall_velocity,
+                            int64_t cap, int64_t* cells, int32_t* dirs, double* wall,
+                            int64_t* n_out);
+
+/* Populations of the core cells, host layout [q][core cells] of doubles (host_type 0) or
+ * floats (host_type 1), f_i - w_i.  The Simulation/Evaluation context switches of the
+ * population columns (gpu/cuda/column.hh:285-296), restricted to the core cells. */
+int lbx_upload_populations(lbx_lattice lattice, const void* host, int32_t host_type, void* stream);
+int lbx_download_populations(lbx_lattice lattice, void* host, int32_t host_type, void* stream);
+
+/* Equilibrium initialisation from moment fields (BlockLattice::iniEquilibrium,
+ * core/blockLattice.hh:201-219): rho [core cells], u [d][core cells], doubles. */
+int lbx_ini_equilibrium(lbx_lattice lattice, const double* rho, const double* u, void* stream);
+
+/* One or more fused collide-and-stream steps (SuperLattice::collideAndStream,
+ * core/superLattice.hh:664-725): collision of every core cell by its dynamics, the
+ * periodic overlap copy, the periodic-shift rotation of every population column
+ * (ConcreteBlockLattice::stream, core/blockLattice.hh:316-338) and the PostStream
+ * bounce-back links.  With LBX_STEP_STATISTICS the last step also accumulates the lattice
+ * statistics (StatisticsPostProcessor, gpu/cuda/statistics.hh:80-117) in FP64. */
+#define LBX_STEP_STATISTICS 1u
+int lbx_collide_and_stream(lbx_lattice lattice, int64_t steps, uint32_t flags, void* stream);
+
+/* Statistics of the last step run with LBX_STEP_STATISTICS: {average rho, average energy
+ * (= mean |u|^2 / 2), max |u|, cell count} (LatticeStatistics, core/latticeStatistics.hh:
+ * 60-90).  Synchronises the stream. */
+int lbx_get_statistics(lbx_lattice lattice, double out[4], void* stream);
+
+/* Moment fields of the core cells, FP64 (the functor path: BlockLatticeDensity/Velocity via
+ * cell.computeRhoU, functors/lattice/latticeVelocity3D.hh:66).  rho [core], u [d][core];
+ * either may be NULL.  Forced dynamics report u = j/rho + F/2 (momenta::ForcedMomentum). */
+int lbx_compute_moments(lbx_lattice lattice, double* rho, double* u, void* stream);
+
+/* FP64 device reductions over the cells with bulk dynamics (SuperLatticeFieldReductionO,
+ * core/superLatticeFieldReductionO.h; host functors SuperLpNorm3D, SuperLatticePhysDrag3D):
+ *   LBX_REDUCE_MASS_MOMENTUM  out = {sum rho, sum j_x, sum j_y, sum j_z}
+ *   LBX_REDUCE_DRAG           out = {F_x, F_y, F_z} momentum exchange over the links
+ *                             (BlockLatticePhysBoundaryForce3D, latticePhysBoundaryForce3D.hh:88-116)
+ *   LBX_REDUCE_RESIDUAL       out = {||u - u_prev||_2, ||u||_2, max |u - u_prev|} against
+ *                             the velocity snapshot of the previous RESIDUAL call, then
+ *                             refreshes the snapshot (ValueTracer-style convergence). */
+#define LBX_REDUCE_MASS_MOMENTUM 1
+#define LBX_REDUCE_DRAG 2
+#define LBX_REDUCE_RESIDUAL 3
+int lbx_reduce(lbx_lattice lattice, int32_t what, double* out, void* stream);
+
+/* Periodic-shift bookkeeping for a platform that keeps the reference's split collide /
+ * stream calls: the device base of population column i at the current shift
+ * (CyclicColumn::operator[] / deviceData, gpu/cuda/column.h:100-171) and a column rotation
+ * by `offset` cells (CyclicColumn::rotate, gpu/cuda/column.h:144-154). */
+int lbx_population_shift(lbx_lattice lattice, int32_t pop, int64_t* shift);
+int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

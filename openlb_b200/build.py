@@ -1,0 +1,93 @@
+"""Build recipe for liblbx.so (sm_100a) -- the CUDA library behind include/lbx.h.
+
+    python -m openlb_b200.build            # compile what changed
+    python -m openlb_b200.build --force    # rebuild everything
+
+Each .cu under csrc/ is compiled by nvcc for sm_100a only (no PTX for other targets) into
+openlb_b200/_build/, then linked into openlb_b200/lib/liblbx.so.  The FP64 instantiation
+unit is compiled with -fmad=false so its rounding matches the reference's CPU build.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "lib" / "liblbx.so"
+INCLUDE = PKG.parent / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+          "-Xptxas", "-warn-spills", "-I", str(INCLUDE), "-I", str(CSRC)]
+PER_UNIT = {"lbx_inst_f64.cu": ["-fmad=false"]}
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; liblbx.so needs the CUDA toolkit to build")
+    return cand
+
+
+def _sources() -> list[Path]:
+    return sorted(CSRC.glob("*.cu"))
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _compile(src: Path, verbose: bool) -> Path:
+    obj = BUILD / (src.stem + ".o")
+    cmd = [nvcc(), *ARCH, *COMMON, *PER_UNIT.get(src.name, []), "-c", str(src), "-o", str(obj)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{proc.stdout}\n{proc.stderr}")
+    if verbose and proc.stderr:
+        sys.stderr.write(proc.stderr)
+    return obj
+
+
+def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> Path:
+    """Compile changed units and (re)link liblbx.so; returns the library path."""
+    BUILD.mkdir(exist_ok=True)
+    LIB.parent.mkdir(exist_ok=True)
+    newest_header = max((p.stat().st_mtime for p in _headers()), default=0.0)
+    todo = []
+    for src in _sources():
+        obj = BUILD / (src.stem + ".o")
+        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header):
+            todo.append(src)
+    jobs = jobs or min(len(todo) or 1, os.cpu_count() or 4)
+    with ThreadPoolExecutor(max_workers=jobs) as pool:
+        list(pool.map(lambda s: _compile(s, verbose), todo))
+    objs = [BUILD / (s.stem + ".o") for s in _sources()]
+    if force or todo or not LIB.exists():
+        cmd = [nvcc(), *ARCH, "-shared", "--cudart", "static", "-o", str(LIB), *map(str, objs)]
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"link failed:\n{proc.stdout}\n{proc.stderr}")
+    return LIB
+
+
+def main(argv: list[str] | None = None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true", help="pass -Xptxas=-v (registers, spills)")
+    ap.add_argument("--jobs", type=int, default=None)
+    a = ap.parse_args(argv)
+    print(build(force=a.force, verbose=a.verbose, jobs=a.jobs))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

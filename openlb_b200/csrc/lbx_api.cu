@@ -1,0 +1,640 @@
+// C ABI of liblbx.so: lattice handles, host-side setters and the step driver.
+// The kernels live in lbx_kernels.cuh and are instantiated per storage type in
+// lbx_inst_*.cu.  See include/lbx.h for the contract of every entry point.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lbx.h"
+#include "lbx_kernels.cuh"
+
+using namespace lbx;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+
+#define LBX_CUDA_TRY(expr)                                                                   \
+  do {                                                                                       \
+    cudaError_t e_ = (expr);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? LBX_ERR_OUT_OF_MEMORY : LBX_ERR_CUDA,    \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+// Makes the lattice's device current for the duration of a call and restores the caller's.
+struct DeviceGuard {
+  int previous = -1;
+  bool ok = false;
+  explicit DeviceGuard(int device) {
+    if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+    ok = (previous == device) || (cudaSetDevice(device) == cudaSuccess);
+  }
+  ~DeviceGuard() {
+    if (previous >= 0) cudaSetDevice(previous);
+  }
+};
+
+size_t storage_bytes(int storage) {
+  switch (storage) {
+  case LBX_F64: return 8;
+  case LBX_F32: return 4;
+  case LBX_F16DEV: return 2;
+  case LBX_BF16DEV: return 2;
+  default: return 0;
+  }
+}
+
+const int* velocity(int q, int i) {
+  static const int c9[9][3] = {{0, 0, 0},  {-1, 1, 0}, {-1, 0, 0}, {-1, -1, 0}, {0, -1, 0},
+                               {1, -1, 0}, {1, 0, 0},  {1, 1, 0},  {0, 1, 0}};
+  switch (q) {
+  case 9: return c9[i];
+  case 19: return Desc<19>::C[i];
+  default: return Desc<27>::C[i];
+  }
+}
+int opposite(int q, int i) {
+  switch (q) {
+  case 9: return Desc<9>::OPP[i];
+  case 19: return Desc<19>::OPP[i];
+  default: return Desc<27>::OPP[i];
+  }
+}
+double weight_of(int q, int i) {
+  switch (q) {
+  case 9: return double(Desc<9>::WN[i]) / double(Desc<9>::WD[i]);
+  case 19: return double(Desc<19>::WN[i]) / double(Desc<19>::WD[i]);
+  default: return double(Desc<27>::WN[i]) / double(Desc<27>::WD[i]);
+  }
+}
+
+}  // namespace
+
+struct lbx_lattice_s {
+  int q = 0, d = 0, storage = 0, device = 0;
+  int core[3] = {1, 1, 1};
+  int padded[3] = {1, 1, 1};
+  int periodic[3] = {0, 0, 0};
+  int64_t n = 0, stride = 0, ncore = 0;
+  int64_t shift[27] = {};
+  void* pop = nullptr;
+  uint8_t* cellDyn = nullptr;
+  uint32_t* linkCell = nullptr;
+  uint8_t* linkDir = nullptr;
+  void* linkDelta = nullptr;
+  int64_t nLinks = 0;
+  StatAcc* stats = nullptr;
+  double* reduceAcc = nullptr;       // 8 doubles + 1 ull of scratch for reductions
+  float* residualSnap = nullptr;
+  void* stage = nullptr;             // ncore doubles
+  int dynamics = LBX_BGK;
+  lbx_params params{1.0, 0.25, 0.12, {0, 0, 0}};
+  int blockX = 256, blockY = 1;
+  int64_t bytes = 0;
+};
+
+namespace {
+
+Geometry geometry_of(const lbx_lattice_s* L) {
+  Geometry g;
+  g.n = L->n;
+  g.stride = L->stride;
+  g.sy = (L->d == 3) ? L->padded[2] : 1;
+  g.sx = int64_t(L->padded[1]) * ((L->d == 3) ? L->padded[2] : 1);
+  g.nx = L->core[0];
+  g.ny = L->core[1];
+  g.nz = (L->d == 3) ? L->core[2] : 1;
+  g.pz = (L->d == 3) ? 1 : 0;
+  g.pmask = (L->periodic[0] ? 1 : 0) | (L->periodic[1] ? 2 : 0) | ((L->d == 3 && L->periodic[2]) ? 4 : 0);
+  return g;
+}
+
+LaunchArgs args_of(const lbx_lattice_s* L) {
+  LaunchArgs a{};
+  a.pop = L->pop;
+  a.g = geometry_of(L);
+  for (int i = 0; i < L->q; ++i) a.shift[i] = L->shift[i];
+  a.dynamics = L->dynamics;
+  a.omega = L->params.omega;
+  a.magic = L->params.magic;
+  a.smagorinsky = L->params.smagorinsky;
+  for (int k = 0; k < 3; ++k) a.force[k] = L->params.force[k];
+  a.cellDyn = L->cellDyn;
+  a.stats = nullptr;
+  a.blockX = L->blockX;
+  a.blockY = L->blockY;
+  return a;
+}
+
+// Dispatch a launcher template on (Q, storage).
+#define LBX_DISPATCH(L, CALL)                                                                     \
+  [&]() -> cudaError_t {                                                                          \
+    switch ((L)->q * 4 + (L)->storage) {                                                          \
+    case 9 * 4 + LBX_F64: { constexpr int Q = 9; using S = double; return CALL; }                 \
+    case 9 * 4 + LBX_F32: { constexpr int Q = 9; using S = float; return CALL; }                  \
+    case 9 * 4 + LBX_F16DEV: { constexpr int Q = 9; using S = __half; return CALL; }              \
+    case 9 * 4 + LBX_BF16DEV: { constexpr int Q = 9; using S = __nv_bfloat16; return CALL; }      \
+    case 19 * 4 + LBX_F64: { constexpr int Q = 19; using S = double; return CALL; }               \
+    case 19 * 4 + LBX_F32: { constexpr int Q = 19; using S = float; return CALL; }                \
+    case 19 * 4 + LBX_F16DEV: { constexpr int Q = 19; using S = __half; return CALL; }            \
+    case 19 * 4 + LBX_BF16DEV: { constexpr int Q = 19; using S = __nv_bfloat16; return CALL; }    \
+    case 27 * 4 + LBX_F64: { constexpr int Q = 27; using S = double; return CALL; }               \
+    case 27 * 4 + LBX_F32: { constexpr int Q = 27; using S = float; return CALL; }                \
+    case 27 * 4 + LBX_F16DEV: { constexpr int Q = 27; using S = __half; return CALL; }            \
+    case 27 * 4 + LBX_BF16DEV: { constexpr int Q = 27; using S = __nv_bfloat16; return CALL; }    \
+    default: return cudaErrorInvalidValue;                                                        \
+    }                                                                                             \
+  }()
+
+int64_t core_index_to_padded(const lbx_lattice_s* L, int64_t c) {
+  const int nz = (L->d == 3) ? L->core[2] : 1;
+  const int64_t z = c % nz;
+  const int64_t y = (c / nz) % L->core[1];
+  const int64_t x = c / (int64_t(nz) * L->core[1]);
+  const Geometry g = geometry_of(L);
+  return (x + 1) * g.sx + (y + 1) * g.sy + (z + g.pz);
+}
+
+void rotate_all(lbx_lattice_s* L) {
+  const Geometry g = geometry_of(L);
+  for (int i = 0; i < L->q; ++i) {
+    const int* c = velocity(L->q, i);
+    const int64_t off = c[0] * g.sx + c[1] * g.sy + ((L->d == 3) ? c[2] : 0);
+    int64_t s = (L->shift[i] - off) % L->n;
+    if (s < 0) s += L->n;
+    L->shift[i] = s;
+  }
+}
+
+void default_block_shape(lbx_lattice_s* L) {
+  const int nf = (L->d == 3) ? L->core[2] : L->core[1];
+  int bx = 32;
+  while (bx < nf && bx < 256) bx *= 2;
+  L->blockX = bx;
+  L->blockY = 256 / bx;
+}
+
+int ensure_stage(lbx_lattice_s* L) {
+  if (!L->stage) LBX_CUDA_TRY(cudaMalloc(&L->stage, size_t(L->ncore) * sizeof(double)));
+  return LBX_OK;
+}
+
+bool device_ok(int device, std::string& why) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    why = "no CUDA device";
+    return false;
+  }
+  if (device < 0 || device >= count) {
+    why = "device index out of range";
+    return false;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+    why = "cudaGetDeviceProperties failed";
+    return false;
+  }
+  if (prop.major != 10) {
+    why = "device is compute capability " + std::to_string(prop.major) + "." + std::to_string(prop.minor) +
+          "; liblbx is built for sm_100a only";
+    return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* lbx_last_error(void) { return g_error.c_str(); }
+
+int lbx_abi_version(void) { return LBX_ABI_VERSION; }
+
+int lbx_device_count(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int usable = 0;
+  for (int d = 0; d < count; ++d) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) ++usable;
+  }
+  return usable;
+}
+
+int lbx_lattice_create(int32_t q, const int32_t core[3], const int32_t periodic[3], int32_t storage,
+                       int32_t device, lbx_lattice* out) {
+  if (!out || !core) return fail(LBX_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (q != 9 && q != 19 && q != 27) return fail(LBX_ERR_UNSUPPORTED, "descriptor must be D2Q9, D3Q19 or D3Q27");
+  if (storage_bytes(storage) == 0) return fail(LBX_ERR_INVALID, "unknown storage");
+  const int d = (q == 9) ? 2 : 3;
+  if (core[0] < 1 || core[1] < 1 || core[2] < 1) return fail(LBX_ERR_INVALID, "core extents must be >= 1");
+  if (d == 2 && core[2] != 1) return fail(LBX_ERR_INVALID, "D2Q9 lattices have core[2] == 1");
+  if (core[0] > 65535 || core[1] > 65535 * 256 || core[2] > (1 << 30))
+    return fail(LBX_ERR_INVALID, "core extent too large");
+  std::string why;
+  if (!device_ok(device, why)) return fail(LBX_ERR_NO_DEVICE, why);
+  DeviceGuard guard(device);
+  if (!guard.ok) return fail(LBX_ERR_CUDA, "cudaSetDevice failed");
+
+  auto* L = new lbx_lattice_s();
+  L->q = q;
+  L->d = d;
+  L->storage = storage;
+  L->device = device;
+  for (int a = 0; a < 3; ++a) {
+    L->core[a] = core[a];
+    L->periodic[a] = periodic ? (periodic[a] != 0) : 0;
+  }
+  if (d == 2) L->periodic[2] = 0;
+  L->padded[0] = core[0] + 2;
+  L->padded[1] = core[1] + 2;
+  L->padded[2] = (d == 3) ? core[2] + 2 : 1;
+  L->n = int64_t(L->padded[0]) * L->padded[1] * L->padded[2];
+  if (L->n >= (int64_t(1) << 32)) {
+    delete L;
+    return fail(LBX_ERR_INVALID, "padded block exceeds 2^32 cells");
+  }
+  L->ncore = int64_t(core[0]) * core[1] * core[2];
+  L->stride = (L->n + 127) / 128 * 128;
+  default_block_shape(L);
+  const size_t popBytes = size_t(q) * size_t(L->stride) * storage_bytes(storage);
+  cudaError_t e = cudaMalloc(&L->pop, popBytes);
+  if (e == cudaSuccess) e = cudaMemset(L->pop, 0, popBytes);
+  if (e == cudaSuccess) e = cudaMalloc(&L->stats, sizeof(StatAcc));
+  if (e == cudaSuccess) e = cudaMemset(L->stats, 0, sizeof(StatAcc));
+  if (e == cudaSuccess) e = cudaMalloc(&L->reduceAcc, 8 * sizeof(double) + sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    const std::string msg = std::string("allocation failed: ") + cudaGetErrorString(e);
+    cudaFree(L->pop);
+    cudaFree(L->stats);
+    cudaFree(L->reduceAcc);
+    delete L;
+    return fail(e == cudaErrorMemoryAllocation ? LBX_ERR_OUT_OF_MEMORY : LBX_ERR_CUDA, msg);
+  }
+  L->bytes = int64_t(popBytes);
+  *out = L;
+  return LBX_OK;
+}
+
+int lbx_lattice_destroy(lbx_lattice L) {
+  if (!L) return LBX_OK;
+  DeviceGuard guard(L->device);
+  cudaFree(L->pop);
+  cudaFree(L->cellDyn);
+  cudaFree(L->linkCell);
+  cudaFree(L->linkDir);
+  cudaFree(L->linkDelta);
+  cudaFree(L->stats);
+  cudaFree(L->reduceAcc);
+  cudaFree(L->residualSnap);
+  cudaFree(L->stage);
+  delete L;
+  return LBX_OK;
+}
+
+int lbx_get_info(lbx_lattice L, lbx_info* info) {
+  if (!L || !info) return fail(LBX_ERR_INVALID, "null argument");
+  std::memset(info, 0, sizeof(*info));
+  info->q = L->q;
+  info->d = L->d;
+  for (int a = 0; a < 3; ++a) {
+    info->core[a] = L->core[a];
+    info->padded[a] = L->padded[a];
+    info->periodic[a] = L->periodic[a];
+  }
+  info->pad = 1;
+  info->storage = L->storage;
+  info->n_cells = L->n;
+  info->n_core = L->ncore;
+  info->column_stride = L->stride;
+  info->bytes = L->bytes;
+  info->n_links = L->nLinks;
+  return LBX_OK;
+}
+
+int lbx_set_dynamics(lbx_lattice L, int32_t dynamics, const lbx_params* params) {
+  if (!L || !params) return fail(LBX_ERR_INVALID, "null argument");
+  if (dynamics < LBX_BGK || dynamics > LBX_SMAGORINSKY_FORCED_BGK) return fail(LBX_ERR_UNSUPPORTED, "unknown dynamics");
+  if (!(params->omega > 0.0 && params->omega < 2.0)) return fail(LBX_ERR_INVALID, "omega must lie in (0, 2)");
+  if (dynamics == LBX_TRT && !(params->magic > 0.0)) return fail(LBX_ERR_INVALID, "TRT magic parameter must be > 0");
+  if ((dynamics == LBX_SMAGORINSKY_BGK || dynamics == LBX_SMAGORINSKY_FORCED_BGK) && !(params->smagorinsky >= 0.0))
+    return fail(LBX_ERR_INVALID, "Smagorinsky constant must be >= 0");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(params->force[k])) return fail(LBX_ERR_INVALID, "force must be finite");
+  L->dynamics = dynamics;
+  L->params = *params;
+  return LBX_OK;
+}
+
+int lbx_set_cell_dynamics(lbx_lattice L, const uint8_t* ids) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  DeviceGuard guard(L->device);
+  if (!ids) {
+    cudaFree(L->cellDyn);
+    L->cellDyn = nullptr;
+    return LBX_OK;
+  }
+  std::vector<uint8_t> padded(static_cast<size_t>(L->n), 0);
+  for (int64_t c = 0; c < L->ncore; ++c) {
+    if (ids[c] > LBX_CELL_BOUNCE_BACK) return fail(LBX_ERR_INVALID, "cell dynamics id out of range");
+    padded[size_t(core_index_to_padded(L, c))] = ids[c];
+  }
+  if (!L->cellDyn) LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
+  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, padded.data(), size_t(L->n), cudaMemcpyHostToDevice));
+  return LBX_OK;
+}
+
+int lbx_set_bouzidi_links(lbx_lattice L, int64_t n, const int64_t* cells, const int32_t* dirs, const double* wall) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (n < 0 || (n > 0 && (!cells || !dirs))) return fail(LBX_ERR_INVALID, "bad link arrays");
+  DeviceGuard guard(L->device);
+  cudaFree(L->linkCell);
+  cudaFree(L->linkDir);
+  cudaFree(L->linkDelta);
+  L->linkCell = nullptr;
+  L->linkDir = nullptr;
+  L->linkDelta = nullptr;
+  L->nLinks = 0;
+  if (n == 0) return LBX_OK;
+  std::vector<uint32_t> hc(static_cast<size_t>(n));
+  std::vector<uint8_t> hd(static_cast<size_t>(n));
+  std::vector<double> delta(static_cast<size_t>(n));
+  bool anyWall = false;
+  for (int64_t l = 0; l < n; ++l) {
+    if (cells[l] < 0 || cells[l] >= L->ncore) return fail(LBX_ERR_INVALID, "link cell out of range");
+    if (dirs[l] < 1 || dirs[l] >= L->q) return fail(LBX_ERR_INVALID, "link direction out of range");
+    hc[size_t(l)] = uint32_t(core_index_to_padded(L, cells[l]));
+    hd[size_t(l)] = uint8_t(dirs[l]);
+    // 2 * veloTerm, veloTerm = (c_k . u_w) * t_k * invCs2 (setBouzidiBoundary.h:146)
+    delta[size_t(l)] = wall ? 2.0 * (wall[l] * weight_of(L->q, dirs[l]) * 3.0) : 0.0;
+    if (delta[size_t(l)] != 0.0) anyWall = true;
+  }
+  LBX_CUDA_TRY(cudaMalloc(&L->linkCell, size_t(n) * sizeof(uint32_t)));
+  LBX_CUDA_TRY(cudaMalloc(&L->linkDir, size_t(n)));
+  LBX_CUDA_TRY(cudaMemcpy(L->linkCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->linkDir, hd.data(), size_t(n), cudaMemcpyHostToDevice));
+  if (anyWall) {
+    if (L->storage == LBX_F64) {
+      LBX_CUDA_TRY(cudaMalloc(&L->linkDelta, size_t(n) * sizeof(double)));
+      LBX_CUDA_TRY(cudaMemcpy(L->linkDelta, delta.data(), size_t(n) * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> df(delta.begin(), delta.end());
+      LBX_CUDA_TRY(cudaMalloc(&L->linkDelta, size_t(n) * sizeof(float)));
+      LBX_CUDA_TRY(cudaMemcpy(L->linkDelta, df.data(), size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  }
+  L->nLinks = n;
+  return LBX_OK;
+}
+
+int lbx_build_bouzidi_links(int32_t q, const int32_t core[3], const int32_t periodic[3], const int32_t* material,
+                            int32_t fluid, int32_t n_solid, const int32_t* solid, const double* wall_velocity,
+                            int64_t cap, int64_t* cells, int32_t* dirs, double* wall, int64_t* n_out) {
+  if (!core || !material || !n_out || (n_solid > 0 && !solid)) return fail(LBX_ERR_INVALID, "null argument");
+  if (q != 9 && q != 19 && q != 27) return fail(LBX_ERR_UNSUPPORTED, "descriptor must be D2Q9, D3Q19 or D3Q27");
+  const int d = (q == 9) ? 2 : 3;
+  const int64_t nx = core[0], ny = core[1], nz = (d == 3) ? core[2] : 1;
+  if (nx < 1 || ny < 1 || nz < 1) return fail(LBX_ERR_INVALID, "core extents must be >= 1");
+  int64_t count = 0;
+  for (int64_t x = 0; x < nx; ++x)
+    for (int64_t y = 0; y < ny; ++y)
+      for (int64_t z = 0; z < nz; ++z) {
+        const int64_t cb = (x * ny + y) * nz + z;
+        if (material[cb] != fluid) continue;
+        for (int k = 1; k < q; ++k) {
+          const int* c = velocity(q, k);
+          int64_t s[3] = {x + c[0], y + c[1], z + ((d == 3) ? c[2] : 0)};
+          const int64_t ext[3] = {nx, ny, nz};
+          bool inside = true;
+          for (int a = 0; a < d; ++a) {
+            if (s[a] < 0 || s[a] >= ext[a]) {
+              if (periodic && periodic[a]) s[a] = (s[a] + ext[a]) % ext[a];
+              else inside = false;
+            }
+          }
+          if (!inside) continue;
+          const int64_t cs = (s[0] * ny + s[1]) * nz + s[2];
+          int which = -1;
+          for (int j = 0; j < n_solid; ++j)
+            if (material[cs] == solid[j]) { which = j; break; }
+          if (which < 0) continue;
+          if (count < cap) {
+            if (cells) cells[count] = cb;
+            if (dirs) dirs[count] = k;
+            if (wall) {
+              double cu = 0.0;
+              if (wall_velocity)
+                for (int a = 0; a < d; ++a) cu += c[a] * wall_velocity[which * 3 + a];
+              wall[count] = cu;
+            }
+          }
+          ++count;
+        }
+      }
+  *n_out = count;
+  return LBX_OK;
+}
+
+int lbx_set_bouzidi_from_materials(lbx_lattice L, const int32_t* material, int32_t fluid, int32_t n_solid,
+                                   const int32_t* solid, const double* wall_velocity) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  int64_t n = 0;
+  int rc = lbx_build_bouzidi_links(L->q, L->core, L->periodic, material, fluid, n_solid, solid, wall_velocity, 0,
+                                   nullptr, nullptr, nullptr, &n);
+  if (rc != LBX_OK) return rc;
+  std::vector<int64_t> cells(static_cast<size_t>(n));
+  std::vector<int32_t> dirs(static_cast<size_t>(n));
+  std::vector<double> wall(static_cast<size_t>(n));
+  rc = lbx_build_bouzidi_links(L->q, L->core, L->periodic, material, fluid, n_solid, solid, wall_velocity, n,
+                               cells.data(), dirs.data(), wall.data(), &n);
+  if (rc != LBX_OK) return rc;
+  return lbx_set_bouzidi_links(L, n, cells.data(), dirs.data(), wall_velocity ? wall.data() : nullptr);
+}
+
+int lbx_upload_populations(lbx_lattice L, const void* host, int32_t host_type, void* stream) {
+  if (!L || !host) return fail(LBX_ERR_INVALID, "null argument");
+  if (host_type != 0 && host_type != 1) return fail(LBX_ERR_INVALID, "host_type must be 0 (double) or 1 (float)");
+  DeviceGuard guard(L->device);
+  if (int rc = ensure_stage(L)) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const LaunchArgs a = args_of(L);
+  const size_t es = host_type == 0 ? sizeof(double) : sizeof(float);
+  for (int i = 0; i < L->q; ++i) {
+    const char* src = static_cast<const char*>(host) + size_t(i) * size_t(L->ncore) * es;
+    LBX_CUDA_TRY(cudaMemcpyAsync(L->stage, src, size_t(L->ncore) * es, cudaMemcpyHostToDevice, s));
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_transfer<Q, S>(a, i, L->stage, host_type, true, s))));
+  }
+  return LBX_OK;
+}
+
+int lbx_download_populations(lbx_lattice L, void* host, int32_t host_type, void* stream) {
+  if (!L || !host) return fail(LBX_ERR_INVALID, "null argument");
+  if (host_type != 0 && host_type != 1) return fail(LBX_ERR_INVALID, "host_type must be 0 (double) or 1 (float)");
+  DeviceGuard guard(L->device);
+  if (int rc = ensure_stage(L)) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const LaunchArgs a = args_of(L);
+  const size_t es = host_type == 0 ? sizeof(double) : sizeof(float);
+  for (int i = 0; i < L->q; ++i) {
+    char* dst = static_cast<char*>(host) + size_t(i) * size_t(L->ncore) * es;
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_transfer<Q, S>(a, i, L->stage, host_type, false, s))));
+    LBX_CUDA_TRY(cudaMemcpyAsync(dst, L->stage, size_t(L->ncore) * es, cudaMemcpyDeviceToHost, s));
+  }
+  LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  return LBX_OK;
+}
+
+int lbx_ini_equilibrium(lbx_lattice L, const double* rho, const double* u, void* stream) {
+  if (!L || !rho || !u) return fail(LBX_ERR_INVALID, "null argument");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t nb = size_t(L->ncore) * sizeof(double);
+  double* dev = nullptr;
+  LBX_CUDA_TRY(cudaMalloc(&dev, nb * size_t(1 + L->d)));
+  cudaError_t e = cudaMemcpyAsync(dev, rho, nb, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dev + L->ncore, u, nb * size_t(L->d), cudaMemcpyHostToDevice, s);
+  const LaunchArgs a = args_of(L);
+  if (e == cudaSuccess) e = LBX_DISPATCH(L, (launch_ini_equilibrium<Q, S>(a, dev, dev + L->ncore, s)));
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dev);
+  LBX_CUDA_TRY(e);
+  return LBX_OK;
+}
+
+int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* stream) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (steps < 0) return fail(LBX_ERR_INVALID, "steps must be >= 0");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  for (int64_t k = 0; k < steps; ++k) {
+    LaunchArgs a = args_of(L);
+    if ((flags & LBX_STEP_STATISTICS) && k == steps - 1) {
+      LBX_CUDA_TRY(cudaMemsetAsync(L->stats, 0, sizeof(StatAcc), s));
+      a.stats = L->stats;
+    }
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_step<Q, S>(a, s))));
+    rotate_all(L);
+    if (L->nLinks > 0) {
+      const LaunchArgs b = args_of(L);
+      LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
+    }
+  }
+  return LBX_OK;
+}
+
+int lbx_get_statistics(lbx_lattice L, double out[4], void* stream) {
+  if (!L || !out) return fail(LBX_ERR_INVALID, "null argument");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  StatAcc h;
+  LBX_CUDA_TRY(cudaMemcpyAsync(&h, L->stats, sizeof(StatAcc), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  double mx;
+  std::memcpy(&mx, &h.maxbits, sizeof(double));
+  const double cnt = double(h.count);
+  out[0] = h.count ? h.sum[0] / cnt : 1.0;
+  out[1] = h.count ? 0.5 * h.sum[1] / cnt : 1.0;
+  out[2] = std::sqrt(mx);
+  out[3] = cnt;
+  return LBX_OK;
+}
+
+int lbx_compute_moments(lbx_lattice L, double* rho, double* u, void* stream) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (!rho && !u) return LBX_OK;
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t nb = size_t(L->ncore) * sizeof(double);
+  double* dev = nullptr;
+  LBX_CUDA_TRY(cudaMalloc(&dev, nb * size_t(1 + L->d)));
+  const LaunchArgs a = args_of(L);
+  cudaError_t e = LBX_DISPATCH(L, (launch_moments<Q, S>(a, dev, dev + L->ncore, s)));
+  if (e == cudaSuccess && rho) e = cudaMemcpyAsync(rho, dev, nb, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && u) e = cudaMemcpyAsync(u, dev + L->ncore, nb * size_t(L->d), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dev);
+  LBX_CUDA_TRY(e);
+  return LBX_OK;
+}
+
+int lbx_reduce(lbx_lattice L, int32_t what, double* out, void* stream) {
+  if (!L || !out) return fail(LBX_ERR_INVALID, "null argument");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const LaunchArgs a = args_of(L);
+  double h[8] = {};
+  unsigned long long mb = 0;
+  unsigned long long* maxbits = reinterpret_cast<unsigned long long*>(L->reduceAcc + 8);
+  LBX_CUDA_TRY(cudaMemsetAsync(L->reduceAcc, 0, 8 * sizeof(double) + sizeof(unsigned long long), s));
+  switch (what) {
+  case LBX_REDUCE_MASS_MOMENTUM:
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_mass_momentum<Q, S>(a, L->reduceAcc, s))));
+    break;
+  case LBX_REDUCE_DRAG:
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_link_force<Q, S>(a, L->linkCell, L->linkDir, L->nLinks, L->reduceAcc, s))));
+    break;
+  case LBX_REDUCE_RESIDUAL:
+    if (!L->residualSnap) {
+      LBX_CUDA_TRY(cudaMalloc(&L->residualSnap, size_t(L->ncore) * size_t(L->d) * sizeof(float)));
+      LBX_CUDA_TRY(cudaMemsetAsync(L->residualSnap, 0, size_t(L->ncore) * size_t(L->d) * sizeof(float), s));
+    }
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_residual<Q, S>(a, L->residualSnap, L->reduceAcc, maxbits, s))));
+    break;
+  default:
+    return fail(LBX_ERR_INVALID, "unknown reduction");
+  }
+  LBX_CUDA_TRY(cudaMemcpyAsync(h, L->reduceAcc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaMemcpyAsync(&mb, maxbits, sizeof(mb), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  switch (what) {
+  case LBX_REDUCE_MASS_MOMENTUM:
+    for (int k = 0; k < 4; ++k) out[k] = h[k];
+    break;
+  case LBX_REDUCE_DRAG:
+    for (int k = 0; k < 3; ++k) out[k] = h[k];
+    break;
+  default: {
+    double m;
+    std::memcpy(&m, &mb, sizeof(double));
+    out[0] = std::sqrt(h[0]);
+    out[1] = std::sqrt(h[1]);
+    out[2] = m;
+  }
+  }
+  return LBX_OK;
+}
+
+int lbx_population_shift(lbx_lattice L, int32_t pop, int64_t* shift) {
+  if (!L || !shift) return fail(LBX_ERR_INVALID, "null argument");
+  if (pop < 0 || pop >= L->q) return fail(LBX_ERR_INVALID, "population index out of range");
+  *shift = L->shift[pop];
+  return LBX_OK;
+}
+
+int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (pop < 0 || pop >= L->q) return fail(LBX_ERR_INVALID, "population index out of range");
+  int64_t s = (L->shift[pop] - offset) % L->n;
+  if (s < 0) s += L->n;
+  L->shift[pop] = s;
+  return LBX_OK;
+}
+
+}  // extern "C"

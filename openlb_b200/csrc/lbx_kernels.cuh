@@ -1,0 +1,556 @@
+// Kernels of the B200 lattice Boltzmann hot path.
+//
+// Storage (HBM): one population column per direction, Q columns of `stride` elements, each
+// column a cyclic array over the N cells of the padded block (pad = 1).  Cell index
+// n = (x+1)*sx + (y+1)*sy + (z+pz) (z fastest; 2D: sy = 1, pz = 0), as the reference's
+// BlockStructure orders cells (src/core/blockStructure.h:71).  Population i of cell n lives
+// at column_i[(n + shift_i) mod N]: the periodic-shift (PS) pattern of the reference's
+// CyclicColumn (src/core/platform/cpu/sisd/column.h:128-221, gpu/cuda/column.h:100-171).
+// Streaming is the rotation shift_i -= c_i . (sx, sy, 1) done on the host between launches
+// (ConcreteBlockLattice::stream, core/blockLattice.hh:316-338): no population moves.
+//
+// The fused step kernel therefore reads and writes every population of a core cell exactly
+// once, in place (2 Q elements per lattice update).  On periodic axes the ghost layer has to
+// carry the post-collision populations of the opposite face before the rotation (the
+// reference's PostCollide overlap copy, core/superLattice.hh:150-155, gpu/cuda/
+// communicator.hh:111-124); the step kernel writes those few values itself, so a periodic
+// step is a single launch.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "lbx_collision.cuh"
+
+namespace lbx {
+
+// ---- storage formats -----------------------------------------------------------------
+template <typename S> struct Storage;
+template <> struct Storage<double> {
+  using R = double;
+  static __device__ __forceinline__ R load(const double* p) { return *p; }
+  static __device__ __forceinline__ void store(double* p, R v) { *p = v; }
+};
+template <> struct Storage<float> {
+  using R = float;
+  static __device__ __forceinline__ R load(const float* p) { return *p; }
+  static __device__ __forceinline__ void store(float* p, R v) { *p = v; }
+};
+template <> struct Storage<__half> {
+  using R = float;
+  static __device__ __forceinline__ R load(const __half* p) { return __half2float(*p); }
+  static __device__ __forceinline__ void store(__half* p, R v) { *p = __float2half_rn(v); }
+};
+template <> struct Storage<__nv_bfloat16> {
+  using R = float;
+  static __device__ __forceinline__ R load(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+  static __device__ __forceinline__ void store(__nv_bfloat16* p, R v) { *p = __float2bfloat16_rn(v); }
+};
+
+// ---- geometry of one lattice as the kernels see it -------------------------------------
+struct Geometry {
+  int64_t n;       // padded cells N (column length)
+  int64_t stride;  // elements between column starts
+  int64_t sx, sy;  // padded strides of x and y (z stride 1)
+  int32_t nx, ny, nz;
+  int32_t pz;      // 1 in 3D (z is padded), 0 in 2D
+  int32_t pmask;   // periodic axes, bit a for axis a
+};
+
+template <int Q>
+struct Shifts {
+  int64_t s[Q];
+};
+
+__device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t s, int64_t n) {
+  const int64_t r = a + s;
+  return r >= n ? r - n : r;
+}
+
+// Statistics accumulator: {sum rho, sum |u|^2} in FP64, {count, max |u|^2 bits}.
+struct StatAcc {
+  double sum[2];
+  unsigned long long count;
+  unsigned long long maxbits;
+};
+
+template <typename R>
+__device__ __forceinline__ void block_stats(R rho, R usq, bool valid, StatAcc* acc) {
+  double a = valid ? double(rho) : 0.0;
+  double b = valid ? double(usq) : 0.0;
+  double m = valid ? double(usq) : 0.0;
+  unsigned int c = valid ? 1u : 0u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  __shared__ double sa[32], sb[32], sm[32];
+  __shared__ unsigned int sc[32];
+  const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+  const int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  if (lane == 0) { sa[warp] = a; sb[warp] = b; sm[warp] = m; sc[warp] = c; }
+  __syncthreads();
+  if (warp == 0) {
+    a = lane < nwarps ? sa[lane] : 0.0;
+    b = lane < nwarps ? sb[lane] : 0.0;
+    m = lane < nwarps ? sm[lane] : 0.0;
+    c = lane < nwarps ? sc[lane] : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (lane == 0 && c > 0) {
+      atomicAdd(&acc->sum[0], a);
+      atomicAdd(&acc->sum[1], b);
+      atomicAdd(&acc->count, (unsigned long long)c);
+      atomicMax(&acc->maxbits, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// ---- fused collide + PS stream --------------------------------------------------------
+// One thread per core cell; threadIdx.x runs along the fastest core axis (z in 3D, y in 2D)
+// so that every population load and store of a warp is one contiguous run.
+template <int Q, typename S, int DYN>
+__global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                        CollisionParams<typename Storage<S>::R> p,
+                                                        const uint8_t* __restrict__ cellDyn,
+                                                        StatAcc* __restrict__ stats) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  int x, y, z;
+  bool inside;
+  {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y * blockDim.y + threadIdx.y;
+    if constexpr (D::d == 3) {
+      z = f; y = m; x = blockIdx.z;
+      inside = z < g.nz && y < g.ny;
+    } else {
+      y = f; x = m; z = 0;
+      inside = y < g.ny && x < g.nx;
+    }
+  }
+  R rho = R(-1), usq = R(-1);
+  bool valid = false;
+  if (inside) {
+    const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+    const uint8_t kind = cellDyn ? cellDyn[n] : uint8_t(1);
+    R f[Q];
+    const bool needPops = kind != 0 || g.pmask != 0;
+    if (needPops) {
+      static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
+    }
+    if (kind == 1) {
+      collide<Q, R, DYN>(f, p, rho, usq);
+      valid = true;
+    } else if (kind == 2) {
+      revert<Q, R>(f);
+    }
+    if (kind != 0) {
+      static_for<Q>([&](auto I) { Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), f[I]); });
+    }
+
+    // periodic overlap: post-collision values that leave the core across a periodic face are
+    // written into the ghost cell from which the rotation will carry them into the opposite face
+    if (g.pmask) {
+      const bool edge = ((g.pmask & 1) && (x == 0 || x == g.nx - 1)) ||
+                        ((g.pmask & 2) && (y == 0 || y == g.ny - 1)) ||
+                        (D::d == 3 && (g.pmask & 4) && (z == 0 || z == g.nz - 1));
+      if (edge) {
+        static_for<Q>([&](auto I) {
+          constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+          int tx = x + cx, ty = y + cy, tz = z + cz;
+          bool crossed = false, lost = false;
+          if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+          if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+          if constexpr (D::d == 3) {
+            if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+          }
+          if (crossed && !lost) {
+            const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+            Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
+          }
+        });
+      }
+    }
+  }
+
+  if (stats) block_stats<R>(rho, usq, valid, stats);
+}
+
+// ---- halfway bounce-back links (PostStream) ---------------------------------------------
+// f_opp(k)(x_b) = f_k(x_b + c_k) - delta, delta = 2 (c_k . u_w) t_k / c_s^2.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_bouzidi(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                 const uint32_t* __restrict__ cell,
+                                                 const uint8_t* __restrict__ dir,
+                                                 const typename Storage<S>::R* __restrict__ delta,
+                                                 int64_t nLinks) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (l >= nLinks) return;
+  const int64_t xb = cell[l];
+  const int k = dir[l];
+  int64_t off = 0;
+  int kopp = 0;
+  static_for<Q>([&](auto I) {
+    if (I == k) {
+      off = D::C[I][0] * g.sx + D::C[I][1] * g.sy + D::C[I][2];
+      kopp = D::OPP[I];
+    }
+  });
+  const int64_t xs = xb + off;
+  const R v = Storage<S>::load(pop + int64_t(k) * g.stride + wrap_add(xs, sh.s[k], g.n));
+  Storage<S>::store(pop + int64_t(kopp) * g.stride + wrap_add(xb, sh.s[kopp], g.n),
+                    v - (delta ? delta[l] : R(0)));
+}
+
+// ---- host <-> column transfers (one population at a time through a staging buffer) -----
+template <typename S, typename H>
+__global__ void k_scatter_pop(S* __restrict__ col, Geometry g, int64_t shift, const H* __restrict__ src) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t ncore = int64_t(g.nx) * g.ny * g.nz;
+  if (c >= ncore) return;
+  const int z = int(c % g.nz);
+  const int y = int((c / g.nz) % g.ny);
+  const int x = int(c / (int64_t(g.nz) * g.ny));
+  const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+  Storage<S>::store(col + wrap_add(n, shift, g.n), typename Storage<S>::R(src[c]));
+}
+
+template <typename S, typename H>
+__global__ void k_gather_pop(const S* __restrict__ col, Geometry g, int64_t shift, H* __restrict__ dst) {
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t ncore = int64_t(g.nx) * g.ny * g.nz;
+  if (c >= ncore) return;
+  const int z = int(c % g.nz);
+  const int y = int((c / g.nz) % g.ny);
+  const int x = int(c / (int64_t(g.nz) * g.ny));
+  const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+  dst[c] = H(Storage<S>::load(col + wrap_add(n, shift, g.n)));
+}
+
+// f^eq - w from moment fields (BlockLattice::iniEquilibrium, core/blockLattice.hh:201-219)
+template <int Q, typename S>
+__global__ void k_ini_equilibrium(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                  const double* __restrict__ rho, const double* __restrict__ u) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t ncore = int64_t(g.nx) * g.ny * g.nz;
+  if (c >= ncore) return;
+  const int z = int(c % g.nz);
+  const int y = int((c / g.nz) % g.ny);
+  const int x = int(c / (int64_t(g.nz) * g.ny));
+  const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+  const R r = R(rho[c]);
+  R uu[3] = {R(0), R(0), R(0)};
+  static_for<D::d>([&](auto A) { uu[A] = R(u[A * ncore + c]); });
+  R usq = R(0);
+  static_for<D::d>([&](auto A) { usq += uu[A] * uu[A]; });
+  static_for<Q>([&](auto I) {
+    Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), equilibrium<Q, I>(r, uu, usq));
+  });
+}
+
+// rho and u of every core cell, FP64 out (forced dynamics: u = j/rho + F/2)
+template <int Q, typename S>
+__global__ void k_moments(const S* __restrict__ pop, Geometry g, Shifts<Q> sh, int forced,
+                          double fx, double fy, double fz, double* __restrict__ rho,
+                          double* __restrict__ u) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t ncore = int64_t(g.nx) * g.ny * g.nz;
+  if (c >= ncore) return;
+  const int z = int(c % g.nz);
+  const int y = int((c / g.nz) % g.ny);
+  const int x = int(c / (int64_t(g.nz) * g.ny));
+  const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+  R f[Q];
+  static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
+  R r, uu[3];
+  const R F[3] = {R(fx), R(fy), R(fz)};
+  if (forced) moments<Q, R, true>(f, F, r, uu);
+  else moments<Q, R, false>(f, F, r, uu);
+  if (rho) rho[c] = double(r);
+  if (u) static_for<D::d>([&](auto A) { u[A * ncore + c] = double(uu[A]); });
+}
+
+// FP64 mass and momentum over the bulk cells: acc = {sum rho, sum j_x, sum j_y, sum j_z}
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_mass_momentum(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                       const uint8_t* __restrict__ cellDyn,
+                                                       double* __restrict__ acc) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t ncore = int64_t(g.nx) * g.ny * g.nz;
+  double v[4] = {0, 0, 0, 0};
+  if (c < ncore) {
+    const int z = int(c % g.nz);
+    const int y = int((c / g.nz) % g.ny);
+    const int x = int(c / (int64_t(g.nz) * g.ny));
+    const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+    if (!cellDyn || cellDyn[n] == 1) {
+      double r = 1.0;
+      static_for<Q>([&](auto I) {
+        const double fi = double(Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)));
+        r += fi;
+        static_for<D::d>([&](auto A) {
+          constexpr int cc = D::C[I][A];
+          if constexpr (cc != 0) v[1 + A] += cc * fi;
+        });
+      });
+      v[0] = r;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    double a = v[k];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(&acc[k], a);
+  }
+}
+
+// Momentum exchange over the bounce-back links after the PostStream step:
+// F = sum_links c_k (f~_k(x_b) + f_opp(k)(x_b)), f~_k(x_b) = the post-collision population
+// that streamed into the solid neighbour (now held there).  Full populations (f - w + w).
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_link_force(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                    const uint32_t* __restrict__ cell,
+                                                    const uint8_t* __restrict__ dir, int64_t nLinks,
+                                                    double* __restrict__ acc) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double fx = 0, fy = 0, fz = 0;
+  if (l < nLinks) {
+    const int64_t xb = cell[l];
+    const int k = dir[l];
+    int64_t off = 0;
+    int kopp = 0;
+    double cx = 0, cy = 0, cz = 0, w = 0;
+    static_for<Q>([&](auto I) {
+      if (I == k) {
+        off = D::C[I][0] * g.sx + D::C[I][1] * g.sy + D::C[I][2];
+        kopp = D::OPP[I];
+        cx = D::C[I][0]; cy = D::C[I][1]; cz = D::C[I][2];
+        w = weight<Q, double>(I);
+      }
+    });
+    const double fin = double(Storage<S>::load(pop + int64_t(k) * g.stride + wrap_add(xb + off, sh.s[k], g.n))) + w;
+    const double fout = double(Storage<S>::load(pop + int64_t(kopp) * g.stride + wrap_add(xb, sh.s[kopp], g.n))) + w;
+    const double s = fin + fout;
+    fx = cx * s; fy = cy * s; fz = cz * s;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc[0], fx);
+    atomicAdd(&acc[1], fy);
+    atomicAdd(&acc[2], fz);
+  }
+}
+
+// Velocity residual against a snapshot: acc = {sum |du|^2, sum |u|^2, max |du| bits}; the
+// snapshot is refreshed with the current velocity.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_residual(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                  const uint8_t* __restrict__ cellDyn, int forced,
+                                                  float fx, float fy, float fz, float* __restrict__ snap,
+                                                  double* __restrict__ acc,
+                                                  unsigned long long* __restrict__ maxbits) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t ncore = int64_t(g.nx) * g.ny * g.nz;
+  double du2 = 0, u2 = 0;
+  if (c < ncore) {
+    const int z = int(c % g.nz);
+    const int y = int((c / g.nz) % g.ny);
+    const int x = int(c / (int64_t(g.nz) * g.ny));
+    const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+    if (!cellDyn || cellDyn[n] == 1) {
+      R f[Q];
+      static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
+      R r, uu[3];
+      const R F[3] = {R(fx), R(fy), R(fz)};
+      if (forced) moments<Q, R, true>(f, F, r, uu);
+      else moments<Q, R, false>(f, F, r, uu);
+      static_for<D::d>([&](auto A) {
+        const double cur = double(uu[A]);
+        const double d = cur - double(snap[A * ncore + c]);
+        du2 += d * d;
+        u2 += cur * cur;
+        snap[A * ncore + c] = float(cur);
+      });
+    }
+  }
+  double m = sqrt(du2);
+  for (int o = 16; o > 0; o >>= 1) {
+    du2 += __shfl_xor_sync(0xffffffffu, du2, o);
+    u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc[0], du2);
+    atomicAdd(&acc[1], u2);
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// ---- launchers (instantiated once per storage type) ------------------------------------
+struct LaunchArgs {
+  void* pop;
+  Geometry g;
+  int64_t shift[27];
+  int32_t dynamics;
+  double omega, magic, smagorinsky, force[3];
+  const uint8_t* cellDyn;
+  StatAcc* stats;
+  int blockX, blockY;
+};
+
+template <int Q, typename S>
+cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_bouzidi(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
+                           const void* delta, int64_t nLinks, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_transfer(const LaunchArgs& a, int pop, const void* stage, int hostType, bool toColumns,
+                            cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_ini_equilibrium(const LaunchArgs& a, const double* rho, const double* u, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_moments(const LaunchArgs& a, double* rho, double* u, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_mass_momentum(const LaunchArgs& a, double* acc, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir, int64_t nLinks,
+                              double* acc, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc, unsigned long long* maxbits,
+                            cudaStream_t stream);
+
+template <int Q>
+inline Shifts<Q> shifts_of(const LaunchArgs& a) {
+  Shifts<Q> s;
+  for (int i = 0; i < Q; ++i) s.s[i] = a.shift[i];
+  return s;
+}
+
+template <typename R>
+inline CollisionParams<R> params_of(const LaunchArgs& a) {
+  CollisionParams<R> p;
+  p.omega = R(a.omega);
+  p.magic = R(a.magic);
+  p.smagorinsky = R(a.smagorinsky);
+  for (int k = 0; k < 3; ++k) p.force[k] = R(a.force[k]);
+  return p;
+}
+
+inline int64_t ncore_of(const Geometry& g) { return int64_t(g.nx) * g.ny * g.nz; }
+
+#ifdef LBX_KERNEL_TU
+// Launcher bodies: compiled only in the per-storage instantiation units.
+template <int Q, typename S>
+cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream) {
+  using R = typename Storage<S>::R;
+  const Geometry& g = a.g;
+  dim3 block(a.blockX, a.blockY, 1);
+  dim3 grid;
+  if (Desc<Q>::d == 3) grid = dim3((g.nz + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
+  else grid = dim3((g.ny + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
+  const auto sh = shifts_of<Q>(a);
+  const auto p = params_of<R>(a);
+  S* pop = static_cast<S*>(a.pop);
+  switch (a.dynamics) {
+  case DYN_BGK: k_collide_stream<Q, S, DYN_BGK><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
+  case DYN_TRT: k_collide_stream<Q, S, DYN_TRT><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
+  case DYN_SMAGORINSKY: k_collide_stream<Q, S, DYN_SMAGORINSKY><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
+  case DYN_FORCED_BGK: k_collide_stream<Q, S, DYN_FORCED_BGK><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
+  case DYN_FORCED_SMAGORINSKY: k_collide_stream<Q, S, DYN_FORCED_SMAGORINSKY><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
+  default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_bouzidi(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
+                                 const void* delta, int64_t nLinks, cudaStream_t stream) {
+  using R = typename Storage<S>::R;
+  if (nLinks <= 0) return cudaSuccess;
+  const int64_t blocks = (nLinks + 255) / 256;
+  k_bouzidi<Q, S><<<unsigned(blocks), 256, 0, stream>>>(static_cast<S*>(a.pop), a.g, shifts_of<Q>(a), cell, dir,
+                                                        static_cast<const R*>(delta), nLinks);
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_transfer(const LaunchArgs& a, int i, const void* stage, int hostType, bool toColumns,
+                                  cudaStream_t stream) {
+  const int64_t nc = ncore_of(a.g);
+  const unsigned blocks = unsigned((nc + 255) / 256);
+  S* col = static_cast<S*>(a.pop) + int64_t(i) * a.g.stride;
+  if (toColumns) {
+    if (hostType == 0) k_scatter_pop<S, double><<<blocks, 256, 0, stream>>>(col, a.g, a.shift[i], static_cast<const double*>(stage));
+    else k_scatter_pop<S, float><<<blocks, 256, 0, stream>>>(col, a.g, a.shift[i], static_cast<const float*>(stage));
+  } else {
+    if (hostType == 0) k_gather_pop<S, double><<<blocks, 256, 0, stream>>>(col, a.g, a.shift[i], static_cast<double*>(const_cast<void*>(stage)));
+    else k_gather_pop<S, float><<<blocks, 256, 0, stream>>>(col, a.g, a.shift[i], static_cast<float*>(const_cast<void*>(stage)));
+  }
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_ini_equilibrium(const LaunchArgs& a, const double* rho, const double* u,
+                                         cudaStream_t stream) {
+  const unsigned blocks = unsigned((ncore_of(a.g) + 255) / 256);
+  k_ini_equilibrium<Q, S><<<blocks, 256, 0, stream>>>(static_cast<S*>(a.pop), a.g, shifts_of<Q>(a), rho, u);
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_moments(const LaunchArgs& a, double* rho, double* u, cudaStream_t stream) {
+  const unsigned blocks = unsigned((ncore_of(a.g) + 255) / 256);
+  const int forced = (a.dynamics == DYN_FORCED_BGK || a.dynamics == DYN_FORCED_SMAGORINSKY);
+  k_moments<Q, S><<<blocks, 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), forced,
+                                              a.force[0], a.force[1], a.force[2], rho, u);
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_mass_momentum(const LaunchArgs& a, double* acc, cudaStream_t stream) {
+  const unsigned blocks = unsigned((ncore_of(a.g) + 255) / 256);
+  k_mass_momentum<Q, S><<<blocks, 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), a.cellDyn, acc);
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
+                                    int64_t nLinks, double* acc, cudaStream_t stream) {
+  if (nLinks <= 0) return cudaSuccess;
+  k_link_force<Q, S><<<unsigned((nLinks + 255) / 256), 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g,
+                                                                          shifts_of<Q>(a), cell, dir, nLinks, acc);
+  return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc,
+                                  unsigned long long* maxbits, cudaStream_t stream) {
+  const unsigned blocks = unsigned((ncore_of(a.g) + 255) / 256);
+  const int forced = (a.dynamics == DYN_FORCED_BGK || a.dynamics == DYN_FORCED_SMAGORINSKY);
+  k_residual<Q, S><<<blocks, 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), a.cellDyn,
+                                               forced, float(a.force[0]), float(a.force[1]),
+                                               float(a.force[2]), snap, acc, maxbits);
+  return cudaGetLastError();
+}
+#endif  // LBX_KERNEL_TU
+
+}  // namespace lbx

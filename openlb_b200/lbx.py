@@ -1,0 +1,267 @@
+"""ctypes binding of liblbx.so (include/lbx.h) and a block-lattice wrapper.
+
+`BlockLattice` mirrors the part of the reference's BlockLattice / SuperLattice interface
+that drives the hot path (OpenLB 1.8r1, paths relative to the reference project):
+
+    defineDynamics / setParameter   core/blockLattice.h:559-576  -> define_dynamics / set_parameter
+    iniEquilibrium                  core/blockLattice.hh:201-219 -> ini_equilibrium
+    collideAndStream                core/superLattice.hh:664-725 -> collide_and_stream
+    getStatistics                   core/latticeStatistics.h:91-93 -> get_statistics
+    setBouzidiBoundary/-Velocity    boundary/setBouzidiBoundary.h:193-420 -> set_bouzidi_boundary
+    setProcessingContext(Evaluation) + cell access                  -> get_populations / compute_moments
+
+There is no CPU fallback: importing this module fails when liblbx.so is missing, and
+creating a lattice fails without an sm_100 GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(os.environ.get("LBX_LIBRARY", Path(__file__).resolve().parent / "lib" / "liblbx.so"))
+
+LBX_OK = 0
+STORAGE = {"f64": 0, "f32": 1, "f16dev": 2, "bf16dev": 3}
+STORAGE_BYTES = {"f64": 8, "f32": 4, "f16dev": 2, "bf16dev": 2}
+DYNAMICS = {"bgk": 1, "trt": 2, "smagorinsky_bgk": 3, "forced_bgk": 4, "smagorinsky_forced_bgk": 5}
+CELL_NONE, CELL_BULK, CELL_BOUNCE_BACK = 0, 1, 2
+STEP_STATISTICS = 1
+REDUCE_MASS_MOMENTUM, REDUCE_DRAG, REDUCE_RESIDUAL = 1, 2, 3
+
+
+class Params(C.Structure):
+    _fields_ = [("omega", C.c_double), ("magic", C.c_double), ("smagorinsky", C.c_double),
+                ("force", C.c_double * 3)]
+
+
+class Info(C.Structure):
+    _fields_ = [("q", C.c_int32), ("d", C.c_int32), ("core", C.c_int32 * 3), ("padded", C.c_int32 * 3),
+                ("pad", C.c_int32), ("periodic", C.c_int32 * 3), ("storage", C.c_int32),
+                ("n_cells", C.c_int64), ("n_core", C.c_int64), ("column_stride", C.c_int64),
+                ("bytes", C.c_int64), ("n_links", C.c_int64)]
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"liblbx.so not built ({LIB_PATH}); run `python -m openlb_b200.build`")
+    lib = C.CDLL(str(LIB_PATH))
+    P, I32, I64, U32, D, VP = C.POINTER, C.c_int32, C.c_int64, C.c_uint32, C.c_double, C.c_void_p
+    sig = {
+        "lbx_last_error": ([], C.c_char_p),
+        "lbx_abi_version": ([], C.c_int),
+        "lbx_device_count": ([], C.c_int),
+        "lbx_lattice_create": ([I32, P(I32), P(I32), I32, I32, P(VP)], C.c_int),
+        "lbx_lattice_destroy": ([VP], C.c_int),
+        "lbx_get_info": ([VP, P(Info)], C.c_int),
+        "lbx_set_dynamics": ([VP, I32, P(Params)], C.c_int),
+        "lbx_set_cell_dynamics": ([VP, VP], C.c_int),
+        "lbx_set_bouzidi_links": ([VP, I64, VP, VP, VP], C.c_int),
+        "lbx_set_bouzidi_from_materials": ([VP, VP, I32, I32, VP, VP], C.c_int),
+        "lbx_build_bouzidi_links": ([I32, P(I32), P(I32), VP, I32, I32, VP, VP, I64, VP, VP, VP, P(I64)], C.c_int),
+        "lbx_upload_populations": ([VP, VP, I32, VP], C.c_int),
+        "lbx_download_populations": ([VP, VP, I32, VP], C.c_int),
+        "lbx_ini_equilibrium": ([VP, VP, VP, VP], C.c_int),
+        "lbx_collide_and_stream": ([VP, I64, U32, VP], C.c_int),
+        "lbx_get_statistics": ([VP, P(D), VP], C.c_int),
+        "lbx_compute_moments": ([VP, VP, VP, VP], C.c_int),
+        "lbx_reduce": ([VP, I32, P(D), VP], C.c_int),
+        "lbx_population_shift": ([VP, I32, P(I64)], C.c_int),
+        "lbx_rotate": ([VP, I32, I64], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
+lib = _load()
+
+
+class LbxError(RuntimeError):
+    """A liblbx call failed (the C++ platform layer raises std::runtime_error likewise)."""
+
+    def __init__(self, code: int, where: str):
+        msg = lib.lbx_last_error().decode(errors="replace")
+        super().__init__(f"{where} failed ({code}): {msg}")
+        self.code = code
+
+
+def check(code: int, where: str) -> None:
+    if code != LBX_OK:
+        raise LbxError(code, where)
+
+
+def _ptr(a: np.ndarray | None) -> C.c_void_p | None:
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _i32x3(v) -> C.Array:
+    return (C.c_int32 * 3)(*[int(x) for x in v])
+
+
+def _stream_ptr(stream) -> C.c_void_p | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(int(stream.cuda_stream))  # torch.cuda.Stream
+
+
+def device_count() -> int:
+    return int(lib.lbx_device_count())
+
+
+def build_bouzidi_links(q: int, core, material: np.ndarray, fluid: int = 1, solid=(2,),
+                        wall_velocity=None, periodic=(False, False, False)):
+    """Halfway bounce-back links of a material map, as setBouzidiBoundary derives them
+    (q = 1/2 fallback).  Returns (cells int64, dirs int32, wall int32) numpy arrays."""
+    mat = np.ascontiguousarray(material, dtype=np.int32).reshape(-1)
+    sol = np.ascontiguousarray(solid, dtype=np.int32)
+    wv = None if wall_velocity is None else np.ascontiguousarray(wall_velocity, dtype=np.float64).reshape(-1)
+    n = C.c_int64(0)
+    args = (q, _i32x3(core), _i32x3(periodic), _ptr(mat), fluid, len(sol), _ptr(sol), _ptr(wv))
+    check(lib.lbx_build_bouzidi_links(*args, 0, None, None, None, C.byref(n)), "lbx_build_bouzidi_links")
+    cells = np.zeros(n.value, np.int64)
+    dirs = np.zeros(n.value, np.int32)
+    wall = np.zeros(n.value, np.float64)
+    check(lib.lbx_build_bouzidi_links(*args, n.value, _ptr(cells), _ptr(dirs), _ptr(wall), C.byref(n)),
+          "lbx_build_bouzidi_links")
+    return cells, dirs, wall
+
+
+class BlockLattice:
+    """One block lattice on one B200 (a ConcreteBlockLattice of the new platform)."""
+
+    def __init__(self, q: int, core, periodic=(False, False, False), storage: str = "f32", device: int = 0):
+        core = list(core) + [1] * (3 - len(core))
+        h = C.c_void_p()
+        check(lib.lbx_lattice_create(q, _i32x3(core), _i32x3(periodic), STORAGE[storage], device, C.byref(h)),
+              "lbx_lattice_create")
+        self._h = h
+        self.q = q
+        self.d = 2 if q == 9 else 3
+        self.core = tuple(core)
+        self.storage = storage
+        self.device = device
+        self.n_core = int(np.prod(core))
+        self._dyn = "bgk"
+        self._params = Params(1.0, 0.25, 0.12, (C.c_double * 3)(0, 0, 0))
+
+    # -- lifetime --------------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.lbx_lattice_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def info(self) -> Info:
+        i = Info()
+        check(lib.lbx_get_info(self._h, C.byref(i)), "lbx_get_info")
+        return i
+
+    # -- dynamics and parameters -----------------------------------------------------------
+    def define_dynamics(self, dynamics: str, omega: float | None = None, magic: float | None = None,
+                        smagorinsky: float | None = None, force=None) -> None:
+        self._dyn = dynamics
+        if omega is not None:
+            self._params.omega = omega
+        if magic is not None:
+            self._params.magic = magic
+        if smagorinsky is not None:
+            self._params.smagorinsky = smagorinsky
+        if force is not None:
+            f = list(force) + [0.0] * (3 - len(force))
+            self._params.force = (C.c_double * 3)(*f)
+        check(lib.lbx_set_dynamics(self._h, DYNAMICS[dynamics], C.byref(self._params)), "lbx_set_dynamics")
+
+    def set_parameter(self, name: str, value) -> None:
+        """setParameter<OMEGA | TRT::MAGIC | LES::SMAGORINSKY | FORCE>."""
+        key = {"omega": "omega", "magic": "magic", "smagorinsky": "smagorinsky", "force": "force"}[name.lower()]
+        self.define_dynamics(self._dyn, **{key: value})
+
+    def set_cell_dynamics(self, ids: np.ndarray | None) -> None:
+        if ids is None:
+            check(lib.lbx_set_cell_dynamics(self._h, None), "lbx_set_cell_dynamics")
+            return
+        a = np.ascontiguousarray(ids, dtype=np.uint8).reshape(-1)
+        if a.size != self.n_core:
+            raise ValueError("cell dynamics map must cover the core cells")
+        check(lib.lbx_set_cell_dynamics(self._h, _ptr(a)), "lbx_set_cell_dynamics")
+
+    def set_bouzidi_links(self, cells, dirs, wall=None) -> None:
+        c = np.ascontiguousarray(cells, dtype=np.int64)
+        d = np.ascontiguousarray(dirs, dtype=np.int32)
+        w = None if wall is None else np.ascontiguousarray(wall, dtype=np.float64)
+        check(lib.lbx_set_bouzidi_links(self._h, len(c), _ptr(c), _ptr(d), _ptr(w)), "lbx_set_bouzidi_links")
+
+    def set_bouzidi_boundary(self, material: np.ndarray, fluid: int = 1, solid=(2,), wall_velocity=None) -> None:
+        mat = np.ascontiguousarray(material, dtype=np.int32).reshape(-1)
+        sol = np.ascontiguousarray(solid, dtype=np.int32)
+        wv = None if wall_velocity is None else np.ascontiguousarray(wall_velocity, dtype=np.float64).reshape(-1)
+        check(lib.lbx_set_bouzidi_from_materials(self._h, _ptr(mat), fluid, len(sol), _ptr(sol), _ptr(wv)),
+              "lbx_set_bouzidi_from_materials")
+
+    # -- data movement -----------------------------------------------------------------------
+    def set_populations(self, f: np.ndarray, stream=None) -> None:
+        a = np.ascontiguousarray(f)
+        if a.dtype not in (np.float64, np.float32) or a.size != self.q * self.n_core:
+            raise ValueError("populations must be float64/float32 [q][core cells]")
+        check(lib.lbx_upload_populations(self._h, _ptr(a), 0 if a.dtype == np.float64 else 1, _stream_ptr(stream)),
+              "lbx_upload_populations")
+
+    def get_populations(self, dtype=np.float64, stream=None, out: np.ndarray | None = None) -> np.ndarray:
+        a = out if out is not None else np.empty((self.q, self.n_core), dtype=dtype)
+        check(lib.lbx_download_populations(self._h, _ptr(a), 0 if a.dtype == np.float64 else 1, _stream_ptr(stream)),
+              "lbx_download_populations")
+        return a
+
+    def ini_equilibrium(self, rho: np.ndarray, u: np.ndarray, stream=None) -> None:
+        r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+        v = np.ascontiguousarray(u, dtype=np.float64).reshape(self.d, -1)
+        check(lib.lbx_ini_equilibrium(self._h, _ptr(r), _ptr(v), _stream_ptr(stream)), "lbx_ini_equilibrium")
+
+    # -- the hot path --------------------------------------------------------------------------
+    def collide_and_stream(self, steps: int = 1, statistics: bool = False, stream=None) -> None:
+        flags = STEP_STATISTICS if statistics else 0
+        check(lib.lbx_collide_and_stream(self._h, steps, flags, _stream_ptr(stream)), "lbx_collide_and_stream")
+
+    def get_statistics(self, stream=None) -> dict:
+        out = (C.c_double * 4)()
+        check(lib.lbx_get_statistics(self._h, out, _stream_ptr(stream)), "lbx_get_statistics")
+        return {"average_rho": out[0], "average_energy": out[1], "max_u": out[2], "cells": int(out[3])}
+
+    def compute_moments(self, stream=None):
+        rho = np.empty(self.n_core, np.float64)
+        u = np.empty((self.d, self.n_core), np.float64)
+        check(lib.lbx_compute_moments(self._h, _ptr(rho), _ptr(u), _stream_ptr(stream)), "lbx_compute_moments")
+        return rho, u
+
+    def reduce(self, what: int, stream=None) -> np.ndarray:
+        out = (C.c_double * 8)()
+        check(lib.lbx_reduce(self._h, what, out, _stream_ptr(stream)), "lbx_reduce")
+        n = {REDUCE_MASS_MOMENTUM: 4, REDUCE_DRAG: 3, REDUCE_RESIDUAL: 3}[what]
+        return np.array(out[:n])
+
+    def population_shift(self, pop: int) -> int:
+        s = C.c_int64()
+        check(lib.lbx_population_shift(self._h, pop, C.byref(s)), "lbx_population_shift")
+        return s.value

@@ -1,0 +1,366 @@
+/*  Reference-side driver (test infrastructure, never part of the shipped path).
+ *
+ *  Runs the reference implementation's OWN CPU code (SuperLattice / dynamics::Tuple /
+ *  post-processors, compiled from the reference sources by oracle/Makefile) on a
+ *  synthetic case and dumps the core-cell populations, so that the CUDA path and the
+ *  C restatement in oracle/lbm_oracle.c can be checked against it.
+ *
+ *  API used (paths relative to the reference project):
+ *    SuperLattice ctor / collideAndStream     src/core/superLattice.h:88, superLattice.hh:664-725
+ *    defineDynamics<...>                      src/core/superLattice.h (BlockLattice::defineDynamics blockLattice.hh:274)
+ *    BGKdynamics / TRTdynamics / ForcedBGK    src/dynamics/dynamics.h:89,223,529
+ *    SmagorinskyBGK / SmagorinskyForcedBGK    src/dynamics/smagorinskyBGKdynamics.h:39,67
+ *    BounceBack (Revert) / NoDynamics         src/dynamics/dynamics.h:51,557
+ *    setBouzidiBoundary / setBouzidiVelocity  src/boundary/setBouzidiBoundary.h:193-420
+ *    Cell::iniEquilibrium                     src/core/cell.h:202
+ *    LatticeStatistics                        src/core/latticeStatistics.h:91-93
+ *
+ *  Build-time selection: REF_T (double|float), REF_Q (9|19|27), REF_NO_FORCE (descriptor
+ *  without the FORCE field; used by the timing build of plain BGK).
+ *
+ *  Usage:
+ *    lbref <periodic|cavity|porous> [--n NX NY [NZ]] [--dyn bgk|trt|smag|fbgk|fsmag]
+ *          [--omega W] [--magic L] [--cs C] [--force FX FY [FZ]] [--steps S]
+ *          [--init tgv|random|rest] [--u0 U] [--amp A] [--seed K] [--ulid U]
+ *          [--walls bouzidi|bounceback] [--solid-frac P] [--out PREFIX]
+ *          [--time W K] [--stats]
+ *  Output (with --out): PREFIX.f0.bin / PREFIX.fS.bin  raw T populations [Q][ext...] of the
+ *  core cells after initialize() and after S steps; PREFIX.mat.bin int32 materials [ext...];
+ *  PREFIX.stats.txt per-step "avgRho avgEnergy maxU"; PREFIX.json the case description.
+ */
+
+#include "olb.h"
+
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+using namespace olb;
+using namespace olb::descriptors;
+
+#ifndef REF_T
+#define REF_T double
+#endif
+using T = REF_T;
+
+#if REF_Q == 9
+#  ifdef REF_NO_FORCE
+using DESCRIPTOR = D2Q9<>;
+#  else
+using DESCRIPTOR = D2Q9<FORCE>;
+#  endif
+#elif REF_Q == 19
+#  ifdef REF_NO_FORCE
+using DESCRIPTOR = D3Q19<>;
+#  else
+using DESCRIPTOR = D3Q19<FORCE>;
+#  endif
+#elif REF_Q == 27
+#  ifdef REF_NO_FORCE
+using DESCRIPTOR = D3Q27<>;
+#  else
+using DESCRIPTOR = D3Q27<FORCE>;
+#  endif
+#else
+#  error "REF_Q must be 9, 19 or 27"
+#endif
+
+constexpr int D = DESCRIPTOR::d;
+constexpr int Q = DESCRIPTOR::q;
+
+namespace {
+
+struct Options {
+  std::string kase = "periodic";
+  int n[3] = {16, 16, 16};
+  std::string dyn = "bgk";
+  double omega = 1.0;
+  double magic = 0.25;
+  double cs = 0.12;
+  double force[3] = {0, 0, 0};
+  long steps = 10;
+  std::string init = "random";
+  double u0 = 0.05;
+  double amp = 0.02;
+  std::uint64_t seed = 1;
+  double ulid = 0.1;
+  std::string walls = "bouzidi";
+  double solidFrac = 0.2;
+  std::string out;
+  long timeWarm = -1;
+  long timeSteps = 0;
+  bool stats = false;
+};
+
+/// splitmix64: deterministic per-(cell, population) values shared with the Python tests.
+std::uint64_t mix(std::uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+double unit(std::uint64_t seed, std::uint64_t a, std::uint64_t b) {
+  return double(mix(seed * 0x100000001B3ull ^ mix(a * 64 + b)) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+/// Indicator whose distance queries always fail: setBouzidiBoundary then falls back to
+/// q = 1/2 on every link (setBouzidiBoundary.h:262-278), i.e. halfway bounce-back.
+template <int DIM> struct Nowhere;
+template <> struct Nowhere<2> : public IndicatorF2D<T> {
+  Nowhere() { this->_myMin = Vector<T,2>(-1e9); this->_myMax = Vector<T,2>(1e9); }
+  bool operator()(bool output[], const T input[]) override { output[0] = false; return true; }
+  bool distance(T& d, const Vector<T,2>&, const Vector<T,2>&, int) override { return false; }
+};
+template <> struct Nowhere<3> : public IndicatorF3D<T> {
+  Nowhere() { this->_myMin = Vector<T,3>(-1e9); this->_myMax = Vector<T,3>(1e9); }
+  bool operator()(bool output[], const T input[]) override { output[0] = false; return true; }
+  bool distance(T& d, const Vector<T,3>&, const Vector<T,3>&, int) override { return false; }
+};
+
+template <typename F>
+void forCore(const int ext[3], F f) {
+  const int ez = (D == 3) ? ext[2] : 1;
+  for (int x = 0; x < ext[0]; ++x)
+    for (int y = 0; y < ext[1]; ++y)
+      for (int z = 0; z < ez; ++z)
+        f(x, y, z);
+}
+
+LatticeR<D> loc(int x, int y, int z) {
+  if constexpr (D == 3) { return LatticeR<D>{x, y, z}; }
+  else { return LatticeR<D>{x, y}; }
+}
+
+Options parse(int argc, char** argv) {
+  Options o;
+  if (argc > 1) o.kase = argv[1];
+  for (int i = 2; i < argc; ++i) {
+    std::string a = argv[i];
+    auto next = [&]() -> const char* {
+      if (i + 1 >= argc) { std::fprintf(stderr, "missing value for %s\n", a.c_str()); std::exit(2); }
+      return argv[++i];
+    };
+    if (a == "--n") { for (int d = 0; d < D; ++d) o.n[d] = std::atoi(next()); }
+    else if (a == "--dyn") o.dyn = next();
+    else if (a == "--omega") o.omega = std::atof(next());
+    else if (a == "--magic") o.magic = std::atof(next());
+    else if (a == "--cs") o.cs = std::atof(next());
+    else if (a == "--force") { for (int d = 0; d < D; ++d) o.force[d] = std::atof(next()); }
+    else if (a == "--steps") o.steps = std::atol(next());
+    else if (a == "--init") o.init = next();
+    else if (a == "--u0") o.u0 = std::atof(next());
+    else if (a == "--amp") o.amp = std::atof(next());
+    else if (a == "--seed") o.seed = std::strtoull(next(), nullptr, 10);
+    else if (a == "--ulid") o.ulid = std::atof(next());
+    else if (a == "--walls") o.walls = next();
+    else if (a == "--solid-frac") o.solidFrac = std::atof(next());
+    else if (a == "--out") o.out = next();
+    else if (a == "--time") { o.timeWarm = std::atol(next()); o.timeSteps = std::atol(next()); }
+    else if (a == "--stats") o.stats = true;
+    else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); std::exit(2); }
+  }
+  return o;
+}
+
+template <typename DYN>
+void defineFluid(SuperLattice<T,DESCRIPTOR>& lat, SuperGeometry<T,D>& geo) {
+  lat.template defineDynamics<DYN>(geo, 1);
+}
+
+void dumpPopulations(SuperLattice<T,DESCRIPTOR>& lat, const int ext[3], const std::string& path) {
+  auto& block = lat.getBlock(0);
+  std::size_t nCells = std::size_t(ext[0]) * ext[1] * ((D == 3) ? ext[2] : 1);
+  std::vector<T> buf(std::size_t(Q) * nCells);
+  std::size_t c = 0;
+  forCore(ext, [&](int x, int y, int z) {
+    auto cell = block.get(loc(x, y, z));
+    for (int i = 0; i < Q; ++i) buf[std::size_t(i) * nCells + c] = cell[i];
+    ++c;
+  });
+  std::ofstream f(path, std::ios::binary);
+  f.write(reinterpret_cast<const char*>(buf.data()), buf.size() * sizeof(T));
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  olb::initialize(&argc, &argv);
+  Options o = parse(argc, argv);
+  OstreamManager clout(std::cout, "lbref");
+
+  const bool periodic = (o.kase == "periodic" || o.kase == "porous");
+  int ext[3] = {1, 1, 1};
+  for (int d = 0; d < D; ++d) ext[d] = o.n[d] + (o.kase == "cavity" ? 2 : 0);
+
+  Vector<T,D> origin(T(0));
+  Vector<int,D> extent;
+  for (int d = 0; d < D; ++d) extent[d] = ext[d];
+  CuboidDecomposition<T,D> cuboids(origin, T(1), extent, 1);
+  if (periodic) {
+    Vector<bool,D> per;
+    for (int d = 0; d < D; ++d) per[d] = true;
+    cuboids.setPeriodicity(per);
+  }
+  HeuristicLoadBalancer<T> balancer(cuboids);
+  SuperGeometry<T,D> geo(cuboids, balancer, 2);
+
+  // --- materials: 1 fluid, 2 solid wall, 3 moving lid --------------------------------
+  std::vector<std::int32_t> mat(std::size_t(ext[0]) * ext[1] * ((D == 3) ? ext[2] : 1), 1);
+  {
+    std::size_t c = 0;
+    forCore(ext, [&](int x, int y, int z) {
+      int m = 1;
+      if (o.kase == "cavity") {
+        const bool wall = x == 0 || x == ext[0] - 1 || y == 0 || (D == 3 && (z == 0 || z == ext[2] - 1));
+        if (y == ext[1] - 1) m = 3;  // lid: the whole top layer, edges included
+        else if (wall) m = 2;
+      } else if (o.kase == "porous") {
+        if (unit(o.seed ^ 0xABCDEFull, c, 63) < o.solidFrac) m = 2;
+      }
+      mat[c++] = m;
+    });
+    auto& bg = geo.getBlockGeometry(0);
+    c = 0;
+    forCore(ext, [&](int x, int y, int z) { bg.set(loc(x, y, z), mat[c++]); });
+    // BlockGeometry::set does not flag the overlap as stale; a rename between two unused
+    // material numbers does (superGeometry.hh:221), so communicate() fills the periodic overlap.
+    geo.rename(1000, 1001);
+    geo.communicate();
+  }
+
+  SuperLattice<T,DESCRIPTOR> lat(geo);
+  {
+    // Lattice units throughout: dx = dt = 1, nu = (1/omega - 1/2) / 3.
+    const T nu = (T(1) / T(o.omega) - T(0.5)) / T(3);
+    const UnitConverter<T,DESCRIPTOR> converter(T(1), T(1), T(1), T(1), nu, T(1));
+    lat.setUnitConverter(converter);
+  }
+  if (!o.stats && o.timeWarm >= 0) lat.setStatisticsOff();
+  lat.template defineDynamics<NoDynamics>(geo, 0);
+
+  if (o.dyn == "bgk") defineFluid<BGKdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "trt") defineFluid<TRTdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "smag") defineFluid<SmagorinskyBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+#ifndef REF_NO_FORCE
+  else if (o.dyn == "fbgk") defineFluid<ForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "fsmag") defineFluid<SmagorinskyForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+#endif
+  else { std::fprintf(stderr, "unsupported --dyn %s\n", o.dyn.c_str()); return 2; }
+
+  Nowhere<D> nowhere;
+  if (o.kase == "cavity") {
+    if (o.walls == "bouzidi") {
+      lat.template defineDynamics<NoDynamics>(geo, 2);
+      lat.template defineDynamics<NoDynamics>(geo, 3);
+      setBouzidiBoundary<T,DESCRIPTOR,BouzidiVelocityPostProcessor>(
+        lat, geo.getMaterialIndicator({2, 3}), geo.getMaterialIndicator({1}), nowhere);
+      Vector<T,D> uw(T(0));
+      uw[0] = T(o.ulid);
+      AnalyticalConst<D,T,T> lidU(uw);
+      setBouzidiVelocity<T,DESCRIPTOR>(lat, geo.getMaterialIndicator({3}), geo.getMaterialIndicator({1}), lidU);
+    } else if (o.walls == "bounceback") {
+      lat.template defineDynamics<BounceBack>(geo, 2);
+      lat.template defineDynamics<BounceBack>(geo, 3);
+    } else { std::fprintf(stderr, "unsupported --walls\n"); return 2; }
+  } else if (o.kase == "porous") {
+    if (o.walls == "bouzidi") {
+      lat.template defineDynamics<NoDynamics>(geo, 2);
+      setBouzidiBoundary<T,DESCRIPTOR,BouzidiPostProcessor>(
+        lat, geo.getMaterialIndicator({2}), geo.getMaterialIndicator({1}), nowhere);
+    } else {
+      lat.template defineDynamics<BounceBack>(geo, 2);
+    }
+  }
+
+  lat.template setParameter<descriptors::OMEGA>(T(o.omega));
+  if (o.dyn == "trt") lat.template setParameter<collision::TRT::MAGIC>(T(o.magic));
+  if (o.dyn == "smag" || o.dyn == "fsmag") lat.template setParameter<collision::LES::SMAGORINSKY>(T(o.cs));
+
+  // --- initial populations --------------------------------------------------------------
+  {
+    auto& block = lat.getBlock(0);
+    std::size_t c = 0;
+    const double twoPi = 2.0 * 3.14159265358979323846;
+    forCore(ext, [&](int x, int y, int z) {
+      auto cell = block.get(loc(x, y, z));
+#ifndef REF_NO_FORCE
+      if (mat[c] == 1) {
+        Vector<T,D> fv;
+        for (int d = 0; d < D; ++d) fv[d] = T(o.force[d]);
+        cell.template setField<FORCE>(fv);
+      }
+#endif
+      T rho = 1;
+      T u[D] = {};
+      if (o.init == "tgv") {
+        const double X = twoPi * x / ext[0], Y = twoPi * y / ext[1], Z = (D == 3) ? twoPi * z / ext[2] : 0.0;
+        u[0] = T(o.u0 * std::sin(X) * std::cos(Y) * std::cos(Z));
+        u[1] = T(-o.u0 * std::cos(X) * std::sin(Y) * std::cos(Z));
+      } else if (o.init == "random") {
+        rho = T(1.0 + o.amp * (unit(o.seed, c, 60) - 0.5));
+        for (int d = 0; d < D; ++d) u[d] = T(o.u0 * (unit(o.seed, c, 61 + d) - 0.5));
+      }
+      if (mat[c] == 1) {
+        cell.iniEquilibrium(rho, u);
+        if (o.init == "random") {
+          for (int i = 0; i < Q; ++i) {
+            cell[i] += T(o.amp * descriptors::t<double,DESCRIPTOR>(i) * (unit(o.seed, c, i) - 0.5));
+          }
+        }
+      } else {
+        for (int i = 0; i < Q; ++i) cell[i] = T(0);
+      }
+      ++c;
+    });
+  }
+  lat.initialize();
+
+  const std::size_t nCore = std::size_t(ext[0]) * ext[1] * ((D == 3) ? ext[2] : 1);
+
+  if (o.timeWarm >= 0) {
+    for (long s = 0; s < o.timeWarm; ++s) lat.collideAndStream();
+    auto t0 = std::chrono::steady_clock::now();
+    for (long s = 0; s < o.timeSteps; ++s) lat.collideAndStream();
+    auto t1 = std::chrono::steady_clock::now();
+    const double sec = std::chrono::duration<double>(t1 - t0).count();
+    int threads = 1;
+#ifdef PARALLEL_MODE_OMP
+    threads = singleton::omp().getSize();
+#endif
+    std::printf("{\"cells\": %zu, \"steps\": %ld, \"seconds\": %.9g, \"mlups\": %.9g, \"threads\": %d, \"q\": %d, \"bytes\": %zu}\n",
+                nCore, o.timeSteps, sec, double(nCore) * o.timeSteps / sec / 1e6, threads, Q, sizeof(T));
+    return 0;
+  }
+
+  std::FILE* statsFile = nullptr;
+  if (!o.out.empty()) {
+    dumpPopulations(lat, ext, o.out + ".f0.bin");
+    std::ofstream m(o.out + ".mat.bin", std::ios::binary);
+    m.write(reinterpret_cast<const char*>(mat.data()), mat.size() * sizeof(std::int32_t));
+    statsFile = std::fopen((o.out + ".stats.txt").c_str(), "w");
+  }
+  for (long s = 0; s < o.steps; ++s) {
+    lat.collideAndStream();
+    if (statsFile) {
+      auto& st = lat.getStatistics();
+      std::fprintf(statsFile, "%.17g %.17g %.17g\n", double(st.getAverageRho()), double(st.getAverageEnergy()), double(st.getMaxU()));
+    }
+  }
+  if (!o.out.empty()) {
+    std::fclose(statsFile);
+    dumpPopulations(lat, ext, o.out + ".fS.bin");
+    std::ofstream j(o.out + ".json");
+    j.precision(17);
+    j << "{\"case\": \"" << o.kase << "\", \"q\": " << Q << ", \"d\": " << D
+      << ", \"ext\": [" << ext[0] << ", " << ext[1] << ", " << ((D == 3) ? ext[2] : 1) << "]"
+      << ", \"dyn\": \"" << o.dyn << "\", \"omega\": " << o.omega << ", \"magic\": " << o.magic
+      << ", \"cs\": " << o.cs << ", \"force\": [" << o.force[0] << ", " << o.force[1] << ", " << o.force[2] << "]"
+      << ", \"steps\": " << o.steps << ", \"init\": \"" << o.init << "\", \"walls\": \"" << o.walls
+      << "\", \"ulid\": " << o.ulid << ", \"bytes\": " << sizeof(T) << "}\n";
+  }
+  return 0;
+}

@@ -1,0 +1,113 @@
+"""Generate the golden fixtures of tests/golden/ from the reference's own CPU code.
+
+Runs the reference drivers built by `make -C oracle ref` (oracle/ref_driver.cpp compiled
+against the reference sources: sequential CPU_SISD, FP64 with and without the generated CSE
+kernels, and FP32) on small seeded cases and stores, per case, the core-cell populations
+after initialize() (f0) and after `steps` steps (fS), the material map and the per-step
+lattice statistics.  Needs the reference tree (this container only); the fixtures it writes
+are committed and are all the tests need.
+
+    python tests/golden/gen_golden.py            # all cases
+    python tests/golden/gen_golden.py NAME ...   # selected cases
+"""
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = HERE.parent.parent / "oracle" / "_ref"
+
+P3 = ["--n", "6", "7", "8"]
+P2 = ["--n", "12", "10"]
+RND = ["--init", "random", "--amp", "0.04", "--u0", "0.08"]
+FORCE3 = ["--force", "1e-3", "-2e-4", "5e-4"]
+FORCE2 = ["--force", "1e-3", "-2e-4"]
+
+# name: (binary suffix, case, args)
+CASES: dict[str, tuple[str, str, list[str]]] = {}
+for q, geo in ((9, P2), (19, P3), (27, P3)):
+    FORCE = FORCE2 if q == 9 else FORCE3
+    for dyn, extra in (("bgk", ["--omega", "1.7"]), ("trt", ["--omega", "1.6", "--magic", "0.25"]),
+                       ("smag", ["--omega", "1.95", "--cs", "0.12"]), ("fbgk", ["--omega", "1.3", *FORCE]),
+                       ("fsmag", ["--omega", "1.95", "--cs", "0.12", *FORCE])):
+        args = ["periodic", *geo, "--dyn", dyn, *extra, *RND, "--steps", "20", "--seed", str(q)]
+        CASES[f"periodic_d{'2' if q == 9 else '3'}q{q}_{dyn}_f64"] = (f"d{'2' if q == 9 else '3'}q{q}_f64_nocse", args[0], args[1:])
+        CASES[f"periodic_d{'2' if q == 9 else '3'}q{q}_{dyn}_f64cse"] = (f"d{'2' if q == 9 else '3'}q{q}_f64", args[0], args[1:])
+        CASES[f"periodic_d{'2' if q == 9 else '3'}q{q}_{dyn}_f32"] = (f"d{'2' if q == 9 else '3'}q{q}_f32", args[0], args[1:])
+
+CASES.update({
+    # lid-driven cavities: halfway bounce-back walls (q = 1/2 Bouzidi) + moving lid
+    "cavity_d2q9_bgk_f64": ("d2q9_f64_nocse", "cavity", ["--n", "16", "14", "--dyn", "bgk", "--omega", "1.2",
+                                                          "--ulid", "0.1", "--init", "rest", "--steps", "150"]),
+    "cavity_d2q9_bgk_f32": ("d2q9_f32", "cavity", ["--n", "16", "14", "--dyn", "bgk", "--omega", "1.2",
+                                                    "--ulid", "0.1", "--init", "rest", "--steps", "150"]),
+    "cavity_d3q19_bgk_f64": ("d3q19_f64_nocse", "cavity", ["--n", "8", "9", "7", "--dyn", "bgk", "--omega", "1.4",
+                                                            "--ulid", "0.05", "--init", "rest", "--steps", "60"]),
+    "cavity_d3q19_trt_f64": ("d3q19_f64_nocse", "cavity", ["--n", "8", "9", "7", "--dyn", "trt", "--omega", "1.4",
+                                                            "--ulid", "0.05", "--init", "rest", "--steps", "60"]),
+    "cavity_d3q27_smag_f64": ("d3q27_f64_nocse", "cavity", ["--n", "7", "8", "6", "--dyn", "smag", "--omega", "1.9",
+                                                             "--cs", "0.12", "--ulid", "0.05", "--init", "rest",
+                                                             "--steps", "60"]),
+    # bounce-back dynamics (collision::Revert) on the walls
+    "cavity_d3q19_bb_f64": ("d3q19_f64_nocse", "cavity", ["--n", "8", "9", "7", "--dyn", "bgk", "--omega", "1.4",
+                                                           "--walls", "bounceback", *RND, "--steps", "40"]),
+    "cavity_d2q9_bb_f64": ("d2q9_f64_nocse", "cavity", ["--n", "12", "11", "--dyn", "trt", "--omega", "1.4",
+                                                         "--walls", "bounceback", *RND, "--steps", "40"]),
+    # periodic porous media: random solid cells with halfway bounce-back, body force
+    "porous_d3q19_fbgk_f64": ("d3q19_f64_nocse", "porous", ["--n", "8", "9", "10", "--dyn", "fbgk", "--omega", "1.5",
+                                                             "--force", "1e-4", "0", "0", "--solid-frac", "0.25",
+                                                             *RND, "--steps", "40"]),
+    "porous_d3q27_fsmag_f64": ("d3q27_f64_nocse", "porous", ["--n", "8", "9", "10", "--dyn", "fsmag", "--omega", "1.9",
+                                                              "--cs", "0.12", "--force", "1e-4", "0", "0",
+                                                              "--solid-frac", "0.25", *RND, "--steps", "40"]),
+    "porous_d2q9_trt_f64": ("d2q9_f64_nocse", "porous", ["--n", "14", "12", "--dyn", "trt", "--omega", "1.5",
+                                                          "--solid-frac", "0.2", *RND, "--steps", "40"]),
+    # Taylor-Green vortex (the benchmark's initial condition), small
+    "tgv_d3q19_bgk_f64": ("d3q19_f64_nocse", "periodic", ["--n", "16", "16", "16", "--dyn", "bgk",
+                                                           "--omega", str(1.0 / (3 * 0.01 + 0.5)), "--init", "tgv",
+                                                           "--u0", "0.05", "--steps", "50"]),
+    "tgv_d3q19_bgk_f32": ("d3q19_f32", "periodic", ["--n", "16", "16", "16", "--dyn", "bgk",
+                                                     "--omega", str(1.0 / (3 * 0.01 + 0.5)), "--init", "tgv",
+                                                     "--u0", "0.05", "--steps", "50"]),
+})
+
+
+def generate(name: str) -> Path:
+    binary, case, args = CASES[name]
+    exe = REF / f"lbref_{binary}"
+    if not exe.exists():
+        raise SystemExit(f"{exe} missing: build it with `make -C oracle ref`")
+    with tempfile.TemporaryDirectory() as tmp:
+        prefix = str(Path(tmp) / "c")
+        subprocess.run([str(exe), case, *args, "--out", prefix], check=True, timeout=600,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        meta = json.loads(Path(prefix + ".json").read_text())
+        dt = np.float64 if meta["bytes"] == 8 else np.float32
+        q = meta["q"]
+        n = int(np.prod(meta["ext"]))
+        f0 = np.fromfile(prefix + ".f0.bin", dtype=dt).reshape(q, n)
+        fS = np.fromfile(prefix + ".fS.bin", dtype=dt).reshape(q, n)
+        mat = np.fromfile(prefix + ".mat.bin", dtype=np.int32)
+        stats = np.loadtxt(prefix + ".stats.txt", ndmin=2)
+    meta["binary"] = binary
+    meta["args"] = [case, *args]
+    out = HERE / f"{name}.npz"
+    np.savez_compressed(out, f0=f0, fS=fS, mat=mat, stats=stats, meta=json.dumps(meta))
+    return out
+
+
+def main(argv: list[str]) -> int:
+    names = argv or list(CASES)
+    for name in names:
+        print(generate(name))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main(sys.argv[1:]))

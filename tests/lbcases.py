@@ -1,0 +1,233 @@
+"""Shared helpers of the test suite: golden fixtures, the CPU oracle binding, link derivation
+and error metrics.  Test infrastructure only.
+
+The oracle (oracle/lbm_oracle.c, built into oracle/_build/liblbmoracle.so) is the checker;
+the CUDA path under test is openlb_b200.lbx.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLDEN = ROOT / "tests" / "golden"
+ORACLE_LIB = ROOT / "oracle" / "_build" / "liblbmoracle.so"
+
+# descriptor tables (src/descriptor/definition/common.h), used for moments and links
+C9 = [(0, 0, 0), (-1, 1, 0), (-1, 0, 0), (-1, -1, 0), (0, -1, 0), (1, -1, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)]
+C19 = [(0, 0, 0), (-1, 0, 0), (0, -1, 0), (0, 0, -1), (-1, -1, 0), (-1, 1, 0), (-1, 0, -1), (-1, 0, 1),
+       (0, -1, -1), (0, -1, 1), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, -1, 0), (1, 0, 1), (1, 0, -1),
+       (0, 1, 1), (0, 1, -1)]
+C27 = [(0, 0, 0), (-1, 0, 0), (0, -1, 0), (0, 0, -1), (-1, -1, 0), (-1, 1, 0), (-1, 0, -1), (-1, 0, 1),
+       (0, -1, -1), (0, -1, 1), (-1, -1, -1), (-1, -1, 1), (-1, 1, -1), (-1, 1, 1), (1, 0, 0), (0, 1, 0),
+       (0, 0, 1), (1, 1, 0), (1, -1, 0), (1, 0, 1), (1, 0, -1), (0, 1, 1), (0, 1, -1), (1, 1, 1), (1, 1, -1),
+       (1, -1, 1), (1, -1, -1)]
+VEL = {9: np.array(C9), 19: np.array(C19), 27: np.array(C27)}
+W = {9: np.array([4 / 9] + [1 / 36, 1 / 9] * 4),
+     19: np.array([1 / 3] + [1 / 18] * 3 + [1 / 36] * 6 + [1 / 18] * 3 + [1 / 36] * 6),
+     27: np.array([8 / 27] + [2 / 27] * 3 + [1 / 54] * 6 + [1 / 216] * 4 + [2 / 27] * 3 + [1 / 54] * 6 + [1 / 216] * 4)}
+DYN_CODE = {"bgk": 0, "trt": 1, "smag": 2, "fbgk": 3, "fsmag": 4}
+GPU_DYN = {"bgk": "bgk", "trt": "trt", "smag": "smagorinsky_bgk", "fbgk": "forced_bgk",
+           "fsmag": "smagorinsky_forced_bgk"}
+
+
+def opposite(q: int) -> np.ndarray:
+    c = VEL[q]
+    return np.array([int(np.where((c == -c[i]).all(axis=1))[0][0]) for i in range(q)])
+
+
+# ---- fixtures -------------------------------------------------------------------------------
+def fixture_names() -> list[str]:
+    return sorted(p.stem for p in GOLDEN.glob("*.npz"))
+
+
+def load_fixture(name: str) -> dict:
+    z = np.load(GOLDEN / f"{name}.npz")
+    meta = json.loads(str(z["meta"]))
+    fx = {k: z[k] for k in ("f0", "fS", "mat", "stats")}
+    fx["meta"] = meta
+    fx["name"] = name
+    return fx
+
+
+def core_of(meta: dict) -> tuple[int, int, int]:
+    e = meta["ext"]
+    return int(e[0]), int(e[1]), int(e[2])
+
+
+def periodic_of(meta: dict) -> tuple[int, int, int]:
+    p = 1 if meta["case"] in ("periodic", "porous") else 0
+    return (p, p, p if meta["d"] == 3 else 0)
+
+
+# ---- halfway bounce-back links: numpy restatement of setBouzidiBoundary's q = 1/2 fallback ----
+def bouzidi_links(q: int, core, material: np.ndarray, fluid: int, solid, wall_velocity=None, periodic=(0, 0, 0)):
+    """Links (x_b, k) with x_b fluid and x_b + c_k solid (boundary/setBouzidiBoundary.h:236-330);
+    wall term c_k . u_wall of the solid material (setBouzidiVelocity, :386-410)."""
+    nx, ny, nz = core
+    mat = material.reshape(nx, ny, nz)
+    c = VEL[q]
+    cells, dirs, wall = [], [], []
+    idx = np.arange(nx * ny * nz).reshape(nx, ny, nz)
+    X, Y, Z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    fl = mat == fluid
+    for k in range(1, q):
+        sx, sy, sz = X + c[k][0], Y + c[k][1], Z + c[k][2]
+        ok = np.ones_like(fl)
+        for s, n, per in ((sx, nx, periodic[0]), (sy, ny, periodic[1]), (sz, nz, periodic[2])):
+            if per:
+                s %= n
+            else:
+                ok &= (s >= 0) & (s < n)
+        sxc, syc, szc = np.clip(sx, 0, nx - 1), np.clip(sy, 0, ny - 1), np.clip(sz, 0, nz - 1)
+        smat = mat[sxc, syc, szc]
+        for j, m in enumerate(solid):
+            hit = fl & ok & (smat == m)
+            n_hit = int(hit.sum())
+            if n_hit:
+                cells.append(idx[hit])
+                dirs.append(np.full(n_hit, k))
+                uw = np.zeros(3) if wall_velocity is None else np.asarray(wall_velocity[j], float)
+                wall.append(np.full(n_hit, float(np.dot(c[k], uw))))
+    if not cells:
+        return np.zeros(0, np.int64), np.zeros(0, np.int32), np.zeros(0)
+    cells = np.concatenate(cells)
+    dirs = np.concatenate(dirs).astype(np.int32)
+    wall = np.concatenate(wall)
+    order = np.lexsort((dirs, cells))
+    return cells[order].astype(np.int64), dirs[order], wall[order]
+
+
+def case_setup(fx: dict) -> dict:
+    """Dynamics, per-cell map and links of a fixture, as the reference driver set them up."""
+    meta = fx["meta"]
+    q = meta["q"]
+    core = core_of(meta)
+    per = periodic_of(meta)
+    mat = fx["mat"]
+    setup = {"q": q, "core": core, "periodic": per, "dyn": meta["dyn"], "omega": meta["omega"],
+             "magic": meta["magic"], "cs": meta["cs"], "force": list(meta["force"]), "links": None,
+             "cell_dyn": None}
+    if meta["case"] == "cavity":
+        if meta["walls"] == "bounceback":
+            cd = np.where(mat == 1, 1, 2).astype(np.uint8)
+        else:
+            cd = np.where(mat == 1, 1, 0).astype(np.uint8)
+            setup["links"] = bouzidi_links(q, core, mat, 1, (2, 3), [(0, 0, 0), (meta["ulid"], 0, 0)], per)
+        setup["cell_dyn"] = cd
+    elif meta["case"] == "porous":
+        if meta["walls"] == "bounceback":
+            setup["cell_dyn"] = np.where(mat == 1, 1, 2).astype(np.uint8)
+        else:
+            setup["cell_dyn"] = np.where(mat == 1, 1, 0).astype(np.uint8)
+            setup["links"] = bouzidi_links(q, core, mat, 1, (2,), None, per)
+    return setup
+
+
+# ---- oracle -----------------------------------------------------------------------------------
+class _Case(C.Structure):
+    _fields_ = [("q", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("periodic", C.c_int32), ("dynamics", C.c_int32), ("omega", C.c_double), ("magic", C.c_double),
+                ("smagorinsky", C.c_double), ("force", C.c_double * 3), ("material", C.c_void_p),
+                ("n_links", C.c_int64), ("link_cell", C.c_void_p), ("link_dir", C.c_void_p),
+                ("link_wall", C.c_void_p)]
+
+
+_oracle = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_LIB.exists():
+            subprocess.run(["make", "-C", str(ROOT / "oracle"), "oracle"], check=True, capture_output=True)
+        lib = C.CDLL(str(ORACLE_LIB))
+        for fn in ("lbo_run_f64", "lbo_run_f32"):
+            getattr(lib, fn).argtypes = [C.POINTER(_Case), C.c_void_p, C.c_int64, C.c_void_p]
+            getattr(lib, fn).restype = C.c_int
+        lib.lbo_run_half.argtypes = [C.POINTER(_Case), C.c_void_p, C.c_int32, C.c_int64, C.c_void_p]
+        lib.lbo_run_half.restype = C.c_int
+        lib.lbo_float_to_half.argtypes = [C.c_float]
+        lib.lbo_float_to_half.restype = C.c_uint16
+        lib.lbo_half_to_float.argtypes = [C.c_uint16]
+        lib.lbo_half_to_float.restype = C.c_float
+        lib.lbo_float_to_bf16.argtypes = [C.c_float]
+        lib.lbo_float_to_bf16.restype = C.c_uint16
+        lib.lbo_bf16_to_float.argtypes = [C.c_uint16]
+        lib.lbo_bf16_to_float.restype = C.c_float
+        _oracle = lib
+    return _oracle
+
+
+def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage: str | None = None):
+    """Run the oracle in place on a copy of f; returns (f, stats[steps, 3])."""
+    lib = oracle()
+    keep = []
+    c = _Case()
+    c.q = setup["q"]
+    c.nx, c.ny, c.nz = setup["core"]
+    c.periodic = 1 if any(setup["periodic"]) else 0
+    c.dynamics = DYN_CODE[setup["dyn"]]
+    c.omega, c.magic, c.smagorinsky = setup["omega"], setup["magic"], setup["cs"]
+    c.force = (C.c_double * 3)(*(list(setup["force"]) + [0.0] * 3)[:3])
+    if setup["cell_dyn"] is not None:
+        m = np.where(setup["cell_dyn"] == 1, 1, np.where(setup["cell_dyn"] == 2, 4, 0)).astype(np.int32)
+        keep.append(m)
+        c.material = m.ctypes.data
+    if setup["links"] is not None:
+        cells, dirs, wall = (np.ascontiguousarray(a) for a in setup["links"])
+        keep += [cells, dirs, wall]
+        c.n_links = len(cells)
+        c.link_cell, c.link_dir, c.link_wall = cells.ctypes.data, dirs.ctypes.data, wall.ctypes.data
+    stats = np.zeros((max(steps, 1), 3))
+    if storage in ("f16dev", "bf16dev"):
+        conv = lib.lbo_float_to_half if storage == "f16dev" else lib.lbo_float_to_bf16
+        flat = np.ascontiguousarray(f, dtype=np.float32).reshape(-1)
+        h = np.array([conv(float(v)) for v in flat], dtype=np.uint16)
+        rc = lib.lbo_run_half(C.byref(c), h.ctypes.data, 1 if storage == "f16dev" else 2, steps, stats.ctypes.data)
+        back = lib.lbo_half_to_float if storage == "f16dev" else lib.lbo_bf16_to_float
+        out = np.array([back(int(v)) for v in h], dtype=np.float32).reshape(f.shape)
+    else:
+        out = np.ascontiguousarray(f, dtype=dtype).copy()
+        fn = lib.lbo_run_f64 if dtype == np.float64 else lib.lbo_run_f32
+        rc = fn(C.byref(c), out.ctypes.data, steps, stats.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle failed: {rc}")
+    return out, stats[:steps]
+
+
+# ---- metrics ------------------------------------------------------------------------------------
+def moments(q: int, f: np.ndarray, force=None):
+    f = np.asarray(f, np.float64)
+    c = VEL[q][:, : (2 if q == 9 else 3)]
+    rho = f.sum(axis=0) + 1.0
+    u = (c.T @ f) / rho
+    if force is not None:
+        u = u + 0.5 * np.asarray(force[: u.shape[0]])[:, None]
+    return rho, u
+
+
+def errors(q: int, a: np.ndarray, b: np.ndarray, mask: np.ndarray | None = None, force=None) -> dict:
+    """Relative errors of a against b over the cells in mask: populations (max abs diff over
+    max |b|), velocity (max and L2) and density (max abs)."""
+    if mask is not None:
+        a, b = a[:, mask], b[:, mask]
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    ra, ua = moments(q, a, force)
+    rb, ub = moments(q, b, force)
+    umax = np.abs(ub).max() or 1.0
+    return {
+        "pop": float(np.abs(a - b).max() / (np.abs(b).max() or 1.0)),
+        "u_inf": float(np.abs(ua - ub).max() / umax),
+        "u_l2": float(np.sqrt(((ua - ub) ** 2).sum() / max((ub ** 2).sum(), 1e-300))),
+        "rho_inf": float(np.abs(ra - rb).max()),
+    }
+
+
+def fluid_mask(fx: dict) -> np.ndarray:
+    return fx["mat"] == 1
