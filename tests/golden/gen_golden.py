@@ -85,7 +85,7 @@ def generate(name: str) -> Path:
         raise SystemExit(f"{exe} missing: build it with `make -C oracle ref`")
     with tempfile.TemporaryDirectory() as tmp:
         prefix = str(Path(tmp) / "c")
-        subprocess.run([str(exe), case, *args, "--out", prefix], check=True, timeout=600,
+        subprocess.run([str(exe), case, *args, "--out", prefix], check=True, timeout=600, cwd=tmp,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         meta = json.loads(Path(prefix + ".json").read_text())
         dt = np.float64 if meta["bytes"] == 8 else np.float32
