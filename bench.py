@@ -1,0 +1,343 @@
+"""Benchmark: D3Q19 BGK fused collide-and-stream on a periodic 256^3 Taylor-Green vortex.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one fused collide + periodic-shift stream over the whole 256^3 lattice (FP32
+storage, nu = 0.01, u0 = 0.05), the bandwidth-roofline configuration of the reference's
+benchmark set.  `value` is MLUPS with the populations resident in HBM; `e2e` is the same
+metric through the C ABI with host buffers (upload of the initial populations from pinned
+memory, every step's lattice statistics read back, download of the final populations).  The
+FP16/BF16 deviation-storage and FP64 forms are timed beside it under "forms".  With N GPUs
+every rank steps its own lattice (replicas; the path needs no collective) and `value`
+aggregates over ranks with the max-over-ranks time.
+
+--impl reference times the reference's own CPU implementation (OpenMP + SIMD build of
+OpenLB, oracle/_ref) on this host's cores on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLUPS (D3Q19 256^3 fused collide-and-stream)"
+NU = 0.01
+U0 = 0.05
+OMEGA = 1.0 / (3.0 * NU + 0.5)
+BYTES_PER_LUP = {"f64": 2 * 19 * 8, "f32": 2 * 19 * 4, "f16dev": 2 * 19 * 2, "bf16dev": 2 * 19 * 2}
+
+
+def hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profile_traffic() -> float | None:
+    """dram read+write bytes per launch of the step kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "k_collide_stream_d3q19_f32_256.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch_256:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------------------------
+def reference_binary() -> Path | None:
+    flags = ""
+    try:
+        flags = Path("/proc/cpuinfo").read_text()
+    except OSError:
+        pass
+    isa = "avx512" if " avx512f" in flags and " avx512bw" in flags else "avx2"
+    exe = ROOT / "oracle" / "_ref" / f"lbref_d3q19_f32_omp_{isa}"
+    return exe if exe.exists() else None
+
+
+def time_reference(n: int, warmup: int, steps: int, threads: int) -> dict:
+    exe = reference_binary()
+    if exe is None:
+        raise FileNotFoundError("reference CPU build missing (make -C oracle ref)")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+    cmd = [str(exe), "periodic", "--n", str(n), str(n), str(n), "--dyn", "bgk", "--omega", repr(OMEGA),
+           "--init", "tgv", "--u0", repr(U0), "--time", str(warmup), str(steps)]
+    with __import__("tempfile").TemporaryDirectory() as tmp:
+        out = subprocess.run(cmd, env=env, cwd=tmp, capture_output=True, text=True, timeout=900, check=True).stdout
+    line = [l for l in out.splitlines() if l.startswith("{")][-1]
+    r = json.loads(line)
+    r["binary"] = exe.name
+    return r
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ---------------------------------------------------------------------------------------------
+def tgv_fields(n: int):
+    x = 2 * np.pi * np.arange(n) / n
+    sx, cx = np.sin(x), np.cos(x)
+    ux = U0 * sx[:, None, None] * cx[None, :, None] * cx[None, None, :]
+    uy = -U0 * cx[:, None, None] * sx[None, :, None] * cx[None, None, :]
+    u = np.stack([ux.reshape(-1), uy.reshape(-1), np.zeros(n ** 3)])
+    return np.ones(n ** 3), u
+
+
+def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
+    import torch
+
+    from openlb_b200 import lbx
+
+    torch.cuda.set_device(device)
+    stream = torch.cuda.Stream(device=device)
+    n = args.size
+    cells = n ** 3
+    rho, u = tgv_fields(n)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(lat, k: int) -> float:
+        """ms for k fused steps, device-timed on the launch stream, max over ranks."""
+        barrier()
+        torch.cuda.synchronize(device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lat.collide_and_stream(k, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    # ---- headline: FP32 storage, populations resident -----------------------------------------
+    lat = lbx.BlockLattice(19, (n, n, n), (1, 1, 1), args.storage, device=device)
+    lat.define_dynamics("bgk", omega=OMEGA)
+    lat.ini_equilibrium(rho, u, stream=stream)
+    lat.collide_and_stream(args.warmup, stream=stream)
+    torch.cuda.synchronize(device)
+    clocks = Clocks(device)
+    clocks.start()
+    ms = timed_steps(lat, args.steps)
+    clk = clocks.stop()
+    per_step_ms = ms / args.steps
+    mlups = world * cells * args.steps / (ms * 1e-3) / 1e6
+    launch_s = per_step_ms * 1e-3
+    bytes_launch = cells * BYTES_PER_LUP[args.storage]
+    peak, peak_kind = hbm_peak()
+    achieved_gbs = bytes_launch / launch_s / 1e9
+    stats = lat.get_statistics()
+
+    # ---- e2e through the C ABI with host buffers -----------------------------------------------
+    f_host = torch.empty((19, cells), dtype=torch.float32 if args.storage != "f64" else torch.float64,
+                         pin_memory=True)
+    f_np = f_host.numpy()
+    lat.get_populations(out=f_np, stream=stream)
+    barrier()
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    lat.set_populations(f_np, stream=stream)
+    for _ in range(args.steps):
+        lat.collide_and_stream(1, statistics=True, stream=stream)
+        lat.get_statistics(stream=stream)
+    lat.get_populations(out=f_np, stream=stream)
+    torch.cuda.synchronize(device)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    e2e_mlups = world * cells * args.steps / e2e_s / 1e6
+    pop_bytes = f_np.nbytes
+    lat.close()
+
+    # ---- other storage forms (shorter runs) ------------------------------------------------------
+    forms = {}
+    if not args.no_forms:
+        for form in ("f16dev", "bf16dev", "f64"):
+            k = max(10, args.steps // 4)
+            fl = lbx.BlockLattice(19, (n, n, n), (1, 1, 1), form, device=device)
+            fl.define_dynamics("bgk", omega=OMEGA)
+            fl.ini_equilibrium(rho, u, stream=stream)
+            fl.collide_and_stream(args.warmup, stream=stream)
+            fms = timed_steps(fl, k)
+            f_mlups = world * cells * k / (fms * 1e-3) / 1e6
+            f_gbs = cells * BYTES_PER_LUP[form] / (fms / k * 1e-3) / 1e9
+            forms[form] = {"mlups": round(f_mlups, 1), "hbm_gbs": round(f_gbs, 1),
+                           "hbm_frac": round(f_gbs / peak, 4), "vs_f32_mlups": round(f_mlups / mlups, 3),
+                           "steps": k}
+            fl.close()
+
+    if rank != 0:
+        return None
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(per_step_ms, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64",
+        "data": "synthetic (Taylor-Green vortex initial state, seeded-free analytic field)",
+        "config": {"workload": f"D3Q19 BGK periodic {n}^3 Taylor-Green u0={U0} nu={NU}, {args.storage} storage",
+                   "cells": cells, "storage": args.storage, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": f"population arrays {bytes_launch / 2 / 1e9:.2f} GB > 126 MB L2; no flush needed"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_gbs / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": bytes_launch},
+        "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(pop_bytes / args.steps),
+                "d2h_bytes_per_step": int(pop_bytes / args.steps + 32)},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "statistics_last_step": stats,
+        "forms": forms,
+    }
+    return line
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--storage", default="f32", choices=["f32", "f64", "f16dev", "bf16dev"])
+    ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        k = min(args.steps, 30)
+        w = min(args.warmup, 2)
+        r = time_reference(args.size, w, k, threads)
+        line = {"impl": "reference", "metric": METRIC, "value": round(r["mlups"], 2), "unit": "MLUPS",
+                "n_gpus": args.gpus, "steps": k, "warmup": w, "ms_per_step": round(1e3 * r["seconds"] / k, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (Taylor-Green vortex initial state)",
+                "config": {"workload": f"D3Q19 BGK periodic {args.size}^3 Taylor-Green u0={U0} nu={NU}, f32 storage",
+                           "cells": args.size ** 3, "storage": "f32", "parallelism": "host cores"},
+                "cpu_baseline": {"value": round(r["mlups"], 2), "unit": "MLUPS", "cores": r["threads"],
+                                 "kind": "reference",
+                                 "sample": f"{args.size}^3 lattice, {w} warm-up + {k} timed steps of OpenLB "
+                                           f"CPU_SIMD+OpenMP ({r['binary']}) on {cpu_model()}"},
+                "e2e": {"value": round(r["mlups"], 2), "unit": "MLUPS", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device(f"cuda:{local}"))
+        dist = tdist
+    line = run_b200(args, rank, world, local, dist)
+    if line is not None and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            k = 40
+            r = time_reference(args.size, 1, k, threads)
+            line["cpu_baseline"] = {"value": round(r["mlups"], 2), "unit": "MLUPS", "cores": r["threads"],
+                                    "kind": "reference",
+                                    "sample": f"{args.size}^3 lattice, 1 warm-up + {k} timed steps of OpenLB "
+                                              f"CPU_SIMD+OpenMP ({r['binary']}) on {cpu_model()}"}
+        except Exception as exc:  # the baseline is reported, never required for the GPU number
+            line["cpu_baseline"] = {"value": None, "unit": "MLUPS", "cores": None, "kind": "reference",
+                                    "sample": f"unavailable: {exc}"}
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

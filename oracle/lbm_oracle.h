@@ -37,7 +37,7 @@ enum lbo_material {
 typedef struct {
   int32_t q;             /* 9, 19 or 27 */
   int32_t nx, ny, nz;    /* core extents; nz = 1 for D2Q9 */
-  int32_t periodic;      /* 1: periodic in every direction */
+  int32_t periodic;      /* bit a set: periodic along axis a (1 x, 2 y, 4 z) */
   int32_t dynamics;      /* enum lbo_dynamics */
   double omega, magic, smagorinsky;
   double force[3];       /* body force (acceleration) of the forced dynamics */

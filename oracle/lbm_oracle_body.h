@@ -126,7 +126,7 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
 
   for (int64_t s = 0; s < steps; ++s) {
     /* collide (ConcreteBlockCollisionO<..CPU_SISD..>::apply, cpu/sisd/operator.h:143-228) */
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n > 200000)
     for (int64_t x = 0; x < n; ++x) {
       const int m = c->material ? c->material[x] : LBO_FLUID;
       cellRho[x] = (REAL)-1;
@@ -168,16 +168,16 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
     memcpy(tmp, f, sizeof(STORE_T) * (size_t)(q * n));
     for (int i = 0; i < q; ++i) {
       const int cx = d->c[i][0], cy = d->c[i][1], cz = (d->d == 3) ? d->c[i][2] : 0;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n > 200000)
       for (int64_t x = 0; x < nx; ++x) {
         for (int64_t y = 0; y < ny; ++y) {
           for (int64_t z = 0; z < nz; ++z) {
             int64_t sx = x - cx, sy = y - cy, sz = z - cz;
             STORE_T v = STORE((REAL)0);
-            if (c->periodic) {
-              sx = (sx + nx) % nx; sy = (sy + ny) % ny; sz = (sz + nz) % nz;
-              v = tmp[i * n + (sx * ny + sy) * nz + sz];
-            } else if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) {
+            if (c->periodic & 1) sx = (sx + nx) % nx;
+            if (c->periodic & 2) sy = (sy + ny) % ny;
+            if (c->periodic & 4) sz = (sz + nz) % nz;
+            if (sx >= 0 && sx < nx && sy >= 0 && sy < ny && sz >= 0 && sz < nz) {
               v = tmp[i * n + (sx * ny + sy) * nz + sz];
             }
             f[i * n + (x * ny + y) * nz + z] = v;
@@ -193,7 +193,9 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
       const int k = c->link_dir[l];
       int64_t bx = xb / (ny * nz), by = (xb / nz) % ny, bz = xb % nz;
       int64_t sx = bx + d->c[k][0], sy = by + d->c[k][1], sz = bz + ((d->d == 3) ? d->c[k][2] : 0);
-      if (c->periodic) { sx = (sx + nx) % nx; sy = (sy + ny) % ny; sz = (sz + nz) % nz; }
+      if (c->periodic & 1) sx = (sx + nx) % nx;
+      if (c->periodic & 2) sy = (sy + ny) % ny;
+      if (c->periodic & 4) sz = (sz + nz) % nz;
       if (sx < 0 || sx >= nx || sy < 0 || sy >= ny || sz < 0 || sz >= nz) continue;
       const int64_t xs = (sx * ny + sy) * nz + sz;
       const REAL tk = (REAL)d->tn[k] / (REAL)d->td[k];

@@ -170,7 +170,8 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
     c = _Case()
     c.q = setup["q"]
     c.nx, c.ny, c.nz = setup["core"]
-    c.periodic = 1 if any(setup["periodic"]) else 0
+    per = setup["periodic"]
+    c.periodic = (1 if per[0] else 0) | (2 if per[1] else 0) | (4 if len(per) > 2 and per[2] else 0)
     c.dynamics = DYN_CODE[setup["dyn"]]
     c.omega, c.magic, c.smagorinsky = setup["omega"], setup["magic"], setup["cs"]
     c.force = (C.c_double * 3)(*(list(setup["force"]) + [0.0] * 3)[:3])
