@@ -82,9 +82,9 @@ typedef struct {
   int32_t pad;
   int32_t periodic[3];
   int32_t storage;
-  int64_t n_cells;       /* padded cell count = length of each population column */
+  int64_t n_cells;       /* padded cell count */
   int64_t n_core;        /* core cell count */
-  int64_t column_stride; /* elements between the starts of consecutive population columns */
+  int64_t column_stride; /* elements between column starts = the cyclic period of a column */
   int64_t bytes;         /* device bytes held by the handle */
   int64_t n_links;       /* halfway bounce-back links */
 } lbx_info;
@@ -187,6 +187,12 @@ int lbx_reduce(lbx_lattice lattice, int32_t what, double* out, void* stream);
  * by `offset` cells (CyclicColumn::rotate, gpu/cuda/column.h:144-154). */
 int lbx_population_shift(lbx_lattice lattice, int32_t pop, int64_t* shift);
 int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
+
+/* Launch configuration of the step kernel, the knob the autotuner turns (no reference
+ * counterpart; the reference's CUDA platform launches fixed 32-thread blocks,
+ * gpu/cuda/operator.hh:425-441).  variant 0: shared-memory staged tiles of 256 cells
+ * (default); variant 1: one cell per thread in (block_x, block_y) blocks. */
+int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y);
 
 #ifdef __cplusplus
 }

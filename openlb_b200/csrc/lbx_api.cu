@@ -102,6 +102,7 @@ struct lbx_lattice_s {
   int dynamics = LBX_BGK;
   lbx_params params{1.0, 0.25, 0.12, {0, 0, 0}};
   int blockX = 256, blockY = 1;
+  int kernel = 0;
   int64_t bytes = 0;
 };
 
@@ -109,7 +110,7 @@ namespace {
 
 Geometry geometry_of(const lbx_lattice_s* L) {
   Geometry g;
-  g.n = L->n;
+  g.n = L->stride;  // cyclic period of every column (>= padded cells, multiple of 128)
   g.stride = L->stride;
   g.sy = (L->d == 3) ? L->padded[2] : 1;
   g.sx = int64_t(L->padded[1]) * ((L->d == 3) ? L->padded[2] : 1);
@@ -135,6 +136,12 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.stats = nullptr;
   a.blockX = L->blockX;
   a.blockY = L->blockY;
+  a.kernel = L->kernel;
+  const Geometry& g = a.g;
+  const int64_t first = g.sx + g.sy + g.pz;
+  const int64_t last = int64_t(g.nx) * g.sx + int64_t(g.ny) * g.sy + (g.nz - 1 + g.pz);
+  a.flatBase = first / 8 * 8;
+  a.flatEnd = last + 1;
   return a;
 }
 
@@ -172,8 +179,8 @@ void rotate_all(lbx_lattice_s* L) {
   for (int i = 0; i < L->q; ++i) {
     const int* c = velocity(L->q, i);
     const int64_t off = c[0] * g.sx + c[1] * g.sy + ((L->d == 3) ? c[2] : 0);
-    int64_t s = (L->shift[i] - off) % L->n;
-    if (s < 0) s += L->n;
+    int64_t s = (L->shift[i] - off) % L->stride;
+    if (s < 0) s += L->stride;
     L->shift[i] = s;
   }
 }
@@ -631,9 +638,22 @@ int lbx_population_shift(lbx_lattice L, int32_t pop, int64_t* shift) {
 int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   if (pop < 0 || pop >= L->q) return fail(LBX_ERR_INVALID, "population index out of range");
-  int64_t s = (L->shift[pop] - offset) % L->n;
-  if (s < 0) s += L->n;
+  int64_t s = (L->shift[pop] - offset) % L->stride;
+  if (s < 0) s += L->stride;
   L->shift[pop] = s;
+  return LBX_OK;
+}
+
+int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32_t block_y) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (variant != 0 && variant != 1) return fail(LBX_ERR_INVALID, "variant must be 0 or 1");
+  if (variant == 1) {
+    if (block_x < 1 || block_y < 1 || block_x * block_y > 256 || (block_x * block_y) % 32 != 0)
+      return fail(LBX_ERR_INVALID, "block must hold a multiple of 32 and at most 256 threads");
+    L->blockX = block_x;
+    L->blockY = block_y;
+  }
+  L->kernel = variant;
   return LBX_OK;
 }
 

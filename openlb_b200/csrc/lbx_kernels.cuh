@@ -186,6 +186,153 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
   if (stats) block_stats<R>(rho, usq, valid, stats);
 }
 
+// ---- fused collide + PS stream, shared-memory staged tiles -----------------------------
+// A block owns TILE consecutive cells of the flat padded index space (ghost and spare cells
+// included; only core cells are computed and stored).  Because every population column is
+// shifted by its own amount, the TILE values of population i sit at an arbitrary, per-
+// population offset in HBM.  The block therefore copies each population's span as aligned
+// 16-byte chunks into shared memory (one extra chunk absorbs the misalignment), computes
+// from shared memory, and writes the span back as aligned 16-byte chunks; only chunks that
+// straddle a non-core cell fall back to element stores, so no slot owned by another block is
+// ever written.  The column period P is a multiple of the vector width, so a chunk never
+// straddles the cyclic wrap.
+constexpr int TILE = 256;
+
+template <typename S> struct Vec;
+template <> struct Vec<double> { static constexpr int V = 2; using T = double2; };
+template <> struct Vec<float> { static constexpr int V = 4; using T = float4; };
+template <> struct Vec<__half> { static constexpr int V = 8; using T = uint4; };
+template <> struct Vec<__nv_bfloat16> { static constexpr int V = 8; using T = uint4; };
+
+template <int Q, typename S>
+constexpr int tile_smem_bytes() {
+  return Q * (TILE / Vec<S>::V + 1) * Vec<S>::V * int(sizeof(S));
+}
+
+template <int Q, typename S, int DYN>
+__global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                               int64_t base, int64_t nFlat,
+                                                               CollisionParams<typename Storage<S>::R> p,
+                                                               const uint8_t* __restrict__ cellDyn,
+                                                               StatAcc* __restrict__ stats) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  using VT = typename Vec<S>::T;
+  constexpr int V = Vec<S>::V;
+  constexpr int NCH = TILE / V + 1;   // chunks per population span
+  constexpr int SPAN = NCH * V;       // shared-memory elements per population
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);
+  __shared__ int64_t sA[Q];  // aligned start of the span in the column
+  __shared__ int sR[Q];      // misalignment of the span
+  __shared__ uint8_t sCore[TILE];
+
+  const int tid = threadIdx.x;
+  const int64_t t0 = base + int64_t(blockIdx.x) * TILE;
+  const int64_t n = t0 + tid;
+
+  // decode the cell of this thread
+  int x = -1, y = -1, z = -1;
+  bool core = false;
+  if (n < nFlat) {
+    const int64_t px = n / g.sx;
+    const int64_t rem = n - px * g.sx;
+    const int64_t py = rem / g.sy;
+    const int64_t pzz = rem - py * g.sy;
+    x = int(px) - 1;
+    y = int(py) - 1;
+    z = int(pzz) - g.pz;
+    core = x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+  }
+  sCore[tid] = core ? 1 : 0;
+  static_for<Q>([&](auto I) {
+    if (tid == I) {
+      const int64_t st = wrap_add(t0, sh.s[I], g.n);
+      const int r = int(st % V);
+      sR[I] = r;
+      sA[I] = st - r;
+    }
+  });
+  if (!__syncthreads_or(core)) return;
+
+  // load: aligned 16-byte chunks of every population span into shared memory
+  for (int c = tid; c < Q * NCH; c += TILE) {
+    const int i = c / NCH;
+    const int k = c - i * NCH;
+    int64_t a = sA[i] + int64_t(k) * V;
+    if (a >= g.n) a -= g.n;
+    *reinterpret_cast<VT*>(sm + i * SPAN + k * V) = *reinterpret_cast<const VT*>(pop + i * g.stride + a);
+  }
+  __syncthreads();
+
+  R rho = R(-1), usq = R(-1);
+  bool valid = false;
+  if (core) {
+    const uint8_t kind = cellDyn ? cellDyn[n] : uint8_t(1);
+    R f[Q];
+    static_for<Q>([&](auto I) { f[I] = Storage<S>::load(sm + I * SPAN + sR[I] + tid); });
+    if (kind == 1) {
+      collide<Q, R, DYN>(f, p, rho, usq);
+      valid = true;
+    } else if (kind == 2) {
+      revert<Q, R>(f);
+    }
+    if (kind != 0) {
+      static_for<Q>([&](auto I) { Storage<S>::store(sm + I * SPAN + sR[I] + tid, f[I]); });
+    }
+    // periodic overlap (see k_collide_stream): values that leave across a periodic face go to
+    // the ghost cell the rotation carries into the opposite face
+    if (g.pmask) {
+      const bool edge = ((g.pmask & 1) && (x == 0 || x == g.nx - 1)) ||
+                        ((g.pmask & 2) && (y == 0 || y == g.ny - 1)) ||
+                        (D::d == 3 && (g.pmask & 4) && (z == 0 || z == g.nz - 1));
+      if (edge) {
+        static_for<Q>([&](auto I) {
+          constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+          int tx = x + cx, ty = y + cy, tz = z + cz;
+          bool crossed = false, lost = false;
+          if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+          if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+          if constexpr (D::d == 3) {
+            if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+          }
+          if (crossed && !lost) {
+            const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+            Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
+          }
+        });
+      }
+    }
+  }
+  if (stats) block_stats<R>(rho, usq, valid, stats);
+  __syncthreads();
+
+  // store: aligned chunks whose cells are all core cells of this tile; element stores elsewhere
+  for (int c = tid; c < Q * NCH; c += TILE) {
+    const int i = c / NCH;
+    const int k = c - i * NCH;
+    const int j0 = k * V - sR[i];
+    int64_t a = sA[i] + int64_t(k) * V;
+    if (a >= g.n) a -= g.n;
+    const S* src = sm + i * SPAN + k * V;
+    S* dst = pop + i * g.stride + a;
+    bool full = j0 >= 0 && j0 + V <= TILE;
+    if (full) {
+#pragma unroll
+      for (int e = 0; e < V; ++e) full = full && sCore[j0 + e];
+    }
+    if (full) {
+      *reinterpret_cast<VT*>(dst) = *reinterpret_cast<const VT*>(src);
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const int j = j0 + e;
+        if (j >= 0 && j < TILE && sCore[j]) dst[e] = src[e];
+      }
+    }
+  }
+}
+
 // ---- halfway bounce-back links (PostStream) ---------------------------------------------
 // f_opp(k)(x_b) = f_k(x_b + c_k) - delta, delta = 2 (c_k . u_w) t_k / c_s^2.
 template <int Q, typename S>
@@ -422,6 +569,9 @@ struct LaunchArgs {
   const uint8_t* cellDyn;
   StatAcc* stats;
   int blockX, blockY;
+  int kernel;          // 0: shared-memory staged tiles, 1: one cell per thread
+  int64_t flatBase;    // first tile start (multiple of 8) and end of the flat cell range
+  int64_t flatEnd;
 };
 
 template <int Q, typename S>
@@ -466,26 +616,46 @@ inline int64_t ncore_of(const Geometry& g) { return int64_t(g.nx) * g.ny * g.nz;
 
 #ifdef LBX_KERNEL_TU
 // Launcher bodies: compiled only in the per-storage instantiation units.
-template <int Q, typename S>
-cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream) {
+template <int Q, typename S, int DYN>
+cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
   using R = typename Storage<S>::R;
   const Geometry& g = a.g;
-  dim3 block(a.blockX, a.blockY, 1);
-  dim3 grid;
-  if (Desc<Q>::d == 3) grid = dim3((g.nz + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
-  else grid = dim3((g.ny + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
   const auto sh = shifts_of<Q>(a);
   const auto p = params_of<R>(a);
   S* pop = static_cast<S*>(a.pop);
-  switch (a.dynamics) {
-  case DYN_BGK: k_collide_stream<Q, S, DYN_BGK><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
-  case DYN_TRT: k_collide_stream<Q, S, DYN_TRT><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
-  case DYN_SMAGORINSKY: k_collide_stream<Q, S, DYN_SMAGORINSKY><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
-  case DYN_FORCED_BGK: k_collide_stream<Q, S, DYN_FORCED_BGK><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
-  case DYN_FORCED_SMAGORINSKY: k_collide_stream<Q, S, DYN_FORCED_SMAGORINSKY><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats); break;
-  default: return cudaErrorInvalidValue;
+  if (a.kernel == 0) {
+    constexpr int smem = tile_smem_bytes<Q, S>();
+    static unsigned long long configured = 0;  // one bit per device ordinal
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured >> (dev & 63) & 1ull)) {
+      cudaError_t e = cudaFuncSetAttribute(k_collide_stream_tiled<Q, S, DYN>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      if (e != cudaSuccess) return e;
+      configured |= 1ull << (dev & 63);
+    }
+    const int64_t tiles = (a.flatEnd - a.flatBase + TILE - 1) / TILE;
+    k_collide_stream_tiled<Q, S, DYN><<<unsigned(tiles), TILE, smem, stream>>>(pop, g, sh, a.flatBase, a.flatEnd, p,
+                                                                                a.cellDyn, a.stats);
+  } else {
+    dim3 block(a.blockX, a.blockY, 1);
+    dim3 grid;
+    if (Desc<Q>::d == 3) grid = dim3((g.nz + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
+    else grid = dim3((g.ny + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
+    k_collide_stream<Q, S, DYN><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats);
   }
   return cudaGetLastError();
+}
+template <int Q, typename S>
+cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream) {
+  switch (a.dynamics) {
+  case DYN_BGK: return launch_step_dyn<Q, S, DYN_BGK>(a, stream);
+  case DYN_TRT: return launch_step_dyn<Q, S, DYN_TRT>(a, stream);
+  case DYN_SMAGORINSKY: return launch_step_dyn<Q, S, DYN_SMAGORINSKY>(a, stream);
+  case DYN_FORCED_BGK: return launch_step_dyn<Q, S, DYN_FORCED_BGK>(a, stream);
+  case DYN_FORCED_SMAGORINSKY: return launch_step_dyn<Q, S, DYN_FORCED_SMAGORINSKY>(a, stream);
+  default: return cudaErrorInvalidValue;
+  }
 }
 template <int Q, typename S>
 cudaError_t launch_bouzidi(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
