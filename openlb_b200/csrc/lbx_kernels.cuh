@@ -235,10 +235,12 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
   int x = -1, y = -1, z = -1;
   bool core = false;
   if (n < nFlat) {
-    const int64_t px = n / g.sx;
-    const int64_t rem = n - px * g.sx;
-    const int64_t py = rem / g.sy;
-    const int64_t pzz = rem - py * g.sy;
+    // the padded block holds fewer than 2^32 cells (checked at creation): 32-bit division
+    const unsigned un = unsigned(n), usx = unsigned(g.sx), usy = unsigned(g.sy);
+    const unsigned px = un / usx;
+    const unsigned rem = un - px * usx;
+    const unsigned py = rem / usy;
+    const unsigned pzz = rem - py * usy;
     x = int(px) - 1;
     y = int(py) - 1;
     z = int(pzz) - g.pz;
@@ -255,14 +257,18 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
   });
   if (!__syncthreads_or(core)) return;
 
-  // load: aligned 16-byte chunks of every population span into shared memory
+  // load: aligned 16-byte chunks of every population span into shared memory, all issued as
+  // asynchronous copies (cp.async, L2 only) before the first wait
   for (int c = tid; c < Q * NCH; c += TILE) {
     const int i = c / NCH;
     const int k = c - i * NCH;
     int64_t a = sA[i] + int64_t(k) * V;
     if (a >= g.n) a -= g.n;
-    *reinterpret_cast<VT*>(sm + i * SPAN + k * V) = *reinterpret_cast<const VT*>(pop + i * g.stride + a);
+    const unsigned dst = unsigned(__cvta_generic_to_shared(sm + i * SPAN + k * V));
+    const S* src = pop + i * g.stride + a;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
 
   R rho = R(-1), usq = R(-1);
