@@ -190,9 +190,12 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
 
 /* Launch configuration of the step kernel, the knob the autotuner turns (no reference
  * counterpart; the reference's CUDA platform launches fixed 32-thread blocks,
- * gpu/cuda/operator.hh:425-441).  variant 0: shared-memory staged tiles of 256 cells
- * (default); variant 1: one cell per thread in (block_x, block_y) blocks. */
-int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y);
+ * gpu/cuda/operator.hh:425-441).  variant 0: pipelined shared-memory tiles of 256 cells;
+ * variant 1: one cell per thread in (block_x, block_y) blocks; variant 2 (default):
+ * cells_per_thread (1, 2 or 4) consecutive cells per thread in (block_x, block_y) blocks,
+ * block_x along the fastest axis. */
+int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y,
+                          int32_t cells_per_thread);
 
 #ifdef __cplusplus
 }

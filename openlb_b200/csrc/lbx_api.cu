@@ -102,7 +102,8 @@ struct lbx_lattice_s {
   int dynamics = LBX_BGK;
   lbx_params params{1.0, 0.25, 0.12, {0, 0, 0}};
   int blockX = 256, blockY = 1;
-  int kernel = 0;
+  int kernel = 2;
+  int cellsPerThread = 1;
   int64_t bytes = 0;
 };
 
@@ -137,6 +138,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.blockX = L->blockX;
   a.blockY = L->blockY;
   a.kernel = L->kernel;
+  a.cellsPerThread = L->cellsPerThread;
   const Geometry& g = a.g;
   const int64_t first = g.sx + g.sy + g.pz;
   const int64_t last = int64_t(g.nx) * g.sx + int64_t(g.ny) * g.sy + (g.nz - 1 + g.pz);
@@ -185,12 +187,22 @@ void rotate_all(lbx_lattice_s* L) {
   }
 }
 
+// Threads along the fastest core axis, filled up to 256 per block; the rest of the block
+// spans the next axis.
+void block_shape_for(int nf, int cellsPerThread, int& bx, int& by) {
+  const int groups = (nf + cellsPerThread - 1) / cellsPerThread;
+  bx = 32;
+  while (bx < groups && bx < 256) bx *= 2;
+  by = 256 / bx;
+}
+
 void default_block_shape(lbx_lattice_s* L) {
   const int nf = (L->d == 3) ? L->core[2] : L->core[1];
-  int bx = 32;
-  while (bx < nf && bx < 256) bx *= 2;
-  L->blockX = bx;
-  L->blockY = 256 / bx;
+  // K cells per thread: one 16-byte span of storage per population and thread
+  L->cellsPerThread = (L->storage == LBX_F64) ? 1 : (L->storage == LBX_F32 ? 2 : 4);
+  L->kernel = (L->stride < (int64_t(1) << 31)) ? 2 : 1;
+  if (L->kernel == 1) L->cellsPerThread = 1;
+  block_shape_for(nf, L->cellsPerThread, L->blockX, L->blockY);
 }
 
 int ensure_stage(lbx_lattice_s* L) {
@@ -644,15 +656,21 @@ int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
   return LBX_OK;
 }
 
-int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32_t block_y) {
+int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32_t block_y,
+                          int32_t cells_per_thread) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
-  if (variant != 0 && variant != 1) return fail(LBX_ERR_INVALID, "variant must be 0 or 1");
-  if (variant == 1) {
+  if (variant < 0 || variant > 2) return fail(LBX_ERR_INVALID, "variant must be 0, 1 or 2");
+  if (variant == 2 && L->stride >= (int64_t(1) << 31))
+    return fail(LBX_ERR_UNSUPPORTED, "variant 2 needs a column period below 2^31 cells");
+  if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2 && cells_per_thread != 4)
+    return fail(LBX_ERR_INVALID, "cells_per_thread must be 1, 2 or 4");
+  if (variant != 0) {
     if (block_x < 1 || block_y < 1 || block_x * block_y > 256 || (block_x * block_y) % 32 != 0)
       return fail(LBX_ERR_INVALID, "block must hold a multiple of 32 and at most 256 threads");
     L->blockX = block_x;
     L->blockY = block_y;
   }
+  L->cellsPerThread = variant == 2 ? cells_per_thread : 1;
   L->kernel = variant;
   return LBX_OK;
 }

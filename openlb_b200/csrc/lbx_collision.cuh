@@ -58,7 +58,12 @@ __device__ __forceinline__ void moments(const R (&f)[Q], const R* force, R& rho,
       else if constexpr (c == -1) u[A] -= f[I];
     });
   });
-  static_for<D::d>([&](auto A) { u[A] /= rho; });
+  if constexpr (sizeof(R) == 8) {
+    static_for<D::d>([&](auto A) { u[A] /= rho; });  // FP64: the reference's exact division
+  } else {
+    const R inv = R(1) / rho;  // FP32 collision: one division, within the FP32 tolerance
+    static_for<D::d>([&](auto A) { u[A] *= inv; });
+  }
   if constexpr (FORCED) {
     static_for<D::d>([&](auto A) { u[A] += force[A] * R(0.5); });
   }

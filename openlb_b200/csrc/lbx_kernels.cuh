@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
     const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
     const uint8_t kind = cellDyn ? cellDyn[n] : uint8_t(1);
     R f[Q];
-    const bool needPops = kind != 0 || g.pmask != 0;
+    const bool needPops = kind != 0;
     if (needPops) {
       static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
     }
@@ -158,44 +158,25 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
       static_for<Q>([&](auto I) { Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), f[I]); });
     }
 
-    // periodic overlap: post-collision values that leave the core across a periodic face are
-    // written into the ghost cell from which the rotation will carry them into the opposite face
-    if (g.pmask) {
-      const bool edge = ((g.pmask & 1) && (x == 0 || x == g.nx - 1)) ||
-                        ((g.pmask & 2) && (y == 0 || y == g.ny - 1)) ||
-                        (D::d == 3 && (g.pmask & 4) && (z == 0 || z == g.nz - 1));
-      if (edge) {
-        static_for<Q>([&](auto I) {
-          constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
-          int tx = x + cx, ty = y + cy, tz = z + cz;
-          bool crossed = false, lost = false;
-          if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
-          if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
-          if constexpr (D::d == 3) {
-            if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
-          }
-          if (crossed && !lost) {
-            const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
-            Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
-          }
-        });
-      }
-    }
   }
 
   if (stats) block_stats<R>(rho, usq, valid, stats);
 }
 
-// ---- fused collide + PS stream, shared-memory staged tiles -----------------------------
-// A block owns TILE consecutive cells of the flat padded index space (ghost and spare cells
-// included; only core cells are computed and stored).  Because every population column is
-// shifted by its own amount, the TILE values of population i sit at an arbitrary, per-
-// population offset in HBM.  The block therefore copies each population's span as aligned
-// 16-byte chunks into shared memory (one extra chunk absorbs the misalignment), computes
-// from shared memory, and writes the span back as aligned 16-byte chunks; only chunks that
-// straddle a non-core cell fall back to element stores, so no slot owned by another block is
-// ever written.  The column period P is a multiple of the vector width, so a chunk never
-// straddles the cyclic wrap.
+// ---- fused collide + PS stream, pipelined shared-memory tiles --------------------------
+// A tile is TILE consecutive cells of the flat padded index space (ghost and spare cells
+// included; only core cells are computed and stored).  Every population column is shifted by
+// its own amount, so the TILE values of population i sit at a per-population offset in HBM.
+// The tile's span of each population is copied as aligned 16-byte chunks into shared memory
+// (one extra chunk absorbs the misalignment), computed there, and written back as aligned
+// 16-byte chunks; only chunks that straddle a non-core cell fall back to element stores, so
+// no slot owned by another tile is ever written.  The column period P is a multiple of the
+// vector width and every tile starts at a multiple of it, so the misalignment of population
+// i is s_i mod V for every tile and a chunk never straddles the cyclic wrap.
+//
+// Blocks are persistent and run a STAGES-deep cp.async pipeline: while tile k is computed
+// and stored, the loads of tiles k+1 .. k+STAGES-1 are in flight, which keeps enough bytes
+// outstanding per SM to saturate HBM independently of the register count.
 constexpr int TILE = 256;
 
 template <typename S> struct Vec;
@@ -205,138 +186,344 @@ template <> struct Vec<__half> { static constexpr int V = 8; using T = uint4; };
 template <> struct Vec<__nv_bfloat16> { static constexpr int V = 8; using T = uint4; };
 
 template <int Q, typename S>
-constexpr int tile_smem_bytes() {
-  return Q * (TILE / Vec<S>::V + 1) * Vec<S>::V * int(sizeof(S));
+struct TileCfg {
+  static constexpr int V = Vec<S>::V;
+  static constexpr int NCH = TILE / V + 1;  // 16-byte chunks per population span
+  static constexpr int SPAN = NCH * V;      // elements per population per stage
+  static constexpr int STAGE_BYTES = Q * SPAN * int(sizeof(S));
+  static constexpr int STAGES = (4 * STAGE_BYTES <= 100 * 1024) ? 4 : ((3 * STAGE_BYTES <= 120 * 1024) ? 3 : 2);
+  static constexpr int SMEM = STAGES * STAGE_BYTES;
+};
+
+// Post-collision values that leave the core across a periodic face are written into the ghost
+// cell from which the next rotation carries them into the opposite face (the reference's
+// PostCollide overlap copy, core/superLattice.hh:150-155, gpu/cuda/communicator.hh:111-124).
+template <int Q, typename S>
+__device__ __forceinline__ void periodic_ghost_writes(S* __restrict__ pop, const Geometry& g, const Shifts<Q>& sh,
+                                                      int x, int y, int z, const typename Storage<S>::R (&f)[Q]) {
+  using D = Desc<Q>;
+  const bool edge = ((g.pmask & 1) && (x == 0 || x == g.nx - 1)) || ((g.pmask & 2) && (y == 0 || y == g.ny - 1)) ||
+                    (D::d == 3 && (g.pmask & 4) && (z == 0 || z == g.nz - 1));
+  if (!edge) return;
+  static_for<Q>([&](auto I) {
+    constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+    int tx = x + cx, ty = y + cy, tz = z + cz;
+    bool crossed = false, lost = false;
+    if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+    if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+    if constexpr (D::d == 3) {
+      if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+    }
+    if (crossed && !lost) {
+      const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+      Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
+    }
+  });
+}
+
+// Core coordinates of flat padded cell n (< 2^32: checked at lattice creation).
+__device__ __forceinline__ bool decode_cell(const Geometry& g, int64_t n, int64_t nFlat, int& x, int& y, int& z) {
+  if (n >= nFlat) return false;
+  const unsigned un = unsigned(n), usx = unsigned(g.sx), usy = unsigned(g.sy);
+  const unsigned px = un / usx;
+  const unsigned rem = un - px * usx;
+  const unsigned py = rem / usy;
+  x = int(px) - 1;
+  y = int(py) - 1;
+  z = int(rem - py * usy) - g.pz;
+  return x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
 }
 
 template <int Q, typename S, int DYN>
 __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
-                                                               int64_t base, int64_t nFlat,
+                                                               int64_t base, int64_t nFlat, int64_t nTiles,
+                                                               CollisionParams<typename Storage<S>::R> p,
+                                                               const uint8_t* __restrict__ cellDyn,
+                                                               StatAcc* __restrict__ stats) {
+  using R = typename Storage<S>::R;
+  using C = TileCfg<Q, S>;
+  using VT = typename Vec<S>::T;
+  constexpr int V = C::V, NCH = C::NCH, SPAN = C::SPAN, STAGES = C::STAGES;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sm = reinterpret_cast<S*>(smem_raw);  // [STAGES][Q][SPAN]
+  __shared__ int64_t sShift[Q];
+  __shared__ int sR[Q];
+  __shared__ uint8_t sCore[STAGES][TILE];
+
+  const int tid = threadIdx.x;
+  static_for<Q>([&](auto I) {
+    if (tid == I) {
+      sShift[I] = sh.s[I];
+      sR[I] = int(sh.s[I] % V);
+    }
+  });
+  __syncthreads();
+
+  // issue the cp.async copies of one tile into one stage (an empty group past the last tile)
+  auto issue = [&](int64_t tile, int st) {
+    if (tile < nTiles) {
+      const int64_t t0 = base + tile * TILE;
+      int x, y, z;
+      sCore[st][tid] = decode_cell(g, t0 + tid, nFlat, x, y, z) ? 1 : 0;
+      S* stage = sm + st * (Q * SPAN);
+      for (int c = tid; c < Q * NCH; c += TILE) {
+        const int i = c / NCH;
+        const int k = c - i * NCH;
+        int64_t a = wrap_add(t0, sShift[i], g.n) - sR[i] + int64_t(k) * V;
+        if (a >= g.n) a -= g.n;
+        const unsigned dst = unsigned(__cvta_generic_to_shared(stage + i * SPAN + k * V));
+        const S* src = pop + i * g.stride + a;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+
+  double accRho = 0.0, accUsq = 0.0, accMax = 0.0;
+  unsigned accCount = 0;
+
+  const int64_t stride = gridDim.x;
+  for (int s = 0; s < STAGES - 1; ++s) issue(blockIdx.x + s * stride, s);
+
+  int k = 0;
+  for (int64_t tile = blockIdx.x; tile < nTiles; tile += stride, ++k) {
+    const int st = k % STAGES;
+    issue(tile + (STAGES - 1) * stride, (k + STAGES - 1) % STAGES);
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(STAGES - 1) : "memory");
+    __syncthreads();
+
+    S* stage = sm + st * (Q * SPAN);
+    const int64_t n = base + tile * TILE + tid;
+    int x, y, z;
+    if (decode_cell(g, n, nFlat, x, y, z)) {
+      const uint8_t kind = cellDyn ? cellDyn[n] : uint8_t(1);
+      R f[Q];
+      static_for<Q>([&](auto I) { f[I] = Storage<S>::load(stage + I * SPAN + sR[I] + tid); });
+      if (kind == 1) {
+        R rho, usq;
+        collide<Q, R, DYN>(f, p, rho, usq);
+        accRho += double(rho);
+        accUsq += double(usq);
+        accMax = fmax(accMax, double(usq));
+        ++accCount;
+      } else if (kind == 2) {
+        revert<Q, R>(f);
+      }
+      if (kind != 0) {
+        static_for<Q>([&](auto I) { Storage<S>::store(stage + I * SPAN + sR[I] + tid, f[I]); });
+      }
+    }
+    __syncthreads();
+
+    const int64_t t0 = base + tile * TILE;
+    for (int c = tid; c < Q * NCH; c += TILE) {
+      const int i = c / NCH;
+      const int kk = c - i * NCH;
+      const int j0 = kk * V - sR[i];
+      int64_t a = wrap_add(t0, sShift[i], g.n) - sR[i] + int64_t(kk) * V;
+      if (a >= g.n) a -= g.n;
+      const S* src = stage + i * SPAN + kk * V;
+      S* dst = pop + i * g.stride + a;
+      bool full = j0 >= 0 && j0 + V <= TILE;
+      if (full) {
+#pragma unroll
+        for (int e = 0; e < V; ++e) full = full && sCore[st][j0 + e];
+      }
+      if (full) {
+        *reinterpret_cast<VT*>(dst) = *reinterpret_cast<const VT*>(src);
+      } else {
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+          const int j = j0 + e;
+          if (j >= 0 && j < TILE && sCore[st][j]) dst[e] = src[e];
+        }
+      }
+    }
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+
+  if (stats) {
+    double a = accRho, b = accUsq, m = accMax;
+    unsigned c = accCount;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if ((tid & 31) == 0 && c > 0) {
+      atomicAdd(&stats->sum[0], a);
+      atomicAdd(&stats->sum[1], b);
+      atomicAdd(&stats->count, (unsigned long long)c);
+      atomicMax(&stats->maxbits, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// ---- fused collide + PS stream, K consecutive cells per thread --------------------------
+// One thread owns K consecutive cells along the fastest core axis (z in 3D, y in 2D).  For
+// every population it forms ONE wrapped column index; the K values are then reached with
+// constant offsets (a separate per-element wrap is only needed in the rare group that
+// straddles the cyclic end of the column).  All K*Q loads are issued before the first
+// collision.  Periodic faces are handled by k_periodic_halo after this kernel, so the hot
+// kernel carries no face logic.  Column indices are 32-bit: the column period is < 2^31.
+template <int Q>
+struct ColumnBases {
+  void* base[Q];   // start of population column i
+  uint32_t s[Q];   // current shift of column i
+};
+
+template <int Q, typename S, int DYN, int K>
+__global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
                                                                StatAcc* __restrict__ stats) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
-  using VT = typename Vec<S>::T;
-  constexpr int V = Vec<S>::V;
-  constexpr int NCH = TILE / V + 1;   // chunks per population span
-  constexpr int SPAN = NCH * V;       // shared-memory elements per population
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* sm = reinterpret_cast<S*>(smem_raw);
-  __shared__ int64_t sA[Q];  // aligned start of the span in the column
-  __shared__ int sR[Q];      // misalignment of the span
-  __shared__ uint8_t sCore[TILE];
-
-  const int tid = threadIdx.x;
-  const int64_t t0 = base + int64_t(blockIdx.x) * TILE;
-  const int64_t n = t0 + tid;
-
-  // decode the cell of this thread
-  int x = -1, y = -1, z = -1;
-  bool core = false;
-  if (n < nFlat) {
-    // the padded block holds fewer than 2^32 cells (checked at creation): 32-bit division
-    const unsigned un = unsigned(n), usx = unsigned(g.sx), usy = unsigned(g.sy);
-    const unsigned px = un / usx;
-    const unsigned rem = un - px * usx;
-    const unsigned py = rem / usy;
-    const unsigned pzz = rem - py * usy;
-    x = int(px) - 1;
-    y = int(py) - 1;
-    z = int(pzz) - g.pz;
-    core = x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+  const uint32_t P = uint32_t(g.n);
+  int x, y, z0, nvalid;
+  bool inside;
+  {
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y * blockDim.y + threadIdx.y;
+    if constexpr (D::d == 3) {
+      z0 = gi * K; y = m; x = blockIdx.z;
+      inside = z0 < g.nz && y < g.ny;
+      nvalid = g.nz - z0;
+    } else {
+      z0 = gi * K; x = m; y = 0;
+      inside = z0 < g.ny && x < g.nx;
+      nvalid = g.ny - z0;
+    }
   }
-  sCore[tid] = core ? 1 : 0;
+  double accRho = 0.0, accUsq = 0.0, accMax = 0.0;
+  unsigned accCount = 0;
+  if (inside) {
+    // 3D: (x+1)*sx + (y+1)*sy + z0 + 1; 2D: the fast axis is y (sy = 1), z absent
+    const uint32_t n0 = (D::d == 3) ? uint32_t((x + 1) * g.sx + (y + 1) * g.sy + z0 + 1)
+                                    : uint32_t((x + 1) * g.sx + z0 + 1);
+    R f[K][Q];
+    static_for<Q>([&](auto I) {
+      uint32_t idx = n0 + cols.s[I];
+      if (idx >= P) idx -= P;
+      const S* col = static_cast<const S*>(cols.base[I]);
+      if (idx + K <= P) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (k < nvalid) f[k][I] = Storage<S>::load(col + idx + k);
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          uint32_t ik = idx + k;
+          if (ik >= P) ik -= P;
+          if (k < nvalid) f[k][I] = Storage<S>::load(col + ik);
+        }
+      }
+    });
+    uint8_t kinds[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      kinds[k] = (k < nvalid) ? (cellDyn ? cellDyn[n0 + k] : uint8_t(1)) : uint8_t(0);
+      if (kinds[k] == 1) {
+        R rho, usq;
+        collide<Q, R, DYN>(f[k], p, rho, usq);
+        accRho += double(rho);
+        accUsq += double(usq);
+        accMax = fmax(accMax, double(usq));
+        ++accCount;
+      } else if (kinds[k] == 2) {
+        revert<Q, R>(f[k]);
+      }
+    }
+    static_for<Q>([&](auto I) {
+      uint32_t idx = n0 + cols.s[I];
+      if (idx >= P) idx -= P;
+      S* col = static_cast<S*>(cols.base[I]);
+      if (idx + K <= P) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          if (kinds[k] != 0) Storage<S>::store(col + idx + k, f[k][I]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          uint32_t ik = idx + k;
+          if (ik >= P) ik -= P;
+          if (kinds[k] != 0) Storage<S>::store(col + ik, f[k][I]);
+        }
+      }
+    });
+  }
+  if (stats) {
+    double a = accRho, b = accUsq, m = accMax;
+    unsigned c = accCount;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      b += __shfl_xor_sync(0xffffffffu, b, o);
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (((threadIdx.x + threadIdx.y * blockDim.x) & 31) == 0 && c > 0) {
+      atomicAdd(&stats->sum[0], a);
+      atomicAdd(&stats->sum[1], b);
+      atomicAdd(&stats->count, (unsigned long long)c);
+      atomicMax(&stats->maxbits, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// ---- periodic overlap copy (PostCollide) --------------------------------------------------
+// After the collision, every population that leaves the core across a periodic face is
+// copied into the ghost cell from which the next rotation carries it into the opposite face
+// -- the single-block form of the reference's periodic overlap communication
+// (core/superLattice.hh:150-155, gpu/cuda/communicator.hh:111-124).  One thread per cell of
+// each periodic face pair; a cell on an edge is visited once per face and writes the same
+// value to the same ghost slot each time.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_periodic_halo(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
+                                                       int64_t cntX, int64_t cntY, int64_t cntZ) {
+  using D = Desc<Q>;
+  int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  int x, y, z;
+  if (t < cntX) {
+    const int64_t plane = int64_t(g.ny) * g.nz;
+    x = (t / plane) ? g.nx - 1 : 0;
+    const int64_t r = t % plane;
+    y = int(r / g.nz);
+    z = int(r % g.nz);
+  } else if ((t -= cntX) < cntY) {
+    const int64_t plane = int64_t(g.nx) * g.nz;
+    y = (t / plane) ? g.ny - 1 : 0;
+    const int64_t r = t % plane;
+    x = int(r / g.nz);
+    z = int(r % g.nz);
+  } else if ((t -= cntY) < cntZ) {
+    const int64_t plane = int64_t(g.nx) * g.ny;
+    z = (t / plane) ? g.nz - 1 : 0;
+    const int64_t r = t % plane;
+    x = int(r / g.ny);
+    y = int(r % g.ny);
+  } else {
+    return;
+  }
+  const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
   static_for<Q>([&](auto I) {
-    if (tid == I) {
-      const int64_t st = wrap_add(t0, sh.s[I], g.n);
-      const int r = int(st % V);
-      sR[I] = r;
-      sA[I] = st - r;
+    constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+    int tx = x + cx, ty = y + cy, tz = z + cz;
+    bool crossed = false, lost = false;
+    if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+    if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+    if constexpr (D::d == 3) {
+      if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+    }
+    if (crossed && !lost) {
+      const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+      S* col = pop + I * g.stride;
+      col[wrap_add(gn, sh.s[I], g.n)] = col[wrap_add(n, sh.s[I], g.n)];
     }
   });
-  if (!__syncthreads_or(core)) return;
-
-  // load: aligned 16-byte chunks of every population span into shared memory, all issued as
-  // asynchronous copies (cp.async, L2 only) before the first wait
-  for (int c = tid; c < Q * NCH; c += TILE) {
-    const int i = c / NCH;
-    const int k = c - i * NCH;
-    int64_t a = sA[i] + int64_t(k) * V;
-    if (a >= g.n) a -= g.n;
-    const unsigned dst = unsigned(__cvta_generic_to_shared(sm + i * SPAN + k * V));
-    const S* src = pop + i * g.stride + a;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-  }
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-  __syncthreads();
-
-  R rho = R(-1), usq = R(-1);
-  bool valid = false;
-  if (core) {
-    const uint8_t kind = cellDyn ? cellDyn[n] : uint8_t(1);
-    R f[Q];
-    static_for<Q>([&](auto I) { f[I] = Storage<S>::load(sm + I * SPAN + sR[I] + tid); });
-    if (kind == 1) {
-      collide<Q, R, DYN>(f, p, rho, usq);
-      valid = true;
-    } else if (kind == 2) {
-      revert<Q, R>(f);
-    }
-    if (kind != 0) {
-      static_for<Q>([&](auto I) { Storage<S>::store(sm + I * SPAN + sR[I] + tid, f[I]); });
-    }
-    // periodic overlap (see k_collide_stream): values that leave across a periodic face go to
-    // the ghost cell the rotation carries into the opposite face
-    if (g.pmask) {
-      const bool edge = ((g.pmask & 1) && (x == 0 || x == g.nx - 1)) ||
-                        ((g.pmask & 2) && (y == 0 || y == g.ny - 1)) ||
-                        (D::d == 3 && (g.pmask & 4) && (z == 0 || z == g.nz - 1));
-      if (edge) {
-        static_for<Q>([&](auto I) {
-          constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
-          int tx = x + cx, ty = y + cy, tz = z + cz;
-          bool crossed = false, lost = false;
-          if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
-          if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
-          if constexpr (D::d == 3) {
-            if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
-          }
-          if (crossed && !lost) {
-            const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
-            Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
-          }
-        });
-      }
-    }
-  }
-  if (stats) block_stats<R>(rho, usq, valid, stats);
-  __syncthreads();
-
-  // store: aligned chunks whose cells are all core cells of this tile; element stores elsewhere
-  for (int c = tid; c < Q * NCH; c += TILE) {
-    const int i = c / NCH;
-    const int k = c - i * NCH;
-    const int j0 = k * V - sR[i];
-    int64_t a = sA[i] + int64_t(k) * V;
-    if (a >= g.n) a -= g.n;
-    const S* src = sm + i * SPAN + k * V;
-    S* dst = pop + i * g.stride + a;
-    bool full = j0 >= 0 && j0 + V <= TILE;
-    if (full) {
-#pragma unroll
-      for (int e = 0; e < V; ++e) full = full && sCore[j0 + e];
-    }
-    if (full) {
-      *reinterpret_cast<VT*>(dst) = *reinterpret_cast<const VT*>(src);
-    } else {
-#pragma unroll
-      for (int e = 0; e < V; ++e) {
-        const int j = j0 + e;
-        if (j >= 0 && j < TILE && sCore[j]) dst[e] = src[e];
-      }
-    }
-  }
 }
 
 // ---- halfway bounce-back links (PostStream) ---------------------------------------------
@@ -575,7 +762,8 @@ struct LaunchArgs {
   const uint8_t* cellDyn;
   StatAcc* stats;
   int blockX, blockY;
-  int kernel;          // 0: shared-memory staged tiles, 1: one cell per thread
+  int kernel;          // 0: pipelined shared-memory tiles, 1: one cell per thread, 2: K cells per thread
+  int cellsPerThread;  // K of kernel 2 (1, 2 or 4)
   int64_t flatBase;    // first tile start (multiple of 8) and end of the flat cell range
   int64_t flatEnd;
 };
@@ -630,26 +818,61 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
   const auto p = params_of<R>(a);
   S* pop = static_cast<S*>(a.pop);
   if (a.kernel == 0) {
-    constexpr int smem = tile_smem_bytes<Q, S>();
+    constexpr int smem = TileCfg<Q, S>::SMEM;
     static unsigned long long configured = 0;  // one bit per device ordinal
+    static int residentBlocks[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (!(configured >> (dev & 63) & 1ull)) {
       cudaError_t e = cudaFuncSetAttribute(k_collide_stream_tiled<Q, S, DYN>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
       if (e != cudaSuccess) return e;
+      int perSM = 0, sms = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_collide_stream_tiled<Q, S, DYN>, TILE, smem);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      residentBlocks[dev & 63] = (perSM > 0 ? perSM : 1) * sms;
       configured |= 1ull << (dev & 63);
     }
     const int64_t tiles = (a.flatEnd - a.flatBase + TILE - 1) / TILE;
-    k_collide_stream_tiled<Q, S, DYN><<<unsigned(tiles), TILE, smem, stream>>>(pop, g, sh, a.flatBase, a.flatEnd, p,
-                                                                                a.cellDyn, a.stats);
-  } else {
+    const int64_t grid = tiles < residentBlocks[dev & 63] ? tiles : residentBlocks[dev & 63];
+    k_collide_stream_tiled<Q, S, DYN><<<unsigned(grid), TILE, smem, stream>>>(pop, g, sh, a.flatBase, a.flatEnd,
+                                                                               tiles, p, a.cellDyn, a.stats);
+  } else if (a.kernel == 1) {
     dim3 block(a.blockX, a.blockY, 1);
     dim3 grid;
     if (Desc<Q>::d == 3) grid = dim3((g.nz + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
     else grid = dim3((g.ny + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
     k_collide_stream<Q, S, DYN><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats);
+  } else {
+    ColumnBases<Q> cols;
+    for (int i = 0; i < Q; ++i) {
+      cols.base[i] = pop + int64_t(i) * g.stride;
+      cols.s[i] = uint32_t(a.shift[i]);
+    }
+    const int K = a.cellsPerThread;
+    const int nf = Desc<Q>::d == 3 ? g.nz : g.ny;
+    const int groups = (nf + K - 1) / K;
+    dim3 block(a.blockX, a.blockY, 1);
+    dim3 grid;
+    if (Desc<Q>::d == 3) grid = dim3((groups + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
+    else grid = dim3((groups + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
+    switch (K) {
+    case 1: k_collide_stream_groups<Q, S, DYN, 1><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    case 2: k_collide_stream_groups<Q, S, DYN, 2><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    case 4: k_collide_stream_groups<Q, S, DYN, 4><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    default: return cudaErrorInvalidValue;
+    }
   }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || g.pmask == 0) return e;
+  // periodic overlap copy after the collision
+  const int64_t cntX = (g.pmask & 1) ? 2 * int64_t(g.ny) * g.nz : 0;
+  const int64_t cntY = (g.pmask & 2) ? 2 * int64_t(g.nx) * g.nz : 0;
+  const int64_t cntZ = (g.pmask & 4) ? 2 * int64_t(g.nx) * g.ny : 0;
+  const int64_t total = cntX + cntY + cntZ;
+  k_periodic_halo<Q, S><<<unsigned((total + 255) / 256), 256, 0, stream>>>(pop, g, sh, cntX, cntY, cntZ);
   return cudaGetLastError();
 }
 template <int Q, typename S>

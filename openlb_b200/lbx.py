@@ -70,7 +70,7 @@ def _load() -> C.CDLL:
         "lbx_reduce": ([VP, I32, P(D), VP], C.c_int),
         "lbx_population_shift": ([VP, I32, P(I64)], C.c_int),
         "lbx_rotate": ([VP, I32, I64], C.c_int),
-        "lbx_set_launch_config": ([VP, I32, I32, I32], C.c_int),
+        "lbx_set_launch_config": ([VP, I32, I32, I32, I32], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -262,8 +262,10 @@ class BlockLattice:
         n = {REDUCE_MASS_MOMENTUM: 4, REDUCE_DRAG: 3, REDUCE_RESIDUAL: 3}[what]
         return np.array(out[:n])
 
-    def set_launch_config(self, variant: int, block_x: int = 256, block_y: int = 1) -> None:
-        check(lib.lbx_set_launch_config(self._h, variant, block_x, block_y), "lbx_set_launch_config")
+    def set_launch_config(self, variant: int, block_x: int = 256, block_y: int = 1,
+                          cells_per_thread: int = 1) -> None:
+        check(lib.lbx_set_launch_config(self._h, variant, block_x, block_y, cells_per_thread),
+              "lbx_set_launch_config")
 
     def population_shift(self, pop: int) -> int:
         s = C.c_int64()

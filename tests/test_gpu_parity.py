@@ -232,15 +232,17 @@ def test_invalid_parameters_raise():
                                   "porous_d2q9_trt_f64", "tgv_d3q19_bgk_f32"])
 @pytest.mark.parametrize("storage", ["f64", "f32", "f16dev"])
 def test_kernel_variants_agree_bitwise(name, storage):
-    """The shared-memory tiled step and the one-cell-per-thread step compute identical bits."""
+    """Every step kernel variant and launch shape computes identical bits."""
     fx = L.load_fixture(name)
     setup = L.case_setup(fx)
     outs = []
-    for variant, bx, by in ((0, 256, 1), (1, 64, 4), (1, 32, 8)):
+    for variant, bx, by, k in ((0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2),
+                               (2, 32, 8, 4)):
         lat = make_lattice(setup, storage)
-        lat.set_launch_config(variant, bx, by)
+        lat.set_launch_config(variant, bx, by, k)
         lat.set_populations(np.asarray(fx["f0"], np.float64))
         lat.collide_and_stream(7)
         outs.append(lat.get_populations())
         lat.close()
-    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    for o in outs[1:]:
+        assert np.array_equal(outs[0], o)
