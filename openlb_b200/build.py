@@ -5,7 +5,8 @@
 
 Each .cu under csrc/ is compiled by nvcc for sm_100a only (no PTX for other targets) into
 openlb_b200/_build/, then linked into openlb_b200/lib/liblbx.so.  The FP64 instantiation
-unit is compiled with -fmad=false so its rounding matches the reference's CPU build.
+units are compiled with -fmad=false: FP64 rounds like the reference's CPU build and the float
+kernels fuse only where the source says so, identically in every kernel variant.
 """
 from __future__ import annotations
 
@@ -26,7 +27,10 @@ INCLUDE = PKG.parent / "include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-warn-spills", "-I", str(INCLUDE), "-I", str(CSRC)]
-PER_UNIT = {"lbx_inst_f64.cu": ["-fmad=false"]}
+# No implicit FMA contraction anywhere: FP64 keeps the reference's rounding, and the float
+# kernels contract only where lbx_collision.cuh says so, identically in every kernel variant.
+PER_UNIT = {}
+COMMON.append("-fmad=false")
 
 
 def nvcc() -> str:

@@ -83,12 +83,20 @@ __device__ __forceinline__ R c_dot(const R (&u)[3]) {
   return cu;
 }
 
-// f_i^eq - w_i (second order).
+// f_i^eq - w_i (second order).  FP64 keeps the reference's operation sequence (no fused
+// operations: the FP64 unit is built with -fmad=false); the float arithmetic of the FP32 and
+// reduced-precision forms uses explicit fused multiply-adds.  Every unit is built without
+// implicit contraction, so each kernel variant and launch shape rounds identically.
 template <int Q, int I, typename R>
 __device__ __forceinline__ R equilibrium(R rho, const R (&u)[3], R uSqr) {
   constexpr R t = weight<Q, R>(I);
   const R cu = c_dot<Q, I>(u);
-  return rho * t * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * uSqr) - t;
+  if constexpr (sizeof(R) == 8) {
+    return rho * t * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * uSqr) - t;
+  } else {
+    const R e = __fmaf_rn(R(4.5) * cu, cu, __fmaf_rn(R(3), cu, R(1) - R(1.5) * uSqr));
+    return __fmaf_rn(rho * t, e, -t);
+  }
 }
 
 // Effective relaxation frequency of the Smagorinsky model.
@@ -174,8 +182,12 @@ __device__ __forceinline__ void collide(R (&f)[Q], const CollisionParams<R>& p, 
     const R keep = R(1) - omega;
     static_for<Q>([&](auto I) {
       const R feq = equilibrium<Q, I>(rho, u, uSqr);
-      f[I] *= keep;
-      f[I] += omega * feq;
+      if constexpr (sizeof(R) == 8) {
+        f[I] *= keep;
+        f[I] += omega * feq;
+      } else {
+        f[I] = __fmaf_rn(omega, feq, f[I] * keep);
+      }
     });
   }
 

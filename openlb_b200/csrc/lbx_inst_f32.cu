@@ -1,4 +1,4 @@
-// FP32 kernel instantiations (FMA contraction on).
+// FP32 kernel instantiations.
 #define LBX_KERNEL_TU
 #include "lbx_kernels.cuh"
 

@@ -404,24 +404,24 @@ __global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> co
     // 3D: (x+1)*sx + (y+1)*sy + z0 + 1; 2D: the fast axis is y (sy = 1), z absent
     const uint32_t n0 = (D::d == 3) ? uint32_t((x + 1) * g.sx + (y + 1) * g.sy + z0 + 1)
                                     : uint32_t((x + 1) * g.sx + z0 + 1);
-    R f[K][Q];
+    // raw loads first, all in straight-line code (the wrap is a select, not a branch), so every
+    // load of the thread is in flight before the first value is used
+    S raw[K][Q];
     static_for<Q>([&](auto I) {
-      uint32_t idx = n0 + cols.s[I];
-      if (idx >= P) idx -= P;
       const S* col = static_cast<const S*>(cols.base[I]);
-      if (idx + K <= P) {
+      uint32_t idx = n0 + cols.s[I];
+      idx = idx >= P ? idx - P : idx;
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-          if (k < nvalid) f[k][I] = Storage<S>::load(col + idx + k);
-      } else {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          uint32_t ik = idx + k;
-          if (ik >= P) ik -= P;
-          if (k < nvalid) f[k][I] = Storage<S>::load(col + ik);
-        }
+      for (int k = 0; k < K; ++k) {
+        uint32_t ik = idx + k;
+        if (k > 0) ik = ik >= P ? ik - P : ik;
+        if (k < nvalid) raw[k][I] = col[ik];
       }
     });
+    R f[K][Q];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      static_for<Q>([&](auto I) { f[k][I] = (k < nvalid) ? Storage<S>::load(&raw[k][I]) : R(0); });
     uint8_t kinds[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
@@ -438,20 +438,14 @@ __global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> co
       }
     }
     static_for<Q>([&](auto I) {
-      uint32_t idx = n0 + cols.s[I];
-      if (idx >= P) idx -= P;
       S* col = static_cast<S*>(cols.base[I]);
-      if (idx + K <= P) {
+      uint32_t idx = n0 + cols.s[I];
+      idx = idx >= P ? idx - P : idx;
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-          if (kinds[k] != 0) Storage<S>::store(col + idx + k, f[k][I]);
-      } else {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          uint32_t ik = idx + k;
-          if (ik >= P) ik -= P;
-          if (kinds[k] != 0) Storage<S>::store(col + ik, f[k][I]);
-        }
+      for (int k = 0; k < K; ++k) {
+        uint32_t ik = idx + k;
+        if (k > 0) ik = ik >= P ? ik - P : ik;
+        if (kinds[k] != 0) Storage<S>::store(col + ik, f[k][I]);
       }
     });
   }
