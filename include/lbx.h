@@ -84,9 +84,11 @@ typedef struct {
   int32_t storage;
   int64_t n_cells;       /* padded cell count */
   int64_t n_core;        /* core cell count */
-  int64_t column_stride; /* elements between column starts = the cyclic period of a column */
-  int64_t bytes;         /* device bytes held by the handle */
+  int64_t column_stride; /* elements between column starts */
+  int64_t bytes;         /* device bytes held by the population columns */
   int64_t n_links;       /* halfway bounce-back links */
+  int64_t column_period; /* cyclic period of a column (= column_stride, or half of it when
+                            every column is mapped twice back to back) */
 } lbx_info;
 
 typedef struct lbx_lattice_s* lbx_lattice;
@@ -192,7 +194,7 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
  * counterpart; the reference's CUDA platform launches fixed 32-thread blocks,
  * gpu/cuda/operator.hh:425-441).  variant 0: pipelined shared-memory tiles of 256 cells;
  * variant 1: one cell per thread in (block_x, block_y) blocks; variant 2 (default):
- * cells_per_thread (1, 2 or 4) consecutive cells per thread in (block_x, block_y) blocks,
+ * cells_per_thread (1 or 2) consecutive cells per thread in (block_x, block_y) blocks,
  * block_x along the fastest axis. */
 int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread);

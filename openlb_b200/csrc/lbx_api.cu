@@ -1,11 +1,13 @@
 // C ABI of liblbx.so: lattice handles, host-side setters and the step driver.
 // The kernels live in lbx_kernels.cuh and are instantiated per storage type in
 // lbx_inst_*.cu.  See include/lbx.h for the contract of every entry point.
+#include <cuda.h>  // driver-API types; the functions are resolved at run time (no libcuda link)
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -87,7 +89,10 @@ struct lbx_lattice_s {
   int core[3] = {1, 1, 1};
   int padded[3] = {1, 1, 1};
   int periodic[3] = {0, 0, 0};
-  int64_t n = 0, stride = 0, ncore = 0;
+  int64_t n = 0, stride = 0, period = 0, ncore = 0;
+  bool doubled = false;                      // columns mapped twice back to back (see alloc_columns)
+  unsigned long long vmmHandles[27] = {};
+  unsigned long long vmmBase = 0, vmmBytes = 0;
   int64_t shift[27] = {};
   void* pop = nullptr;
   uint8_t* cellDyn = nullptr;
@@ -111,7 +116,7 @@ namespace {
 
 Geometry geometry_of(const lbx_lattice_s* L) {
   Geometry g;
-  g.n = L->stride;  // cyclic period of every column (>= padded cells, multiple of 128)
+  g.n = L->period;  // cyclic period of every column (>= padded cells)
   g.stride = L->stride;
   g.sy = (L->d == 3) ? L->padded[2] : 1;
   g.sx = int64_t(L->padded[1]) * ((L->d == 3) ? L->padded[2] : 1);
@@ -138,6 +143,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.blockX = L->blockX;
   a.blockY = L->blockY;
   a.kernel = L->kernel;
+  a.doubled = L->doubled ? 1 : 0;
   a.cellsPerThread = L->cellsPerThread;
   const Geometry& g = a.g;
   const int64_t first = g.sx + g.sy + g.pz;
@@ -181,8 +187,8 @@ void rotate_all(lbx_lattice_s* L) {
   for (int i = 0; i < L->q; ++i) {
     const int* c = velocity(L->q, i);
     const int64_t off = c[0] * g.sx + c[1] * g.sy + ((L->d == 3) ? c[2] : 0);
-    int64_t s = (L->shift[i] - off) % L->stride;
-    if (s < 0) s += L->stride;
+    int64_t s = (L->shift[i] - off) % L->period;
+    if (s < 0) s += L->period;
     L->shift[i] = s;
   }
 }
@@ -198,9 +204,8 @@ void block_shape_for(int nf, int cellsPerThread, int& bx, int& by) {
 
 void default_block_shape(lbx_lattice_s* L) {
   const int nf = (L->d == 3) ? L->core[2] : L->core[1];
-  // K cells per thread: one 16-byte span of storage per population and thread
-  L->cellsPerThread = (L->storage == LBX_F64) ? 1 : (L->storage == LBX_F32 ? 2 : 4);
-  L->kernel = (L->stride < (int64_t(1) << 31)) ? 2 : 1;
+  L->cellsPerThread = 1;
+  L->kernel = (L->period < (int64_t(1) << 31)) ? 2 : 1;
   if (L->kernel == 1) L->cellsPerThread = 1;
   block_shape_for(nf, L->cellsPerThread, L->blockX, L->blockY);
 }
@@ -208,6 +213,152 @@ void default_block_shape(lbx_lattice_s* L) {
 int ensure_stage(lbx_lattice_s* L) {
   if (!L->stage) LBX_CUDA_TRY(cudaMalloc(&L->stage, size_t(L->ncore) * sizeof(double)));
   return LBX_OK;
+}
+
+// ---- population columns in doubled virtual mappings -------------------------------------
+// Each column's physical memory (one allocation of C bytes) is mapped twice, back to back,
+// into one reserved virtual range: element j and element j + P alias.  A population index
+// n + shift (< 2P) then never needs the modulo of the periodic-shift pattern, which removes
+// the wrap arithmetic from every access of the step kernel.  This is the technique of the
+// reference's CUDA CyclicColumn (gpu/cuda/column.hh:217-256), built here on the CUDA VMM
+// API.  Without it (entry points missing, or any step failing) the columns fall back to one
+// plain allocation and the kernels wrap explicitly.
+namespace vmm {
+using FnGran = CUresult (*)(size_t*, const CUmemAllocationProp*, CUmemAllocationGranularity_flags);
+using FnCreate = CUresult (*)(CUmemGenericAllocationHandle*, size_t, const CUmemAllocationProp*, unsigned long long);
+using FnRelease = CUresult (*)(CUmemGenericAllocationHandle);
+using FnReserve = CUresult (*)(CUdeviceptr*, size_t, size_t, CUdeviceptr, unsigned long long);
+using FnAddrFree = CUresult (*)(CUdeviceptr, size_t);
+using FnMap = CUresult (*)(CUdeviceptr, size_t, size_t, CUmemGenericAllocationHandle, unsigned long long);
+using FnUnmap = CUresult (*)(CUdeviceptr, size_t);
+using FnAccess = CUresult (*)(CUdeviceptr, size_t, const CUmemAccessDesc*, size_t);
+
+struct Api {
+  FnGran gran = nullptr;
+  FnCreate create = nullptr;
+  FnRelease release = nullptr;
+  FnReserve reserve = nullptr;
+  FnAddrFree addrFree = nullptr;
+  FnMap map = nullptr;
+  FnUnmap unmap = nullptr;
+  FnAccess access = nullptr;
+  bool ok = false;
+};
+
+template <typename F>
+bool entry(const char* name, F& fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) {
+    cudaGetLastError();
+    return false;
+  }
+  fn = reinterpret_cast<F>(p);
+  return true;
+}
+
+const Api& api() {
+  static Api a = [] {
+    Api r;
+    r.ok = entry("cuMemGetAllocationGranularity", r.gran) && entry("cuMemCreate", r.create) &&
+           entry("cuMemRelease", r.release) && entry("cuMemAddressReserve", r.reserve) &&
+           entry("cuMemAddressFree", r.addrFree) && entry("cuMemMap", r.map) && entry("cuMemUnmap", r.unmap) &&
+           entry("cuMemSetAccess", r.access);
+    return r;
+  }();
+  return a;
+}
+}  // namespace vmm
+
+void release_columns(lbx_lattice_s* L) {
+  if (L->doubled) {
+    const auto& a = vmm::api();
+    if (L->vmmBase) a.unmap(CUdeviceptr(L->vmmBase), size_t(L->vmmBytes));
+    for (int i = 0; i < L->q; ++i)
+      if (L->vmmHandles[i]) a.release(CUmemGenericAllocationHandle(L->vmmHandles[i]));
+    if (L->vmmBase) a.addrFree(CUdeviceptr(L->vmmBase), size_t(L->vmmBytes));
+    L->vmmBase = 0;
+    L->doubled = false;
+  } else {
+    cudaFree(L->pop);
+  }
+  L->pop = nullptr;
+}
+
+bool try_doubled_columns(lbx_lattice_s* L, size_t es) {
+  const auto& a = vmm::api();
+  if (!a.ok) return false;
+  CUmemAllocationProp prop{};
+  prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+  prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  prop.location.id = L->device;
+  size_t gran = 0;
+  if (a.gran(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_MINIMUM) != CUDA_SUCCESS || gran == 0) return false;
+  const size_t colBytes = (size_t(L->n) * es + gran - 1) / gran * gran;
+  const size_t total = size_t(L->q) * 2 * colBytes;
+  CUdeviceptr base = 0;
+  if (a.reserve(&base, total, gran, 0, 0) != CUDA_SUCCESS) return false;
+  L->vmmBase = base;
+  L->vmmBytes = total;
+  L->doubled = true;
+  bool ok = true;
+  for (int i = 0; i < L->q && ok; ++i) {
+    CUmemGenericAllocationHandle h;
+    if (a.create(&h, colBytes, &prop, 0) != CUDA_SUCCESS) { ok = false; break; }
+    L->vmmHandles[i] = h;
+    ok = a.map(base + CUdeviceptr(2 * i * colBytes), colBytes, 0, h, 0) == CUDA_SUCCESS &&
+         a.map(base + CUdeviceptr((2 * i + 1) * colBytes), colBytes, 0, h, 0) == CUDA_SUCCESS;
+  }
+  if (ok) {
+    CUmemAccessDesc acc{};
+    acc.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+    acc.location.id = L->device;
+    acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+    ok = a.access(base, total, &acc, 1) == CUDA_SUCCESS;
+  }
+  if (!ok) {
+    // unmap whatever was mapped: unmapping the whole range is allowed only if fully mapped, so
+    // unmap column by column
+    for (int i = 0; i < L->q; ++i) {
+      if (!L->vmmHandles[i]) continue;
+      a.unmap(base + CUdeviceptr(2 * i * colBytes), colBytes);
+      a.unmap(base + CUdeviceptr((2 * i + 1) * colBytes), colBytes);
+      a.release(CUmemGenericAllocationHandle(L->vmmHandles[i]));
+      L->vmmHandles[i] = 0;
+    }
+    a.addrFree(base, total);
+    L->vmmBase = 0;
+    L->doubled = false;
+    cudaGetLastError();
+    return false;
+  }
+  L->pop = reinterpret_cast<void*>(base);
+  L->period = int64_t(colBytes / es);
+  L->stride = 2 * L->period;
+  L->bytes = int64_t(size_t(L->q) * colBytes);
+  return true;
+}
+
+// Allocate the Q population columns: doubled mappings when the VMM API is available, one plain
+// allocation otherwise.  Contents start at zero.
+cudaError_t alloc_columns(lbx_lattice_s* L) {
+  const size_t es = storage_bytes(L->storage);
+  if (!std::getenv("LBX_PLAIN_COLUMNS") && try_doubled_columns(L, es)) {
+    // zero the first copy of every column (the second aliases it)
+    for (int i = 0; i < L->q; ++i) {
+      cudaError_t e = cudaMemset(static_cast<char*>(L->pop) + size_t(i) * size_t(L->stride) * es, 0,
+                                 size_t(L->period) * es);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  L->period = (L->n + 127) / 128 * 128;
+  L->stride = L->period;
+  const size_t bytes = size_t(L->q) * size_t(L->stride) * es;
+  cudaError_t e = cudaMalloc(&L->pop, bytes);
+  if (e == cudaSuccess) e = cudaMemset(L->pop, 0, bytes);
+  L->bytes = int64_t(bytes);
+  return e;
 }
 
 bool device_ok(int device, std::string& why) {
@@ -291,23 +442,19 @@ int lbx_lattice_create(int32_t q, const int32_t core[3], const int32_t periodic[
     return fail(LBX_ERR_INVALID, "padded block exceeds 2^32 cells");
   }
   L->ncore = int64_t(core[0]) * core[1] * core[2];
-  L->stride = (L->n + 127) / 128 * 128;
+  cudaError_t e = alloc_columns(L);
   default_block_shape(L);
-  const size_t popBytes = size_t(q) * size_t(L->stride) * storage_bytes(storage);
-  cudaError_t e = cudaMalloc(&L->pop, popBytes);
-  if (e == cudaSuccess) e = cudaMemset(L->pop, 0, popBytes);
   if (e == cudaSuccess) e = cudaMalloc(&L->stats, sizeof(StatAcc));
   if (e == cudaSuccess) e = cudaMemset(L->stats, 0, sizeof(StatAcc));
   if (e == cudaSuccess) e = cudaMalloc(&L->reduceAcc, 8 * sizeof(double) + sizeof(unsigned long long));
   if (e != cudaSuccess) {
     const std::string msg = std::string("allocation failed: ") + cudaGetErrorString(e);
-    cudaFree(L->pop);
+    release_columns(L);
     cudaFree(L->stats);
     cudaFree(L->reduceAcc);
     delete L;
     return fail(e == cudaErrorMemoryAllocation ? LBX_ERR_OUT_OF_MEMORY : LBX_ERR_CUDA, msg);
   }
-  L->bytes = int64_t(popBytes);
   *out = L;
   return LBX_OK;
 }
@@ -315,7 +462,8 @@ int lbx_lattice_create(int32_t q, const int32_t core[3], const int32_t periodic[
 int lbx_lattice_destroy(lbx_lattice L) {
   if (!L) return LBX_OK;
   DeviceGuard guard(L->device);
-  cudaFree(L->pop);
+  cudaDeviceSynchronize();
+  release_columns(L);
   cudaFree(L->cellDyn);
   cudaFree(L->linkCell);
   cudaFree(L->linkDir);
@@ -343,6 +491,7 @@ int lbx_get_info(lbx_lattice L, lbx_info* info) {
   info->n_cells = L->n;
   info->n_core = L->ncore;
   info->column_stride = L->stride;
+  info->column_period = L->period;
   info->bytes = L->bytes;
   info->n_links = L->nLinks;
   return LBX_OK;
@@ -650,8 +799,8 @@ int lbx_population_shift(lbx_lattice L, int32_t pop, int64_t* shift) {
 int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   if (pop < 0 || pop >= L->q) return fail(LBX_ERR_INVALID, "population index out of range");
-  int64_t s = (L->shift[pop] - offset) % L->stride;
-  if (s < 0) s += L->stride;
+  int64_t s = (L->shift[pop] - offset) % L->period;
+  if (s < 0) s += L->period;
   L->shift[pop] = s;
   return LBX_OK;
 }
@@ -660,10 +809,10 @@ int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32
                           int32_t cells_per_thread) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   if (variant < 0 || variant > 2) return fail(LBX_ERR_INVALID, "variant must be 0, 1 or 2");
-  if (variant == 2 && L->stride >= (int64_t(1) << 31))
+  if (variant == 2 && L->period >= (int64_t(1) << 31))
     return fail(LBX_ERR_UNSUPPORTED, "variant 2 needs a column period below 2^31 cells");
-  if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2 && cells_per_thread != 4)
-    return fail(LBX_ERR_INVALID, "cells_per_thread must be 1, 2 or 4");
+  if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2)
+    return fail(LBX_ERR_INVALID, "cells_per_thread must be 1 or 2");
   if (variant != 0) {
     if (block_x < 1 || block_y < 1 || block_x * block_y > 256 || (block_x * block_y) % 32 != 0)
       return fail(LBX_ERR_INVALID, "block must hold a multiple of 32 and at most 256 threads");

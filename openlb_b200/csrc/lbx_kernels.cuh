@@ -371,11 +371,11 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
 // kernel carries no face logic.  Column indices are 32-bit: the column period is < 2^31.
 template <int Q>
 struct ColumnBases {
-  void* base[Q];   // start of population column i
-  uint32_t s[Q];   // current shift of column i
+  void* base[Q];   // start of population column i (doubled columns: start + shift)
+  uint32_t s[Q];   // current shift of column i (doubled columns: 0)
 };
 
-template <int Q, typename S, int DYN, int K>
+template <int Q, typename S, int DYN, int K, bool DOUBLED>
 __global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
@@ -409,13 +409,19 @@ __global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> co
     S raw[K][Q];
     static_for<Q>([&](auto I) {
       const S* col = static_cast<const S*>(cols.base[I]);
-      uint32_t idx = n0 + cols.s[I];
-      idx = idx >= P ? idx - P : idx;
+      if constexpr (DOUBLED) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        uint32_t ik = idx + k;
-        if (k > 0) ik = ik >= P ? ik - P : ik;
-        if (k < nvalid) raw[k][I] = col[ik];
+        for (int k = 0; k < K; ++k)
+          if (k < nvalid) raw[k][I] = col[n0 + k];
+      } else {
+        uint32_t idx = n0 + cols.s[I];
+        idx = idx >= P ? idx - P : idx;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          uint32_t ik = idx + k;
+          if (k > 0) ik = ik >= P ? ik - P : ik;
+          if (k < nvalid) raw[k][I] = col[ik];
+        }
       }
     });
     R f[K][Q];
@@ -439,13 +445,19 @@ __global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> co
     }
     static_for<Q>([&](auto I) {
       S* col = static_cast<S*>(cols.base[I]);
-      uint32_t idx = n0 + cols.s[I];
-      idx = idx >= P ? idx - P : idx;
+      if constexpr (DOUBLED) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        uint32_t ik = idx + k;
-        if (k > 0) ik = ik >= P ? ik - P : ik;
-        if (kinds[k] != 0) Storage<S>::store(col + ik, f[k][I]);
+        for (int k = 0; k < K; ++k)
+          if (kinds[k] != 0) Storage<S>::store(col + n0 + k, f[k][I]);
+      } else {
+        uint32_t idx = n0 + cols.s[I];
+        idx = idx >= P ? idx - P : idx;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          uint32_t ik = idx + k;
+          if (k > 0) ik = ik >= P ? ik - P : ik;
+          if (kinds[k] != 0) Storage<S>::store(col + ik, f[k][I]);
+        }
       }
     });
   }
@@ -758,6 +770,7 @@ struct LaunchArgs {
   int blockX, blockY;
   int kernel;          // 0: pipelined shared-memory tiles, 1: one cell per thread, 2: K cells per thread
   int cellsPerThread;  // K of kernel 2 (1, 2 or 4)
+  int doubled;         // columns mapped twice back to back: index n + shift needs no wrap
   int64_t flatBase;    // first tile start (multiple of 8) and end of the flat cell range
   int64_t flatEnd;
 };
@@ -842,8 +855,8 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
   } else {
     ColumnBases<Q> cols;
     for (int i = 0; i < Q; ++i) {
-      cols.base[i] = pop + int64_t(i) * g.stride;
-      cols.s[i] = uint32_t(a.shift[i]);
+      cols.base[i] = pop + int64_t(i) * g.stride + (a.doubled ? a.shift[i] : 0);
+      cols.s[i] = a.doubled ? 0u : uint32_t(a.shift[i]);
     }
     const int K = a.cellsPerThread;
     const int nf = Desc<Q>::d == 3 ? g.nz : g.ny;
@@ -852,10 +865,12 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     dim3 grid;
     if (Desc<Q>::d == 3) grid = dim3((groups + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
     else grid = dim3((groups + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
-    switch (K) {
-    case 1: k_collide_stream_groups<Q, S, DYN, 1><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
-    case 2: k_collide_stream_groups<Q, S, DYN, 2><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
-    case 4: k_collide_stream_groups<Q, S, DYN, 4><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    const int sel = K * 2 + (a.doubled ? 1 : 0);
+    switch (sel) {
+    case 2: k_collide_stream_groups<Q, S, DYN, 1, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
     default: return cudaErrorInvalidValue;
     }
   }

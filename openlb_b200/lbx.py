@@ -41,7 +41,7 @@ class Info(C.Structure):
     _fields_ = [("q", C.c_int32), ("d", C.c_int32), ("core", C.c_int32 * 3), ("padded", C.c_int32 * 3),
                 ("pad", C.c_int32), ("periodic", C.c_int32 * 3), ("storage", C.c_int32),
                 ("n_cells", C.c_int64), ("n_core", C.c_int64), ("column_stride", C.c_int64),
-                ("bytes", C.c_int64), ("n_links", C.c_int64)]
+                ("bytes", C.c_int64), ("n_links", C.c_int64), ("column_period", C.c_int64)]
 
 
 def _load() -> C.CDLL:
