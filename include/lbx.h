@@ -199,6 +199,26 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
 int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread);
 
+/* Mass/momentum sums for callers that cannot allocate device memory.  No counterpart in the
+ * reference.  lbx_reduce(LBX_REDUCE_MASS_MOMENTUM) needs a lattice handle, whose creation
+ * calls cudaMalloc; a host program whose device memory is all owned by its own pool or arena,
+ * or that must not enter the CUDA allocator where it runs, can still reduce populations it
+ * already holds on the device with this entry point.  It allocates nothing: its scratch is a
+ * static device array of (LBX_NOALLOC_MAX_BLOCKS + 1) * 4 doubles (256 KiB), present on every
+ * GPU that loads the library until the process exits.
+ *   populations  device array in the exchange layout, column i starting at element
+ *                i * column_stride, n_cells cells per column, values f_i - w_i of `storage`;
+ *   out          host array {sum rho, sum j_x, sum j_y, sum j_z} (rho = sum_i f_i + 1), FP64;
+ *   n_cells      at most LBX_NOALLOC_MAX_CELLS, otherwise LBX_ERR_INVALID before any device work.
+ * Runs on the current device and `stream`, and synchronises the stream.  The first call on a
+ * device looks up the scratch's device address; make it before any stream capture.  All calls
+ * share the one scratch array: calls that overlap on the GPU race, so serialise them. */
+#define LBX_NOALLOC_MAX_BLOCKS 8192
+#define LBX_NOALLOC_CELLS_PER_BLOCK 4096
+#define LBX_NOALLOC_MAX_CELLS ((int64_t)LBX_NOALLOC_MAX_BLOCKS * LBX_NOALLOC_CELLS_PER_BLOCK)
+int lbx_mass_momentum_noalloc(int32_t q, int32_t storage, const void* populations, int64_t n_cells,
+                              int64_t column_stride, double out[4], void* stream);
+
 #ifdef __cplusplus
 }
 #endif

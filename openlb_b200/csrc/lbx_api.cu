@@ -84,6 +84,10 @@ double weight_of(int q, int i) {
 
 }  // namespace
 
+namespace lbx {
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace lbx
+
 struct lbx_lattice_s {
   int q = 0, d = 0, storage = 0, device = 0;
   int core[3] = {1, 1, 1};
