@@ -178,16 +178,32 @@ __device__ __forceinline__ void collide(R (&f)[Q], const CollisionParams<R>& p, 
       f[i] = fi - (omega * (fpi - epi) + omega2 * (fmi - emi));
       f[j] = fj - (omega * (fpj - epj) + omega2 * (fmj - emj));
     });
-  } else {
+  } else if constexpr (sizeof(R) == 8) {
     const R keep = R(1) - omega;
     static_for<Q>([&](auto I) {
       const R feq = equilibrium<Q, I>(rho, u, uSqr);
-      if constexpr (sizeof(R) == 8) {
-        f[I] *= keep;
-        f[I] += omega * feq;
-      } else {
-        f[I] = __fmaf_rn(omega, feq, f[I] * keep);
-      }
+      f[I] *= keep;
+      f[I] += omega * feq;
+    });
+  } else {
+    // float: opposite directions share t_i and |c_i . u|, so their equilibria are
+    // sym +- asym with sym = rho t (1 - 1.5 u^2 + 4.5 (c.u)^2) - t and asym = 3 rho t (c.u)
+    const R keep = R(1) - omega;
+    const R base = R(1) - R(1.5) * uSqr;
+    {
+      constexpr R t0 = weight<Q, R>(0);
+      f[0] = __fmaf_rn(omega, __fmaf_rn(rho * t0, base, -t0), f[0] * keep);
+    }
+    static_for<Q / 2>([&](auto K) {
+      constexpr int i = K + 1;
+      constexpr int j = D::OPP[i];
+      constexpr R t = weight<Q, R>(i);
+      const R cu = c_dot<Q, i>(u);
+      const R rt = rho * t;
+      const R sym = __fmaf_rn(rt, __fmaf_rn(R(4.5) * cu, cu, base), -t);
+      const R asym = (rho * R(3 * t)) * cu;
+      f[i] = __fmaf_rn(omega, sym + asym, f[i] * keep);
+      f[j] = __fmaf_rn(omega, sym - asym, f[j] * keep);
     });
   }
 

@@ -375,8 +375,17 @@ struct ColumnBases {
   uint32_t s[Q];   // current shift of column i (doubled columns: 0)
 };
 
+// Resident blocks per SM the step kernel is compiled for: the 16-bit forms move half the
+// bytes per request, so they need more warps in flight to keep HBM busy.
+// (D3Q27 keeps the compiler's choice: at 6 blocks its 27 values spill.)
+template <int Q, typename S> struct StepOccupancy { static constexpr int blocks = 1; };
+template <> struct StepOccupancy<19, __half> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<19, __nv_bfloat16> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<9, __half> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<9, __nv_bfloat16> { static constexpr int blocks = 6; };
+
 template <int Q, typename S, int DYN, int K, bool DOUBLED>
-__global__ void __launch_bounds__(256) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
+__global__ void __launch_bounds__(256, StepOccupancy<Q, S>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
                                                                StatAcc* __restrict__ stats) {
