@@ -199,6 +199,15 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
 int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread);
 
+/* Per-kernel device timing of lbx_collide_and_stream, for profiling and the roofline (no
+ * reference counterpart; the reference's util::Timer times whole steps on the host,
+ * utilities/timer.hh:55-86).  enable != 0 records CUDA events around the kernels of every
+ * following step and clears the totals; lbx_get_kernel_timing synchronises and returns the
+ * summed device milliseconds of the collision, periodic-overlap and bounce-back-link kernels in
+ * out[0..2] and their launch counts in out[3..5]. */
+int lbx_set_kernel_timing(lbx_lattice lattice, int32_t enable);
+int lbx_get_kernel_timing(lbx_lattice lattice, double out[6]);
+
 /* Mass/momentum sums for callers that cannot allocate device memory.  No counterpart in the
  * reference.  lbx_reduce(LBX_REDUCE_MASS_MOMENTUM) needs a lattice handle, whose creation
  * calls cudaMalloc; a host program whose device memory is all owned by its own pool or arena,

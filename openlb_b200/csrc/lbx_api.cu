@@ -67,13 +67,6 @@ const int* velocity(int q, int i) {
   default: return Desc<27>::C[i];
   }
 }
-int opposite(int q, int i) {
-  switch (q) {
-  case 9: return Desc<9>::OPP[i];
-  case 19: return Desc<19>::OPP[i];
-  default: return Desc<27>::OPP[i];
-  }
-}
 double weight_of(int q, int i) {
   switch (q) {
   case 9: return double(Desc<9>::WN[i]) / double(Desc<9>::WD[i]);
@@ -114,6 +107,12 @@ struct lbx_lattice_s {
   int kernel = 2;
   int cellsPerThread = 1;
   int64_t bytes = 0;
+  // optional per-kernel event timing (lbx_set_kernel_timing)
+  bool timing = false;
+  std::vector<cudaEvent_t> eventPool;
+  std::vector<cudaEvent_t> pending;  // groups of 4: before/after collision, after halo, after links
+  double timedMs[3] = {0, 0, 0};
+  int64_t timedLaunches[3] = {0, 0, 0};
 };
 
 namespace {
@@ -365,6 +364,38 @@ cudaError_t alloc_columns(lbx_lattice_s* L) {
   return e;
 }
 
+cudaEvent_t take_event(lbx_lattice_s* L) {
+  if (!L->eventPool.empty()) {
+    cudaEvent_t e = L->eventPool.back();
+    L->eventPool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) e = nullptr;
+  return e;
+}
+
+// Fold the recorded groups into the totals (waits for them) and recycle their events.
+void drain_timing(lbx_lattice_s* L) {
+  for (size_t g = 0; g + 4 <= L->pending.size(); g += 4) {
+    cudaEvent_t* e = &L->pending[g];
+    float ms = 0.f;
+    if (cudaEventSynchronize(e[3]) == cudaSuccess) {
+      if (cudaEventElapsedTime(&ms, e[0], e[1]) == cudaSuccess) { L->timedMs[0] += ms; ++L->timedLaunches[0]; }
+      if (L->periodic[0] || L->periodic[1] || L->periodic[2]) {
+        if (cudaEventElapsedTime(&ms, e[1], e[2]) == cudaSuccess) { L->timedMs[1] += ms; ++L->timedLaunches[1]; }
+      }
+      if (L->nLinks > 0) {
+        if (cudaEventElapsedTime(&ms, e[2], e[3]) == cudaSuccess) { L->timedMs[2] += ms; ++L->timedLaunches[2]; }
+      }
+    }
+    for (int k = 0; k < 4; ++k) L->eventPool.push_back(e[k]);
+  }
+  L->pending.clear();
+  cudaGetLastError();
+}
+
+
 bool device_ok(int device, std::string& why) {
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -467,6 +498,8 @@ int lbx_lattice_destroy(lbx_lattice L) {
   if (!L) return LBX_OK;
   DeviceGuard guard(L->device);
   cudaDeviceSynchronize();
+  drain_timing(L);
+  for (cudaEvent_t e : L->eventPool) cudaEventDestroy(e);
   release_columns(L);
   cudaFree(L->cellDyn);
   cudaFree(L->linkCell);
@@ -701,12 +734,50 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
       LBX_CUDA_TRY(cudaMemsetAsync(L->stats, 0, sizeof(StatAcc), s));
       a.stats = L->stats;
     }
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (L->timing) {
+      if (L->pending.size() >= 4 * 2048) drain_timing(L);
+      for (auto& e : ev) e = take_event(L);
+      if (ev[0]) cudaEventRecord(ev[0], s);
+    }
     LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_step<Q, S>(a, s))));
+    if (ev[1]) cudaEventRecord(ev[1], s);
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_halo<Q, S>(a, s))));
+    if (ev[2]) cudaEventRecord(ev[2], s);
     rotate_all(L);
     if (L->nLinks > 0) {
       const LaunchArgs b = args_of(L);
       LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
     }
+    if (ev[3]) {
+      cudaEventRecord(ev[3], s);
+      if (ev[0] && ev[1] && ev[2]) {
+        for (auto e : ev) L->pending.push_back(e);
+      }
+    }
+  }
+  return LBX_OK;
+}
+
+int lbx_set_kernel_timing(lbx_lattice L, int32_t enable) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  DeviceGuard guard(L->device);
+  drain_timing(L);
+  L->timing = enable != 0;
+  for (int k = 0; k < 3; ++k) {
+    L->timedMs[k] = 0;
+    L->timedLaunches[k] = 0;
+  }
+  return LBX_OK;
+}
+
+int lbx_get_kernel_timing(lbx_lattice L, double out[6]) {
+  if (!L || !out) return fail(LBX_ERR_INVALID, "null argument");
+  DeviceGuard guard(L->device);
+  drain_timing(L);
+  for (int k = 0; k < 3; ++k) {
+    out[k] = L->timedMs[k];
+    out[3 + k] = double(L->timedLaunches[k]);
   }
   return LBX_OK;
 }

@@ -787,6 +787,8 @@ struct LaunchArgs {
 template <int Q, typename S>
 cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream);
 template <int Q, typename S>
+cudaError_t launch_halo(const LaunchArgs& a, cudaStream_t stream);
+template <int Q, typename S>
 cudaError_t launch_bouzidi(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
                            const void* delta, int64_t nLinks, cudaStream_t stream);
 template <int Q, typename S>
@@ -883,9 +885,15 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     default: return cudaErrorInvalidValue;
     }
   }
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || g.pmask == 0) return e;
-  // periodic overlap copy after the collision
+  return cudaGetLastError();
+}
+// Periodic overlap copy after the collision (no launch for a lattice without periodic axes).
+template <int Q, typename S>
+cudaError_t launch_halo(const LaunchArgs& a, cudaStream_t stream) {
+  const Geometry& g = a.g;
+  if (g.pmask == 0) return cudaSuccess;
+  const auto sh = shifts_of<Q>(a);
+  S* pop = static_cast<S*>(a.pop);
   const int64_t cntX = (g.pmask & 1) ? 2 * int64_t(g.ny) * g.nz : 0;
   const int64_t cntY = (g.pmask & 2) ? 2 * int64_t(g.nx) * g.nz : 0;
   const int64_t cntZ = (g.pmask & 4) ? 2 * int64_t(g.nx) * g.ny : 0;
@@ -968,6 +976,19 @@ cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc,
                                                float(a.force[2]), snap, acc, maxbits);
   return cudaGetLastError();
 }
+// Explicit instantiation of every launcher for one (descriptor, storage) pair.
+#define LBX_INSTANTIATE(Q, S)                                                                          \
+  template cudaError_t launch_step<Q, S>(const LaunchArgs&, cudaStream_t);                            \
+  template cudaError_t launch_halo<Q, S>(const LaunchArgs&, cudaStream_t);                            \
+  template cudaError_t launch_bouzidi<Q, S>(const LaunchArgs&, const uint32_t*, const uint8_t*,       \
+                                            const void*, int64_t, cudaStream_t);                      \
+  template cudaError_t launch_transfer<Q, S>(const LaunchArgs&, int, const void*, int, bool, cudaStream_t); \
+  template cudaError_t launch_ini_equilibrium<Q, S>(const LaunchArgs&, const double*, const double*, cudaStream_t); \
+  template cudaError_t launch_moments<Q, S>(const LaunchArgs&, double*, double*, cudaStream_t);       \
+  template cudaError_t launch_mass_momentum<Q, S>(const LaunchArgs&, double*, cudaStream_t);          \
+  template cudaError_t launch_link_force<Q, S>(const LaunchArgs&, const uint32_t*, const uint8_t*,    \
+                                               int64_t, double*, cudaStream_t);                       \
+  template cudaError_t launch_residual<Q, S>(const LaunchArgs&, float*, double*, unsigned long long*, cudaStream_t);
 #endif  // LBX_KERNEL_TU
 
 }  // namespace lbx

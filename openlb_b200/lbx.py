@@ -71,6 +71,8 @@ def _load() -> C.CDLL:
         "lbx_population_shift": ([VP, I32, P(I64)], C.c_int),
         "lbx_rotate": ([VP, I32, I64], C.c_int),
         "lbx_set_launch_config": ([VP, I32, I32, I32, I32], C.c_int),
+        "lbx_set_kernel_timing": ([VP, I32], C.c_int),
+        "lbx_get_kernel_timing": ([VP, P(D)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -266,6 +268,16 @@ class BlockLattice:
                           cells_per_thread: int = 1) -> None:
         check(lib.lbx_set_launch_config(self._h, variant, block_x, block_y, cells_per_thread),
               "lbx_set_launch_config")
+
+    def set_kernel_timing(self, enable: bool) -> None:
+        check(lib.lbx_set_kernel_timing(self._h, 1 if enable else 0), "lbx_set_kernel_timing")
+
+    def kernel_timing(self) -> dict:
+        """Summed device ms and launch counts per kernel kind since set_kernel_timing(True)."""
+        out = (C.c_double * 6)()
+        check(lib.lbx_get_kernel_timing(self._h, out), "lbx_get_kernel_timing")
+        return {"collision": (out[0], int(out[3])), "periodic_overlap": (out[1], int(out[4])),
+                "links": (out[2], int(out[5]))}
 
     def population_shift(self, pop: int) -> int:
         s = C.c_int64()
