@@ -272,11 +272,13 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
                      "traffic": traffic, "algorithmic_bytes_per_launch": bytes_launch},
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(pop_bytes / args.steps),
                 "d2h_bytes_per_step": int(pop_bytes / args.steps + 32)},
-        "gpu_launches": 2 * args.steps,
-        "kernels": {"k_collide_stream_groups": {"avg_ms": round(coll_ms / max(coll_n, 1), 5), "launches": coll_n,
-                                                "share": round(coll_ms / max(coll_ms + halo_ms, 1e-12), 4)},
-                    "k_periodic_halo": {"avg_ms": round(halo_ms / max(halo_n, 1), 5), "launches": halo_n,
-                                        "share": round(halo_ms / max(coll_ms + halo_ms, 1e-12), 4)}},
+        "gpu_launches": coll_n + halo_n,
+        "kernels": {k: v for k, v in {
+            "k_collide_stream_groups": {"avg_ms": round(coll_ms / max(coll_n, 1), 5), "launches": coll_n,
+                                        "share": round(coll_ms / max(coll_ms + halo_ms, 1e-12), 4)},
+            "k_periodic_halo": {"avg_ms": round(halo_ms / max(halo_n, 1), 5), "launches": halo_n,
+                                "share": round(halo_ms / max(coll_ms + halo_ms, 1e-12), 4)}}.items()
+            if v["launches"] > 0},
         "clocks": clk,
         "statistics": stats,
         "forms": forms,

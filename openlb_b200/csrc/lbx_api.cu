@@ -98,6 +98,8 @@ struct lbx_lattice_s {
   void* linkDelta = nullptr;
   int64_t nLinks = 0;
   StatAcc* stats = nullptr;
+  double* statPart = nullptr;        // per-block statistics partials
+  int64_t statCapacity = 0;          // blocks statPart holds
   double* reduceAcc = nullptr;       // 8 doubles + 1 ull of scratch for reductions
   float* residualSnap = nullptr;
   void* stage = nullptr;             // ncore doubles
@@ -211,6 +213,34 @@ void default_block_shape(lbx_lattice_s* L) {
   L->kernel = (L->period < (int64_t(1) << 31)) ? 2 : 1;
   if (L->kernel == 1) L->cellsPerThread = 1;
   block_shape_for(nf, L->cellsPerThread, L->blockX, L->blockY);
+}
+
+// Blocks the step kernel of the current launch configuration runs (the statistics partials
+// hold one entry per block).
+int64_t step_blocks(const lbx_lattice_s* L) {
+  const Geometry g = geometry_of(L);
+  const int nf = (L->d == 3) ? g.nz : g.ny;
+  const int nm = (L->d == 3) ? g.ny : g.nx;
+  const int ns = (L->d == 3) ? g.nx : 1;
+  if (L->kernel == 0) {
+    const LaunchArgs a = args_of(L);
+    return (a.flatEnd - a.flatBase + TILE - 1) / TILE;
+  }
+  const int k = L->kernel == 2 ? L->cellsPerThread : 1;
+  const int64_t groups = (nf + k - 1) / k;
+  return ((groups + L->blockX - 1) / L->blockX) * int64_t((nm + L->blockY - 1) / L->blockY) * ns;
+}
+
+int ensure_stat_capacity(lbx_lattice_s* L) {
+  const int64_t need = step_blocks(L);
+  if (need > L->statCapacity) {
+    cudaFree(L->statPart);
+    L->statPart = nullptr;
+    L->statCapacity = 0;
+    LBX_CUDA_TRY(cudaMalloc(&L->statPart, size_t(need) * 4 * sizeof(double)));
+    L->statCapacity = need;
+  }
+  return LBX_OK;
 }
 
 int ensure_stage(lbx_lattice_s* L) {
@@ -382,7 +412,7 @@ void drain_timing(lbx_lattice_s* L) {
     float ms = 0.f;
     if (cudaEventSynchronize(e[3]) == cudaSuccess) {
       if (cudaEventElapsedTime(&ms, e[0], e[1]) == cudaSuccess) { L->timedMs[0] += ms; ++L->timedLaunches[0]; }
-      if (L->periodic[0] || L->periodic[1] || L->periodic[2]) {
+      if ((L->periodic[0] || L->periodic[1] || L->periodic[2]) && L->kernel != 2) {  // variant 2: no copy launch
         if (cudaEventElapsedTime(&ms, e[1], e[2]) == cudaSuccess) { L->timedMs[1] += ms; ++L->timedLaunches[1]; }
       }
       if (L->nLinks > 0) {
@@ -506,6 +536,7 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->linkDir);
   cudaFree(L->linkDelta);
   cudaFree(L->stats);
+  cudaFree(L->statPart);
   cudaFree(L->reduceAcc);
   cudaFree(L->residualSnap);
   cudaFree(L->stage);
@@ -731,8 +762,10 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
   for (int64_t k = 0; k < steps; ++k) {
     LaunchArgs a = args_of(L);
     if ((flags & LBX_STEP_STATISTICS) && k == steps - 1) {
-      LBX_CUDA_TRY(cudaMemsetAsync(L->stats, 0, sizeof(StatAcc), s));
+      if (int rc = ensure_stat_capacity(L)) return rc;
       a.stats = L->stats;
+      a.statPart = L->statPart;
+      a.statCapacity = L->statCapacity;
     }
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     if (L->timing) {

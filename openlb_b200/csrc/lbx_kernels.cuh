@@ -115,6 +115,77 @@ __device__ __forceinline__ void block_stats(R rho, R usq, bool valid, StatAcc* a
   }
 }
 
+// Block partial of the lattice statistics {sum rho, sum |u|^2, max |u|^2, count}: a warp
+// butterfly, then the warps in index order, written to part[4 * block] without atomics.  With
+// k_stats_finalize summing the partials in a fixed order, the statistics are bitwise
+// reproducible from run to run.
+__device__ __forceinline__ void block_partial(double a, double b, double m, double c, double* __restrict__ part) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  __shared__ double red[4][32];
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  if ((tid & 31) == 0) {
+    red[0][tid >> 5] = a;
+    red[1][tid >> 5] = b;
+    red[2][tid >> 5] = m;
+    red[3][tid >> 5] = c;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int w = 0; w < nwarps; ++w) {
+      s0 += red[0][w];
+      s1 += red[1][w];
+      s2 = fmax(s2, red[2][w]);
+      s3 += red[3][w];
+    }
+    const int64_t bid = blockIdx.x + int64_t(gridDim.x) * (blockIdx.y + int64_t(gridDim.y) * blockIdx.z);
+    part[4 * bid + 0] = s0;
+    part[4 * bid + 1] = s1;
+    part[4 * bid + 2] = s2;
+    part[4 * bid + 3] = s3;
+  }
+}
+
+// The block partials summed in a fixed order into the StatAcc the host reads.
+static __global__ void __launch_bounds__(256) k_stats_finalize(const double* __restrict__ part, int64_t nblocks,
+                                                        StatAcc* __restrict__ out) {
+  double a = 0, b = 0, m = 0, c = 0;
+  for (int64_t i = threadIdx.x; i < nblocks; i += 256) {
+    a += part[4 * i + 0];
+    b += part[4 * i + 1];
+    m = fmax(m, part[4 * i + 2]);
+    c += part[4 * i + 3];
+  }
+  __shared__ double s[4][256];
+  s[0][threadIdx.x] = a;
+  s[1][threadIdx.x] = b;
+  s[2][threadIdx.x] = m;
+  s[3][threadIdx.x] = c;
+  __syncthreads();
+  for (int stride = 128; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride) {
+      s[0][threadIdx.x] += s[0][threadIdx.x + stride];
+      s[1][threadIdx.x] += s[1][threadIdx.x + stride];
+      s[2][threadIdx.x] = fmax(s[2][threadIdx.x], s[2][threadIdx.x + stride]);
+      s[3][threadIdx.x] += s[3][threadIdx.x + stride];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out->sum[0] = s[0][0];
+    out->sum[1] = s[1][0];
+    out->count = (unsigned long long)s[3][0];
+    out->maxbits = (unsigned long long)__double_as_longlong(s[2][0]);
+  }
+}
+
 // ---- fused collide + PS stream --------------------------------------------------------
 // One thread per core cell; threadIdx.x runs along the fastest core axis (z in 3D, y in 2D)
 // so that every population load and store of a warp is one contiguous run.
@@ -122,7 +193,7 @@ template <int Q, typename S, int DYN>
 __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                         CollisionParams<typename Storage<S>::R> p,
                                                         const uint8_t* __restrict__ cellDyn,
-                                                        StatAcc* __restrict__ stats) {
+                                                        double* __restrict__ statPart) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   int x, y, z;
@@ -160,7 +231,8 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
 
   }
 
-  if (stats) block_stats<R>(rho, usq, valid, stats);
+  if (statPart) block_partial(valid ? double(rho) : 0.0, valid ? double(usq) : 0.0, valid ? double(usq) : 0.0,
+                              valid ? 1.0 : 0.0, statPart);
 }
 
 // ---- fused collide + PS stream, pipelined shared-memory tiles --------------------------
@@ -239,7 +311,7 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
                                                                int64_t base, int64_t nFlat, int64_t nTiles,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
-                                                               StatAcc* __restrict__ stats) {
+                                                               double* __restrict__ statPart) {
   using R = typename Storage<S>::R;
   using C = TileCfg<Q, S>;
   using VT = typename Vec<S>::T;
@@ -343,23 +415,7 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 
-  if (stats) {
-    double a = accRho, b = accUsq, m = accMax;
-    unsigned c = accCount;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      c += __shfl_xor_sync(0xffffffffu, c, o);
-    }
-    if ((tid & 31) == 0 && c > 0) {
-      atomicAdd(&stats->sum[0], a);
-      atomicAdd(&stats->sum[1], b);
-      atomicAdd(&stats->count, (unsigned long long)c);
-      atomicMax(&stats->maxbits, (unsigned long long)__double_as_longlong(m));
-    }
-  }
+  if (statPart) block_partial(accRho, accUsq, accMax, double(accCount), statPart);
 }
 
 // ---- fused collide + PS stream, K consecutive cells per thread --------------------------
@@ -388,7 +444,7 @@ template <int Q, typename S, int DYN, int K, bool DOUBLED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
-                                                               StatAcc* __restrict__ stats) {
+                                                               double* __restrict__ statPart) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const uint32_t P = uint32_t(g.n);
@@ -452,6 +508,63 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S>::blocks) k_collide_st
         revert<Q, R>(f[k]);
       }
     }
+    // periodic overlap (the reference's PostCollide copy, done here so a step is one launch):
+    //  - rows on a periodic slower face (whole warps, ~1% of the rows) copy every leaving
+    //    population to its ghost slot with the full wrap, edges and corners included;
+    //  - other rows copy only what leaves across the fastest axis, which lands in the same
+    //    row's ghost cell at the other end (n -+ nf).
+    const int nf = D::d == 3 ? g.nz : g.ny;
+    const bool slowFace = ((g.pmask & 1) && (x == 0 || x == g.nx - 1)) ||
+                          (D::d == 3 && (g.pmask & 2) && (y == 0 || y == g.ny - 1));
+    auto ghost_store = [&](auto I, int k, uint32_t slot) {
+      S* col = static_cast<S*>(cols.base[I]);
+      if constexpr (DOUBLED) {
+        Storage<S>::store(col + slot, f[k][I]);
+      } else {
+        uint32_t idx = slot + cols.s[I];
+        idx = idx >= P ? idx - P : idx;
+        Storage<S>::store(col + idx, f[k][I]);
+      }
+    };
+    if (slowFace) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (k >= nvalid) continue;
+        const int cz0 = D::d == 3 ? z0 + k : 0;
+        const int cy0 = D::d == 3 ? y : z0 + k;
+        static_for<Q>([&](auto I) {
+          constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+          int tx = x + cx, ty = cy0 + cy, tz = cz0 + cz;
+          bool crossed = false, lost = false;
+          if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+          if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+          if constexpr (D::d == 3) {
+            if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+          }
+          if (crossed && !lost) {
+            const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+            ghost_store(I, k, uint32_t(gn));
+          }
+        });
+      }
+    } else if (g.pmask & (D::d == 3 ? 4 : 2)) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int fk = z0 + k;
+        if (k >= nvalid || (fk != 0 && fk != nf - 1)) continue;
+        static_for<Q>([&](auto I) {
+          constexpr int cf = D::d == 3 ? D::C[I][2] : D::C[I][1];
+          if constexpr (cf != 0) {
+            if ((cf > 0 && fk == nf - 1) || (cf < 0 && fk == 0)) {
+              constexpr int cx = D::C[I][0], cy = D::C[I][1];
+              bool inside = x + cx >= 0 && x + cx < g.nx;
+              if constexpr (D::d == 3) inside = inside && y + cy >= 0 && y + cy < g.ny;
+              if (inside) ghost_store(I, k, n0 + k - uint32_t(cf * nf));
+            }
+          }
+        });
+      }
+    }
     static_for<Q>([&](auto I) {
       S* col = static_cast<S*>(cols.base[I]);
       if constexpr (DOUBLED) {
@@ -470,70 +583,73 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S>::blocks) k_collide_st
       }
     });
   }
-  if (stats) {
-    double a = accRho, b = accUsq, m = accMax;
-    unsigned c = accCount;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      c += __shfl_xor_sync(0xffffffffu, c, o);
-    }
-    if (((threadIdx.x + threadIdx.y * blockDim.x) & 31) == 0 && c > 0) {
-      atomicAdd(&stats->sum[0], a);
-      atomicAdd(&stats->sum[1], b);
-      atomicAdd(&stats->count, (unsigned long long)c);
-      atomicMax(&stats->maxbits, (unsigned long long)__double_as_longlong(m));
-    }
-  }
+  if (statPart) block_partial(accRho, accUsq, accMax, double(accCount), statPart);
 }
 
 // ---- periodic overlap copy (PostCollide) --------------------------------------------------
 // After the collision, every population that leaves the core across a periodic face is
 // copied into the ghost cell from which the next rotation carries it into the opposite face
 // -- the single-block form of the reference's periodic overlap communication
-// (core/superLattice.hh:150-155, gpu/cuda/communicator.hh:111-124).  One thread per cell of
-// each periodic face pair; a cell on an edge is visited once per face and writes the same
-// value to the same ghost slot each time.
+// (core/superLattice.hh:150-155, gpu/cuda/communicator.hh:111-124).  One thread per (face
+// cell, leaving population); the threads are ordered (axis, side, population, cell) so that a
+// warp copies one population of consecutive face cells.  A population leaving across two faces
+// at once (an edge) is copied by both faces' threads to the same ghost slot with the same value.
+template <int Q> struct FaceCount { static constexpr int n = Q == 9 ? 3 : (Q == 19 ? 5 : 9); };
+
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_periodic_halo(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                        int64_t cntX, int64_t cntY, int64_t cntZ) {
   using D = Desc<Q>;
+  constexpr int NF = FaceCount<Q>::n;
   int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  int x, y, z;
+  int axis;
+  int64_t plane;
   if (t < cntX) {
-    const int64_t plane = int64_t(g.ny) * g.nz;
-    x = (t / plane) ? g.nx - 1 : 0;
-    const int64_t r = t % plane;
-    y = int(r / g.nz);
-    z = int(r % g.nz);
+    axis = 0;
+    plane = int64_t(g.ny) * g.nz;
   } else if ((t -= cntX) < cntY) {
-    const int64_t plane = int64_t(g.nx) * g.nz;
-    y = (t / plane) ? g.ny - 1 : 0;
-    const int64_t r = t % plane;
-    x = int(r / g.nz);
-    z = int(r % g.nz);
+    axis = 1;
+    plane = int64_t(g.nx) * g.nz;
   } else if ((t -= cntY) < cntZ) {
-    const int64_t plane = int64_t(g.nx) * g.ny;
-    z = (t / plane) ? g.nz - 1 : 0;
-    const int64_t r = t % plane;
-    x = int(r / g.ny);
-    y = int(r % g.ny);
+    axis = 2;
+    plane = int64_t(g.nx) * g.ny;
   } else {
     return;
   }
+  const int64_t perSide = plane * NF;
+  const int side = t >= perSide ? 1 : -1;  // -1: the low face (leaving with c_axis = -1)
+  const int64_t rs = t >= perSide ? t - perSide : t;
+  const int j = int(rs / plane);
+  const int64_t cell = rs - int64_t(j) * plane;
+  int x, y, z;
+  if (axis == 0) {
+    x = side < 0 ? 0 : g.nx - 1;
+    y = int(cell / g.nz);
+    z = int(cell % g.nz);
+  } else if (axis == 1) {
+    y = side < 0 ? 0 : g.ny - 1;
+    x = int(cell / g.nz);
+    z = int(cell % g.nz);
+  } else {
+    z = side < 0 ? 0 : g.nz - 1;
+    x = int(cell / g.ny);
+    y = int(cell % g.ny);
+  }
   const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+  int count = 0;
   static_for<Q>([&](auto I) {
     constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+    const int ca = axis == 0 ? cx : (axis == 1 ? cy : cz);
+    if (ca != side) return;
+    if (count++ != j) return;
     int tx = x + cx, ty = y + cy, tz = z + cz;
-    bool crossed = false, lost = false;
-    if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
-    if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+    bool lost = false;
+    if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) tx = tx < 0 ? tx + g.nx : tx - g.nx; else lost = true; }
+    if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) ty = ty < 0 ? ty + g.ny : ty - g.ny; else lost = true; }
     if constexpr (D::d == 3) {
-      if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+      if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) tz = tz < 0 ? tz + g.nz : tz - g.nz; else lost = true; }
     }
-    if (crossed && !lost) {
+    if (!lost) {
       const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
       S* col = pop + I * g.stride;
       col[wrap_add(gn, sh.s[I], g.n)] = col[wrap_add(n, sh.s[I], g.n)];
@@ -775,7 +891,9 @@ struct LaunchArgs {
   int32_t dynamics;
   double omega, magic, smagorinsky, force[3];
   const uint8_t* cellDyn;
-  StatAcc* stats;
+  StatAcc* stats;       // statistics of this step requested: totals land here
+  double* statPart;     // block partials of the statistics (4 doubles per block)
+  int64_t statCapacity; // blocks statPart can hold
   int blockX, blockY;
   int kernel;          // 0: pipelined shared-memory tiles, 1: one cell per thread, 2: K cells per thread
   int cellsPerThread;  // K of kernel 2 (1, 2 or 4)
@@ -835,6 +953,7 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
   const auto sh = shifts_of<Q>(a);
   const auto p = params_of<R>(a);
   S* pop = static_cast<S*>(a.pop);
+  int64_t nblocks = 0;
   if (a.kernel == 0) {
     constexpr int smem = TileCfg<Q, S>::SMEM;
     static unsigned long long configured = 0;  // one bit per device ordinal
@@ -855,14 +974,19 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     }
     const int64_t tiles = (a.flatEnd - a.flatBase + TILE - 1) / TILE;
     const int64_t grid = tiles < residentBlocks[dev & 63] ? tiles : residentBlocks[dev & 63];
+    if (a.stats && grid > a.statCapacity) return cudaErrorInvalidValue;
     k_collide_stream_tiled<Q, S, DYN><<<unsigned(grid), TILE, smem, stream>>>(pop, g, sh, a.flatBase, a.flatEnd,
-                                                                               tiles, p, a.cellDyn, a.stats);
+                                                                               tiles, p, a.cellDyn,
+                                                                               a.stats ? a.statPart : nullptr);
+    nblocks = grid;
   } else if (a.kernel == 1) {
     dim3 block(a.blockX, a.blockY, 1);
     dim3 grid;
     if (Desc<Q>::d == 3) grid = dim3((g.nz + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
     else grid = dim3((g.ny + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
-    k_collide_stream<Q, S, DYN><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats);
+    nblocks = int64_t(grid.x) * grid.y * grid.z;
+    if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
+    k_collide_stream<Q, S, DYN><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats ? a.statPart : nullptr);
   } else {
     ColumnBases<Q> cols;
     for (int i = 0; i < Q; ++i) {
@@ -877,14 +1001,20 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     if (Desc<Q>::d == 3) grid = dim3((groups + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
     else grid = dim3((groups + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
     const int sel = K * 2 + (a.doubled ? 1 : 0);
+    nblocks = int64_t(grid.x) * grid.y * grid.z;
+    if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
+    double* part = a.stats ? a.statPart : nullptr;
     switch (sel) {
-    case 2: k_collide_stream_groups<Q, S, DYN, 1, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
-    case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
-    case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
-    case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.stats); break;
+    case 2: k_collide_stream_groups<Q, S, DYN, 1, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
+    case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
+    case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
+    case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
     default: return cudaErrorInvalidValue;
     }
   }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !a.stats) return e;
+  k_stats_finalize<<<1, 256, 0, stream>>>(a.statPart, nblocks, a.stats);
   return cudaGetLastError();
 }
 // Periodic overlap copy after the collision (no launch for a lattice without periodic axes).
@@ -894,9 +1024,13 @@ cudaError_t launch_halo(const LaunchArgs& a, cudaStream_t stream) {
   if (g.pmask == 0) return cudaSuccess;
   const auto sh = shifts_of<Q>(a);
   S* pop = static_cast<S*>(a.pop);
-  const int64_t cntX = (g.pmask & 1) ? 2 * int64_t(g.ny) * g.nz : 0;
-  const int64_t cntY = (g.pmask & 2) ? 2 * int64_t(g.nx) * g.nz : 0;
-  const int64_t cntZ = (g.pmask & 4) ? 2 * int64_t(g.nx) * g.ny : 0;
+  constexpr int NF = FaceCount<Q>::n;
+  // the K-cells step kernel (variant 2) does the whole overlap copy itself
+  if (a.kernel == 2) return cudaSuccess;
+  const int mask = g.pmask;
+  const int64_t cntX = (mask & 1) ? 2 * NF * int64_t(g.ny) * g.nz : 0;
+  const int64_t cntY = (mask & 2) ? 2 * NF * int64_t(g.nx) * g.nz : 0;
+  const int64_t cntZ = (mask & 4) ? 2 * NF * int64_t(g.nx) * g.ny : 0;
   const int64_t total = cntX + cntY + cntZ;
   k_periodic_halo<Q, S><<<unsigned((total + 255) / 256), 256, 0, stream>>>(pop, g, sh, cntX, cntY, cntZ);
   return cudaGetLastError();
