@@ -160,6 +160,11 @@ int lbx_ini_equilibrium(lbx_lattice lattice, const double* rho, const double* u,
 #define LBX_STEP_STATISTICS 1u
 int lbx_collide_and_stream(lbx_lattice lattice, int64_t steps, uint32_t flags, void* stream);
 
+/* Run the PostStream post-processors once (the bounce-back links) without a step: what
+ * BlockLattice::postProcess does (core/blockLattice.hh:483-489) and what the reference's
+ * SuperLattice::initialize() runs once before the first collideAndStream. */
+int lbx_post_process(lbx_lattice lattice, void* stream);
+
 /* Statistics of the last step run with LBX_STEP_STATISTICS: {average rho, average energy
  * (= mean |u|^2 / 2), max |u|, cell count} (LatticeStatistics, core/latticeStatistics.hh:
  * 60-90).  Synchronises the stream. */
@@ -207,6 +212,63 @@ int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x,
  * out[0..2] and their launch counts in out[3..5]. */
 int lbx_set_kernel_timing(lbx_lattice lattice, int32_t enable);
 int lbx_get_kernel_timing(lbx_lattice lattice, double out[6]);
+
+/* ---- ensemble engine: many independent lattices stepped together ----------------------
+ * No reference counterpart (the reference steps one SuperLattice at a time).  An ensemble owns
+ * one slab of device memory; each admitted request is a box cavity of its own size: all core
+ * cells fluid with the given bulk dynamics, halfway bounce-back walls on every face, the +y
+ * face moving in +x with lid_velocity (setBouzidiBoundary + setBouzidiVelocity semantics with
+ * q = 1/2, boundary/setBouzidiBoundary.h:129-162, the lid taking the edges).  A persistent kernel
+ * steps every running lattice through a tile -> lattice map, checks the relative L2 velocity
+ * residual ||u(t) - u(t - check)|| / ||u(t)|| every `check_interval` steps and stops a lattice
+ * when it falls below `tolerance` or after `max_steps`. */
+typedef struct lbx_ensemble_s* lbx_ensemble;
+
+typedef struct {
+  int32_t core[3];        /* nx, ny, nz */
+  int32_t dynamics;       /* LBX_BGK or LBX_TRT */
+  lbx_params params;      /* omega (and magic for TRT) */
+  double lid_velocity;    /* x velocity of the +y wall */
+  double tolerance;       /* stop at residual < tolerance */
+  int64_t max_steps;      /* stop after this many steps */
+} lbx_ensemble_request;
+
+typedef enum {
+  LBX_SLOT_FREE = 0,
+  LBX_SLOT_RUNNING = 1,
+  LBX_SLOT_CONVERGED = 2,
+  LBX_SLOT_MAX_STEPS = 3,
+  LBX_SLOT_DIVERGED = 4     /* residual or velocity not finite */
+} lbx_slot_state;
+
+typedef struct {
+  int32_t state;          /* lbx_slot_state */
+  int32_t pad;
+  int64_t steps;          /* steps taken */
+  double residual;        /* last checked residual */
+} lbx_ensemble_status;
+
+/* Slab bytes a request needs (populations + velocity snapshot). */
+int lbx_ensemble_footprint(int32_t q, int32_t storage, const lbx_ensemble_request* req, int64_t* bytes);
+int lbx_ensemble_create(int32_t q, int32_t storage, int64_t slab_bytes, int32_t max_lattices, int32_t device,
+                        lbx_ensemble* out);
+int lbx_ensemble_destroy(lbx_ensemble ens);
+/* Admit a request (populations at rest, rho = 1).  LBX_ERR_OUT_OF_MEMORY when the slab has no
+ * room or all slots are taken: the caller retries after retiring finished lattices. */
+int lbx_ensemble_admit(lbx_ensemble ens, const lbx_ensemble_request* req, int32_t* slot);
+/* Run `steps` steps of every running lattice in one persistent launch (replayed from a CUDA
+ * graph after the first call with the same step count), ordered on `stream`. */
+int lbx_ensemble_run(lbx_ensemble ens, int32_t steps, void* stream);
+/* Status of every slot (synchronises the stream); n = number of entries in `out`. */
+int lbx_ensemble_statuses(lbx_ensemble ens, lbx_ensemble_status* out, int32_t n, void* stream);
+/* rho [cells] and u [3][cells] of a slot's core cells, FP64 (with the wall links applied). */
+int lbx_ensemble_moments(lbx_ensemble ens, int32_t slot, double* rho, double* u, void* stream);
+/* Free a slot and its slab space (no effect on the others). */
+int lbx_ensemble_retire(lbx_ensemble ens, int32_t slot);
+/* Launch shape of the persistent kernel (the autotuner's knob): threads per block (multiple of
+ * 32, <= 256; cells per tile = threads), resident blocks per SM (0: occupancy maximum), and the
+ * residual check interval in steps. */
+int lbx_ensemble_set_config(lbx_ensemble ens, int32_t threads, int32_t blocks_per_sm, int32_t check_interval);
 
 /* Mass/momentum sums for callers that cannot allocate device memory.  No counterpart in the
  * reference.  lbx_reduce(LBX_REDUCE_MASS_MOMENTUM) needs a lattice handle, whose creation

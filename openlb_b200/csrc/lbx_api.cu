@@ -792,6 +792,16 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
   return LBX_OK;
 }
 
+int lbx_post_process(lbx_lattice L, void* stream) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (L->nLinks == 0) return LBX_OK;
+  DeviceGuard guard(L->device);
+  const LaunchArgs b = args_of(L);
+  LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks,
+                                                     static_cast<cudaStream_t>(stream)))));
+  return LBX_OK;
+}
+
 int lbx_set_kernel_timing(lbx_lattice L, int32_t enable) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   DeviceGuard guard(L->device);

@@ -44,6 +44,18 @@ class Info(C.Structure):
                 ("bytes", C.c_int64), ("n_links", C.c_int64), ("column_period", C.c_int64)]
 
 
+class EnsembleRequest(C.Structure):
+    _fields_ = [("core", C.c_int32 * 3), ("dynamics", C.c_int32), ("params", Params), ("lid_velocity", C.c_double),
+                ("tolerance", C.c_double), ("max_steps", C.c_int64)]
+
+
+class EnsembleStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("pad", C.c_int32), ("steps", C.c_int64), ("residual", C.c_double)]
+
+
+SLOT_FREE, SLOT_RUNNING, SLOT_CONVERGED, SLOT_MAX_STEPS, SLOT_DIVERGED = 0, 1, 2, 3, 4
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"liblbx.so not built ({LIB_PATH}); run `python -m openlb_b200.build`")
@@ -72,6 +84,16 @@ def _load() -> C.CDLL:
         "lbx_rotate": ([VP, I32, I64], C.c_int),
         "lbx_set_launch_config": ([VP, I32, I32, I32, I32], C.c_int),
         "lbx_set_kernel_timing": ([VP, I32], C.c_int),
+        "lbx_post_process": ([VP, VP], C.c_int),
+        "lbx_ensemble_footprint": ([I32, I32, P(EnsembleRequest), P(I64)], C.c_int),
+        "lbx_ensemble_create": ([I32, I32, I64, I32, I32, P(VP)], C.c_int),
+        "lbx_ensemble_destroy": ([VP], C.c_int),
+        "lbx_ensemble_admit": ([VP, P(EnsembleRequest), P(I32)], C.c_int),
+        "lbx_ensemble_run": ([VP, I32, VP], C.c_int),
+        "lbx_ensemble_statuses": ([VP, P(EnsembleStatus), I32, VP], C.c_int),
+        "lbx_ensemble_moments": ([VP, I32, VP, VP, VP], C.c_int),
+        "lbx_ensemble_retire": ([VP, I32], C.c_int),
+        "lbx_ensemble_set_config": ([VP, I32, I32, I32], C.c_int),
         "lbx_get_kernel_timing": ([VP, P(D)], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -247,6 +269,10 @@ class BlockLattice:
         flags = STEP_STATISTICS if statistics else 0
         check(lib.lbx_collide_and_stream(self._h, steps, flags, _stream_ptr(stream)), "lbx_collide_and_stream")
 
+    def post_process(self, stream=None) -> None:
+        """The PostStream post-processors once (what the reference's initialize() runs)."""
+        check(lib.lbx_post_process(self._h, _stream_ptr(stream)), "lbx_post_process")
+
     def get_statistics(self, stream=None) -> dict:
         out = (C.c_double * 4)()
         check(lib.lbx_get_statistics(self._h, out, _stream_ptr(stream)), "lbx_get_statistics")
@@ -283,3 +309,85 @@ class BlockLattice:
         s = C.c_int64()
         check(lib.lbx_population_shift(self._h, pop, C.byref(s)), "lbx_population_shift")
         return s.value
+
+
+def make_request(core, omega: float, lid_velocity: float, tolerance: float = 1e-6, max_steps: int = 50000,
+                 dynamics: str = "bgk", magic: float = 0.25) -> EnsembleRequest:
+    r = EnsembleRequest()
+    r.core = (C.c_int32 * 3)(*[int(v) for v in core])
+    r.dynamics = DYNAMICS[dynamics]
+    r.params = Params(omega, magic, 0.0, (C.c_double * 3)(0, 0, 0))
+    r.lid_velocity = lid_velocity
+    r.tolerance = tolerance
+    r.max_steps = max_steps
+    return r
+
+
+class Ensemble:
+    """Many independent box cavities stepped by one persistent kernel (lbx_ensemble_*)."""
+
+    def __init__(self, q: int = 19, storage: str = "f32", slab_bytes: int = 8 << 30, max_lattices: int = 1024,
+                 device: int = 0):
+        h = C.c_void_p()
+        check(lib.lbx_ensemble_create(q, STORAGE[storage], slab_bytes, max_lattices, device, C.byref(h)),
+              "lbx_ensemble_create")
+        self._h = h
+        self.q = q
+        self.storage = storage
+        self.max_lattices = max_lattices
+        self.cells: dict[int, int] = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.lbx_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def footprint(self, req: EnsembleRequest) -> int:
+        b = C.c_int64()
+        check(lib.lbx_ensemble_footprint(self.q, STORAGE[self.storage], C.byref(req), C.byref(b)),
+              "lbx_ensemble_footprint")
+        return b.value
+
+    def admit(self, req: EnsembleRequest) -> int | None:
+        """Slot of the admitted request, or None when the slab or the slot table is full."""
+        slot = C.c_int32()
+        rc = lib.lbx_ensemble_admit(self._h, C.byref(req), C.byref(slot))
+        if rc == -5:
+            return None
+        check(rc, "lbx_ensemble_admit")
+        self.cells[slot.value] = int(req.core[0]) * int(req.core[1]) * int(req.core[2])
+        return slot.value
+
+    def run(self, steps: int, stream=None) -> None:
+        check(lib.lbx_ensemble_run(self._h, steps, _stream_ptr(stream)), "lbx_ensemble_run")
+
+    def statuses(self, stream=None) -> list[tuple[int, int, float]]:
+        arr = (EnsembleStatus * self.max_lattices)()
+        check(lib.lbx_ensemble_statuses(self._h, arr, self.max_lattices, _stream_ptr(stream)), "lbx_ensemble_statuses")
+        return [(a.state, a.steps, a.residual) for a in arr]
+
+    def moments(self, slot: int, stream=None):
+        n = self.cells[slot]
+        rho = np.empty(n, np.float64)
+        u = np.empty((3, n), np.float64)
+        check(lib.lbx_ensemble_moments(self._h, slot, _ptr(rho), _ptr(u), _stream_ptr(stream)), "lbx_ensemble_moments")
+        return rho, u
+
+    def retire(self, slot: int) -> None:
+        check(lib.lbx_ensemble_retire(self._h, slot), "lbx_ensemble_retire")
+        self.cells.pop(slot, None)
+
+    def set_config(self, threads: int = 256, blocks_per_sm: int = 0, check_interval: int = 100) -> None:
+        check(lib.lbx_ensemble_set_config(self._h, threads, blocks_per_sm, check_interval), "lbx_ensemble_set_config")
