@@ -155,6 +155,26 @@ def tgv_fields(n: int):
     return np.ones(n ** 3), u
 
 
+STEP_KERNEL = {0: "k_collide_stream_tiled", 1: "k_collide_stream", 2: "k_collide_stream_groups"}
+
+
+def current_config(tuning: list[dict]) -> dict:
+    """The launch shape in use: the autotuner's pick (fastest timed candidate), else the default."""
+    timed = [t for t in tuning if t["ms_per_step"] > 0]
+    if not timed:
+        return {"variant": 2, "block_x": None, "block_y": None, "cells_per_thread": 1, "source": "default"}
+    best = min(timed, key=lambda t: t["ms_per_step"])
+    return {k: best[k] for k in ("variant", "block_x", "block_y", "cells_per_thread")} | {"source": "autotune"}
+
+
+def launch_config(cfg: dict, tuning: list[dict]) -> dict:
+    out = dict(cfg)
+    out["candidates"] = len(tuning)
+    out["tuned_ms_per_step"] = {f"v{t['variant']}/{t['block_x']}x{t['block_y']}/k{t['cells_per_thread']}":
+                                round(t["ms_per_step"], 4) for t in tuning}
+    return out
+
+
 def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     import torch
 
@@ -195,6 +215,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     lat.define_dynamics("bgk", omega=OMEGA)
     lat.ini_equilibrium(rho, u, stream=stream)
     lat.collide_and_stream(args.warmup, stream=stream)
+    tuning = lat.autotune(steps=10, stream=stream) if not args.no_autotune else []
     torch.cuda.synchronize(device)
     clocks = Clocks(device)
     clocks.start()
@@ -205,6 +226,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     kt = lat.kernel_timing()
     lat.set_kernel_timing(False)
     clk = clocks.stop()
+    lat_cfg = current_config(tuning)
     per_step_ms = ms / args.steps
     mlups = world * cells * args.steps / (ms * 1e-3) / 1e6
     coll_ms, coll_n = kt["collision"]
@@ -245,6 +267,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
             fl.define_dynamics("bgk", omega=OMEGA)
             fl.ini_equilibrium(rho, u, stream=stream)
             fl.collide_and_stream(args.warmup, stream=stream)
+            f_tuning = fl.autotune(steps=10, stream=stream) if not args.no_autotune else []
             fms = timed_steps(fl, k)
             fl.set_kernel_timing(True)
             timed_steps(fl, k)
@@ -253,8 +276,10 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
             f_gbs = cells * BYTES_PER_LUP[form] / (fk_ms / max(fk_n, 1) * 1e-3) / 1e9
             forms[form] = {"mlups": round(f_mlups, 1), "hbm_gbs": round(f_gbs, 1),
                            "hbm_frac": round(f_gbs / peak, 4), "vs_f32_mlups": round(f_mlups / mlups, 3),
-                           "steps": k}
+                           "steps": k, "launch_config": current_config(f_tuning)}
             fl.close()
+
+    ensemble = None if args.ensemble_requests <= 0 else run_ensemble(args, device, stream)
 
     if rank != 0:
         return None
@@ -273,8 +298,9 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
         "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(pop_bytes / args.steps),
                 "d2h_bytes_per_step": int(pop_bytes / args.steps + 32)},
         "gpu_launches": coll_n + halo_n,
+        "launch_config": launch_config(lat_cfg, tuning),
         "kernels": {k: v for k, v in {
-            "k_collide_stream_groups": {"avg_ms": round(coll_ms / max(coll_n, 1), 5), "launches": coll_n,
+            STEP_KERNEL[lat_cfg["variant"]]: {"avg_ms": round(coll_ms / max(coll_n, 1), 5), "launches": coll_n,
                                         "share": round(coll_ms / max(coll_ms + halo_ms, 1e-12), 4)},
             "k_periodic_halo": {"avg_ms": round(halo_ms / max(halo_n, 1), 5), "launches": halo_n,
                                 "share": round(halo_ms / max(coll_ms + halo_ms, 1e-12), 4)}}.items()
@@ -283,7 +309,56 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
         "statistics": stats,
         "forms": forms,
     }
+    if ensemble is not None:
+        line["ensemble"] = ensemble
     return line
+
+
+def run_ensemble(args, device: int, stream) -> dict:
+    """Serving form: a bounded sample of the lid-driven cavity parameter sweep (D3Q19 BGK, FP32,
+    edges {32..192}, Re log-uniform [10, 1000], lid 0.05, Poisson arrivals at 200/s, residual
+    tolerance 1e-6 with the step count capped) served by the continuous-batching ensemble server,
+    then the same requests solved one after another on the single-lattice path."""
+    import torch
+
+    from openlb_b200 import lbx, serving
+
+    reqs = serving.sample_requests(args.ensemble_requests, seed=2024, max_steps=args.ensemble_max_steps)
+    check = 100
+    with lbx.Ensemble(19, "f32", slab_bytes=24 << 30, max_lattices=256, device=device) as ens:
+        ens.set_config(threads=256, blocks_per_sm=0, check_interval=check)
+        # tune the persistent kernel once on one cavity of every edge length, then empty the slab
+        probe = [ens.admit(serving.CavityRequest(i, e, 100.0).engine_request())
+                 for i, e in enumerate((32, 48, 64, 96, 128, 192))]
+        tuning = ens.autotune(steps=10, stream=stream)
+        for slot in probe:
+            ens.retire(slot)
+        timed = [t for t in tuning if t["ms_per_step"] > 0]
+        pick = min(timed, key=lambda t: t["ms_per_step"]) if timed else None
+        server = serving.EnsembleServer(ens, chunk=500, stream=stream)
+        serving_warm = serving.sample_requests(4, seed=1, edges=(16,), max_steps=1000)
+        server.serve(serving_warm, realtime=False)  # graph capture and first-launch costs
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        recs = server.serve(reqs)
+        torch.cuda.synchronize(device)
+        wall = time.perf_counter() - t0
+    served = serving.summarise(recs, wall)
+    t0 = time.perf_counter()
+    seq = serving.solve_sequential(reqs, check_interval=check, device=device)
+    torch.cuda.synchronize(device)
+    seq_wall = time.perf_counter() - t0
+    sequential = serving.summarise(seq, seq_wall)
+    return {"workload": f"{len(reqs)} D3Q19 BGK lid-driven cavity requests, edge ~ U{{32,48,64,96,128,192}}, "
+                        f"Re ~ logU[10,1000], lid 0.05, Poisson 200/s (seed 2024), stop at L2 velocity "
+                        f"residual < 1e-6 (delta {check} steps) or {args.ensemble_max_steps} steps; f32 storage",
+            "sample": f"{len(reqs)} requests with the step cap lowered from 50000 to {args.ensemble_max_steps} "
+                      f"so the run ends in seconds",
+            "launch_config": None if pick is None else {"threads": pick["threads"],
+                                                        "blocks_per_sm": pick["blocks_per_sm"],
+                                                        "candidates": len(tuning), "source": "autotune"},
+            "server": served, "sequential": sequential,
+            "speedup_vs_sequential": round(sequential["wall_s"] / served["wall_s"], 3)}
 
 
 def main() -> int:
@@ -296,6 +371,9 @@ def main() -> int:
     ap.add_argument("--storage", default="f32", choices=["f32", "f64", "f16dev", "bf16dev"])
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--ensemble-requests", type=int, default=32)
+    ap.add_argument("--ensemble-max-steps", type=int, default=2000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

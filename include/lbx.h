@@ -266,9 +266,33 @@ int lbx_ensemble_moments(lbx_ensemble ens, int32_t slot, double* rho, double* u,
 /* Free a slot and its slab space (no effect on the others). */
 int lbx_ensemble_retire(lbx_ensemble ens, int32_t slot);
 /* Launch shape of the persistent kernel (the autotuner's knob): threads per block (multiple of
- * 32, <= 256; cells per tile = threads), resident blocks per SM (0: occupancy maximum), and the
- * residual check interval in steps. */
+ * 32, <= 256; a tile is 256 cells whatever the block size, so results and residuals do not
+ * depend on it), resident blocks per SM (0: occupancy maximum), and the residual check interval
+ * in steps. */
 int lbx_ensemble_set_config(lbx_ensemble ens, int32_t threads, int32_t blocks_per_sm, int32_t check_interval);
+
+/* ---- autotuner ----------------------------------------------------------------------------
+ * No reference counterpart (the reference's CUDA platform launches fixed 32-thread blocks,
+ * gpu/cuda/operator.hh:425-441).  Both calls time every candidate launch shape on the caller's
+ * own data with CUDA events on `stream`, each candidate starting from the same saved state, then
+ * keep the fastest and put the state back as it was: populations, column shifts (and for an
+ * ensemble every lattice's step count, residual and state) are unchanged on return, and since
+ * every launch shape computes identical bits the tuned run continues exactly as an untuned one
+ * would.  The saved state is a temporary device copy (populations of the lattice, or the used
+ * part of the ensemble slab); LBX_ERR_OUT_OF_MEMORY if it does not fit, config unchanged.
+ * out[0 .. min(capacity, candidates) - 1] lists what was tried, *n_out the number of candidates;
+ * ms_per_step < 0 marks a shape the device or the lattice does not accept. */
+typedef struct {
+  int32_t variant, block_x, block_y, cells_per_thread;  /* lbx_autotune: lbx_set_launch_config */
+  int32_t threads, blocks_per_sm;                       /* lbx_ensemble_autotune: set_config */
+  double ms_per_step;
+} lbx_tune_entry;
+/* Tunes the step kernel of one lattice over `steps` timed steps per candidate. */
+int lbx_autotune(lbx_lattice lattice, int32_t steps, lbx_tune_entry* out, int32_t capacity, int32_t* n_out,
+                 void* stream);
+/* Tunes the persistent kernel over `steps` timed steps of the admitted lattices (at least one). */
+int lbx_ensemble_autotune(lbx_ensemble ens, int32_t steps, lbx_tune_entry* out, int32_t capacity,
+                          int32_t* n_out, void* stream);
 
 /* Mass/momentum sums for callers that cannot allocate device memory.  No counterpart in the
  * reference.  lbx_reduce(LBX_REDUCE_MASS_MOMENTUM) needs a lattice handle, whose creation

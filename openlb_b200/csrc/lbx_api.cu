@@ -942,4 +942,94 @@ int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32
   return LBX_OK;
 }
 
+
+int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capacity, int32_t* n_out, void* stream) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (steps < 1 || capacity < 0 || (capacity > 0 && !out)) return fail(LBX_ERR_INVALID, "bad steps or output array");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // Candidates: the three kernels, block shapes along the fastest axis from 32 to 256 cells,
+  // full (256-thread) and half (128-thread) blocks, one or two cells per thread for variant 2.
+  struct Cand { int variant, bx, by, k; };
+  std::vector<Cand> cands;
+  const int nf = (L->d == 3) ? L->core[2] : L->core[1];
+  for (int k = 1; k <= 2; ++k)
+    for (int bx = 32; bx <= 256; bx *= 2) {
+      if (bx > 32 && bx >= 2 * ((nf + k - 1) / k)) break;  // wider blocks only idle more threads
+      for (int threads = 256; threads >= 128; threads /= 2)
+        if (threads / bx >= 1) cands.push_back({2, bx, threads / bx, k});
+    }
+  {
+    int bx, by;
+    block_shape_for(nf, 1, bx, by);
+    cands.push_back({1, bx, by, 1});
+    cands.push_back({0, 256, 1, 1});
+  }
+  if (n_out) *n_out = int32_t(cands.size());
+  const Cand keep{L->kernel, L->blockX, L->blockY, L->cellsPerThread};
+  // saved state: every column's period of populations and the shifts
+  const size_t es = storage_bytes(L->storage);
+  const size_t colBytes = size_t(L->period) * es, pitch = size_t(L->stride) * es;
+  void* saved = nullptr;
+  cudaError_t e = cudaMalloc(&saved, colBytes * size_t(L->q));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? LBX_ERR_OUT_OF_MEMORY : LBX_ERR_CUDA,
+                std::string("autotune state copy: ") + cudaGetErrorString(e));
+  }
+  int64_t shift0[27];
+  std::memcpy(shift0, L->shift, sizeof(shift0));
+  const bool timing0 = L->timing;
+  if (timing0) drain_timing(L);
+  L->timing = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto restore = [&]() -> cudaError_t {
+    std::memcpy(L->shift, shift0, sizeof(shift0));
+    return cudaMemcpy2DAsync(L->pop, pitch, saved, colBytes, colBytes, size_t(L->q), cudaMemcpyDeviceToDevice, s);
+  };
+  e = cudaMemcpy2DAsync(saved, colBytes, L->pop, pitch, colBytes, size_t(L->q), cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int best = -1;
+  float bestMs = 0.f;
+  int rc = LBX_OK;
+  for (size_t i = 0; i < cands.size() && e == cudaSuccess && rc == LBX_OK; ++i) {
+    const Cand& c = cands[i];
+    float ms = -1.f;
+    if (lbx_set_launch_config(L, c.variant, c.bx, c.by, c.k) == LBX_OK) {
+      e = restore();
+      if (e == cudaSuccess) rc = lbx_collide_and_stream(L, 1, 0, stream);  // warm-up
+      if (e == cudaSuccess && rc == LBX_OK) e = cudaEventRecord(e0, s);
+      if (e == cudaSuccess && rc == LBX_OK) rc = lbx_collide_and_stream(L, steps, 0, stream);
+      if (e == cudaSuccess && rc == LBX_OK) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess && rc == LBX_OK) e = cudaEventSynchronize(e1);
+      if (e == cudaSuccess && rc == LBX_OK) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e == cudaSuccess && rc == LBX_OK) {
+        ms /= float(steps);
+        if (best < 0 || ms < bestMs) {
+          best = int(i);
+          bestMs = ms;
+        }
+      }
+    }
+    if (out && int32_t(i) < capacity) out[i] = lbx_tune_entry{c.variant, c.bx, c.by, c.k, 0, 0, double(ms)};
+  }
+  const std::string err = rc != LBX_OK ? std::string(lbx_last_error()) : std::string();
+  cudaError_t e2 = restore();
+  if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = e2;
+  cudaFree(saved);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  L->timing = timing0;
+  const Cand pick = best >= 0 ? cands[size_t(best)] : keep;
+  L->kernel = pick.variant;
+  L->blockX = pick.bx;
+  L->blockY = pick.by;
+  L->cellsPerThread = pick.k;
+  if (rc != LBX_OK) return fail(rc, "autotune: " + err);
+  if (e != cudaSuccess) return fail(LBX_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+  return LBX_OK;
+}
+
 }  // extern "C"

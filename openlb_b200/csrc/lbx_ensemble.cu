@@ -3,19 +3,20 @@
 // Each admitted request owns a region of one device slab: Q population columns of period P
 // (its padded cell count rounded up to 64; the periodic-shift layout of lbx_kernels.cuh, the
 // ghost layer being the walls) and a velocity snapshot for the convergence residual.  A tile
-// is up to `threads` consecutive core cells of one lattice; the persistent kernel runs
+// is up to 2048 consecutive core cells of one lattice; the persistent kernel runs
 // `steps` steps, in each of which its blocks stride over the tile list, and two grid-wide
 // barriers per step separate the steps from the per-lattice bookkeeping done by block 0
 // (column shifts of the next step, step count, residual, state).  Lattices stop on their own
 // residual and are retired by the host between runs while the others keep going, so requests
 // of different sizes and ages are stepped together.
 //
-// Walls: halfway bounce-back on every face, applied when a boundary cell loads its
-// populations: the population arriving from a wall direction k is the one the cell sent the
-// step before, f_opp(k)(x_b) = f_k(x_b + c_k) - 2 t_k (c_k . u_w) / c_s^2 (the post-stream
-// BouzidiVelocityPostProcessor with q = 1/2, boundary/setBouzidiBoundary.h:129-162, evaluated
-// one step later: the collision sees identical values, only the stored between-step state of
-// the boundary cells differs, and lbx_ensemble_moments applies the same rule).
+// Walls: halfway bounce-back on every face, fused into the store of the boundary cells: the
+// population a cell sends into a wall direction k comes back as the opposite one,
+// f_opp(k)(x_b) = f_k(x_b) - 2 t_k (c_k . u_w) / c_s^2 (the post-stream
+// BouzidiVelocityPostProcessor with q = 1/2, boundary/setBouzidiBoundary.h:129-162), written to
+// the slot the next step's load of x_b reads: in periodic-shift storage that is the slot of the
+// ghost cell x_b + c_k in column opp(k) at the current shift, the same slot the single-lattice
+// link kernel writes after its stream, so both paths hold identical populations between steps.
 //
 // Memory ordering inside the persistent kernel: populations written by one block are read by
 // another block in the next step (a streamed population crosses tile boundaries), so every
@@ -43,6 +44,7 @@ namespace {
 using namespace lbx;
 
 constexpr int kMaxQ = 27;
+constexpr int kTileCells = 2048;  // cells per tile, independent of the block size
 
 struct EnsLattice {
   void* pop;        // column 0; column i starts at element i * P
@@ -51,6 +53,8 @@ struct EnsLattice {
   int32_t nx, ny, nz;
   int32_t sx, sy;   // padded strides
   int32_t ncore;
+  uint32_t mz, my;  // round-up multipliers for division by nz and ny (FastDiv)
+  int32_t lz, ly;   // and their shifts
   int32_t dynamics;
   int32_t state;
   int32_t pad0;
@@ -91,6 +95,20 @@ template <> struct CgLoad<__nv_bfloat16> {
 
 __device__ __forceinline__ uint32_t wrap32(uint32_t a, uint32_t P) { return a >= P ? a - P : a; }
 
+// Division by an invariant divisor d >= 1 for dividends below 2^31 (the round-up method of
+// Granlund and Montgomery, "Division by invariant integers using multiplication", 1994):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, n / d = (umulhi(m, n) + n) >> l.
+struct FastDiv {
+  static void make(uint32_t d, uint32_t& m, int32_t& l) {
+    l = 0;
+    while ((uint64_t(1) << l) < d) ++l;
+    m = uint32_t(((uint64_t(1) << 32) * ((uint64_t(1) << l) - d)) / d + 1);
+  }
+  static __device__ __forceinline__ uint32_t div(uint32_t n, uint32_t m, int32_t l) {
+    return (__umulhi(m, n) + n) >> l;
+  }
+};
+
 // Grid-wide barrier for a co-resident grid (cooperative launch).  Returns false when another
 // block gave up or this block waited longer than the bound; the kernel then returns.
 __device__ bool grid_barrier(unsigned* barrier, int* err) {
@@ -121,13 +139,20 @@ __device__ bool grid_barrier(unsigned* barrier, int* err) {
   return ok != 0;
 }
 
+// Resident 256-thread blocks per SM the register budget is cut for: three for the 32- and
+// 16-bit D3Q19 forms (80 registers; a few bytes spill), the compiler's choice otherwise.
+template <int Q, typename S> struct EnsOccupancy { static constexpr int blocks = 1; };
+template <> struct EnsOccupancy<19, float> { static constexpr int blocks = 3; };
+template <> struct EnsOccupancy<19, __half> { static constexpr int blocks = 3; };
+template <> struct EnsOccupancy<19, __nv_bfloat16> { static constexpr int blocks = 3; };
+
 template <int Q, typename S>
-__global__ void __launch_bounds__(256) k_ensemble(EnsArgs a) {
+__global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble(EnsArgs a) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   __shared__ uint32_t sShift[Q];
   __shared__ float sDelta[Q];
-  __shared__ double red[2][8];
+  __shared__ double red[2][kTileCells / 32];
   const int tid = threadIdx.x;
   for (int step = 0; step < a.steps; ++step) {
     const long long g = *reinterpret_cast<volatile long long*>(a.globalStep);
@@ -147,69 +172,91 @@ __global__ void __launch_bounds__(256) k_ensemble(EnsArgs a) {
       }
       __syncthreads();
       const uint32_t P = L->P;
-      const int nx = L->nx, ny = L->ny, nz = L->nz, sx = L->sx, sy = L->sy, ncore = L->ncore;
+      const int nx = L->nx, ny = L->ny, nz = L->nz, sx = L->sx, sy = L->sy;
+      const uint32_t mz = L->mz, my = L->my;
+      const int32_t lz = L->lz, ly = L->ly;
+      const int last = min(kTileCells, L->ncore - t.y);  // cells of this tile
+      const int ncore = L->ncore;
       S* pop = static_cast<S*>(L->pop);
-      double du2 = 0.0, u2 = 0.0;
-      const int c = t.y + tid;
-      if (c < ncore) {
-        const int z = c % nz;
-        const int y = (c / nz) % ny;
-        const int x = c / (nz * ny);
-        const uint32_t n = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
-        R f[Q];
-        static_for<Q>([&](auto I) { f[I] = CgLoad<S>::ld(pop + I * int64_t(P) + wrap32(n + sShift[I], P)); });
-        // halfway bounce-back on load for the links that leave the core
-        if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
-          static_for<Q>([&](auto K) {
-            constexpr int cx = D::C[K][0], cy = D::C[K][1], cz = D::C[K][2];
-            if constexpr (cx != 0 || cy != 0 || cz != 0) {
-              const int tx = x + cx, ty = y + cy, tz = z + cz;
-              if (tx < 0 || tx >= nx || ty < 0 || ty >= ny || tz < 0 || tz >= nz) {
-                const uint32_t nb = uint32_t(int(n) + cx * sx + cy * sy + cz);
-                const R v = CgLoad<S>::ld(pop + K * int64_t(P) + wrap32(nb + sShift[K], P));
-                f[D::OPP[K]] = v - (ty == ny ? R(sDelta[K]) : R(0));
-              }
-            }
-          });
-        }
-        if (check) {
-          R rho, u[3];
-          moments<Q, R, false>(f, nullptr, rho, u);
-          float* snap = L->snap;
+      CollisionParams<R> cp;
+      cp.omega = R(L->omega);
+      cp.magic = R(L->magic);
+      cp.smagorinsky = R(0);
+      cp.force[0] = cp.force[1] = cp.force[2] = R(0);
+      const int dyn = L->dynamics;
+      // The block walks the tile's cells in rounds of blockDim.x; each warp's 32 consecutive
+      // cells form one residual slot, reduced by the same shuffle tree whatever the block size,
+      // so the residual does not depend on the launch shape.
+      const int rounds = (last + 31) / 32 * 32;
+      for (int cl = tid; cl < rounds; cl += blockDim.x) {
+        double du2 = 0.0, u2 = 0.0;
+        const int c = t.y + cl;
+        if (cl < last) {
+          const uint32_t xy = FastDiv::div(uint32_t(c), mz, lz);
+          const int z = c - int(xy) * nz;
+          const int x = int(FastDiv::div(xy, my, ly));
+          const int y = int(xy) - x * ny;
+          const uint32_t n = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
+          R f[Q];
+          static_for<Q>([&](auto I) { f[I] = CgLoad<S>::ld(pop + I * int64_t(P) + wrap32(n + sShift[I], P)); });
+          if (check) {
+            R rho, u[3];
+            moments<Q, R, false>(f, nullptr, rho, u);
+            float* snap = L->snap;
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const double cur = double(u[d]);
-            const double dd = cur - double(__ldcg(snap + int64_t(d) * ncore + c));
-            du2 += dd * dd;
-            u2 += cur * cur;
-            snap[int64_t(d) * ncore + c] = float(cur);
+            for (int d = 0; d < 3; ++d) {
+              const double cur = double(u[d]);
+              const double dd = cur - double(__ldcg(snap + int64_t(d) * ncore + c));
+              du2 += dd * dd;
+              u2 += cur * cur;
+              snap[int64_t(d) * ncore + c] = float(cur);
+            }
+          }
+          R rho, usq;
+          if (dyn == LBX_TRT) collide<Q, R, DYN_TRT>(f, cp, rho, usq);
+          else collide<Q, R, DYN_BGK>(f, cp, rho, usq);
+          if (!(usq == usq) || usq > R(1)) du2 = __longlong_as_double(0x7ff8000000000000ll);  // NaN flags divergence
+          // store addresses recomputed from shared memory (volatile: not kept live in registers
+          // across the collision, which would cost two registers per population)
+          static_for<Q>([&](auto I) {
+            const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&sShift[I]);
+            Storage<S>::store(pop + I * int64_t(P) + wrap32(n + sh, P), f[I]);
+          });
+          // Halfway bounce-back of the links that leave the core: the population sent into the
+          // wall comes back as the opposite one, written where the next step's load of this
+          // cell finds it (the slot of ghost cell x + c_K in column opp(K) at this step's shift).
+          if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
+            static_for<Q>([&](auto K) {
+              constexpr int cx = D::C[K][0], cy = D::C[K][1], cz = D::C[K][2];
+              if constexpr (cx != 0 || cy != 0 || cz != 0) {
+                const int tx = x + cx, ty = y + cy, tz = z + cz;
+                if (tx < 0 || tx >= nx || ty < 0 || ty >= ny || tz < 0 || tz >= nz) {
+                  constexpr int O = D::OPP[K];
+                  const uint32_t gh = uint32_t(int(n) + cx * sx + cy * sy + cz);
+                  const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&sShift[O]);
+                  Storage<S>::store(pop + O * int64_t(P) + wrap32(gh + sh, P), f[K] - (ty == ny ? R(sDelta[K]) : R(0)));
+                }
+              }
+            });
           }
         }
-        CollisionParams<R> cp;
-        cp.omega = R(L->omega);
-        cp.magic = R(L->magic);
-        cp.smagorinsky = R(0);
-        cp.force[0] = cp.force[1] = cp.force[2] = R(0);
-        R rho, usq;
-        if (L->dynamics == LBX_TRT) collide<Q, R, DYN_TRT>(f, cp, rho, usq);
-        else collide<Q, R, DYN_BGK>(f, cp, rho, usq);
-        if (!(usq == usq) || usq > R(1)) du2 = __longlong_as_double(0x7ff8000000000000ll);  // NaN flags divergence
-        static_for<Q>([&](auto I) { Storage<S>::store(pop + I * int64_t(P) + wrap32(n + sShift[I], P), f[I]); });
+        if (check) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            du2 += __shfl_xor_sync(0xffffffffu, du2, o);
+            u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+          }
+          if ((tid & 31) == 0) {
+            red[0][cl >> 5] = du2;
+            red[1][cl >> 5] = u2;
+          }
+        }
       }
       if (check) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          du2 += __shfl_xor_sync(0xffffffffu, du2, o);
-          u2 += __shfl_xor_sync(0xffffffffu, u2, o);
-        }
-        if ((tid & 31) == 0) {
-          red[0][tid >> 5] = du2;
-          red[1][tid >> 5] = u2;
-        }
         __syncthreads();
         if (tid == 0) {
           double s0 = 0, s1 = 0;
-          for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+          for (int w = 0; w < (last + 31) / 32; ++w) {
             s0 += red[0][w];
             s1 += red[1][w];
           }
@@ -256,7 +303,8 @@ __global__ void __launch_bounds__(256) k_ensemble(EnsArgs a) {
   }
 }
 
-// rho and u of one lattice's core cells with the wall links applied (FP64 out).
+// rho and u of one lattice's core cells (FP64 out); the wall links were applied by the step that
+// wrote them.
 template <int Q, typename S>
 __global__ void k_ensemble_moments(const EnsLattice* __restrict__ lat, const long long* globalStep, double* rho,
                                    double* u) {
@@ -267,28 +315,40 @@ __global__ void k_ensemble_moments(const EnsLattice* __restrict__ lat, const lon
   if (c >= L.ncore) return;
   const int par = int(*globalStep & 1);
   const uint32_t P = L.P;
-  const int nx = L.nx, ny = L.ny, nz = L.nz, sx = L.sx, sy = L.sy;
+  const int ny = L.ny, nz = L.nz, sx = L.sx, sy = L.sy;
   const int z = c % nz, y = (c / nz) % ny, x = c / (nz * ny);
   const uint32_t n = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
   const S* pop = static_cast<const S*>(L.pop);
   R f[Q];
   static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * int64_t(P) + wrap32(n + L.shift[par][I], P)); });
-  static_for<Q>([&](auto K) {
-    constexpr int cx = D::C[K][0], cy = D::C[K][1], cz = D::C[K][2];
-    if constexpr (cx != 0 || cy != 0 || cz != 0) {
-      const int tx = x + cx, ty = y + cy, tz = z + cz;
-      if (tx < 0 || tx >= nx || ty < 0 || ty >= ny || tz < 0 || tz >= nz) {
-        const uint32_t nb = uint32_t(int(n) + cx * sx + cy * sy + cz);
-        f[D::OPP[K]] = Storage<S>::load(pop + K * int64_t(P) + wrap32(nb + L.shift[par][K], P)) -
-                       (ty == ny ? R(L.delta[K]) : R(0));
-      }
-    }
-  });
   R r, uu[3];
   moments<Q, R, false>(f, nullptr, r, uu);
   if (rho) rho[c] = double(r);
   if (u)
     for (int d = 0; d < 3; ++d) u[int64_t(d) * L.ncore + c] = double(uu[d]);
+}
+
+// Admission: the links through the moving lid start as if the rest state had been bounced once
+// (the reference applies its post-processors once at initialisation): population opp(K) of a
+// top-layer cell becomes 0 - delta_K, in the cell's own slot (the initial shifts are zero and
+// the first step loads the cell's populations where they are).
+template <int Q, typename S>
+__global__ void k_ensemble_init_links(const EnsLattice* __restrict__ lat) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const EnsLattice& L = *lat;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.nx * L.nz) return;
+  const int x = i / L.nz, z = i % L.nz, y = L.ny - 1;
+  const uint32_t n = uint32_t((x + 1) * L.sx + (y + 1) * L.sy + z + 1);
+  S* pop = static_cast<S*>(L.pop);
+  static_for<Q>([&](auto K) {
+    constexpr int cy = D::C[K][1];
+    if constexpr (cy == 1) {
+      constexpr int O = D::OPP[K];
+      Storage<S>::store(pop + O * int64_t(L.P) + n, R(0) - R(L.delta[K]));
+    }
+  });
 }
 
 size_t elem_bytes(int storage) {
@@ -312,23 +372,25 @@ int64_t region_bytes(int q, int storage, const lbx_ensemble_request* r, uint32_t
 
 using KernelFn = void (*)(EnsArgs);
 using MomentsFn = void (*)(const EnsLattice*, const long long*, double*, double*);
+using InitFn = void (*)(const EnsLattice*);
 
 template <int Q, typename S>
-void pick(KernelFn& k, MomentsFn& m) {
+void pick(KernelFn& k, MomentsFn& m, InitFn& i) {
   k = k_ensemble<Q, S>;
   m = k_ensemble_moments<Q, S>;
+  i = k_ensemble_init_links<Q, S>;
 }
 
-bool kernels_for(int q, int storage, KernelFn& k, MomentsFn& m) {
+bool kernels_for(int q, int storage, KernelFn& k, MomentsFn& m, InitFn& i) {
   switch (q * 4 + storage) {
-  case 19 * 4 + LBX_F64: pick<19, double>(k, m); return true;
-  case 19 * 4 + LBX_F32: pick<19, float>(k, m); return true;
-  case 19 * 4 + LBX_F16DEV: pick<19, __half>(k, m); return true;
-  case 19 * 4 + LBX_BF16DEV: pick<19, __nv_bfloat16>(k, m); return true;
-  case 27 * 4 + LBX_F64: pick<27, double>(k, m); return true;
-  case 27 * 4 + LBX_F32: pick<27, float>(k, m); return true;
-  case 27 * 4 + LBX_F16DEV: pick<27, __half>(k, m); return true;
-  case 27 * 4 + LBX_BF16DEV: pick<27, __nv_bfloat16>(k, m); return true;
+  case 19 * 4 + LBX_F64: pick<19, double>(k, m, i); return true;
+  case 19 * 4 + LBX_F32: pick<19, float>(k, m, i); return true;
+  case 19 * 4 + LBX_F16DEV: pick<19, __half>(k, m, i); return true;
+  case 19 * 4 + LBX_BF16DEV: pick<19, __nv_bfloat16>(k, m, i); return true;
+  case 27 * 4 + LBX_F64: pick<27, double>(k, m, i); return true;
+  case 27 * 4 + LBX_F32: pick<27, float>(k, m, i); return true;
+  case 27 * 4 + LBX_F16DEV: pick<27, __half>(k, m, i); return true;
+  case 27 * 4 + LBX_BF16DEV: pick<27, __nv_bfloat16>(k, m, i); return true;
   default: return false;
   }
 }
@@ -376,6 +438,7 @@ struct lbx_ensemble_s {
   int grid = 0;
   KernelFn kernel = nullptr;
   MomentsFn momentsKernel = nullptr;
+  InitFn initKernel = nullptr;
   std::map<int, cudaGraphExec_t> graphs;
   cudaGraph_t graphTemplate = nullptr;
 };
@@ -433,7 +496,7 @@ int upload_tiles(lbx_ensemble_s* E, cudaStream_t s) {
   for (int slot = 0; slot < E->maxLattices; ++slot) {
     if (!E->slotUsed[size_t(slot)]) continue;
     const int first = int(tiles.size());
-    for (int c = 0; c < E->slotCells[size_t(slot)]; c += E->threads) tiles.push_back(int2{slot, c});
+    for (int c = 0; c < E->slotCells[size_t(slot)]; c += kTileCells) tiles.push_back(int2{slot, c});
     range[size_t(slot)] = int2{first, int(tiles.size()) - first};
   }
   if (int(tiles.size()) > E->tileCapacity) {
@@ -467,6 +530,8 @@ int lbx_ensemble_footprint(int32_t q, int32_t storage, const lbx_ensemble_reques
   if (q != 19 && q != 27) return lbx::set_error(LBX_ERR_UNSUPPORTED, "ensembles are D3Q19 or D3Q27");
   for (int a = 0; a < 3; ++a)
     if (req->core[a] < 1 || req->core[a] > 4096) return lbx::set_error(LBX_ERR_INVALID, "core extent out of range");
+  if (int64_t(req->core[0] + 2) * (req->core[1] + 2) * (req->core[2] + 2) >= (int64_t(1) << 31) - 64)
+    return lbx::set_error(LBX_ERR_UNSUPPORTED, "an ensemble lattice holds fewer than 2^31 padded cells");
   *bytes = region_bytes(q, storage, req, nullptr);
   return LBX_OK;
 }
@@ -491,7 +556,7 @@ int lbx_ensemble_create(int32_t q, int32_t storage, int64_t slab_bytes, int32_t 
   E->slotBytes.assign(size_t(max_lattices), 0);
   E->slotUsed.assign(size_t(max_lattices), 0);
   E->slotCells.assign(size_t(max_lattices), 0);
-  kernels_for(q, storage, E->kernel, E->momentsKernel);
+  kernels_for(q, storage, E->kernel, E->momentsKernel, E->initKernel);
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&E->slab), size_t(E->slabBytes));
   if (e == cudaSuccess) e = cudaMalloc(&E->dLat, size_t(max_lattices) * sizeof(EnsLattice));
   if (e == cudaSuccess) e = cudaMemset(E->dLat, 0, size_t(max_lattices) * sizeof(EnsLattice));
@@ -547,6 +612,103 @@ int lbx_ensemble_set_config(lbx_ensemble E, int32_t threads, int32_t blocks_per_
   return LBX_OK;
 }
 
+int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, int32_t capacity, int32_t* n_out,
+                          void* stream) {
+  if (!E) return lbx::set_error(LBX_ERR_INVALID, "null ensemble");
+  if (steps < 1 || capacity < 0 || (capacity > 0 && !out)) return lbx::set_error(LBX_ERR_INVALID, "bad steps or output array");
+  int64_t hi = 0;
+  for (int i = 0; i < E->maxLattices; ++i)
+    if (E->slotUsed[size_t(i)]) hi = std::max(hi, E->slotOffset[size_t(i)] + E->slotBytes[size_t(i)]);
+  if (hi == 0) return lbx::set_error(LBX_ERR_STATE, "autotune needs at least one admitted lattice");
+  DeviceScope scope(E->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // Candidates: block sizes 64..256, resident blocks per SM from 1 to the occupancy maximum
+  // (the grid, and with it the cost of each grid barrier, grows with both).
+  struct Cand { int threads, perSM; };
+  std::vector<Cand> cands;
+  for (int threads = 64; threads <= 256; threads *= 2) {
+    int maxPerSM = 0;
+    ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxPerSM, E->kernel, threads, 0));
+    for (int b = 1; b <= std::min(maxPerSM, 8); b *= 2) cands.push_back({threads, b});
+    if (maxPerSM > 8) cands.push_back({threads, maxPerSM});
+  }
+  if (n_out) *n_out = int32_t(cands.size());
+  const Cand keep{E->threads, E->blocksPerSM};
+  const size_t latBytes = size_t(E->maxLattices) * sizeof(EnsLattice);
+  char* saved = nullptr;
+  cudaError_t e = cudaMalloc(&saved, size_t(hi) + latBytes + sizeof(long long));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return lbx::set_error(e == cudaErrorMemoryAllocation ? LBX_ERR_OUT_OF_MEMORY : LBX_ERR_CUDA,
+                          std::string("autotune state copy: ") + cudaGetErrorString(e));
+  }
+  auto copy_state = [&](bool save) -> cudaError_t {
+    char* a = save ? saved : E->slab;
+    const char* b = save ? E->slab : saved;
+    cudaError_t r = cudaMemcpyAsync(a, b, size_t(hi), cudaMemcpyDeviceToDevice, s);
+    char* la = save ? saved + hi : reinterpret_cast<char*>(E->dLat);
+    const char* lb = save ? reinterpret_cast<const char*>(E->dLat) : saved + hi;
+    if (r == cudaSuccess) r = cudaMemcpyAsync(la, lb, latBytes, cudaMemcpyDeviceToDevice, s);
+    char* ga = save ? saved + hi + latBytes : reinterpret_cast<char*>(E->dGlobalStep);
+    const char* gb = save ? reinterpret_cast<const char*>(E->dGlobalStep) : saved + hi + latBytes;
+    if (r == cudaSuccess) r = cudaMemcpyAsync(ga, gb, sizeof(long long), cudaMemcpyDeviceToDevice, s);
+    return r;
+  };
+  e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = copy_state(true);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int best = -1, rc = LBX_OK;
+  float bestMs = 0.f;
+  auto apply = [&](const Cand& c) {
+    E->threads = c.threads;
+    E->blocksPerSM = c.perSM;
+    E->grid = 0;
+    E->dirty = true;
+    drop_graphs(E);
+  };
+  for (size_t i = 0; i < cands.size() && e == cudaSuccess && rc == LBX_OK; ++i) {
+    const Cand& c = cands[i];
+    float ms = -1.f;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    apply(c);
+    if (e == cudaSuccess) e = copy_state(false);
+    if (e == cudaSuccess) rc = lbx_ensemble_run(E, steps, stream);  // warm-up, captures the graph
+    if (e == cudaSuccess && rc == LBX_OK) e = copy_state(false);
+    if (e == cudaSuccess && rc == LBX_OK) e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess && rc == LBX_OK) rc = lbx_ensemble_run(E, steps, stream);
+    if (e == cudaSuccess && rc == LBX_OK) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess && rc == LBX_OK) e = cudaEventSynchronize(e1);
+    int kerr = 0;
+    if (e == cudaSuccess && rc == LBX_OK) e = cudaMemcpy(&kerr, E->dErr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && rc == LBX_OK && kerr == 0) {
+      e = cudaEventElapsedTime(&ms, e0, e1);
+      ms /= float(steps);
+      if (e == cudaSuccess && (best < 0 || ms < bestMs)) {
+        best = int(i);
+        bestMs = ms;
+      }
+    } else if (kerr != 0) {
+      ms = -1.f;
+    }
+    if (out && int32_t(i) < capacity) out[i] = lbx_tune_entry{0, 0, 0, 0, c.threads, c.perSM, double(ms)};
+  }
+  const std::string err = rc != LBX_OK ? std::string(lbx_last_error()) : std::string();
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e2 == cudaSuccess) e2 = copy_state(false);
+  if (e2 == cudaSuccess) e2 = cudaMemsetAsync(E->dErr, 0, sizeof(int), s);
+  if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = e2;
+  cudaFree(saved);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  apply(best >= 0 ? cands[size_t(best)] : keep);
+  if (rc != LBX_OK) return lbx::set_error(rc, "autotune: " + err);
+  if (e != cudaSuccess) return lbx::set_error(LBX_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+  return LBX_OK;
+}
+
 int lbx_ensemble_admit(lbx_ensemble E, const lbx_ensemble_request* req, int32_t* slot) {
   if (!E || !req || !slot) return lbx::set_error(LBX_ERR_INVALID, "null argument");
   int64_t bytes = 0;
@@ -578,6 +740,8 @@ int lbx_ensemble_admit(lbx_ensemble E, const lbx_ensemble_request* req, int32_t*
   L.sy = req->core[2] + 2;
   L.sx = (req->core[1] + 2) * L.sy;
   L.ncore = req->core[0] * req->core[1] * req->core[2];
+  FastDiv::make(uint32_t(L.nz), L.mz, L.lz);
+  FastDiv::make(uint32_t(L.ny), L.my, L.ly);
   L.dynamics = req->dynamics;
   L.state = LBX_SLOT_RUNNING;
   L.steps = 0;
@@ -594,6 +758,12 @@ int lbx_ensemble_admit(lbx_ensemble E, const lbx_ensemble_request* req, int32_t*
   }
   cudaError_t e = cudaMemset(E->slab + off, 0, size_t(bytes));  // rest state (f - w = 0) and snapshot
   if (e == cudaSuccess) e = cudaMemcpy(E->dLat + s, &L, sizeof(L), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const int lid = L.nx * L.nz;
+    E->initKernel<<<(lid + 255) / 256, 256>>>(E->dLat + s);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     give_space(E, off, bytes);
     return lbx::set_error(LBX_ERR_CUDA, std::string("admit failed: ") + cudaGetErrorString(e));

@@ -53,6 +53,20 @@ class EnsembleStatus(C.Structure):
     _fields_ = [("state", C.c_int32), ("pad", C.c_int32), ("steps", C.c_int64), ("residual", C.c_double)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("variant", C.c_int32), ("block_x", C.c_int32), ("block_y", C.c_int32),
+                ("cells_per_thread", C.c_int32), ("threads", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("ms_per_step", C.c_double)]
+
+
+def _tune(fn, handle, steps: int, stream, where: str) -> list[dict]:
+    cap = 64
+    arr = (TuneEntry * cap)()
+    n = C.c_int32()
+    check(fn(handle, steps, arr, cap, C.byref(n), _stream_ptr(stream)), where)
+    return [{k: getattr(arr[i], k) for k, _ in TuneEntry._fields_} for i in range(min(n.value, cap))]
+
+
 SLOT_FREE, SLOT_RUNNING, SLOT_CONVERGED, SLOT_MAX_STEPS, SLOT_DIVERGED = 0, 1, 2, 3, 4
 
 
@@ -305,6 +319,11 @@ class BlockLattice:
         return {"collision": (out[0], int(out[3])), "periodic_overlap": (out[1], int(out[4])),
                 "links": (out[2], int(out[5]))}
 
+    def autotune(self, steps: int = 20, stream=None) -> list[dict]:
+        """Time every launch shape of the step kernel on this lattice's data, keep the fastest;
+        the populations are left as they were.  Returns the candidates with their ms/step."""
+        return _tune(lib.lbx_autotune, self._h, steps, stream, "lbx_autotune")
+
     def population_shift(self, pop: int) -> int:
         s = C.c_int64()
         check(lib.lbx_population_shift(self._h, pop, C.byref(s)), "lbx_population_shift")
@@ -388,6 +407,11 @@ class Ensemble:
     def retire(self, slot: int) -> None:
         check(lib.lbx_ensemble_retire(self._h, slot), "lbx_ensemble_retire")
         self.cells.pop(slot, None)
+
+    def autotune(self, steps: int = 50, stream=None) -> list[dict]:
+        """Time every launch shape of the persistent kernel on the admitted lattices, keep the
+        fastest; every lattice's state is left as it was."""
+        return _tune(lib.lbx_ensemble_autotune, self._h, steps, stream, "lbx_ensemble_autotune")
 
     def set_config(self, threads: int = 256, blocks_per_sm: int = 0, check_interval: int = 100) -> None:
         check(lib.lbx_ensemble_set_config(self._h, threads, blocks_per_sm, check_interval), "lbx_ensemble_set_config")

@@ -1,0 +1,196 @@
+"""Continuous-batching request server over the ensemble engine, and the sequential baseline.
+
+Parameter-sweep requests (lid-driven box cavities of different sizes and Reynolds numbers)
+arrive over time.  `EnsembleServer.serve` admits every waiting request whose slab footprint
+fits (skipping over ones that do not fit yet, so a large request does not block small ones
+behind it), steps all admitted lattices together in chunks of `chunk` steps through one
+persistent launch, and retires each lattice as soon as the engine reports it converged (relative
+L2 velocity residual below its tolerance), capped or diverged, freeing its slot and memory for
+the queue.  Requests that arrive while others are on the GPU join at the next chunk boundary.
+
+`solve_sequential` solves the same requests one after another on the single-lattice path
+(one lattice per launch sequence), the way a plain OpenLB run would.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import lbx
+
+
+@dataclass
+class CavityRequest:
+    rid: int
+    edge: int
+    reynolds: float
+    lid: float = 0.05
+    tolerance: float = 1e-6
+    max_steps: int = 50000
+    arrival: float = 0.0  # seconds after the start of the run
+
+    @property
+    def viscosity(self) -> float:
+        return self.lid * self.edge / self.reynolds
+
+    @property
+    def omega(self) -> float:
+        return 1.0 / (3.0 * self.viscosity + 0.5)
+
+    @property
+    def cells(self) -> int:
+        return self.edge ** 3
+
+    def engine_request(self) -> lbx.EnsembleRequest:
+        e = self.edge
+        return lbx.make_request((e, e, e), self.omega, self.lid, self.tolerance, self.max_steps)
+
+
+@dataclass
+class Record:
+    rid: int
+    cells: int
+    arrival: float
+    admitted: float = math.nan
+    finished: float = math.nan
+    steps: int = 0
+    state: int = 0
+    residual: float = math.nan
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def sample_requests(n: int, seed: int = 0, rate: float = 200.0, edges=(32, 48, 64, 96, 128, 192),
+                    re_range=(10.0, 1000.0), lid: float = 0.05, tolerance: float = 1e-6,
+                    max_steps: int = 50000) -> list[CavityRequest]:
+    """Seeded parameter sweep: edge uniform over `edges`, Re log-uniform over `re_range`,
+    Poisson arrivals at `rate` per second."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    es = rng.choice(np.asarray(edges), n)
+    res = np.exp(rng.uniform(math.log(re_range[0]), math.log(re_range[1]), n))
+    return [CavityRequest(i, int(es[i]), float(res[i]), lid, tolerance, max_steps, float(arrivals[i])) for i in range(n)]
+
+
+class EnsembleServer:
+    def __init__(self, ensemble: lbx.Ensemble, chunk: int = 200, stream=None):
+        self.ens = ensemble
+        self.chunk = chunk
+        self.stream = stream
+
+    def serve(self, requests: list[CavityRequest], realtime: bool = True, keep_fields: bool = False) -> list[Record]:
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        queue: list[CavityRequest] = []
+        active: dict[int, tuple[CavityRequest, Record]] = {}
+        records: list[Record] = []
+        t0 = time.perf_counter()
+        clock = (lambda: time.perf_counter() - t0) if realtime else None
+        virtual = 0.0
+
+        def now() -> float:
+            return clock() if clock else virtual
+
+        while pending or queue or active:
+            t = now()
+            while pending and pending[0].arrival <= t:
+                queue.append(pending.popleft())
+            still = []
+            for r in queue:
+                slot = self.ens.admit(r.engine_request())
+                if slot is None:
+                    still.append(r)
+                    continue
+                active[slot] = (r, Record(r.rid, r.cells, r.arrival, admitted=now()))
+            queue = still
+            if not active:
+                if pending:
+                    wait = pending[0].arrival - now()
+                    if clock and wait > 0:
+                        time.sleep(min(wait, 0.05))
+                    elif not clock:
+                        virtual = max(virtual, pending[0].arrival)
+                    continue
+                if queue:  # nothing running and the head does not fit: it never will
+                    raise RuntimeError(f"request {queue[0].rid} does not fit into an empty ensemble")
+                continue
+            t_run = time.perf_counter()
+            self.ens.run(self.chunk, stream=self.stream)
+            st = self.ens.statuses(stream=self.stream)
+            if not clock:
+                virtual += time.perf_counter() - t_run
+            for slot in list(active):
+                state, steps, residual = st[slot]
+                if state == lbx.SLOT_RUNNING:
+                    continue
+                r, rec = active.pop(slot)
+                if keep_fields:
+                    rec.extra["moments"] = self.ens.moments(slot, stream=self.stream)
+                rec.finished = now()
+                rec.steps = steps
+                rec.state = state
+                rec.residual = residual
+                self.ens.retire(slot)
+                records.append(rec)
+        return sorted(records, key=lambda r: r.rid)
+
+
+def solve_sequential(requests: list[CavityRequest], check_interval: int = 100, storage: str = "f32",
+                     device: int = 0, keep_fields: bool = False) -> list[Record]:
+    """The same requests solved one at a time on the single-lattice path (cavity with a solid
+    shell, halfway bounce-back links, residual checked every `check_interval` steps)."""
+    records = []
+    t0 = time.perf_counter()
+    for r in sorted(requests, key=lambda q: q.arrival):
+        e = r.edge
+        ext = (e + 2, e + 2, e + 2)
+        mat = np.full(ext, 2, np.int32)
+        mat[1:-1, 1:-1, 1:-1] = 1
+        mat[:, -1, :] = 3
+        rec = Record(r.rid, r.cells, r.arrival, admitted=time.perf_counter() - t0)
+        with lbx.BlockLattice(19, ext, (0, 0, 0), storage, device=device) as lat:
+            lat.define_dynamics("bgk", omega=r.omega)
+            lat.set_cell_dynamics((mat.reshape(-1) == 1).astype(np.uint8))
+            lat.set_bouzidi_boundary(mat, 1, (2, 3), [(0, 0, 0), (r.lid, 0, 0)])
+            lat.post_process()
+            steps, state, res = 0, lbx.SLOT_RUNNING, math.inf
+            lat.reduce(lbx.REDUCE_RESIDUAL)  # snapshot of the initial velocity
+            while state == lbx.SLOT_RUNNING:
+                k = min(check_interval, r.max_steps - steps)
+                lat.collide_and_stream(k)
+                steps += k
+                d, un, _ = lat.reduce(lbx.REDUCE_RESIDUAL)
+                if k == check_interval:
+                    res = d / un if un > 0 else (math.inf if d > 0 else 0.0)
+                    if not math.isfinite(res) or not math.isfinite(un):
+                        state = lbx.SLOT_DIVERGED
+                    elif res < r.tolerance:
+                        state = lbx.SLOT_CONVERGED
+                if state == lbx.SLOT_RUNNING and steps >= r.max_steps:
+                    state = lbx.SLOT_MAX_STEPS
+            if keep_fields:
+                rho, u = lat.compute_moments()
+                fluid = mat.reshape(-1) == 1
+                rec.extra["moments"] = (rho[fluid], u[:, fluid])
+        rec.finished = time.perf_counter() - t0
+        rec.steps, rec.state, rec.residual = steps, state, res
+        records.append(rec)
+    return records
+
+
+def summarise(records: list[Record], wall_seconds: float) -> dict:
+    lat = np.array([r.latency for r in records])
+    updates = float(sum(r.cells * r.steps for r in records))
+    states = {name: sum(1 for r in records if r.state == code) for name, code in
+              (("converged", lbx.SLOT_CONVERGED), ("max_steps", lbx.SLOT_MAX_STEPS), ("diverged", lbx.SLOT_DIVERGED))}
+    return {"requests": len(records), "wall_s": round(wall_seconds, 3),
+            "mlups": round(updates / wall_seconds / 1e6, 1),
+            "p50_s": round(float(np.percentile(lat, 50)), 4), "p99_s": round(float(np.percentile(lat, 99)), 4),
+            "lattice_updates": updates, "states": states}
