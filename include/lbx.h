@@ -63,8 +63,15 @@ typedef enum {
 typedef enum {
   LBX_CELL_NONE = 0,        /* NoDynamics (dynamics.h:51-63) */
   LBX_CELL_BULK = 1,        /* the lattice's bulk dynamics */
-  LBX_CELL_BOUNCE_BACK = 2  /* BounceBack = collision::Revert (collision.h:465-484) */
+  LBX_CELL_BOUNCE_BACK = 2, /* BounceBack = collision::Revert (collision.h:465-484) */
+  LBX_CELL_FD_BOUNDARY = 3  /* a cell of the lbx_set_fd_boundaries list (set by that call) */
 } lbx_cell_dynamics;
+
+/* Kinds of flat-face boundary cells (lbx_set_fd_boundaries). */
+typedef enum {
+  LBX_FD_VELOCITY = 1,      /* boundary::InterpolatedVelocity, boundary/interpolatedVelocity3D.h:45-52 */
+  LBX_FD_PRESSURE = 2       /* boundary::InterpolatedPressure, boundary/interpolatedPressure3D.h:48-90 */
+} lbx_fd_kind;
 
 /* Parameters of the bulk dynamics (the ParametersD fields OMEGA, TRT::MAGIC,
  * LES::SMAGORINSKY and the FORCE field, here uniform over the lattice). */
@@ -116,6 +123,27 @@ int lbx_set_dynamics(lbx_lattice lattice, int32_t dynamics, const lbx_params* pa
 /* Per-cell dynamics ids for the core cells ([core cells], lbx_cell_dynamics); NULL resets
  * to "bulk everywhere" (defineDynamics over a material, core/blockLattice.hh:274-286). */
 int lbx_set_cell_dynamics(lbx_lattice lattice, const uint8_t* ids);
+
+/* Flat-face velocity and pressure boundaries: what boundary::set<InterpolatedVelocity> and
+ * boundary::set<InterpolatedPressure> install on a flat face (boundary/setBoundary.h:80-100):
+ * the cell collides with BGKdynamics whose momenta are the boundary's
+ * (momenta::BasicDirichletVelocityBoundaryTuple / BasicDirichletPressureBoundaryTuple,
+ * dynamics/momenta/aliases.h:173-198; velocity: u imposed, rho from velocityBMRho; pressure:
+ * rho imposed, u_normal from the populations, the tangential velocity imposed), and after each
+ * stream PlaneFdBoundaryProcessor3D / StraightFdBoundaryProcessor2D
+ * (boundary/boundaryPostProcessors3D.hh:39-93, boundaryPostProcessors2D.hh:39-76) rebuilds all
+ * its populations as f^eq(rho, u) + f^neq(Pi) with Pi from finite-difference velocity gradients.
+ * cells: core cell indices; kinds: lbx_fd_kind; dirs: normal axis; orients: +1 or -1, the
+ * direction of the outward normal along that axis; values[4 * i ...]: the imposed velocity
+ * (velocity cells) or {rho, tangential velocity} (pressure cells).  Flat faces only: every
+ * cell needs two cells inward along its normal, and its neighbours along the face must be on
+ * the face or across a periodic axis (edges and corners are rejected with
+ * LBX_ERR_UNSUPPORTED).  The cells become LBX_CELL_FD_BOUNDARY in the cell dynamics map and
+ * keep that id through later lbx_set_cell_dynamics calls; n = 0 removes the list.  A neighbour
+ * reached across a periodic face contributes its j / rho, as the reference's overlap copy of
+ * that cell does (it carries bulk dynamics). */
+int lbx_set_fd_boundaries(lbx_lattice lattice, int64_t n, const int64_t* cells, const int32_t* kinds,
+                          const int32_t* dirs, const int32_t* orients, const double* values);
 
 /* Halfway bounce-back links: BouzidiVelocityPostProcessor with q = 1/2
  * (boundary/setBouzidiBoundary.h:129-162), applied after streaming.  Link l acts on core

@@ -97,6 +97,13 @@ struct lbx_lattice_s {
   uint8_t* linkDir = nullptr;
   void* linkDelta = nullptr;
   int64_t nLinks = 0;
+  // flat-face velocity / pressure boundary cells (lbx_set_fd_boundaries)
+  int64_t nFd = 0;
+  uint32_t* fdCell = nullptr;
+  uint8_t* fdMeta = nullptr;
+  double* fdValue = nullptr;
+  double* fdMom = nullptr;
+  std::vector<uint32_t> fdHostCells;  // padded indices, to re-mark after lbx_set_cell_dynamics
   StatAcc* stats = nullptr;
   double* statPart = nullptr;        // per-block statistics partials
   int64_t statCapacity = 0;          // blocks statPart holds
@@ -155,6 +162,11 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   const int64_t last = int64_t(g.nx) * g.sx + int64_t(g.ny) * g.sy + (g.nz - 1 + g.pz);
   a.flatBase = first / 8 * 8;
   a.flatEnd = last + 1;
+  a.nFd = L->nFd;
+  a.fdCell = L->fdCell;
+  a.fdMeta = L->fdMeta;
+  a.fdValue = L->fdValue;
+  a.fdMom = L->fdMom;
   return a;
 }
 
@@ -232,7 +244,7 @@ int64_t step_blocks(const lbx_lattice_s* L) {
 }
 
 int ensure_stat_capacity(lbx_lattice_s* L) {
-  const int64_t need = step_blocks(L);
+  const int64_t need = step_blocks(L) + fd_blocks(L->nFd);
   if (need > L->statCapacity) {
     cudaFree(L->statPart);
     L->statPart = nullptr;
@@ -535,6 +547,10 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->linkCell);
   cudaFree(L->linkDir);
   cudaFree(L->linkDelta);
+  cudaFree(L->fdCell);
+  cudaFree(L->fdMeta);
+  cudaFree(L->fdValue);
+  cudaFree(L->fdMom);
   cudaFree(L->stats);
   cudaFree(L->statPart);
   cudaFree(L->reduceAcc);
@@ -589,11 +605,90 @@ int lbx_set_cell_dynamics(lbx_lattice L, const uint8_t* ids) {
   }
   std::vector<uint8_t> padded(static_cast<size_t>(L->n), 0);
   for (int64_t c = 0; c < L->ncore; ++c) {
-    if (ids[c] > LBX_CELL_BOUNCE_BACK) return fail(LBX_ERR_INVALID, "cell dynamics id out of range");
+    if (ids[c] > LBX_CELL_FD_BOUNDARY) return fail(LBX_ERR_INVALID, "cell dynamics id out of range");
     padded[size_t(core_index_to_padded(L, c))] = ids[c];
   }
+  for (uint32_t n : L->fdHostCells) padded[n] = LBX_CELL_FD_BOUNDARY;  // the boundary list wins
   if (!L->cellDyn) LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
   LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, padded.data(), size_t(L->n), cudaMemcpyHostToDevice));
+  return LBX_OK;
+}
+
+int lbx_set_fd_boundaries(lbx_lattice L, int64_t n, const int64_t* cells, const int32_t* kinds,
+                          const int32_t* dirs, const int32_t* orients, const double* values) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (n < 0 || (n > 0 && (!cells || !kinds || !dirs || !orients || !values)))
+    return fail(LBX_ERR_INVALID, "bad boundary arrays");
+  DeviceGuard guard(L->device);
+  // validate and sort by cell (the kernels binary-search the list)
+  std::vector<int64_t> order(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    order[size_t(i)] = i;
+    if (cells[i] < 0 || cells[i] >= L->ncore) return fail(LBX_ERR_INVALID, "boundary cell out of range");
+    if (kinds[i] != LBX_FD_VELOCITY && kinds[i] != LBX_FD_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+    if (dirs[i] < 0 || dirs[i] >= L->d) return fail(LBX_ERR_INVALID, "normal axis out of range");
+    if (orients[i] != 1 && orients[i] != -1) return fail(LBX_ERR_INVALID, "orientation must be +1 or -1");
+    if (L->periodic[dirs[i]]) return fail(LBX_ERR_INVALID, "a boundary normal cannot lie along a periodic axis");
+    for (int k = 0; k < 4; ++k)
+      if (!std::isfinite(values[4 * i + k])) return fail(LBX_ERR_INVALID, "boundary values must be finite");
+    if (kinds[i] == LBX_FD_PRESSURE && !(values[4 * i] > 0)) return fail(LBX_ERR_INVALID, "boundary density must be > 0");
+  }
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cells[a] < cells[b]; });
+  for (int64_t i = 1; i < n; ++i)
+    if (cells[order[size_t(i)]] == cells[order[size_t(i - 1)]]) return fail(LBX_ERR_INVALID, "duplicate boundary cell");
+  // Flat faces only: the two cells inward along the normal must lie in the core, and along
+  // every other axis the face must continue (or the axis be periodic).
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t c = cells[i];
+    const int64_t ny = L->core[1], nz = L->core[2];
+    const int p[3] = {int(c / (ny * nz)), int((c / nz) % ny), int(c % nz)};
+    const int a = dirs[i];
+    const int in2 = p[a] - 2 * orients[i];
+    if (in2 < 0 || in2 >= L->core[a]) return fail(LBX_ERR_INVALID, "a boundary cell needs two cells inward along its normal");
+    for (int b = 0; b < L->d; ++b)
+      if (b != a && !L->periodic[b] && (p[b] == 0 || p[b] == L->core[b] - 1))
+        return fail(LBX_ERR_UNSUPPORTED, "boundary cell on an edge or corner (flat faces only)");
+  }
+  std::vector<uint32_t> hc(static_cast<size_t>(n));
+  std::vector<uint8_t> hm(static_cast<size_t>(n));
+  std::vector<double> hv(static_cast<size_t>(4 * n));
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t i = order[size_t(k)];
+    hc[size_t(k)] = uint32_t(core_index_to_padded(L, cells[i]));
+    hm[size_t(k)] = uint8_t(dirs[i] | (orients[i] > 0 ? 4 : 0) | (kinds[i] == LBX_FD_PRESSURE ? 8 : 0));
+    for (int v = 0; v < 4; ++v) hv[size_t(4 * k + v)] = values[4 * i + v];
+  }
+  cudaDeviceSynchronize();
+  cudaFree(L->fdCell);
+  cudaFree(L->fdMeta);
+  cudaFree(L->fdValue);
+  cudaFree(L->fdMom);
+  L->fdCell = nullptr;
+  L->fdMeta = nullptr;
+  L->fdValue = nullptr;
+  L->fdMom = nullptr;
+  L->nFd = 0;
+  // cell map: the listed cells become LBX_CELL_FD_BOUNDARY, the ones of an old list bulk
+  std::vector<uint8_t> map(static_cast<size_t>(L->n), 0);
+  if (L->cellDyn) {
+    LBX_CUDA_TRY(cudaMemcpy(map.data(), L->cellDyn, size_t(L->n), cudaMemcpyDeviceToHost));
+  } else {
+    for (int64_t c = 0; c < L->ncore; ++c) map[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
+    LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
+  }
+  for (uint32_t old : L->fdHostCells) map[old] = LBX_CELL_BULK;
+  for (uint32_t c : hc) map[c] = LBX_CELL_FD_BOUNDARY;
+  L->fdHostCells = hc;
+  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, map.data(), size_t(L->n), cudaMemcpyHostToDevice));
+  if (n == 0) return LBX_OK;
+  LBX_CUDA_TRY(cudaMalloc(&L->fdCell, size_t(n) * sizeof(uint32_t)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdMeta, size_t(n)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdValue, size_t(4 * n) * sizeof(double)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdMom, size_t(7 * n) * sizeof(double)));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdMeta, hm.data(), size_t(n), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdValue, hv.data(), size_t(4 * n) * sizeof(double), cudaMemcpyHostToDevice));
+  L->nFd = n;
   return LBX_OK;
 }
 
@@ -778,9 +873,11 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
     LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_halo<Q, S>(a, s))));
     if (ev[2]) cudaEventRecord(ev[2], s);
     rotate_all(L);
-    if (L->nLinks > 0) {
+    if (L->nLinks > 0 || L->nFd > 0) {
       const LaunchArgs b = args_of(L);
-      LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
+      if (L->nLinks > 0)
+        LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
+      if (L->nFd > 0) LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_fd_boundary<Q, S>(b, s))));
     }
     if (ev[3]) {
       cudaEventRecord(ev[3], s);
@@ -794,11 +891,13 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
 
 int lbx_post_process(lbx_lattice L, void* stream) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
-  if (L->nLinks == 0) return LBX_OK;
+  if (L->nLinks == 0 && L->nFd == 0) return LBX_OK;
   DeviceGuard guard(L->device);
   const LaunchArgs b = args_of(L);
-  LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks,
-                                                     static_cast<cudaStream_t>(stream)))));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (L->nLinks > 0)
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
+  if (L->nFd > 0) LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_fd_boundary<Q, S>(b, s))));
   return LBX_OK;
 }
 

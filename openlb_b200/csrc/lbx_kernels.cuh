@@ -685,6 +685,274 @@ __global__ void __launch_bounds__(256) k_bouzidi(S* __restrict__ pop, Geometry g
                     v - (delta ? delta[l] : R(0)));
 }
 
+// ---- flat-face velocity / pressure boundaries (InterpolatedVelocity / InterpolatedPressure)
+// A boundary cell carries a meta byte: bits 0-1 the normal axis d, bit 2 set for an outward
+// normal along +d (orientation +1, else -1), bit 3 set for a pressure cell (else velocity), and
+// four values: the imposed velocity, or {rho, tangential velocity}.  Reference: the boundary
+// momenta momenta::BasicDirichletVelocityBoundaryTuple / BasicDirichletPressureBoundaryTuple
+// (dynamics/momenta/aliases.h:173-198) mixed into BGKdynamics for the collision, and the
+// post-stream PlaneFdBoundaryProcessor3D / StraightFdBoundaryProcessor2D
+// (boundary/boundaryPostProcessors3D.hh:39-93, boundaryPostProcessors2D.hh:39-76).
+struct FdMeta {
+  int dir, orient, pressure;
+  __device__ __forceinline__ explicit FdMeta(uint8_t m)
+      : dir(m & 3), orient((m & 4) ? 1 : -1), pressure((m >> 3) & 1) {}
+};
+
+// rho and u of a boundary cell from its momenta (velocityBMRho, dynamics/momenta/elements.h:54-71;
+// FixedPressureMomentum::computeU, elements.h:653-690): rho_onWall sums the populations with
+// c_d = 0, rho_normal those with c_d = orientation, each in index order.
+template <int Q, typename R>
+__device__ __forceinline__ void fd_momenta(const R (&f)[Q], FdMeta m, const double* __restrict__ v, R& rho,
+                                           R (&u)[3]) {
+  using D = Desc<Q>;
+  R onWall = R(0), normal = R(0);
+  static_for<Q>([&](auto I) {
+    constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+    const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+    if (c == 0) onWall += f[I];
+  });
+  static_for<Q>([&](auto I) {
+    constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+    const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+    if (c == m.orient) normal += f[I];
+  });
+  u[0] = u[1] = u[2] = R(0);
+  if (!m.pressure) {
+    static_for<D::d>([&](auto A) { u[A] = R(v[A]); });
+    rho = (R(2) * normal + onWall + R(1)) / (R(1) + R(m.orient) * u[m.dir]);
+  } else {
+    static_for<D::d>([&](auto A) { u[A] = R(v[1 + A]); });
+    rho = R(v[0]);
+    u[m.dir] = R(m.orient) * ((R(2) * normal + onWall + R(1)) / rho - R(1));
+  }
+}
+
+// f_i^eq - w_i in the reference's generic operation order for every precision (the boundary
+// cells are few; their float arithmetic is left unfused).
+template <int Q, int I, typename R>
+__device__ __forceinline__ R equilibrium_plain(R rho, const R (&u)[3], R uSqr) {
+  constexpr R t = weight<Q, R>(I);
+  const R cu = c_dot<Q, I>(u);
+  return rho * t * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * uSqr) - t;
+}
+
+// Plain j / rho of a cell (BulkMomentum::computeU, dynamics/momenta/elements.h:500-508).
+template <int Q, typename R>
+__device__ __forceinline__ void bulk_velocity(const R (&f)[Q], R (&u)[3]) {
+  using D = Desc<Q>;
+  R rho = R(0);
+  static_for<Q>([&](auto I) { rho += f[I]; });
+  rho += R(1);
+  u[0] = u[1] = u[2] = R(0);
+  static_for<Q>([&](auto I) {
+    static_for<D::d>([&](auto A) {
+      constexpr int c = D::C[I][A];
+      if constexpr (c == 1) u[A] += f[I];
+      else if constexpr (c == -1) u[A] -= f[I];
+    });
+  });
+  static_for<D::d>([&](auto A) { u[A] /= rho; });
+}
+
+__device__ __forceinline__ void fd_decode(const Geometry& g, int64_t n, int& x, int& y, int& z) {
+  x = int(n / g.sx) - 1;
+  const int64_t r = n - int64_t(x + 1) * g.sx;
+  y = int(r / g.sy) - 1;
+  z = int(r - int64_t(y + 1) * g.sy) - int(g.pz);
+}
+
+// Collision of the boundary cells: BGKdynamics with the boundary momenta
+// (collision::BGK::apply with lbm::bgkCollision, dynamics/collision.h:68-78, lbm.h:395-403),
+// in place at the current shifts, after the bulk step kernel left these cells untouched.  A cell
+// on a periodic face also refreshes the ghost slots of its leaving populations (the bulk
+// kernel wrote them before this collision).  Statistics partials go after the bulk kernel's.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometry g, Shifts<Q> sh, double omega,
+                                                    int64_t nFd, const uint32_t* __restrict__ fdCell,
+                                                    const uint8_t* __restrict__ fdMeta,
+                                                    const double* __restrict__ fdValue, double* __restrict__ statPart) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double aR = 0.0, aU = 0.0, aC = 0.0;
+  if (b < nFd) {
+    const int64_t n = fdCell[b];
+    const FdMeta m(fdMeta[b]);
+    R f[Q];
+    static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
+    R rho, u[3];
+    fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
+    R uSqr = R(0);
+    static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+    const R w = R(omega);
+    static_for<Q>([&](auto I) {
+      f[I] *= R(1) - w;
+      f[I] += w * equilibrium_plain<Q, I>(rho, u, uSqr);
+    });
+    static_for<Q>([&](auto I) { Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), f[I]); });
+    if (g.pmask) {
+      int x, y, z;
+      fd_decode(g, n, x, y, z);
+      static_for<Q>([&](auto I) {
+        constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+        int tx = x + cx, ty = y + cy, tz = z + cz;
+        bool crossed = false, lost = false;
+        if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+        if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+        if constexpr (D::d == 3) {
+          if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+        }
+        if (crossed && !lost) {
+          const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+          Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
+        }
+      });
+    }
+    aR = double(rho);
+    aU = double(uSqr);
+    aC = 1.0;
+  }
+  if (statPart) block_partial(aR, aU, aU, aC, statPart);
+}
+
+// Post-stream pass 1: every boundary cell's velocity from its momenta, its plain j / rho (what a
+// neighbour reached across a periodic face sees: the reference's overlap copy of the cell,
+// which carries bulk dynamics) and its rho, from the populations before any cell is rewritten.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_fd_momenta(const S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t nFd,
+                                                    const uint32_t* __restrict__ fdCell,
+                                                    const uint8_t* __restrict__ fdMeta,
+                                                    const double* __restrict__ fdValue, double* __restrict__ fdMom) {
+  using R = typename Storage<S>::R;
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= nFd) return;
+  const int64_t n = fdCell[b];
+  R f[Q];
+  static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
+  R rho, u[3], ub[3];
+  fd_momenta<Q, R>(f, FdMeta(fdMeta[b]), fdValue + 4 * b, rho, u);
+  bulk_velocity<Q, R>(f, ub);
+  double* out = fdMom + 7 * b;
+  for (int a = 0; a < 3; ++a) {
+    out[a] = double(u[a]);
+    out[3 + a] = double(ub[a]);
+  }
+  out[6] = double(rho);
+}
+
+// Index of padded cell n in the ascending boundary list, or -1.
+__device__ __forceinline__ int64_t fd_find(const uint32_t* __restrict__ fdCell, int64_t nFd, uint32_t n) {
+  int64_t lo = 0, hi = nFd - 1;
+  while (lo <= hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    const uint32_t v = fdCell[mid];
+    if (v == n) return mid;
+    if (v < n) lo = mid + 1;
+    else hi = mid - 1;
+  }
+  return -1;
+}
+
+// Post-stream pass 2: the regularised populations of every boundary cell
+// (PlaneFdBoundaryProcessor3D::apply / StraightFdBoundaryProcessor2D::apply): velocity gradients
+// by fd::DirectedGradients (utilities/finiteDifference3D.h:74-210) -- along the normal the
+// one-sided -o (-3 u0 + 4 u1 - u2) / 2 from the cell and the two cells inward, along the face
+// the central (u(+1) - u(-1)) / 2 --, Pi = -rho / (c_s^-2 omega) (grad u + grad u^T) and
+// f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270).  Neighbours' velocities
+// come from pass 1 (boundary cells) or their populations (bulk cells, not written here), so
+// the result does not depend on the order the cells are processed in.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geometry g, Shifts<Q> sh, double omega,
+                                                       int64_t nFd, const uint32_t* __restrict__ fdCell,
+                                                       const uint8_t* __restrict__ fdMeta,
+                                                       const double* __restrict__ fdMom) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (b >= nFd) return;
+  const int64_t n = fdCell[b];
+  const FdMeta m(fdMeta[b]);
+  int pos[3];
+  fd_decode(g, n, pos[0], pos[1], pos[2]);
+  const int ext[3] = {g.nx, g.ny, g.nz};
+  const double* own = fdMom + 7 * b;
+  const R rho = R(own[6]);
+  R u[3] = {R(own[0]), R(own[1]), R(own[2])};
+  auto velocity_at = [&](int px, int py, int pz, bool wrapped, R (&v)[3]) {
+    const int64_t nn = int64_t(px + 1) * g.sx + int64_t(py + 1) * g.sy + (pz + g.pz);
+    const int64_t j = fd_find(fdCell, nFd, uint32_t(nn));
+    if (j >= 0) {
+      const double* mm = fdMom + 7 * j + (wrapped ? 3 : 0);
+      v[0] = R(mm[0]);
+      v[1] = R(mm[1]);
+      v[2] = R(mm[2]);
+    } else {
+      R f[Q];
+      static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(nn, sh.s[I], g.n)); });
+      bulk_velocity<Q, R>(f, v);
+    }
+  };
+  R grad[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
+  for (int a = 0; a < D::d; ++a) {
+    R ua[3] = {R(0), R(0), R(0)}, ub[3] = {R(0), R(0), R(0)};
+    if (a == m.dir) {
+      int p1[3] = {pos[0], pos[1], pos[2]}, p2[3] = {pos[0], pos[1], pos[2]};
+      p1[a] -= m.orient;
+      p2[a] -= 2 * m.orient;
+      velocity_at(p1[0], p1[1], p1[2], false, ua);
+      velocity_at(p2[0], p2[1], p2[2], false, ub);
+      for (int iD = 0; iD < D::d; ++iD)
+        grad[a][iD] = R(-m.orient) * (((R(-3) * u[iD] + R(4) * ua[iD]) - R(1) * ub[iD]) / R(2));
+    } else {
+      int pp[3] = {pos[0], pos[1], pos[2]}, pm[3] = {pos[0], pos[1], pos[2]};
+      pp[a] += 1;
+      pm[a] -= 1;
+      const bool wp = pp[a] >= ext[a], wm = pm[a] < 0;  // across a periodic face (flat faces only)
+      if (wp) pp[a] -= ext[a];
+      if (wm) pm[a] += ext[a];
+      velocity_at(pp[0], pp[1], pp[2], wp, ua);
+      velocity_at(pm[0], pm[1], pm[2], wm, ub);
+      for (int iD = 0; iD < D::d; ++iD) grad[a][iD] = (ua[iD] - ub[iD]) / R(2);
+    }
+  }
+  const R sToPi = -rho / R(3) / R(omega);
+  R pi[6];
+  if constexpr (D::d == 3) {
+    pi[0] = R(2) * grad[0][0] * sToPi;
+    pi[3] = R(2) * grad[1][1] * sToPi;
+    pi[5] = R(2) * grad[2][2] * sToPi;
+    pi[1] = (grad[0][1] + grad[1][0]) * sToPi;
+    pi[2] = (grad[0][2] + grad[2][0]) * sToPi;
+    pi[4] = (grad[1][2] + grad[2][1]) * sToPi;
+  } else {
+    pi[0] = R(2) * grad[0][0] * sToPi;
+    pi[2] = R(2) * grad[1][1] * sToPi;
+    pi[1] = (grad[0][1] + grad[1][0]) * sToPi;
+  }
+  R uSqr = R(0);
+  static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+  static_for<Q>([&](auto I) {
+    constexpr R t = weight<Q, R>(I);
+    R fneq = R(0);
+    int ip = 0;
+    static_for<D::d>([&](auto AL) {
+      static_for<D::d>([&](auto BE) {
+        if constexpr (BE >= AL) {
+          constexpr int ca = D::C[I][AL], cb = D::C[I][BE];
+          R add = R(ca) * R(cb);
+          if constexpr (AL == BE) add -= R(1) / R(3);
+          else add *= R(2);
+          add *= pi[ip++];
+          fneq += add;
+        }
+      });
+    });
+    fneq *= t * R(3) * R(3) / R(2);
+    Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), equilibrium_plain<Q, I>(rho, u, uSqr) + fneq);
+  });
+}
+
 // ---- host <-> column transfers (one population at a time through a staging buffer) -----
 template <typename S, typename H>
 __global__ void k_scatter_pop(S* __restrict__ col, Geometry g, int64_t shift, const H* __restrict__ src) {
@@ -900,12 +1168,22 @@ struct LaunchArgs {
   int doubled;         // columns mapped twice back to back: index n + shift needs no wrap
   int64_t flatBase;    // first tile start (multiple of 8) and end of the flat cell range
   int64_t flatEnd;
+  int64_t nFd;               // flat-face velocity/pressure boundary cells
+  const uint32_t* fdCell;    // their padded indices, ascending
+  const uint8_t* fdMeta;     // normal axis, orientation, kind (FdMeta)
+  const double* fdValue;     // 4 imposed values per cell
+  double* fdMom;             // 7 doubles per cell of scratch (k_fd_momenta)
 };
+
+// Blocks of 256 threads the boundary-cell collision adds to a step's statistics partials.
+inline int64_t fd_blocks(int64_t nFd) { return (nFd + 255) / 256; }
 
 template <int Q, typename S>
 cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream);
 template <int Q, typename S>
 cudaError_t launch_halo(const LaunchArgs& a, cudaStream_t stream);
+template <int Q, typename S>
+cudaError_t launch_fd_boundary(const LaunchArgs& a, cudaStream_t stream);
 template <int Q, typename S>
 cudaError_t launch_bouzidi(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
                            const void* delta, int64_t nLinks, cudaStream_t stream);
@@ -1013,8 +1291,31 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     }
   }
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess || !a.stats) return e;
-  k_stats_finalize<<<1, 256, 0, stream>>>(a.statPart, nblocks, a.stats);
+  if (e != cudaSuccess) return e;
+  int64_t fdb = 0;
+  if (a.nFd > 0) {
+    fdb = fd_blocks(a.nFd);
+    if (a.stats && nblocks + fdb > a.statCapacity) return cudaErrorInvalidValue;
+    k_fd_collide<Q, S><<<unsigned(fdb), 256, 0, stream>>>(pop, g, sh, a.omega, a.nFd, a.fdCell, a.fdMeta, a.fdValue,
+                                                          a.stats ? a.statPart + 4 * nblocks : nullptr);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (!a.stats) return cudaSuccess;
+  k_stats_finalize<<<1, 256, 0, stream>>>(a.statPart, nblocks + fdb, a.stats);
+  return cudaGetLastError();
+}
+// Post-stream regularisation of the flat-face boundary cells (two passes, see k_fd_regularize).
+template <int Q, typename S>
+cudaError_t launch_fd_boundary(const LaunchArgs& a, cudaStream_t stream) {
+  if (a.nFd <= 0) return cudaSuccess;
+  const unsigned blocks = unsigned(fd_blocks(a.nFd));
+  S* pop = static_cast<S*>(a.pop);
+  const auto sh = shifts_of<Q>(a);
+  k_fd_momenta<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.nFd, a.fdCell, a.fdMeta, a.fdValue, a.fdMom);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_fd_regularize<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.omega, a.nFd, a.fdCell, a.fdMeta, a.fdMom);
   return cudaGetLastError();
 }
 // Periodic overlap copy after the collision (no launch for a lattice without periodic axes).
@@ -1114,6 +1415,7 @@ cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc,
 #define LBX_INSTANTIATE(Q, S)                                                                          \
   template cudaError_t launch_step<Q, S>(const LaunchArgs&, cudaStream_t);                            \
   template cudaError_t launch_halo<Q, S>(const LaunchArgs&, cudaStream_t);                            \
+  template cudaError_t launch_fd_boundary<Q, S>(const LaunchArgs&, cudaStream_t);                     \
   template cudaError_t launch_bouzidi<Q, S>(const LaunchArgs&, const uint32_t*, const uint8_t*,       \
                                             const void*, int64_t, cudaStream_t);                      \
   template cudaError_t launch_transfer<Q, S>(const LaunchArgs&, int, const void*, int, bool, cudaStream_t); \

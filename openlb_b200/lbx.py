@@ -99,6 +99,9 @@ def _load() -> C.CDLL:
         "lbx_set_launch_config": ([VP, I32, I32, I32, I32], C.c_int),
         "lbx_set_kernel_timing": ([VP, I32], C.c_int),
         "lbx_post_process": ([VP, VP], C.c_int),
+        "lbx_set_fd_boundaries": ([VP, I64, VP, VP, VP, VP, VP], C.c_int),
+        "lbx_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
+        "lbx_ensemble_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_footprint": ([I32, I32, P(EnsembleRequest), P(I64)], C.c_int),
         "lbx_ensemble_create": ([I32, I32, I64, I32, I32, P(VP)], C.c_int),
         "lbx_ensemble_destroy": ([VP], C.c_int),
@@ -170,6 +173,51 @@ def build_bouzidi_links(q: int, core, material: np.ndarray, fluid: int = 1, soli
     check(lib.lbx_build_bouzidi_links(*args, n.value, _ptr(cells), _ptr(dirs), _ptr(wall), C.byref(n)),
           "lbx_build_bouzidi_links")
     return cells, dirs, wall
+
+
+FD_VELOCITY, FD_PRESSURE = 1, 2
+
+
+def fd_boundaries_from_materials(material: np.ndarray, boundary: int, fluid=(1,), outside=(0,),
+                                 periodic=(False, False, False)):
+    """Flat-face cells of material `boundary` with their discrete normal, as boundary::set
+    classifies them (geometry/discreteNormals.h): the normal points to the one axis direction
+    whose neighbour is outside (a material in `outside`, or past a non-periodic domain edge)
+    while the opposite neighbour is fluid.  Returns (cells, dirs, orients) for the cells with
+    exactly one such direction; other cells of the material (edges, corners) are left out."""
+    mat = np.asarray(material)
+    d = mat.ndim
+    fluid_m = np.isin(mat, fluid)
+    outside_m = np.isin(mat, outside)
+    cells, dirs, orients = [], [], []
+
+    def look(pt, a, mask):
+        if 0 <= pt[a] < mat.shape[a]:
+            return bool(mask[tuple(pt)])
+        if periodic[a]:
+            pt = list(pt)
+            pt[a] %= mat.shape[a]
+            return bool(mask[tuple(pt)])
+        return mask is outside_m  # past a non-periodic edge: outside
+
+    for idx in zip(*np.nonzero(mat == boundary)):
+        open_sides = []  # (axis, orientation) of every outside neighbour along the axes
+        for a in range(d):
+            for o in (-1, 1):
+                p = list(idx)
+                p[a] += o
+                if look(p, a, outside_m):
+                    open_sides.append((a, o))
+        if len(open_sides) != 1:
+            continue  # interior of the material, or an edge / corner
+        a, o = open_sides[0]
+        q = list(idx)
+        q[a] -= o
+        if look(q, a, fluid_m):
+            cells.append(int(np.ravel_multi_index(idx, mat.shape)))
+            dirs.append(a)
+            orients.append(o)
+    return np.array(cells, np.int64), np.array(dirs, np.int32), np.array(orients, np.int32)
 
 
 class BlockLattice:
@@ -251,6 +299,20 @@ class BlockLattice:
         d = np.ascontiguousarray(dirs, dtype=np.int32)
         w = None if wall is None else np.ascontiguousarray(wall, dtype=np.float64)
         check(lib.lbx_set_bouzidi_links(self._h, len(c), _ptr(c), _ptr(d), _ptr(w)), "lbx_set_bouzidi_links")
+
+    def set_fd_boundaries(self, cells, kinds, dirs, orients, values) -> None:
+        """Flat-face velocity (kind 1) / pressure (kind 2) boundary cells: the cells of
+        boundary::set<InterpolatedVelocity | InterpolatedPressure>; values [n, 4] = the imposed
+        velocity, or {rho, tangential velocity}."""
+        c = np.ascontiguousarray(cells, dtype=np.int64)
+        k = np.ascontiguousarray(kinds, dtype=np.int32)
+        d = np.ascontiguousarray(dirs, dtype=np.int32)
+        o = np.ascontiguousarray(orients, dtype=np.int32)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1, 4)
+        if not (len(c) == len(k) == len(d) == len(o) == len(v)):
+            raise ValueError("boundary arrays differ in length")
+        check(lib.lbx_set_fd_boundaries(self._h, len(c), _ptr(c), _ptr(k), _ptr(d), _ptr(o), _ptr(v)),
+              "lbx_set_fd_boundaries")
 
     def set_bouzidi_boundary(self, material: np.ndarray, fluid: int = 1, solid=(2,), wall_velocity=None) -> None:
         mat = np.ascontiguousarray(material, dtype=np.int32).reshape(-1)

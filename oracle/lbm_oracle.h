@@ -31,7 +31,8 @@ enum lbo_dynamics {
 enum lbo_material {
   LBO_SOLID = 0,      /* NoDynamics: left untouched (dynamics.h:51-63) */
   LBO_FLUID = 1,      /* the case's bulk dynamics */
-  LBO_BOUNCE_BACK = 4 /* BounceBack = collision::Revert (collision.h:465-484) */
+  LBO_BOUNCE_BACK = 4,/* BounceBack = collision::Revert (collision.h:465-484) */
+  LBO_FD_BOUNDARY = 5 /* flat-face Dirichlet cell: BGK with boundary momenta (fd_* below) */
 };
 
 typedef struct {
@@ -46,6 +47,15 @@ typedef struct {
   const int64_t* link_cell;  /* fluid boundary cell x_b */
   const int32_t* link_dir;   /* k: direction from x_b into the solid neighbour x_b + c_k */
   const double* link_wall;   /* c_k . u_wall per link (NULL: resting walls) */
+  /* Flat-face velocity / pressure boundary cells (boundary::InterpolatedVelocity and
+   * boundary::InterpolatedPressure on faces whose tangential axes are periodic):
+   * src/boundary/interpolatedVelocity3D.h:45-52,78-80, interpolatedPressure3D.h:48-90. */
+  int64_t n_fd;
+  const int64_t* fd_cell;    /* core cell, ascending */
+  const int32_t* fd_kind;    /* 1 velocity, 2 pressure */
+  const int32_t* fd_dir;     /* normal axis */
+  const int32_t* fd_orient;  /* outward normal sign, -1 or +1 */
+  const double* fd_value;    /* 4 per cell: the velocity, or {rho, tangential velocity} */
 } lbo_case;
 
 /* Run `steps` collide-and-stream steps in place.  stats (may be NULL) receives per step

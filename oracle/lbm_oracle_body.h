@@ -112,6 +112,182 @@ static void FN(collide)(const lbo_desc* d, const lbo_case* c, REAL* g, REAL* rho
   *usq_out = uSqr;
 }
 
+/* Density and velocity of a flat-face boundary cell from its momenta
+ * (momenta::BasicDirichletVelocityBoundaryTuple / BasicDirichletPressureBoundaryTuple,
+ * src/dynamics/momenta/aliases.h:173-198):
+ *  velocity: u = imposed (FixedVelocityMomentumGeneric, elements.h:603-630), rho from
+ *            velocityBMRho (elements.h:54-71) = (2 rho_normal + rho_onWall + 1) / (1 + o u_d);
+ *  pressure: rho = imposed (FixedDensity, elements.h:270-280), u = imposed tangential
+ *            velocity with u_d = o ((2 rho_normal + rho_onWall + 1) / rho - 1)
+ *            (FixedPressureMomentum::computeU, elements.h:653-690).
+ * rho_onWall sums the populations with c_d = 0, rho_normal those with c_d = o, in index order. */
+static void FN(fd_momenta)(const lbo_desc* d, const REAL* g, int kind, int dir, int orient,
+                           const double* value, REAL* rho, REAL* u)
+{
+  const int q = d->q, dim = d->d;
+  REAL onWall = 0, normal = 0;
+  for (int i = 0; i < q; ++i)
+    if (d->c[i][dir] == 0) onWall += g[i];
+  for (int i = 0; i < q; ++i)
+    if (d->c[i][dir] == orient) normal += g[i];
+  if (kind == 1) {
+    for (int a = 0; a < dim; ++a) u[a] = (REAL)value[a];
+    *rho = ((REAL)2 * normal + onWall + (REAL)1) / ((REAL)1 + (REAL)orient * u[dir]);
+  } else {
+    for (int a = 0; a < dim; ++a) u[a] = (REAL)value[1 + a];
+    *rho = (REAL)value[0];
+    u[dir] = (REAL)orient * (((REAL)2 * normal + onWall + (REAL)1) / *rho - (REAL)1);
+  }
+}
+
+/* BGK collision with given rho, u: lbm::bgkCollision (src/dynamics/lbm.h:395-403). */
+static REAL FN(bgk_with)(const lbo_desc* d, REAL omega, REAL rho, const REAL* u, REAL* g)
+{
+  const int q = d->q, dim = d->d;
+  const REAL invCs2 = (REAL)3;
+  REAL uSqr = 0;
+  for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+  for (int i = 0; i < q; ++i) {
+    const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+    REAL cu = 0;
+    for (int a = 0; a < dim; ++a) cu += (REAL)d->c[i][a] * u[a];
+    const REAL feq = rho * t * ((REAL)1 + invCs2 * cu + invCs2 * invCs2 * (REAL)0.5 * cu * cu
+                                - invCs2 * (REAL)0.5 * uSqr) - t;
+    g[i] *= (REAL)1 - omega;
+    g[i] += omega * feq;
+  }
+  return uSqr;
+}
+
+/* u of a bulk cell: BulkMomentum::computeU (elements.h:500-508) = j / rho. */
+static void FN(bulk_u)(const lbo_desc* d, const REAL* g, REAL* u)
+{
+  const int q = d->q, dim = d->d;
+  for (int a = 0; a < dim; ++a) u[a] = 0;
+  for (int i = 0; i < q; ++i)
+    for (int a = 0; a < dim; ++a) u[a] += g[i] * (REAL)d->c[i][a];
+  REAL rho = 0;
+  for (int i = 0; i < q; ++i) rho += g[i];
+  rho += (REAL)1;
+  for (int a = 0; a < dim; ++a) u[a] /= rho;
+}
+
+/* Velocity u of the cell a finite difference reads (cell.computeU through its dynamics):
+ * a boundary cell of the list uses its momenta on the current (in-place updated) populations;
+ * a bulk cell j / rho.  A neighbour reached across a periodic face is the overlap copy of the
+ * partner cell, which the post-stream communication filled with the partner's populations
+ * before any post-processor ran (core/superLattice.hh:800-820, boundary/setBoundary3D.h:56-110)
+ * and which carries bulk dynamics (boundary::set skips the overlap, setBoundary.h:83-86). */
+static void FN(fd_u_of)(const lbo_desc* d, const lbo_case* c, const STORE_T* f, const STORE_T* pre,
+                        const int64_t* fdIndex, int64_t m, int wrapped, REAL* u)
+{
+  const int q = d->q;
+  const int64_t n = (int64_t)c->nx * c->ny * c->nz;
+  REAL g[27];
+  if (wrapped) {
+    for (int i = 0; i < q; ++i) g[i] = LOAD(pre[i * n + m]);
+    FN(bulk_u)(d, g, u);
+    return;
+  }
+  for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + m]);
+  const int64_t b = fdIndex[m];
+  if (b >= 0) {
+    REAL rho;
+    FN(fd_momenta)(d, g, c->fd_kind[b], c->fd_dir[b], c->fd_orient[b], c->fd_value + 4 * b, &rho, u);
+  } else {
+    FN(bulk_u)(d, g, u);
+  }
+}
+
+/* PlaneFdBoundaryProcessor3D::apply (src/boundary/boundaryPostProcessors3D.hh:39-93) and
+ * StraightFdBoundaryProcessor2D::apply (boundaryPostProcessors2D.hh:39-76), one cell after the
+ * other in ascending cell order and in place, as the CPU post-processor loop runs them
+ * (core/platform/cpu/sisd/operator.h:368-385): velocity gradients by
+ * fd::DirectedGradients (utilities/finiteDifference3D.h:74-210: one-sided second order along
+ * the normal, central along the face), Pi = -rho / (c_s^-2 omega) (grad u + grad u^T), and
+ * f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270). */
+static void FN(fd_postprocess)(const lbo_desc* d, const lbo_case* c, STORE_T* f, const STORE_T* pre,
+                               const int64_t* fdIndex)
+{
+  const int q = d->q, dim = d->d;
+  const int64_t nx = c->nx, ny = c->ny, nz = c->nz, n = nx * ny * nz;
+  const int64_t ext[3] = {nx, ny, nz};
+  const REAL invCs2 = (REAL)3;
+  const REAL omega = (REAL)c->omega;
+  for (int64_t b = 0; b < c->n_fd; ++b) {
+    const int64_t cell = c->fd_cell[b];
+    const int dir = c->fd_dir[b], orient = c->fd_orient[b];
+    const int64_t pos[3] = {cell / (ny * nz), (cell / nz) % ny, cell % nz};
+    REAL g[27], rho, u[3] = {0, 0, 0};
+    for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + cell]);
+    FN(fd_momenta)(d, g, c->fd_kind[b], dir, orient, c->fd_value + 4 * b, &rho, u);
+    REAL grad[3][3] = {{0}};  /* grad[a][iD] = d u_iD / d x_a */
+    for (int a = 0; a < dim; ++a) {
+      /* neighbour at offset s along axis a: index and whether it wrapped periodically */
+      REAL ua[3] = {0, 0, 0}, ub[3] = {0, 0, 0};
+      if (a == dir) {
+        for (int k = 1; k <= 2; ++k) {
+          int64_t p[3] = {pos[0], pos[1], pos[2]};
+          p[a] -= k * orient;
+          const int64_t m = (p[0] * ny + p[1]) * nz + p[2];
+          FN(fd_u_of)(d, c, f, pre, fdIndex, m, 0, k == 1 ? ua : ub);
+        }
+        for (int iD = 0; iD < dim; ++iD)
+          grad[a][iD] = (REAL)(-orient) * (((REAL)-3 * u[iD] + (REAL)4 * ua[iD]) - (REAL)1 * ub[iD]) / (REAL)2;
+      } else {
+        for (int k = 0; k < 2; ++k) {
+          int64_t p[3] = {pos[0], pos[1], pos[2]};
+          p[a] += k == 0 ? 1 : -1;
+          int wrapped = 0;
+          if (p[a] < 0 || p[a] >= ext[a]) {
+            p[a] = (p[a] + ext[a]) % ext[a];
+            wrapped = 1;
+          }
+          const int64_t m = (p[0] * ny + p[1]) * nz + p[2];
+          FN(fd_u_of)(d, c, f, pre, fdIndex, m, wrapped, k == 0 ? ua : ub);
+        }
+        for (int iD = 0; iD < dim; ++iD) grad[a][iD] = (ua[iD] - ub[iD]) / (REAL)2;
+      }
+    }
+    const REAL sToPi = -rho / invCs2 / omega;
+    REAL pi[6];
+    if (dim == 3) {
+      pi[0] = (REAL)2 * grad[0][0] * sToPi;             /* xx */
+      pi[3] = (REAL)2 * grad[1][1] * sToPi;             /* yy */
+      pi[5] = (REAL)2 * grad[2][2] * sToPi;             /* zz */
+      pi[1] = (grad[0][1] + grad[1][0]) * sToPi;        /* xy */
+      pi[2] = (grad[0][2] + grad[2][0]) * sToPi;        /* xz */
+      pi[4] = (grad[1][2] + grad[2][1]) * sToPi;        /* yz */
+    } else {
+      pi[0] = (REAL)2 * grad[0][0] * sToPi;             /* xx */
+      pi[2] = (REAL)2 * grad[1][1] * sToPi;             /* yy */
+      pi[1] = (grad[0][1] + grad[1][0]) * sToPi;        /* xy */
+    }
+    REAL uSqr = 0;
+    for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+    for (int i = 0; i < q; ++i) {
+      const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+      REAL cu = 0;
+      for (int a = 0; a < dim; ++a) cu += (REAL)d->c[i][a] * u[a];
+      const REAL feq = rho * t * ((REAL)1 + invCs2 * cu + invCs2 * invCs2 * (REAL)0.5 * cu * cu
+                                  - invCs2 * (REAL)0.5 * uSqr) - t;
+      REAL fneq = 0;
+      int ip = 0;
+      for (int al = 0; al < dim; ++al) {
+        for (int be = al; be < dim; ++be) {
+          REAL add = (REAL)d->c[i][al] * (REAL)d->c[i][be];
+          if (al == be) add -= (REAL)1 / invCs2;
+          else add *= (REAL)2;
+          add *= pi[ip++];
+          fneq += add;
+        }
+      }
+      fneq *= t * invCs2 * invCs2 / (REAL)2;
+      f[i * n + cell] = STORE(feq + fneq);
+    }
+  }
+}
+
 static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
 {
   const lbo_desc* d = lbo_get_desc(c->q);
@@ -122,7 +298,14 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
   STORE_T* tmp = (STORE_T*)malloc(sizeof(STORE_T) * (size_t)(q * n));
   REAL* cellRho = (REAL*)malloc(sizeof(REAL) * (size_t)n);
   REAL* cellUsq = (REAL*)malloc(sizeof(REAL) * (size_t)n);
-  if (!tmp || !cellRho || !cellUsq) { free(tmp); free(cellRho); free(cellUsq); return -2; }
+  int64_t* fdIndex = (int64_t*)malloc(sizeof(int64_t) * (size_t)n);
+  STORE_T* pre = c->n_fd > 0 ? (STORE_T*)malloc(sizeof(STORE_T) * (size_t)(q * n)) : NULL;
+  if (!tmp || !cellRho || !cellUsq || !fdIndex || (c->n_fd > 0 && !pre)) {
+    free(tmp); free(cellRho); free(cellUsq); free(fdIndex); free(pre);
+    return -2;
+  }
+  for (int64_t x = 0; x < n; ++x) fdIndex[x] = -1;
+  for (int64_t b = 0; b < c->n_fd; ++b) fdIndex[c->fd_cell[b]] = b;
 
   for (int64_t s = 0; s < steps; ++s) {
     /* collide (ConcreteBlockCollisionO<..CPU_SISD..>::apply, cpu/sisd/operator.h:143-228) */
@@ -135,6 +318,16 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
         REAL g[27];
         for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
         FN(collide)(d, c, g, &cellRho[x], &cellUsq[x]);
+        for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);
+      } else if (m == LBO_FD_BOUNDARY && fdIndex[x] >= 0) {
+        /* BGKdynamics with the boundary momenta exchanged in (collision::BGK::apply,
+         * collision.h:68-78, with MOMENTA::computeRhoU of the tuple above) */
+        const int64_t b = fdIndex[x];
+        REAL g[27], rho, u[3] = {0, 0, 0};
+        for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
+        FN(fd_momenta)(d, g, c->fd_kind[b], c->fd_dir[b], c->fd_orient[b], c->fd_value + 4 * b, &rho, u);
+        cellUsq[x] = FN(bgk_with)(d, (REAL)c->omega, rho, u, g);
+        cellRho[x] = rho;
         for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);
       } else if (m == LBO_BOUNCE_BACK) {
         for (int i = 1; i <= q / 2; ++i) {
@@ -202,7 +395,11 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
       const REAL veloTerm = (c->link_wall ? (REAL)c->link_wall[l] : (REAL)0) * tk * (REAL)3;
       f[d->opp[k] * n + xb] = STORE(LOAD(f[k * n + xs]) - (REAL)2 * veloTerm);
     }
+    if (c->n_fd > 0) {
+      memcpy(pre, f, sizeof(STORE_T) * (size_t)(q * n));
+      FN(fd_postprocess)(d, c, f, pre, fdIndex);
+    }
   }
-  free(tmp); free(cellRho); free(cellUsq);
+  free(tmp); free(cellRho); free(cellUsq); free(fdIndex); free(pre);
   return 0;
 }

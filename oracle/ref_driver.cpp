@@ -12,6 +12,8 @@
  *    SmagorinskyBGK / SmagorinskyForcedBGK    src/dynamics/smagorinskyBGKdynamics.h:39,67
  *    BounceBack (Revert) / NoDynamics         src/dynamics/dynamics.h:51,557
  *    setBouzidiBoundary / setBouzidiVelocity  src/boundary/setBouzidiBoundary.h:193-420
+ *    boundary::set<InterpolatedVelocity/Pressure>  src/boundary/setBoundary.h:80-160,
+ *                                             interpolatedVelocity3D.h, interpolatedPressure3D.h
  *    Cell::iniEquilibrium                     src/core/cell.h:202
  *    LatticeStatistics                        src/core/latticeStatistics.h:91-93
  *
@@ -19,7 +21,7 @@
  *  without the FORCE field; used by the timing build of plain BGK).
  *
  *  Usage:
- *    lbref <periodic|cavity|porous> [--n NX NY [NZ]] [--dyn bgk|trt|smag|fbgk|fsmag]
+ *    lbref <periodic|cavity|porous|channel> [--n NX NY [NZ]] [--dyn bgk|trt|smag|fbgk|fsmag]
  *          [--omega W] [--magic L] [--cs C] [--force FX FY [FZ]] [--steps S]
  *          [--init tgv|random|rest] [--u0 U] [--amp A] [--seed K] [--ulid U]
  *          [--walls bouzidi|bounceback] [--solid-frac P] [--out PREFIX]
@@ -27,6 +29,11 @@
  *  Output (with --out): PREFIX.f0.bin / PREFIX.fS.bin  raw T populations [Q][ext...] of the
  *  core cells after initialize() and after S steps; PREFIX.mat.bin int32 materials [ext...];
  *  PREFIX.stats.txt per-step "avgRho avgEnergy maxU"; PREFIX.json the case description.
+ *  The channel case (x: a bounce-back layer, the velocity inlet, NX fluid layers ... the
+ *  pressure outlet and a bounce-back layer, i.e. NX + 2 cells along x; periodic in the other
+ *  axes, so every boundary cell is on a flat face) also writes PREFIX.bnd.bin: per
+ *  boundary cell {core cell index, kind (1 velocity, 2 pressure), direction, orientation,
+ *  value[4]} as doubles, value = the imposed velocity, or {rho, tangential velocity}.
  */
 
 #include "olb.h"
@@ -193,16 +200,17 @@ int main(int argc, char** argv) {
   OstreamManager clout(std::cout, "lbref");
 
   const bool periodic = (o.kase == "periodic" || o.kase == "porous");
+  const bool channel = o.kase == "channel";
   int ext[3] = {1, 1, 1};
-  for (int d = 0; d < D; ++d) ext[d] = o.n[d] + (o.kase == "cavity" ? 2 : 0);
+  for (int d = 0; d < D; ++d) ext[d] = o.n[d] + (o.kase == "cavity" || (o.kase == "channel" && d == 0) ? 2 : 0);
 
   Vector<T,D> origin(T(0));
   Vector<int,D> extent;
   for (int d = 0; d < D; ++d) extent[d] = ext[d];
   CuboidDecomposition<T,D> cuboids(origin, T(1), extent, 1);
-  if (periodic) {
+  if (periodic || channel) {
     Vector<bool,D> per;
-    for (int d = 0; d < D; ++d) per[d] = true;
+    for (int d = 0; d < D; ++d) per[d] = !(channel && d == 0);
     cuboids.setPeriodicity(per);
   }
   HeuristicLoadBalancer<T> balancer(cuboids);
@@ -220,6 +228,10 @@ int main(int argc, char** argv) {
         else if (wall) m = 2;
       } else if (o.kase == "porous") {
         if (unit(o.seed ^ 0xABCDEFull, c, 63) < o.solidFrac) m = 2;
+      } else if (channel) {
+        if (x == 0 || x == ext[0] - 1) m = 2;  // bounce-back layer behind the open faces
+        else if (x == 1) m = 3;                // velocity inlet
+        else if (x == ext[0] - 2) m = 4;       // pressure outlet
       }
       mat[c++] = m;
     });
@@ -276,6 +288,28 @@ int main(int argc, char** argv) {
     }
   }
 
+  // inlet profile and outlet density of the channel (lattice units)
+  const double twoPiC = 2.0 * 3.14159265358979323846;
+  auto inletU = [&](int y, int z, T u[3]) {
+    const double Y = twoPiC * y / ext[1], Z = (D == 3) ? twoPiC * z / ext[2] : 0.0;
+    u[0] = T(o.u0 * (1.0 + 0.5 * std::sin(Y)) * (1.0 + 0.3 * std::cos(Z)));
+    u[1] = T(0.2 * o.u0 * std::cos(Y));
+    u[2] = T(0.1 * o.u0 * std::sin(Z));
+  };
+  const T rhoOut = T(1.0 - 0.2 * o.u0);
+  if (channel) {
+    lat.template defineDynamics<BGKdynamics<T,DESCRIPTOR>>(geo, 3);
+    lat.template defineDynamics<BGKdynamics<T,DESCRIPTOR>>(geo, 4);
+    // The layer behind each open face is bounce-back (material 2), so that the populations
+    // the faces receive from outside are defined; it is the "outside" of the discrete
+    // normals.
+    lat.template defineDynamics<BounceBack>(geo, 2);
+    boundary::set<T, DESCRIPTOR, boundary::InterpolatedVelocity<T,DESCRIPTOR>>(lat, geo.getMaterialIndicator({3}),
+                                                  geo.getMaterialIndicator({1}), geo.getMaterialIndicator({0, 2}));
+    boundary::set<T, DESCRIPTOR, boundary::InterpolatedPressure<T,DESCRIPTOR>>(lat, geo.getMaterialIndicator({4}),
+                                                  geo.getMaterialIndicator({1}), geo.getMaterialIndicator({0, 2}));
+  }
+
   lat.template setParameter<descriptors::OMEGA>(T(o.omega));
   if (o.dyn == "trt") lat.template setParameter<collision::TRT::MAGIC>(T(o.magic));
   if (o.dyn == "smag" || o.dyn == "fsmag") lat.template setParameter<collision::LES::SMAGORINSKY>(T(o.cs));
@@ -304,7 +338,7 @@ int main(int argc, char** argv) {
         rho = T(1.0 + o.amp * (unit(o.seed, c, 60) - 0.5));
         for (int d = 0; d < D; ++d) u[d] = T(o.u0 * (unit(o.seed, c, 61 + d) - 0.5));
       }
-      if (mat[c] == 1) {
+      if (mat[c] == 1 || mat[c] == 3 || mat[c] == 4) {
         cell.iniEquilibrium(rho, u);
         if (o.init == "random") {
           for (int i = 0; i < Q; ++i) {
@@ -313,6 +347,28 @@ int main(int argc, char** argv) {
         }
       } else {
         for (int i = 0; i < Q; ++i) cell[i] = T(0);
+      }
+      ++c;
+    });
+  }
+  std::vector<double> bnd;
+  if (channel) {
+    auto& block = lat.getBlock(0);
+    std::size_t c = 0;
+    forCore(ext, [&](int x, int y, int z) {
+      auto cell = block.get(loc(x, y, z));
+      if (mat[c] == 3) {
+        T u[3];
+        inletU(y, z, u);
+        Vector<T,D> uv;
+        for (int d = 0; d < D; ++d) uv[d] = u[d];
+        cell.defineU(uv.data());
+        const double row[8] = {double(c), 1, 0, -1, double(u[0]), double(u[1]), D == 3 ? double(u[2]) : 0.0, 0};
+        bnd.insert(bnd.end(), row, row + 8);
+      } else if (mat[c] == 4) {
+        cell.defineRho(rhoOut);
+        const double row[8] = {double(c), 2, 0, 1, double(rhoOut), 0, 0, 0};
+        bnd.insert(bnd.end(), row, row + 8);
       }
       ++c;
     });
@@ -342,6 +398,10 @@ int main(int argc, char** argv) {
     std::ofstream m(o.out + ".mat.bin", std::ios::binary);
     m.write(reinterpret_cast<const char*>(mat.data()), mat.size() * sizeof(std::int32_t));
     statsFile = std::fopen((o.out + ".stats.txt").c_str(), "w");
+    if (channel) {
+      std::ofstream b(o.out + ".bnd.bin", std::ios::binary);
+      b.write(reinterpret_cast<const char*>(bnd.data()), bnd.size() * sizeof(double));
+    }
   }
   for (long s = 0; s < o.steps; ++s) {
     lat.collideAndStream();

@@ -68,6 +68,18 @@ CASES.update({
                                                               "--solid-frac", "0.25", *RND, "--steps", "40"]),
     "porous_d2q9_trt_f64": ("d2q9_f64_nocse", "porous", ["--n", "14", "12", "--dyn", "trt", "--omega", "1.5",
                                                           "--solid-frac", "0.2", *RND, "--steps", "40"]),
+    # channels with a velocity inlet and a pressure outlet on flat faces (InterpolatedVelocity /
+    # InterpolatedPressure), periodic across, bounce-back layers behind the open faces
+    "channel_d2q9_bgk_f64": ("d2q9_f64_nocse", "channel", ["--n", "14", "11", "--dyn", "bgk", "--omega", "1.3",
+                                                            *RND, "--u0", "0.05", "--steps", "200"]),
+    "channel_d3q19_bgk_f64": ("d3q19_f64_nocse", "channel", ["--n", "12", "10", "8", "--dyn", "bgk", "--omega", "1.2",
+                                                              *RND, "--u0", "0.05", "--steps", "60"]),
+    "channel_d3q19_trt_f64": ("d3q19_f64_nocse", "channel", ["--n", "12", "10", "8", "--dyn", "trt", "--omega", "1.6",
+                                                              "--magic", "0.25", *RND, "--u0", "0.05", "--steps", "60"]),
+    "channel_d3q27_bgk_f64": ("d3q27_f64_nocse", "channel", ["--n", "10", "8", "6", "--dyn", "bgk", "--omega", "1.5",
+                                                              *RND, "--u0", "0.05", "--steps", "40"]),
+    "channel_d3q19_bgk_f32": ("d3q19_f32", "channel", ["--n", "12", "10", "8", "--dyn", "bgk", "--omega", "1.2",
+                                                        *RND, "--u0", "0.05", "--steps", "60"]),
     # Taylor-Green vortex (the benchmark's initial condition), small
     "tgv_d3q19_bgk_f64": ("d3q19_f64_nocse", "periodic", ["--n", "16", "16", "16", "--dyn", "bgk",
                                                            "--omega", str(1.0 / (3 * 0.01 + 0.5)), "--init", "tgv",
@@ -95,10 +107,12 @@ def generate(name: str) -> Path:
         fS = np.fromfile(prefix + ".fS.bin", dtype=dt).reshape(q, n)
         mat = np.fromfile(prefix + ".mat.bin", dtype=np.int32)
         stats = np.loadtxt(prefix + ".stats.txt", ndmin=2)
+        bnd = Path(prefix + ".bnd.bin")
+        extra = {"bnd": np.fromfile(bnd, dtype=np.float64).reshape(-1, 8)} if bnd.exists() else {}
     meta["binary"] = binary
     meta["args"] = [case, *args]
     out = HERE / f"{name}.npz"
-    np.savez_compressed(out, f0=f0, fS=fS, mat=mat, stats=stats, meta=json.dumps(meta))
+    np.savez_compressed(out, f0=f0, fS=fS, mat=mat, stats=stats, meta=json.dumps(meta), **extra)
     return out
 
 

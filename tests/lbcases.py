@@ -49,6 +49,8 @@ def load_fixture(name: str) -> dict:
     z = np.load(GOLDEN / f"{name}.npz")
     meta = json.loads(str(z["meta"]))
     fx = {k: z[k] for k in ("f0", "fS", "mat", "stats")}
+    if "bnd" in z.files:
+        fx["bnd"] = z["bnd"]
     fx["meta"] = meta
     fx["name"] = name
     return fx
@@ -60,6 +62,8 @@ def core_of(meta: dict) -> tuple[int, int, int]:
 
 
 def periodic_of(meta: dict) -> tuple[int, int, int]:
+    if meta["case"] == "channel":  # inlet/outlet along x, periodic across
+        return (0, 1, 1 if meta["d"] == 3 else 0)
     p = 1 if meta["case"] in ("periodic", "porous") else 0
     return (p, p, p if meta["d"] == 3 else 0)
 
@@ -111,7 +115,7 @@ def case_setup(fx: dict) -> dict:
     mat = fx["mat"]
     setup = {"q": q, "core": core, "periodic": per, "dyn": meta["dyn"], "omega": meta["omega"],
              "magic": meta["magic"], "cs": meta["cs"], "force": list(meta["force"]), "links": None,
-             "cell_dyn": None}
+             "cell_dyn": None, "fd": None}
     if meta["case"] == "cavity":
         if meta["walls"] == "bounceback":
             cd = np.where(mat == 1, 1, 2).astype(np.uint8)
@@ -125,7 +129,21 @@ def case_setup(fx: dict) -> dict:
         else:
             setup["cell_dyn"] = np.where(mat == 1, 1, 0).astype(np.uint8)
             setup["links"] = bouzidi_links(q, core, mat, 1, (2,), None, per)
+    elif meta["case"] == "channel":
+        # bulk dynamics on 1, bounce-back on the layers behind the open faces (2), BGK with
+        # the boundary momenta on the inlet (3) and outlet (4) faces
+        setup["cell_dyn"] = np.select([mat == 1, mat == 2], [1, 2], 3).astype(np.uint8)
+        setup["fd"] = fd_boundaries(fx["bnd"])
     return setup
+
+
+def fd_boundaries(bnd: np.ndarray) -> dict:
+    """Flat-face boundary list of the reference driver's channel case (rows of
+    {cell, kind, direction, orientation, value[4]})."""
+    b = np.asarray(bnd, np.float64).reshape(-1, 8)
+    return {"cells": b[:, 0].astype(np.int64), "kinds": b[:, 1].astype(np.int32),
+            "dirs": b[:, 2].astype(np.int32), "orients": b[:, 3].astype(np.int32),
+            "values": np.ascontiguousarray(b[:, 4:8])}
 
 
 # ---- oracle -----------------------------------------------------------------------------------
@@ -134,7 +152,9 @@ class _Case(C.Structure):
                 ("periodic", C.c_int32), ("dynamics", C.c_int32), ("omega", C.c_double), ("magic", C.c_double),
                 ("smagorinsky", C.c_double), ("force", C.c_double * 3), ("material", C.c_void_p),
                 ("n_links", C.c_int64), ("link_cell", C.c_void_p), ("link_dir", C.c_void_p),
-                ("link_wall", C.c_void_p)]
+                ("link_wall", C.c_void_p), ("n_fd", C.c_int64), ("fd_cell", C.c_void_p),
+                ("fd_kind", C.c_void_p), ("fd_dir", C.c_void_p), ("fd_orient", C.c_void_p),
+                ("fd_value", C.c_void_p)]
 
 
 _oracle = None
@@ -176,9 +196,16 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
     c.omega, c.magic, c.smagorinsky = setup["omega"], setup["magic"], setup["cs"]
     c.force = (C.c_double * 3)(*(list(setup["force"]) + [0.0] * 3)[:3])
     if setup["cell_dyn"] is not None:
-        m = np.where(setup["cell_dyn"] == 1, 1, np.where(setup["cell_dyn"] == 2, 4, 0)).astype(np.int32)
+        cd = setup["cell_dyn"]
+        m = np.where(cd == 1, 1, np.where(cd == 2, 4, np.where(cd == 3, 5, 0))).astype(np.int32)
         keep.append(m)
         c.material = m.ctypes.data
+    if setup.get("fd") is not None:
+        fd = setup["fd"]
+        arrs = [np.ascontiguousarray(fd[k]) for k in ("cells", "kinds", "dirs", "orients", "values")]
+        keep += arrs
+        c.n_fd = len(arrs[0])
+        c.fd_cell, c.fd_kind, c.fd_dir, c.fd_orient, c.fd_value = (a.ctypes.data for a in arrs)
     if setup["links"] is not None:
         cells, dirs, wall = (np.ascontiguousarray(a) for a in setup["links"])
         keep += [cells, dirs, wall]
@@ -231,4 +258,8 @@ def errors(q: int, a: np.ndarray, b: np.ndarray, mask: np.ndarray | None = None,
 
 
 def fluid_mask(fx: dict) -> np.ndarray:
+    """Cells whose populations are compared: the bulk fluid, and in the channel also the
+    inlet and outlet faces (materials 3 and 4; in the cavity those numbers are walls)."""
+    if fx["meta"]["case"] == "channel":
+        return np.isin(fx["mat"], (1, 3, 4))
     return fx["mat"] == 1

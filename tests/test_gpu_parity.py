@@ -31,6 +31,9 @@ def make_lattice(setup: dict, storage: str) -> lbx.BlockLattice:
         lat.set_cell_dynamics(setup["cell_dyn"])
     if setup["links"] is not None:
         lat.set_bouzidi_links(*setup["links"])
+    if setup.get("fd") is not None:
+        fd = setup["fd"]
+        lat.set_fd_boundaries(fd["cells"], fd["kinds"], fd["dirs"], fd["orients"], fd["values"])
     return lat
 
 
