@@ -260,8 +260,9 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
 
     # ---- other storage forms (shorter runs) ------------------------------------------------------
     forms = {}
+    fields = {}
     if not args.no_forms:
-        for form in ("f16dev", "bf16dev", "f64"):
+        for form in ("f16dev", "bf16dev", "f32", "f64"):
             k = max(10, args.steps // 4)
             fl = lbx.BlockLattice(19, (n, n, n), (1, 1, 1), form, device=device)
             fl.define_dynamics("bgk", omega=OMEGA)
@@ -277,7 +278,22 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
             forms[form] = {"mlups": round(f_mlups, 1), "hbm_gbs": round(f_gbs, 1),
                            "hbm_frac": round(f_gbs / peak, 4), "vs_f32_mlups": round(f_mlups / mlups, 3),
                            "steps": k, "launch_config": current_config(f_tuning)}
+            f_rho, f_u = fl.compute_moments(stream=stream)
+            fields[form] = (f_rho.astype(np.float64), f_u.astype(np.float32 if form != "f64" else np.float64))
+            del f_rho, f_u
             fl.close()
+        # accuracy of every storage form against the FP64 run after the same steps from the same
+        # initial state (the FP64 kernel reproduces the reference's FP64 arithmetic)
+        rho64, u64 = fields["f64"]
+        for form in ("f16dev", "bf16dev", "f32"):
+            r, uu = fields[form]
+            du = uu.astype(np.float64) - u64
+            forms[form]["error_vs_f64"] = {
+                "u_l2_rel": float(np.sqrt((du ** 2).sum() / (u64 ** 2).sum())),
+                "u_linf_rel": float(np.abs(du).max() / np.abs(u64).max()),
+                "rho_linf": float(np.abs(r - rho64).max()),
+                "after_steps": int(args.warmup + 2 * max(10, args.steps // 4))}
+        del fields
 
     ensemble = None if args.ensemble_requests <= 0 else run_ensemble(args, device, stream)
 

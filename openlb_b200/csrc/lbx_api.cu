@@ -1028,8 +1028,9 @@ int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32
   if (variant < 0 || variant > 2) return fail(LBX_ERR_INVALID, "variant must be 0, 1 or 2");
   if (variant == 2 && L->period >= (int64_t(1) << 31))
     return fail(LBX_ERR_UNSUPPORTED, "variant 2 needs a column period below 2^31 cells");
-  if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2)
-    return fail(LBX_ERR_INVALID, "cells_per_thread must be 1 or 2");
+  if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2 &&
+      !(cells_per_thread == 4 && storage_bytes(L->storage) == 2))
+    return fail(LBX_ERR_INVALID, "cells_per_thread must be 1 or 2 (or 4 for 16-bit storage)");
   if (variant != 0) {
     if (block_x < 1 || block_y < 1 || block_x * block_y > 256 || (block_x * block_y) % 32 != 0)
       return fail(LBX_ERR_INVALID, "block must hold a multiple of 32 and at most 256 threads");
@@ -1052,7 +1053,8 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
   struct Cand { int variant, bx, by, k; };
   std::vector<Cand> cands;
   const int nf = (L->d == 3) ? L->core[2] : L->core[1];
-  for (int k = 1; k <= 2; ++k)
+  const int maxK = storage_bytes(L->storage) == 2 ? 4 : 2;
+  for (int k = 1; k <= maxK; k *= 2)
     for (int bx = 32; bx <= 256; bx *= 2) {
       if (bx > 32 && bx >= 2 * ((nf + k - 1) / k)) break;  // wider blocks only idle more threads
       for (int threads = 256; threads >= 128; threads /= 2)

@@ -434,14 +434,24 @@ struct ColumnBases {
 // Resident blocks per SM the step kernel is compiled for: the 16-bit forms move half the
 // bytes per request, so they need more warps in flight to keep HBM busy.
 // (D3Q27 keeps the compiler's choice: at 6 blocks its 27 values spill.)
-template <int Q, typename S> struct StepOccupancy { static constexpr int blocks = 1; };
-template <> struct StepOccupancy<19, __half> { static constexpr int blocks = 6; };
-template <> struct StepOccupancy<19, __nv_bfloat16> { static constexpr int blocks = 6; };
-template <> struct StepOccupancy<9, __half> { static constexpr int blocks = 6; };
-template <> struct StepOccupancy<9, __nv_bfloat16> { static constexpr int blocks = 6; };
+template <int Q, typename S, int K> struct StepOccupancy { static constexpr int blocks = 1; };
+template <> struct StepOccupancy<19, __half, 1> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<19, __nv_bfloat16, 1> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<9, __half, 1> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<9, __nv_bfloat16, 1> { static constexpr int blocks = 6; };
+// two cells per thread: 64 registers (four blocks)
+template <> struct StepOccupancy<19, __half, 2> { static constexpr int blocks = 4; };
+template <> struct StepOccupancy<19, __nv_bfloat16, 2> { static constexpr int blocks = 4; };
+template <> struct StepOccupancy<9, __half, 2> { static constexpr int blocks = 4; };
+template <> struct StepOccupancy<9, __nv_bfloat16, 2> { static constexpr int blocks = 4; };
+// four cells per thread: 128 registers (two blocks)
+template <> struct StepOccupancy<19, __half, 4> { static constexpr int blocks = 2; };
+template <> struct StepOccupancy<19, __nv_bfloat16, 4> { static constexpr int blocks = 2; };
+template <> struct StepOccupancy<9, __half, 4> { static constexpr int blocks = 2; };
+template <> struct StepOccupancy<9, __nv_bfloat16, 4> { static constexpr int blocks = 2; };
 
 template <int Q, typename S, int DYN, int K, bool DOUBLED>
-__global__ void __launch_bounds__(256, StepOccupancy<Q, S>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
+__global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
                                                                double* __restrict__ statPart) {
@@ -1287,6 +1297,16 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
     case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
     case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
+    case 8:
+    case 9:
+      // four cells per thread: the 16-bit forms only (their per-cell arithmetic, not HBM, is
+      // what limits them; four cells share one thread's index and address work)
+      if constexpr (sizeof(S) == 2) {
+        if (sel == 8) k_collide_stream_groups<Q, S, DYN, 4, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part);
+        else k_collide_stream_groups<Q, S, DYN, 4, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part);
+        break;
+      }
+      return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
     }
   }

@@ -233,14 +233,17 @@ def test_invalid_parameters_raise():
 
 @pytest.mark.parametrize("name", ["periodic_d3q27_fsmag_f64", "cavity_d3q19_bb_f64", "porous_d3q19_fbgk_f64",
                                   "porous_d2q9_trt_f64", "tgv_d3q19_bgk_f32"])
-@pytest.mark.parametrize("storage", ["f64", "f32", "f16dev"])
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16dev", "bf16dev"])
 def test_kernel_variants_agree_bitwise(name, storage):
-    """Every step kernel variant and launch shape computes identical bits."""
+    """Every step kernel variant and launch shape computes identical bits (the 16-bit forms also
+    with two cells per thread in paired 32-bit words, and four cells per thread)."""
     fx = L.load_fixture(name)
     setup = L.case_setup(fx)
     outs = []
-    for variant, bx, by, k in ((0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2),
-                               (2, 256, 1, 1)):
+    shapes = [(0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2), (2, 256, 1, 1)]
+    if storage in ("f16dev", "bf16dev"):
+        shapes += [(2, 32, 4, 4), (2, 128, 1, 2)]
+    for variant, bx, by, k in shapes:
         lat = make_lattice(setup, storage)
         lat.set_launch_config(variant, bx, by, k)
         lat.set_populations(np.asarray(fx["f0"], np.float64))
