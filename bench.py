@@ -175,6 +175,23 @@ def launch_config(cfg: dict, tuning: list[dict]) -> dict:
     return out
 
 
+def rank_max(dist, v: float, device: str = "cpu") -> float:
+    """Max of a per-rank time over all ranks (every rank calls it; the replicas' job time is
+    the slowest rank's)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(world: int, cells: int, steps: int, max_ms: float) -> float:
+    """Whole-job throughput of N replicas: every rank updates `cells` cells `steps` times; the
+    job takes the slowest rank's time."""
+    return world * cells * steps / (max_ms * 1e-3) / 1e6
+
+
 def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     import torch
 
@@ -191,11 +208,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
             dist.barrier()
 
     def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(dist, v, f"cuda:{device}")
 
     def timed_steps(lat, k: int) -> float:
         """ms for k fused steps, device-timed on the launch stream, max over ranks."""
@@ -215,7 +228,12 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     lat.define_dynamics("bgk", omega=OMEGA)
     lat.ini_equilibrium(rho, u, stream=stream)
     lat.collide_and_stream(args.warmup, stream=stream)
-    tuning = lat.autotune(steps=10, stream=stream) if not args.no_autotune else []
+    tuning = lat.autotune(steps=10, stream=stream) if not (args.no_autotune or args.launch_config) else []
+    if args.launch_config:
+        lat.set_launch_config(*args.launch_config)
+        tuning = [{"variant": args.launch_config[0], "block_x": args.launch_config[1],
+                   "block_y": args.launch_config[2], "cells_per_thread": args.launch_config[3],
+                   "ms_per_step": 1.0}]
     torch.cuda.synchronize(device)
     clocks = Clocks(device)
     clocks.start()
@@ -227,8 +245,10 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     lat.set_kernel_timing(False)
     clk = clocks.stop()
     lat_cfg = current_config(tuning)
+    if args.launch_config:
+        lat_cfg["source"] = "fixed (--launch-config)"
     per_step_ms = ms / args.steps
-    mlups = world * cells * args.steps / (ms * 1e-3) / 1e6
+    mlups = job_mlups(world, cells, args.steps, ms)
     coll_ms, coll_n = kt["collision"]
     halo_ms, halo_n = kt["periodic_overlap"]
     launch_s = coll_ms / max(coll_n, 1) * 1e-3
@@ -254,7 +274,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     torch.cuda.synchronize(device)
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     barrier()
-    e2e_mlups = world * cells * args.steps / e2e_s / 1e6
+    e2e_mlups = job_mlups(world, cells, args.steps, e2e_s * 1e3)
     pop_bytes = f_np.nbytes
     lat.close()
 
@@ -273,7 +293,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
             fl.set_kernel_timing(True)
             timed_steps(fl, k)
             fk_ms, fk_n = fl.kernel_timing()["collision"]
-            f_mlups = world * cells * k / (fms * 1e-3) / 1e6
+            f_mlups = job_mlups(world, cells, k, fms)
             f_gbs = cells * BYTES_PER_LUP[form] / (fk_ms / max(fk_n, 1) * 1e-3) / 1e9
             forms[form] = {"mlups": round(f_mlups, 1), "hbm_gbs": round(f_gbs, 1),
                            "hbm_frac": round(f_gbs / peak, 4), "vs_f32_mlups": round(f_mlups / mlups, 3),
@@ -388,6 +408,8 @@ def main() -> int:
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--launch-config", type=int, nargs=4, metavar=("VARIANT", "BX", "BY", "K"),
+                    help="fixed launch shape of the headline lattice instead of the autotuner's")
     ap.add_argument("--ensemble-requests", type=int, default=32)
     ap.add_argument("--ensemble-max-steps", type=int, default=2000)
     args = ap.parse_args()

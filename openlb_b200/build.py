@@ -23,6 +23,8 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "lib" / "liblbx.so"
 INCLUDE = PKG.parent / "include"
+PLATFORM = PKG / "platform"
+HOST_EXAMPLES = {"cavity3d": PLATFORM / "cavity3d.cpp"}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -80,7 +82,26 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:
             raise RuntimeError(f"link failed:\n{proc.stdout}\n{proc.stderr}")
+    build_host_examples()
     return LIB
+
+
+def build_host_examples() -> list[Path]:
+    """C++ programs over the C++ host layer (platform/lbx.hpp), linked against liblbx.so with
+    an rpath to it: g++, no CUDA headers."""
+    gxx = shutil.which("g++") or "/usr/bin/g++"
+    out = []
+    for name, src in HOST_EXAMPLES.items():
+        exe = LIB.parent / name
+        deps = [src, PLATFORM / "lbx.hpp", INCLUDE / "lbx.h", LIB]
+        if not exe.exists() or exe.stat().st_mtime < max(p.stat().st_mtime for p in deps):
+            cmd = [gxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-I", str(INCLUDE), "-I", str(PLATFORM), str(src),
+                   "-L", str(LIB.parent), "-llbx", "-Wl,-rpath,$ORIGIN", "-o", str(exe)]
+            proc = subprocess.run(cmd, capture_output=True, text=True)
+            if proc.returncode != 0:
+                raise RuntimeError(f"g++ failed for {src.name}:\n{proc.stdout}\n{proc.stderr}")
+        out.append(exe)
+    return out
 
 
 def main(argv: list[str] | None = None) -> int:

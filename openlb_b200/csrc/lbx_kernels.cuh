@@ -153,23 +153,41 @@ __device__ __forceinline__ void block_partial(double a, double b, double m, doub
   }
 }
 
-// The block partials summed in a fixed order into the StatAcc the host reads.
-static __global__ void __launch_bounds__(256) k_stats_finalize(const double* __restrict__ part, int64_t nblocks,
-                                                        StatAcc* __restrict__ out) {
+// The block partials summed in a fixed order into the StatAcc the host reads: thread t adds
+// partials t, t + 1024, ... in index order (eight loads in flight per thread), then a fixed
+// shared-memory tree.  One block of 1024 threads; the result depends only on the partials.
+constexpr int kFinalizeThreads = 1024;
+static __global__ void __launch_bounds__(kFinalizeThreads) k_stats_finalize(const double* __restrict__ part,
+                                                                           int64_t nblocks,
+                                                                           StatAcc* __restrict__ out) {
   double a = 0, b = 0, m = 0, c = 0;
-  for (int64_t i = threadIdx.x; i < nblocks; i += 256) {
+  constexpr int U = 8;
+  int64_t i = threadIdx.x;
+  for (; i + int64_t(U - 1) * kFinalizeThreads < nblocks; i += int64_t(U) * kFinalizeThreads) {
+    double4 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = *reinterpret_cast<const double4*>(part + 4 * (i + int64_t(u) * kFinalizeThreads));
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      a += v[u].x;
+      b += v[u].y;
+      m = fmax(m, v[u].z);
+      c += v[u].w;
+    }
+  }
+  for (; i < nblocks; i += kFinalizeThreads) {
     a += part[4 * i + 0];
     b += part[4 * i + 1];
     m = fmax(m, part[4 * i + 2]);
     c += part[4 * i + 3];
   }
-  __shared__ double s[4][256];
+  __shared__ double s[4][kFinalizeThreads];
   s[0][threadIdx.x] = a;
   s[1][threadIdx.x] = b;
   s[2][threadIdx.x] = m;
   s[3][threadIdx.x] = c;
   __syncthreads();
-  for (int stride = 128; stride > 0; stride >>= 1) {
+  for (int stride = kFinalizeThreads / 2; stride > 0; stride >>= 1) {
     if (threadIdx.x < stride) {
       s[0][threadIdx.x] += s[0][threadIdx.x + stride];
       s[1][threadIdx.x] += s[1][threadIdx.x + stride];
@@ -1322,7 +1340,7 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     if (e != cudaSuccess) return e;
   }
   if (!a.stats) return cudaSuccess;
-  k_stats_finalize<<<1, 256, 0, stream>>>(a.statPart, nblocks + fdb, a.stats);
+  k_stats_finalize<<<1, kFinalizeThreads, 0, stream>>>(a.statPart, nblocks + fdb, a.stats);
   return cudaGetLastError();
 }
 // Post-stream regularisation of the flat-face boundary cells (two passes, see k_fd_regularize).

@@ -80,6 +80,16 @@ def sample_requests(n: int, seed: int = 0, rate: float = 200.0, edges=(32, 48, 6
     return [CavityRequest(i, int(es[i]), float(res[i]), lid, tolerance, max_steps, float(arrivals[i])) for i in range(n)]
 
 
+def shard_requests(requests: list[CavityRequest], rank: int, world: int) -> list[CavityRequest]:
+    """Requests of one rank when `world` GPUs serve one arrival stream: dealt round-robin in
+    arrival order, so every rank sees the same rate and size mix and no request is served twice.
+    The requests are independent, so the ranks need no collective on the data path."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    ordered = sorted(requests, key=lambda r: (r.arrival, r.rid))
+    return ordered[rank::world]
+
+
 class EnsembleServer:
     def __init__(self, ensemble: lbx.Ensemble, chunk: int = 200, stream=None):
         self.ens = ensemble
