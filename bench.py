@@ -390,7 +390,9 @@ def run_ensemble(args, device: int, stream) -> dict:
                         f"residual < 1e-6 (delta {check} steps) or {args.ensemble_max_steps} steps; f32 storage",
             "sample": f"{len(reqs)} requests with the step cap lowered from 50000 to {args.ensemble_max_steps} "
                       f"so the run ends in seconds",
-            "launch_config": None if pick is None else {"threads": pick["threads"],
+            "launch_config": None if pick is None else {"launch_mode": ("persistent" if pick["variant"] == 0
+                                                                        else "graph of step launches"),
+                                                        "threads": pick["threads"],
                                                         "blocks_per_sm": pick["blocks_per_sm"],
                                                         "candidates": len(tuning), "source": "autotune"},
             "server": served, "sequential": sequential,

@@ -298,6 +298,11 @@ int lbx_ensemble_retire(lbx_ensemble ens, int32_t slot);
  * depend on it), resident blocks per SM (0: occupancy maximum), and the residual check interval
  * in steps. */
 int lbx_ensemble_set_config(lbx_ensemble ens, int32_t threads, int32_t blocks_per_sm, int32_t check_interval);
+/* How a run is launched: 0 (default) one persistent cooperative kernel per run, steps separated
+ * by grid-wide barriers; 1 one launch per step plus a one-block bookkeeping launch, chained in a
+ * CUDA graph (the launch boundaries order the steps, and populations may then be read through
+ * L1).  Both give identical results. */
+int lbx_ensemble_set_launch_mode(lbx_ensemble ens, int32_t mode);
 
 /* ---- autotuner ----------------------------------------------------------------------------
  * No reference counterpart (the reference's CUDA platform launches fixed 32-thread blocks,
@@ -311,7 +316,8 @@ int lbx_ensemble_set_config(lbx_ensemble ens, int32_t threads, int32_t blocks_pe
  * out[0 .. min(capacity, candidates) - 1] lists what was tried, *n_out the number of candidates;
  * ms_per_step < 0 marks a shape the device or the lattice does not accept. */
 typedef struct {
-  int32_t variant, block_x, block_y, cells_per_thread;  /* lbx_autotune: lbx_set_launch_config */
+  int32_t variant, block_x, block_y, cells_per_thread;  /* lbx_autotune: lbx_set_launch_config;
+                                                           lbx_ensemble_autotune: variant = launch mode */
   int32_t threads, blocks_per_sm;                       /* lbx_ensemble_autotune: set_config */
   double ms_per_step;
 } lbx_tune_entry;

@@ -108,6 +108,8 @@ struct lbx_lattice_s {
   double* statPart = nullptr;        // per-block statistics partials
   int64_t statCapacity = 0;          // blocks statPart holds
   double* reduceAcc = nullptr;       // 8 doubles + 1 ull of scratch for reductions
+  double* reducePart = nullptr;      // per-block entries of the FP64 reductions (4 doubles each)
+  int64_t reducePartCapacity = 0;    // blocks reducePart holds
   float* residualSnap = nullptr;
   void* stage = nullptr;             // ncore doubles
   int dynamics = LBX_BGK;
@@ -554,6 +556,7 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->stats);
   cudaFree(L->statPart);
   cudaFree(L->reduceAcc);
+  cudaFree(L->reducePart);
   cudaFree(L->residualSnap);
   cudaFree(L->stage);
   delete L;
@@ -961,32 +964,37 @@ int lbx_compute_moments(lbx_lattice L, double* rho, double* u, void* stream) {
 
 int lbx_reduce(lbx_lattice L, int32_t what, double* out, void* stream) {
   if (!L || !out) return fail(LBX_ERR_INVALID, "null argument");
+  if (what != LBX_REDUCE_MASS_MOMENTUM && what != LBX_REDUCE_DRAG && what != LBX_REDUCE_RESIDUAL)
+    return fail(LBX_ERR_INVALID, "unknown reduction");
   DeviceGuard guard(L->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const LaunchArgs a = args_of(L);
-  double h[8] = {};
-  unsigned long long mb = 0;
-  unsigned long long* maxbits = reinterpret_cast<unsigned long long*>(L->reduceAcc + 8);
-  LBX_CUDA_TRY(cudaMemsetAsync(L->reduceAcc, 0, 8 * sizeof(double) + sizeof(unsigned long long), s));
+  // per-block entries (4 doubles per block of 256 cells or links), then a fixed-order sum
+  const int64_t need = reduce_blocks(std::max<int64_t>(L->ncore, L->nLinks)) + 1;
+  if (need > L->reducePartCapacity) {
+    cudaFree(L->reducePart);
+    L->reducePart = nullptr;
+    L->reducePartCapacity = 0;
+    LBX_CUDA_TRY(cudaMalloc(&L->reducePart, size_t(need) * 4 * sizeof(double)));
+    L->reducePartCapacity = need;
+  }
+  double h[4] = {};
   switch (what) {
   case LBX_REDUCE_MASS_MOMENTUM:
-    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_mass_momentum<Q, S>(a, L->reduceAcc, s))));
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_mass_momentum<Q, S>(a, L->reducePart, L->reduceAcc, s))));
     break;
   case LBX_REDUCE_DRAG:
-    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_link_force<Q, S>(a, L->linkCell, L->linkDir, L->nLinks, L->reduceAcc, s))));
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_link_force<Q, S>(a, L->linkCell, L->linkDir, L->nLinks, L->reducePart,
+                                                          L->reduceAcc, s))));
     break;
-  case LBX_REDUCE_RESIDUAL:
+  default:
     if (!L->residualSnap) {
       LBX_CUDA_TRY(cudaMalloc(&L->residualSnap, size_t(L->ncore) * size_t(L->d) * sizeof(float)));
       LBX_CUDA_TRY(cudaMemsetAsync(L->residualSnap, 0, size_t(L->ncore) * size_t(L->d) * sizeof(float), s));
     }
-    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_residual<Q, S>(a, L->residualSnap, L->reduceAcc, maxbits, s))));
-    break;
-  default:
-    return fail(LBX_ERR_INVALID, "unknown reduction");
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_residual<Q, S>(a, L->residualSnap, L->reducePart, L->reduceAcc, s))));
   }
-  LBX_CUDA_TRY(cudaMemcpyAsync(h, L->reduceAcc, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
-  LBX_CUDA_TRY(cudaMemcpyAsync(&mb, maxbits, sizeof(mb), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaMemcpyAsync(h, L->reduceAcc, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
   LBX_CUDA_TRY(cudaStreamSynchronize(s));
   switch (what) {
   case LBX_REDUCE_MASS_MOMENTUM:
@@ -995,13 +1003,10 @@ int lbx_reduce(lbx_lattice L, int32_t what, double* out, void* stream) {
   case LBX_REDUCE_DRAG:
     for (int k = 0; k < 3; ++k) out[k] = h[k];
     break;
-  default: {
-    double m;
-    std::memcpy(&m, &mb, sizeof(double));
+  default:
     out[0] = std::sqrt(h[0]);
     out[1] = std::sqrt(h[1]);
-    out[2] = m;
-  }
+    out[2] = h[2];
   }
   return LBX_OK;
 }

@@ -146,161 +146,246 @@ template <> struct EnsOccupancy<19, float> { static constexpr int blocks = 3; };
 template <> struct EnsOccupancy<19, __half> { static constexpr int blocks = 3; };
 template <> struct EnsOccupancy<19, __nv_bfloat16> { static constexpr int blocks = 3; };
 
-template <int Q, typename S>
-__global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble(EnsArgs a) {
+// Loads of populations inside a step: through L1 when every step is its own launch (the L1
+// starts clean at each launch), around it (ld.global.cg) in the persistent kernel, where a
+// line another block wrote in the previous step may still sit in this SM's L1.
+template <typename S, bool CACHED> struct EnsLoad {
+  static __device__ __forceinline__ typename Storage<S>::R ld(const S* p) {
+    if constexpr (CACHED) return Storage<S>::load(p);
+    else return CgLoad<S>::ld(p);
+  }
+};
+
+// Per-block scratch of the tile loop.
+template <int Q, typename S> struct EnsShared {
+  uint32_t sShift[Q];
+  float sDelta[Q];
+  // column i's base pointer with the shift folded in, valid for every cell of the tile when
+  // sWrap == 0 (no column's cyclic wrap point falls inside the tile's index range)
+  S* sCol[Q];
+  int sWrap;
+  double red[2][kTileCells / 32];
+};
+
+// One step of every running lattice: this block's share of the tile list.
+template <int Q, typename S, bool CACHED>
+__device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nTiles, EnsShared<Q, S>& sm) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
-  __shared__ uint32_t sShift[Q];
-  __shared__ float sDelta[Q];
-  __shared__ double red[2][kTileCells / 32];
+  uint32_t* sShift = sm.sShift;
+  float* sDelta = sm.sDelta;
+  S** sCol = sm.sCol;
+  int& sWrap = sm.sWrap;
+  double (*red)[kTileCells / 32] = sm.red;
   const int tid = threadIdx.x;
-  for (int step = 0; step < a.steps; ++step) {
-    const long long g = *reinterpret_cast<volatile long long*>(a.globalStep);
-    const int par = int(g & 1);
-    const int nTiles = *a.nTiles;
-    for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
-      const int2 t = a.tiles[tile];
-      EnsLattice* L = a.lat + t.x;
-      const int state = __ldcg(&L->state);
-      if (state != LBX_SLOT_RUNNING) continue;  // uniform over the block
-      const int64_t steps = __ldcg(reinterpret_cast<const long long*>(&L->steps));
-      const bool check = ((steps + 1) % a.check) == 0;
-      __syncthreads();  // the previous tile's readers of sShift/sDelta are done
-      if (tid < Q) {
-        sShift[tid] = __ldcg(&L->shift[par][tid]);
-        sDelta[tid] = __ldcg(&L->delta[tid]);
-      }
-      __syncthreads();
+  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+    const int2 t = a.tiles[tile];
+    EnsLattice* L = a.lat + t.x;
+    const int state = __ldcg(&L->state);
+    if (state != LBX_SLOT_RUNNING) continue;  // uniform over the block
+    const int64_t steps = __ldcg(reinterpret_cast<const long long*>(&L->steps));
+    const bool check = ((steps + 1) % a.check) == 0;
+    __syncthreads();  // the previous tile's readers of sShift/sDelta are done
+    if (tid == 0) sWrap = 0;
+    __syncthreads();
+    if (tid < Q) {
+      const uint32_t sh = __ldcg(&L->shift[par][tid]);
+      sShift[tid] = sh;
+      sDelta[tid] = __ldcg(&L->delta[tid]);
+      // padded index range of the tile's cells: rows of the first and the last cell
+      const int c0 = t.y, c1 = min(t.y + kTileCells, L->ncore) - 1;
+      const uint32_t q0 = FastDiv::div(uint32_t(c0), L->mz, L->lz), q1 = FastDiv::div(uint32_t(c1), L->mz, L->lz);
+      const uint32_t x0 = FastDiv::div(q0, L->my, L->ly), x1 = FastDiv::div(q1, L->my, L->ly);
+      const uint32_t lo = (x0 + 1) * uint32_t(L->sx) + (q0 - x0 * uint32_t(L->ny) + 1) * uint32_t(L->sy) +
+                          (uint32_t(c0) - q0 * uint32_t(L->nz)) + 1;
+      const uint32_t hi = (x1 + 1) * uint32_t(L->sx) + (q1 - x1 * uint32_t(L->ny) + 1) * uint32_t(L->sy) +
+                          (uint32_t(c1) - q1 * uint32_t(L->nz)) + 1;
       const uint32_t P = L->P;
-      const int nx = L->nx, ny = L->ny, nz = L->nz, sx = L->sx, sy = L->sy;
-      const uint32_t mz = L->mz, my = L->my;
-      const int32_t lz = L->lz, ly = L->ly;
-      const int last = min(kTileCells, L->ncore - t.y);  // cells of this tile
-      const int ncore = L->ncore;
-      S* pop = static_cast<S*>(L->pop);
-      CollisionParams<R> cp;
-      cp.omega = R(L->omega);
-      cp.magic = R(L->magic);
-      cp.smagorinsky = R(0);
-      cp.force[0] = cp.force[1] = cp.force[2] = R(0);
-      const int dyn = L->dynamics;
-      // The block walks the tile's cells in rounds of blockDim.x; each warp's 32 consecutive
-      // cells form one residual slot, reduced by the same shuffle tree whatever the block size,
-      // so the residual does not depend on the launch shape.
-      const int rounds = (last + 31) / 32 * 32;
-      for (int cl = tid; cl < rounds; cl += blockDim.x) {
-        double du2 = 0.0, u2 = 0.0;
-        const int c = t.y + cl;
-        if (cl < last) {
-          const uint32_t xy = FastDiv::div(uint32_t(c), mz, lz);
-          const int z = c - int(xy) * nz;
-          const int x = int(FastDiv::div(xy, my, ly));
-          const int y = int(xy) - x * ny;
-          const uint32_t n = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
-          R f[Q];
-          static_for<Q>([&](auto I) { f[I] = CgLoad<S>::ld(pop + I * int64_t(P) + wrap32(n + sShift[I], P)); });
-          if (check) {
-            R rho, u[3];
-            moments<Q, R, false>(f, nullptr, rho, u);
-            float* snap = L->snap;
+      // the bounce-back stores reach one padded row beyond the tile's range on either side
+      const uint32_t span = uint32_t(L->sx) + uint32_t(L->sy) + 1;
+      const int64_t a = int64_t(lo) - span + sh, b = int64_t(hi) + span + sh;
+      int64_t off;
+      if (b < int64_t(P) && a >= 0) off = sh;
+      else if (a >= int64_t(P)) off = int64_t(sh) - int64_t(P);
+      else { off = 0; atomicOr(&sWrap, 1); }
+      sCol[tid] = static_cast<S*>(L->pop) + int64_t(tid) * int64_t(P) + off;
+    }
+    __syncthreads();
+    const bool straight = sWrap == 0;  // uniform over the block
+    const uint32_t P = L->P;
+    const int nx = L->nx, ny = L->ny, nz = L->nz, sx = L->sx, sy = L->sy;
+    const uint32_t mz = L->mz, my = L->my;
+    const int32_t lz = L->lz, ly = L->ly;
+    const int last = min(kTileCells, L->ncore - t.y);  // cells of this tile
+    const int ncore = L->ncore;
+    S* pop = static_cast<S*>(L->pop);
+    CollisionParams<R> cp;
+    cp.omega = R(L->omega);
+    cp.magic = R(L->magic);
+    cp.smagorinsky = R(0);
+    cp.force[0] = cp.force[1] = cp.force[2] = R(0);
+    const int dyn = L->dynamics;
+    // The block walks the tile's cells in rounds of blockDim.x; each warp's 32 consecutive
+    // cells form one residual slot, reduced by the same shuffle tree whatever the block size,
+    // so the residual does not depend on the launch shape.
+    const int rounds = (last + 31) / 32 * 32;
+    for (int cl = tid; cl < rounds; cl += blockDim.x) {
+      double du2 = 0.0, u2 = 0.0;
+      const int c = t.y + cl;
+      if (cl < last) {
+        const uint32_t xy = FastDiv::div(uint32_t(c), mz, lz);
+        const int z = c - int(xy) * nz;
+        const int x = int(FastDiv::div(xy, my, ly));
+        const int y = int(xy) - x * ny;
+        const uint32_t n = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
+        R f[Q];
+        if (straight) static_for<Q>([&](auto I) { f[I] = EnsLoad<S, CACHED>::ld(sCol[I] + n); });
+        else static_for<Q>([&](auto I) { f[I] = EnsLoad<S, CACHED>::ld(pop + I * int64_t(P) + wrap32(n + sShift[I], P)); });
+        if (check) {
+          R rho, u[3];
+          moments<Q, R, false>(f, nullptr, rho, u);
+          float* snap = L->snap;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const double cur = double(u[d]);
-              const double dd = cur - double(__ldcg(snap + int64_t(d) * ncore + c));
-              du2 += dd * dd;
-              u2 += cur * cur;
-              snap[int64_t(d) * ncore + c] = float(cur);
-            }
+          for (int d = 0; d < 3; ++d) {
+            const double cur = double(u[d]);
+            const double dd = cur - double(__ldcg(snap + int64_t(d) * ncore + c));
+            du2 += dd * dd;
+            u2 += cur * cur;
+            snap[int64_t(d) * ncore + c] = float(cur);
           }
-          R rho, usq;
-          if (dyn == LBX_TRT) collide<Q, R, DYN_TRT>(f, cp, rho, usq);
-          else collide<Q, R, DYN_BGK>(f, cp, rho, usq);
-          if (!(usq == usq) || usq > R(1)) du2 = __longlong_as_double(0x7ff8000000000000ll);  // NaN flags divergence
-          // store addresses recomputed from shared memory (volatile: not kept live in registers
-          // across the collision, which would cost two registers per population)
+        }
+        R rho, usq;
+        if (dyn == LBX_TRT) collide<Q, R, DYN_TRT>(f, cp, rho, usq);
+        else collide<Q, R, DYN_BGK>(f, cp, rho, usq);
+        if (!(usq == usq) || usq > R(1)) du2 = __longlong_as_double(0x7ff8000000000000ll);  // NaN flags divergence
+        // store addresses recomputed from shared memory (volatile: not kept live in registers
+        // across the collision, which would cost two registers per population)
+        if (straight) {
+          static_for<Q>([&](auto I) { Storage<S>::store(*reinterpret_cast<S* volatile*>(&sCol[I]) + n, f[I]); });
+        } else {
           static_for<Q>([&](auto I) {
             const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&sShift[I]);
             Storage<S>::store(pop + I * int64_t(P) + wrap32(n + sh, P), f[I]);
           });
-          // Halfway bounce-back of the links that leave the core: the population sent into the
-          // wall comes back as the opposite one, written where the next step's load of this
-          // cell finds it (the slot of ghost cell x + c_K in column opp(K) at this step's shift).
-          if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
-            static_for<Q>([&](auto K) {
-              constexpr int cx = D::C[K][0], cy = D::C[K][1], cz = D::C[K][2];
-              if constexpr (cx != 0 || cy != 0 || cz != 0) {
-                const int tx = x + cx, ty = y + cy, tz = z + cz;
-                if (tx < 0 || tx >= nx || ty < 0 || ty >= ny || tz < 0 || tz >= nz) {
-                  constexpr int O = D::OPP[K];
-                  const uint32_t gh = uint32_t(int(n) + cx * sx + cy * sy + cz);
+        }
+        // Halfway bounce-back of the links that leave the core: the population sent into the
+        // wall comes back as the opposite one, written where the next step's load of this
+        // cell finds it (the slot of ghost cell x + c_K in column opp(K) at this step's shift).
+        if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
+          static_for<Q>([&](auto K) {
+            constexpr int cx = D::C[K][0], cy = D::C[K][1], cz = D::C[K][2];
+            if constexpr (cx != 0 || cy != 0 || cz != 0) {
+              const int tx = x + cx, ty = y + cy, tz = z + cz;
+              if (tx < 0 || tx >= nx || ty < 0 || ty >= ny || tz < 0 || tz >= nz) {
+                constexpr int O = D::OPP[K];
+                const uint32_t gh = uint32_t(int(n) + cx * sx + cy * sy + cz);
+                const R v = f[K] - (ty == ny ? R(sDelta[K]) : R(0));
+                if (straight) {
+                  Storage<S>::store(*reinterpret_cast<S* volatile*>(&sCol[O]) + gh, v);
+                } else {
                   const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&sShift[O]);
-                  Storage<S>::store(pop + O * int64_t(P) + wrap32(gh + sh, P), f[K] - (ty == ny ? R(sDelta[K]) : R(0)));
+                  Storage<S>::store(pop + O * int64_t(P) + wrap32(gh + sh, P), v);
                 }
               }
-            });
-          }
-        }
-        if (check) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            du2 += __shfl_xor_sync(0xffffffffu, du2, o);
-            u2 += __shfl_xor_sync(0xffffffffu, u2, o);
-          }
-          if ((tid & 31) == 0) {
-            red[0][cl >> 5] = du2;
-            red[1][cl >> 5] = u2;
-          }
+            }
+          });
         }
       }
       if (check) {
-        __syncthreads();
-        if (tid == 0) {
-          double s0 = 0, s1 = 0;
-          for (int w = 0; w < (last + 31) / 32; ++w) {
-            s0 += red[0][w];
-            s1 += red[1][w];
-          }
-          a.tilePart[2 * int64_t(tile)] = s0;
-          a.tilePart[2 * int64_t(tile) + 1] = s1;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          du2 += __shfl_xor_sync(0xffffffffu, du2, o);
+          u2 += __shfl_xor_sync(0xffffffffu, u2, o);
+        }
+        if ((tid & 31) == 0) {
+          red[0][cl >> 5] = du2;
+          red[1][cl >> 5] = u2;
         }
       }
     }
+    if (check) {
+      __syncthreads();
+      if (tid == 0) {
+        double s0 = 0, s1 = 0;
+        for (int w = 0; w < (last + 31) / 32; ++w) {
+          s0 += red[0][w];
+          s1 += red[1][w];
+        }
+        a.tilePart[2 * int64_t(tile)] = s0;
+        a.tilePart[2 * int64_t(tile) + 1] = s1;
+      }
+    }
+  }
+}
+
+// Per-lattice bookkeeping after a step (one block): step count, the next step's column shifts,
+// and at check steps the residual (tile partials summed in tile order) and the state.
+template <int Q>
+__device__ __forceinline__ void ensemble_book(const EnsArgs& a, int par) {
+  using D = Desc<Q>;
+  for (int s = threadIdx.x; s < a.maxLattices; s += blockDim.x) {
+    EnsLattice* L = a.lat + s;
+    if (__ldcg(&L->state) != LBX_SLOT_RUNNING) continue;
+    const int64_t steps = __ldcg(reinterpret_cast<const long long*>(&L->steps));
+    const bool check = ((steps + 1) % a.check) == 0;
+    L->steps = steps + 1;
+    const uint32_t P = L->P;
+    const int sx = L->sx, sy = L->sy;
+    static_for<Q>([&](auto I) {
+      const int64_t off = D::C[I][0] * int64_t(sx) + D::C[I][1] * int64_t(sy) + D::C[I][2];
+      int64_t ns = (int64_t(__ldcg(&L->shift[par][I])) - off) % int64_t(P);
+      if (ns < 0) ns += P;
+      L->shift[par ^ 1][I] = uint32_t(ns);
+    });
+    int state = LBX_SLOT_RUNNING;
+    if (check) {
+      const int2 r = a.range[s];
+      double s0 = 0, s1 = 0;
+      for (int k = 0; k < r.y; ++k) {
+        s0 += __ldcg(a.tilePart + 2 * int64_t(r.x + k));
+        s1 += __ldcg(a.tilePart + 2 * int64_t(r.x + k) + 1);
+      }
+      const double res = s1 > 0 ? sqrt(s0 / s1) : (s0 > 0 ? INFINITY : 0.0);
+      L->residual = res;
+      if (!(res == res) || !(s1 == s1) || isinf(s1)) state = LBX_SLOT_DIVERGED;
+      else if (res < L->tol) state = LBX_SLOT_CONVERGED;
+    }
+    if (state == LBX_SLOT_RUNNING && steps + 1 >= L->maxSteps) state = LBX_SLOT_MAX_STEPS;
+    if (state != LBX_SLOT_RUNNING) L->state = state;
+  }
+}
+
+template <int Q, typename S>
+__global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble(EnsArgs a) {
+  __shared__ EnsShared<Q, S> sm;
+  for (int step = 0; step < a.steps; ++step) {
+    const long long g = *reinterpret_cast<volatile long long*>(a.globalStep);
+    const int par = int(g & 1);
+    ensemble_tiles<Q, S, false>(a, par, *a.nTiles, sm);
     if (!grid_barrier(a.barrier, a.err)) return;
     if (blockIdx.x == 0) {
-      for (int s = tid; s < a.maxLattices; s += blockDim.x) {
-        EnsLattice* L = a.lat + s;
-        if (__ldcg(&L->state) != LBX_SLOT_RUNNING) continue;
-        const int64_t steps = __ldcg(reinterpret_cast<const long long*>(&L->steps));
-        const bool check = ((steps + 1) % a.check) == 0;
-        L->steps = steps + 1;
-        const uint32_t P = L->P;
-        const int sx = L->sx, sy = L->sy;
-        static_for<Q>([&](auto I) {
-          const int64_t off = D::C[I][0] * int64_t(sx) + D::C[I][1] * int64_t(sy) + D::C[I][2];
-          int64_t ns = (int64_t(__ldcg(&L->shift[par][I])) - off) % int64_t(P);
-          if (ns < 0) ns += P;
-          L->shift[par ^ 1][I] = uint32_t(ns);
-        });
-        int state = LBX_SLOT_RUNNING;
-        if (check) {
-          const int2 r = a.range[s];
-          double s0 = 0, s1 = 0;
-          for (int k = 0; k < r.y; ++k) {
-            s0 += __ldcg(a.tilePart + 2 * int64_t(r.x + k));
-            s1 += __ldcg(a.tilePart + 2 * int64_t(r.x + k) + 1);
-          }
-          const double res = s1 > 0 ? sqrt(s0 / s1) : (s0 > 0 ? INFINITY : 0.0);
-          L->residual = res;
-          if (!(res == res) || !(s1 == s1) || isinf(s1)) state = LBX_SLOT_DIVERGED;
-          else if (res < L->tol) state = LBX_SLOT_CONVERGED;
-        }
-        if (state == LBX_SLOT_RUNNING && steps + 1 >= L->maxSteps) state = LBX_SLOT_MAX_STEPS;
-        if (state != LBX_SLOT_RUNNING) L->state = state;
-      }
-      if (tid == 0) *a.globalStep = g + 1;
+      ensemble_book<Q>(a, par);
+      if (threadIdx.x == 0) *a.globalStep = g + 1;
     }
     if (!grid_barrier(a.barrier, a.err)) return;
   }
+}
+
+// The same step as one ordinary launch (launch mode 1: a CUDA graph chains step and
+// bookkeeping launches; the launch boundaries order the blocks, so no grid barrier is needed).
+template <int Q, typename S>
+__global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble_step(EnsArgs a) {
+  __shared__ EnsShared<Q, S> sm;
+  const long long g = *a.globalStep;
+  ensemble_tiles<Q, S, true>(a, int(g & 1), *a.nTiles, sm);
+}
+
+template <int Q>
+__global__ void __launch_bounds__(256) k_ensemble_book(EnsArgs a) {
+  const long long g = *a.globalStep;
+  ensemble_book<Q>(a, int(g & 1));
+  __syncthreads();
+  if (threadIdx.x == 0) *a.globalStep = g + 1;
 }
 
 // rho and u of one lattice's core cells (FP64 out); the wall links were applied by the step that
@@ -373,24 +458,27 @@ int64_t region_bytes(int q, int storage, const lbx_ensemble_request* r, uint32_t
 using KernelFn = void (*)(EnsArgs);
 using MomentsFn = void (*)(const EnsLattice*, const long long*, double*, double*);
 using InitFn = void (*)(const EnsLattice*);
+using BookFn = void (*)(EnsArgs);
 
 template <int Q, typename S>
-void pick(KernelFn& k, MomentsFn& m, InitFn& i) {
+void pick(KernelFn& k, MomentsFn& m, InitFn& i, KernelFn& step, BookFn& book) {
   k = k_ensemble<Q, S>;
   m = k_ensemble_moments<Q, S>;
   i = k_ensemble_init_links<Q, S>;
+  step = k_ensemble_step<Q, S>;
+  book = k_ensemble_book<Q>;
 }
 
-bool kernels_for(int q, int storage, KernelFn& k, MomentsFn& m, InitFn& i) {
+bool kernels_for(int q, int storage, KernelFn& k, MomentsFn& m, InitFn& i, KernelFn& step, BookFn& book) {
   switch (q * 4 + storage) {
-  case 19 * 4 + LBX_F64: pick<19, double>(k, m, i); return true;
-  case 19 * 4 + LBX_F32: pick<19, float>(k, m, i); return true;
-  case 19 * 4 + LBX_F16DEV: pick<19, __half>(k, m, i); return true;
-  case 19 * 4 + LBX_BF16DEV: pick<19, __nv_bfloat16>(k, m, i); return true;
-  case 27 * 4 + LBX_F64: pick<27, double>(k, m, i); return true;
-  case 27 * 4 + LBX_F32: pick<27, float>(k, m, i); return true;
-  case 27 * 4 + LBX_F16DEV: pick<27, __half>(k, m, i); return true;
-  case 27 * 4 + LBX_BF16DEV: pick<27, __nv_bfloat16>(k, m, i); return true;
+  case 19 * 4 + LBX_F64: pick<19, double>(k, m, i, step, book); return true;
+  case 19 * 4 + LBX_F32: pick<19, float>(k, m, i, step, book); return true;
+  case 19 * 4 + LBX_F16DEV: pick<19, __half>(k, m, i, step, book); return true;
+  case 19 * 4 + LBX_BF16DEV: pick<19, __nv_bfloat16>(k, m, i, step, book); return true;
+  case 27 * 4 + LBX_F64: pick<27, double>(k, m, i, step, book); return true;
+  case 27 * 4 + LBX_F32: pick<27, float>(k, m, i, step, book); return true;
+  case 27 * 4 + LBX_F16DEV: pick<27, __half>(k, m, i, step, book); return true;
+  case 27 * 4 + LBX_BF16DEV: pick<27, __nv_bfloat16>(k, m, i, step, book); return true;
   default: return false;
   }
 }
@@ -439,6 +527,9 @@ struct lbx_ensemble_s {
   KernelFn kernel = nullptr;
   MomentsFn momentsKernel = nullptr;
   InitFn initKernel = nullptr;
+  KernelFn stepKernel = nullptr;  // launch mode 1: one launch per step ...
+  BookFn bookKernel = nullptr;    // ... and one bookkeeping launch, chained in a CUDA graph
+  int mode = 0;                   // 0: persistent cooperative kernel, 1: per-step launches
   std::map<int, cudaGraphExec_t> graphs;
   cudaGraph_t graphTemplate = nullptr;
 };
@@ -481,7 +572,7 @@ void drop_graphs(lbx_ensemble_s* E) {
 int ensure_grid(lbx_ensemble_s* E) {
   if (E->grid > 0) return LBX_OK;
   int perSM = 0, sms = 0;
-  ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, E->kernel, E->threads, 0));
+  ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, E->mode ? E->stepKernel : E->kernel, E->threads, 0));
   ENS_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device));
   if (E->blocksPerSM > 0) perSM = std::min(perSM, E->blocksPerSM);
   if (perSM < 1) return lbx::set_error(LBX_ERR_UNSUPPORTED, "ensemble kernel does not fit on an SM");
@@ -556,7 +647,7 @@ int lbx_ensemble_create(int32_t q, int32_t storage, int64_t slab_bytes, int32_t 
   E->slotBytes.assign(size_t(max_lattices), 0);
   E->slotUsed.assign(size_t(max_lattices), 0);
   E->slotCells.assign(size_t(max_lattices), 0);
-  kernels_for(q, storage, E->kernel, E->momentsKernel, E->initKernel);
+  kernels_for(q, storage, E->kernel, E->momentsKernel, E->initKernel, E->stepKernel, E->bookKernel);
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&E->slab), size_t(E->slabBytes));
   if (e == cudaSuccess) e = cudaMalloc(&E->dLat, size_t(max_lattices) * sizeof(EnsLattice));
   if (e == cudaSuccess) e = cudaMemset(E->dLat, 0, size_t(max_lattices) * sizeof(EnsLattice));
@@ -612,6 +703,17 @@ int lbx_ensemble_set_config(lbx_ensemble E, int32_t threads, int32_t blocks_per_
   return LBX_OK;
 }
 
+int lbx_ensemble_set_launch_mode(lbx_ensemble E, int32_t mode) {
+  if (!E) return lbx::set_error(LBX_ERR_INVALID, "null ensemble");
+  if (mode != 0 && mode != 1) return lbx::set_error(LBX_ERR_INVALID, "launch mode must be 0 or 1");
+  DeviceScope scope(E->device);
+  cudaDeviceSynchronize();
+  E->mode = mode;
+  E->grid = 0;
+  drop_graphs(E);
+  return LBX_OK;
+}
+
 int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, int32_t capacity, int32_t* n_out,
                           void* stream) {
   if (!E) return lbx::set_error(LBX_ERR_INVALID, "null ensemble");
@@ -624,16 +726,17 @@ int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, in
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // Candidates: block sizes 64..256, resident blocks per SM from 1 to the occupancy maximum
   // (the grid, and with it the cost of each grid barrier, grows with both).
-  struct Cand { int threads, perSM; };
+  struct Cand { int mode, threads, perSM; };
   std::vector<Cand> cands;
-  for (int threads = 64; threads <= 256; threads *= 2) {
-    int maxPerSM = 0;
-    ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxPerSM, E->kernel, threads, 0));
-    for (int b = 1; b <= std::min(maxPerSM, 8); b *= 2) cands.push_back({threads, b});
-    if (maxPerSM > 8) cands.push_back({threads, maxPerSM});
-  }
+  for (int mode = 0; mode <= 1; ++mode)
+    for (int threads = 64; threads <= 256; threads *= 2) {
+      int maxPerSM = 0;
+      ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxPerSM, mode ? E->stepKernel : E->kernel, threads, 0));
+      for (int b = 1; b <= std::min(maxPerSM, 8); b *= 2) cands.push_back({mode, threads, b});
+      if (maxPerSM > 8) cands.push_back({mode, threads, maxPerSM});
+    }
   if (n_out) *n_out = int32_t(cands.size());
-  const Cand keep{E->threads, E->blocksPerSM};
+  const Cand keep{E->mode, E->threads, E->blocksPerSM};
   const size_t latBytes = size_t(E->maxLattices) * sizeof(EnsLattice);
   char* saved = nullptr;
   cudaError_t e = cudaMalloc(&saved, size_t(hi) + latBytes + sizeof(long long));
@@ -662,6 +765,7 @@ int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, in
   int best = -1, rc = LBX_OK;
   float bestMs = 0.f;
   auto apply = [&](const Cand& c) {
+    E->mode = c.mode;
     E->threads = c.threads;
     E->blocksPerSM = c.perSM;
     E->grid = 0;
@@ -692,7 +796,7 @@ int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, in
     } else if (kerr != 0) {
       ms = -1.f;
     }
-    if (out && int32_t(i) < capacity) out[i] = lbx_tune_entry{0, 0, 0, 0, c.threads, c.perSM, double(ms)};
+    if (out && int32_t(i) < capacity) out[i] = lbx_tune_entry{c.mode, 0, 0, 0, c.threads, c.perSM, double(ms)};
   }
   const std::string err = rc != LBX_OK ? std::string(lbx_last_error()) : std::string();
   cudaError_t e2 = cudaStreamSynchronize(s);
@@ -822,14 +926,23 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    // capture { reset the error flag; persistent kernel } once per step count and replay it
+    // capture once per step count and replay: mode 0 { reset the error flag; persistent
+    // kernel }, mode 1 { step launch; bookkeeping launch } x steps
     cudaStream_t cap;
     ENS_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     cfg.stream = cap;
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaMemsetAsync(E->dErr, 0, sizeof(int), cap);
-    if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, E->kernel, a);
+    if (E->mode == 0) {
+      if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, E->kernel, a);
+    } else {
+      for (int k = 0; k < steps && e == cudaSuccess; ++k) {
+        E->stepKernel<<<unsigned(E->grid), unsigned(E->threads), 0, cap>>>(a);
+        E->bookKernel<<<1, 256, 0, cap>>>(a);
+        e = cudaGetLastError();
+      }
+    }
     cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
     cudaStreamDestroy(cap);
     if (e == cudaSuccess) e = e2;
@@ -841,7 +954,15 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
       cudaGetLastError();
       cfg.stream = s;
       ENS_TRY(cudaMemsetAsync(E->dErr, 0, sizeof(int), s));
-      ENS_TRY(cudaLaunchKernelEx(&cfg, E->kernel, a));
+      if (E->mode == 0) {
+        ENS_TRY(cudaLaunchKernelEx(&cfg, E->kernel, a));
+      } else {
+        for (int k = 0; k < steps; ++k) {
+          E->stepKernel<<<unsigned(E->grid), unsigned(E->threads), 0, s>>>(a);
+          E->bookKernel<<<1, 256, 0, s>>>(a);
+        }
+        ENS_TRY(cudaGetLastError());
+      }
       return LBX_OK;
     }
     it = E->graphs.emplace(steps, exec).first;

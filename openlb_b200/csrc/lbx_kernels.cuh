@@ -74,47 +74,6 @@ struct StatAcc {
   unsigned long long maxbits;
 };
 
-template <typename R>
-__device__ __forceinline__ void block_stats(R rho, R usq, bool valid, StatAcc* acc) {
-  double a = valid ? double(rho) : 0.0;
-  double b = valid ? double(usq) : 0.0;
-  double m = valid ? double(usq) : 0.0;
-  unsigned int c = valid ? 1u : 0u;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    c += __shfl_xor_sync(0xffffffffu, c, o);
-  }
-  __shared__ double sa[32], sb[32], sm[32];
-  __shared__ unsigned int sc[32];
-  const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
-  const int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
-  const int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
-  if (lane == 0) { sa[warp] = a; sb[warp] = b; sm[warp] = m; sc[warp] = c; }
-  __syncthreads();
-  if (warp == 0) {
-    a = lane < nwarps ? sa[lane] : 0.0;
-    b = lane < nwarps ? sb[lane] : 0.0;
-    m = lane < nwarps ? sm[lane] : 0.0;
-    c = lane < nwarps ? sc[lane] : 0u;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      b += __shfl_xor_sync(0xffffffffu, b, o);
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      c += __shfl_xor_sync(0xffffffffu, c, o);
-    }
-    if (lane == 0 && c > 0) {
-      atomicAdd(&acc->sum[0], a);
-      atomicAdd(&acc->sum[1], b);
-      atomicAdd(&acc->count, (unsigned long long)c);
-      atomicMax(&acc->maxbits, (unsigned long long)__double_as_longlong(m));
-    }
-  }
-}
-
 // Block partial of the lattice statistics {sum rho, sum |u|^2, max |u|^2, count}: a warp
 // butterfly, then the warps in index order, written to part[4 * block] without atomics.  With
 // k_stats_finalize summing the partials in a fixed order, the statistics are bitwise
@@ -202,6 +161,56 @@ static __global__ void __launch_bounds__(kFinalizeThreads) k_stats_finalize(cons
     out->count = (unsigned long long)s[3][0];
     out->maxbits = (unsigned long long)__double_as_longlong(s[2][0]);
   }
+}
+
+// Deterministic 4-component block reduction for the FP64 field reductions: component k is a
+// sum, or a max when bit k of MAXMASK is set.  Warp butterfly, then the warps in index order;
+// one entry of 4 doubles per block, no atomics.
+template <int MAXMASK>
+__device__ __forceinline__ void block_partial4(double v0, double v1, double v2, double v3, double* __restrict__ part) {
+  double v[4] = {v0, v1, v2, v3};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    for (int o = 16; o > 0; o >>= 1) {
+      const double w = __shfl_xor_sync(0xffffffffu, v[k], o);
+      v[k] = ((MAXMASK >> k) & 1) ? fmax(v[k], w) : v[k] + w;
+    }
+  __shared__ double red[4][32];
+  const int tid = threadIdx.x;
+  const int nwarps = (blockDim.x + 31) >> 5;
+  if ((tid & 31) == 0)
+    for (int k = 0; k < 4; ++k) red[k][tid >> 5] = v[k];
+  __syncthreads();
+  if (tid < 4) {
+    double a = 0.0;
+    for (int w = 0; w < nwarps; ++w) a = ((MAXMASK >> tid) & 1) ? fmax(a, red[tid][w]) : a + red[tid][w];
+    part[4 * int64_t(blockIdx.x) + tid] = a;
+  }
+}
+
+// The block entries combined in a fixed order (thread t: entries t, t + 1024, ...; then a fixed
+// tree) into out[0..3].
+template <int MAXMASK>
+static __global__ void __launch_bounds__(kFinalizeThreads) k_finalize4(const double* __restrict__ part, int64_t n,
+                                                                      double* __restrict__ out) {
+  double v[4] = {0, 0, 0, 0};
+  for (int64_t i = threadIdx.x; i < n; i += kFinalizeThreads) {
+    const double4 p = *reinterpret_cast<const double4*>(part + 4 * i);
+    const double q[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = ((MAXMASK >> k) & 1) ? fmax(v[k], q[k]) : v[k] + q[k];
+  }
+  __shared__ double s[4][kFinalizeThreads];
+  for (int k = 0; k < 4; ++k) s[k][threadIdx.x] = v[k];
+  __syncthreads();
+  for (int stride = kFinalizeThreads / 2; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride)
+      for (int k = 0; k < 4; ++k)
+        s[k][threadIdx.x] = ((MAXMASK >> k) & 1) ? fmax(s[k][threadIdx.x], s[k][threadIdx.x + stride])
+                                                : s[k][threadIdx.x] + s[k][threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
 }
 
 // ---- fused collide + PS stream --------------------------------------------------------
@@ -1053,11 +1062,11 @@ __global__ void k_moments(const S* __restrict__ pop, Geometry g, Shifts<Q> sh, i
   if (u) static_for<D::d>([&](auto A) { u[A * ncore + c] = double(uu[A]); });
 }
 
-// FP64 mass and momentum over the bulk cells: acc = {sum rho, sum j_x, sum j_y, sum j_z}
+// FP64 mass and momentum over the bulk cells: block entries {sum rho, sum j_x, sum j_y, sum j_z}
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_mass_momentum(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                        const uint8_t* __restrict__ cellDyn,
-                                                       double* __restrict__ acc) {
+                                                       double* __restrict__ part) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1081,12 +1090,7 @@ __global__ void __launch_bounds__(256) k_mass_momentum(const S* __restrict__ pop
       v[0] = r;
     }
   }
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    double a = v[k];
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if ((threadIdx.x & 31) == 0 && a != 0.0) atomicAdd(&acc[k], a);
-  }
+  block_partial4<0>(v[0], v[1], v[2], v[3], part);
 }
 
 // Momentum exchange over the bounce-back links after the PostStream step:
@@ -1096,7 +1100,7 @@ template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_link_force(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                     const uint32_t* __restrict__ cell,
                                                     const uint8_t* __restrict__ dir, int64_t nLinks,
-                                                    double* __restrict__ acc) {
+                                                    double* __restrict__ part) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1120,26 +1124,16 @@ __global__ void __launch_bounds__(256) k_link_force(const S* __restrict__ pop, G
     const double s = fin + fout;
     fx = cx * s; fy = cy * s; fz = cz * s;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-    fz += __shfl_xor_sync(0xffffffffu, fz, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&acc[0], fx);
-    atomicAdd(&acc[1], fy);
-    atomicAdd(&acc[2], fz);
-  }
+  block_partial4<0>(fx, fy, fz, 0.0, part);
 }
 
-// Velocity residual against a snapshot: acc = {sum |du|^2, sum |u|^2, max |du| bits}; the
+// Velocity residual against a snapshot: block entries {sum |du|^2, sum |u|^2, max |du|}; the
 // snapshot is refreshed with the current velocity.
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_residual(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                   const uint8_t* __restrict__ cellDyn, int forced,
                                                   float fx, float fy, float fz, float* __restrict__ snap,
-                                                  double* __restrict__ acc,
-                                                  unsigned long long* __restrict__ maxbits) {
+                                                  double* __restrict__ part) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1166,17 +1160,7 @@ __global__ void __launch_bounds__(256) k_residual(const S* __restrict__ pop, Geo
       });
     }
   }
-  double m = sqrt(du2);
-  for (int o = 16; o > 0; o >>= 1) {
-    du2 += __shfl_xor_sync(0xffffffffu, du2, o);
-    u2 += __shfl_xor_sync(0xffffffffu, u2, o);
-    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&acc[0], du2);
-    atomicAdd(&acc[1], u2);
-    atomicMax(maxbits, (unsigned long long)__double_as_longlong(m));
-  }
+  block_partial4<4>(du2, u2, sqrt(du2), 0.0, part);
 }
 
 // ---- launchers (instantiated once per storage type) ------------------------------------
@@ -1222,14 +1206,16 @@ template <int Q, typename S>
 cudaError_t launch_ini_equilibrium(const LaunchArgs& a, const double* rho, const double* u, cudaStream_t stream);
 template <int Q, typename S>
 cudaError_t launch_moments(const LaunchArgs& a, double* rho, double* u, cudaStream_t stream);
+// FP64 reductions: per-block entries into `part` (4 doubles per block, sized by
+// reduce_blocks), combined in a fixed order into out[0..3].
+inline int64_t reduce_blocks(int64_t items) { return (items + 255) / 256; }
 template <int Q, typename S>
-cudaError_t launch_mass_momentum(const LaunchArgs& a, double* acc, cudaStream_t stream);
+cudaError_t launch_mass_momentum(const LaunchArgs& a, double* part, double* out, cudaStream_t stream);
 template <int Q, typename S>
 cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir, int64_t nLinks,
-                              double* acc, cudaStream_t stream);
+                              double* part, double* out, cudaStream_t stream);
 template <int Q, typename S>
-cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc, unsigned long long* maxbits,
-                            cudaStream_t stream);
+cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, double* out, cudaStream_t stream);
 
 template <int Q>
 inline Shifts<Q> shifts_of(const LaunchArgs& a) {
@@ -1426,27 +1412,38 @@ cudaError_t launch_moments(const LaunchArgs& a, double* rho, double* u, cudaStre
   return cudaGetLastError();
 }
 template <int Q, typename S>
-cudaError_t launch_mass_momentum(const LaunchArgs& a, double* acc, cudaStream_t stream) {
-  const unsigned blocks = unsigned((ncore_of(a.g) + 255) / 256);
-  k_mass_momentum<Q, S><<<blocks, 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), a.cellDyn, acc);
+cudaError_t launch_mass_momentum(const LaunchArgs& a, double* part, double* out, cudaStream_t stream) {
+  const int64_t blocks = reduce_blocks(ncore_of(a.g));
+  k_mass_momentum<Q, S><<<unsigned(blocks), 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a),
+                                                              a.cellDyn, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_finalize4<0><<<1, kFinalizeThreads, 0, stream>>>(part, blocks, out);
   return cudaGetLastError();
 }
 template <int Q, typename S>
 cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
-                                    int64_t nLinks, double* acc, cudaStream_t stream) {
-  if (nLinks <= 0) return cudaSuccess;
-  k_link_force<Q, S><<<unsigned((nLinks + 255) / 256), 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g,
-                                                                          shifts_of<Q>(a), cell, dir, nLinks, acc);
+                                    int64_t nLinks, double* part, double* out, cudaStream_t stream) {
+  const int64_t blocks = reduce_blocks(nLinks);
+  if (nLinks > 0) {
+    k_link_force<Q, S><<<unsigned(blocks), 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), cell,
+                                                             dir, nLinks, part);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  k_finalize4<0><<<1, kFinalizeThreads, 0, stream>>>(part, blocks, out);
   return cudaGetLastError();
 }
 template <int Q, typename S>
-cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc,
-                                  unsigned long long* maxbits, cudaStream_t stream) {
-  const unsigned blocks = unsigned((ncore_of(a.g) + 255) / 256);
+cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, double* out, cudaStream_t stream) {
+  const int64_t blocks = reduce_blocks(ncore_of(a.g));
   const int forced = (a.dynamics == DYN_FORCED_BGK || a.dynamics == DYN_FORCED_SMAGORINSKY);
-  k_residual<Q, S><<<blocks, 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), a.cellDyn,
-                                               forced, float(a.force[0]), float(a.force[1]),
-                                               float(a.force[2]), snap, acc, maxbits);
+  k_residual<Q, S><<<unsigned(blocks), 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), a.cellDyn,
+                                                         forced, float(a.force[0]), float(a.force[1]),
+                                                         float(a.force[2]), snap, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_finalize4<4><<<1, kFinalizeThreads, 0, stream>>>(part, blocks, out);
   return cudaGetLastError();
 }
 // Explicit instantiation of every launcher for one (descriptor, storage) pair.
@@ -1459,10 +1456,10 @@ cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* acc,
   template cudaError_t launch_transfer<Q, S>(const LaunchArgs&, int, const void*, int, bool, cudaStream_t); \
   template cudaError_t launch_ini_equilibrium<Q, S>(const LaunchArgs&, const double*, const double*, cudaStream_t); \
   template cudaError_t launch_moments<Q, S>(const LaunchArgs&, double*, double*, cudaStream_t);       \
-  template cudaError_t launch_mass_momentum<Q, S>(const LaunchArgs&, double*, cudaStream_t);          \
+  template cudaError_t launch_mass_momentum<Q, S>(const LaunchArgs&, double*, double*, cudaStream_t); \
   template cudaError_t launch_link_force<Q, S>(const LaunchArgs&, const uint32_t*, const uint8_t*,    \
-                                               int64_t, double*, cudaStream_t);                       \
-  template cudaError_t launch_residual<Q, S>(const LaunchArgs&, float*, double*, unsigned long long*, cudaStream_t);
+                                               int64_t, double*, double*, cudaStream_t);              \
+  template cudaError_t launch_residual<Q, S>(const LaunchArgs&, float*, double*, double*, cudaStream_t);
 #endif  // LBX_KERNEL_TU
 
 }  // namespace lbx

@@ -102,6 +102,7 @@ def _load() -> C.CDLL:
         "lbx_set_fd_boundaries": ([VP, I64, VP, VP, VP, VP, VP], C.c_int),
         "lbx_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
+        "lbx_ensemble_set_launch_mode": ([VP, I32], C.c_int),
         "lbx_ensemble_footprint": ([I32, I32, P(EnsembleRequest), P(I64)], C.c_int),
         "lbx_ensemble_create": ([I32, I32, I64, I32, I32, P(VP)], C.c_int),
         "lbx_ensemble_destroy": ([VP], C.c_int),
@@ -474,6 +475,10 @@ class Ensemble:
         """Time every launch shape of the persistent kernel on the admitted lattices, keep the
         fastest; every lattice's state is left as it was."""
         return _tune(lib.lbx_ensemble_autotune, self._h, steps, stream, "lbx_ensemble_autotune")
+
+    def set_launch_mode(self, mode: int) -> None:
+        """0: one persistent kernel per run; 1: one launch per step, chained in a CUDA graph."""
+        check(lib.lbx_ensemble_set_launch_mode(self._h, mode), "lbx_ensemble_set_launch_mode")
 
     def set_config(self, threads: int = 256, blocks_per_sm: int = 0, check_interval: int = 100) -> None:
         check(lib.lbx_ensemble_set_config(self._h, threads, blocks_per_sm, check_interval), "lbx_ensemble_set_config")
