@@ -80,6 +80,12 @@ CASES.update({
                                                               *RND, "--u0", "0.05", "--steps", "40"]),
     "channel_d3q19_bgk_f32": ("d3q19_f32", "channel", ["--n", "12", "10", "8", "--dyn", "bgk", "--omega", "1.2",
                                                         *RND, "--u0", "0.05", "--steps", "60"]),
+    # the 2D cavity at its full size: 128^2 fluid cells, nu = 0.1 * 128 / 100, lid 0.1, 20 000
+    # steps from rest (statistics kept every 100th step and the last)
+    "full_cavity_d2q9_bgk_128_f64": ("d2q9_f64_nocse", "cavity", ["--n", "128", "128", "--dyn", "bgk",
+                                                                   "--omega", str(1.0 / (3 * 0.128 + 0.5)),
+                                                                   "--ulid", "0.1", "--init", "rest",
+                                                                   "--steps", "20000"]),
     # Taylor-Green vortex (the benchmark's initial condition), small
     "tgv_d3q19_bgk_f64": ("d3q19_f64_nocse", "periodic", ["--n", "16", "16", "16", "--dyn", "bgk",
                                                            "--omega", str(1.0 / (3 * 0.01 + 0.5)), "--init", "tgv",
@@ -88,6 +94,14 @@ CASES.update({
                                                      "--omega", str(1.0 / (3 * 0.01 + 0.5)), "--init", "tgv",
                                                      "--u0", "0.05", "--steps", "50"]),
 })
+
+
+STATS_EVERY = {"full_cavity_d2q9_bgk_128_f64": 100}
+
+
+def select_stats(stats: np.ndarray, every: int) -> np.ndarray:
+    """Every `every`-th row of per-step statistics, and the last row."""
+    return np.vstack([stats[::every], stats[-1:]]) if every > 1 else stats
 
 
 def generate(name: str) -> Path:
@@ -109,6 +123,9 @@ def generate(name: str) -> Path:
         stats = np.loadtxt(prefix + ".stats.txt", ndmin=2)
         bnd = Path(prefix + ".bnd.bin")
         extra = {"bnd": np.fromfile(bnd, dtype=np.float64).reshape(-1, 8)} if bnd.exists() else {}
+    every = STATS_EVERY.get(name, 1)
+    stats = select_stats(stats, every)
+    meta["stats_every"] = every
     meta["binary"] = binary
     meta["args"] = [case, *args]
     out = HERE / f"{name}.npz"
