@@ -155,7 +155,8 @@ def tgv_fields(n: int):
     return np.ones(n ** 3), u
 
 
-STEP_KERNEL = {0: "k_collide_stream_tiled", 1: "k_collide_stream", 2: "k_collide_stream_groups"}
+STEP_KERNEL = {0: "k_collide_stream_tiled", 1: "k_collide_stream", 2: "k_collide_stream_groups",
+               3: "k_collide_stream_bulk"}
 
 
 def current_config(tuning: list[dict]) -> dict:

@@ -109,6 +109,7 @@ struct lbx_lattice_s {
   int64_t statCapacity = 0;          // blocks statPart holds
   double* reduceAcc = nullptr;       // 8 doubles + 1 ull of scratch for reductions
   double* reducePart = nullptr;      // per-block entries of the FP64 reductions (4 doubles each)
+  int* devErr = nullptr;             // set by a step kernel whose bounded wait gave up
   int64_t reducePartCapacity = 0;    // blocks reducePart holds
   float* residualSnap = nullptr;
   void* stage = nullptr;             // ncore doubles
@@ -169,6 +170,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.fdMeta = L->fdMeta;
   a.fdValue = L->fdValue;
   a.fdMom = L->fdMom;
+  a.err = L->devErr;
   return a;
 }
 
@@ -239,6 +241,19 @@ int64_t step_blocks(const lbx_lattice_s* L) {
   if (L->kernel == 0) {
     const LaunchArgs a = args_of(L);
     return (a.flatEnd - a.flatBase + TILE - 1) / TILE;
+  }
+  if (L->kernel == 3) {  // at most one persistent block per tile (the grid is capped by residency)
+    const LaunchArgs a = args_of(L);
+    int64_t bt = 0;
+    switch (L->q * 4 + L->storage) {
+#define LBX_BT(QQ, SS, ST) case QQ * 4 + ST: bt = BulkCfg<QQ, SS>::BT; break;
+      LBX_BT(9, double, LBX_F64) LBX_BT(9, float, LBX_F32) LBX_BT(9, __half, LBX_F16DEV) LBX_BT(9, __nv_bfloat16, LBX_BF16DEV)
+      LBX_BT(19, double, LBX_F64) LBX_BT(19, float, LBX_F32) LBX_BT(19, __half, LBX_F16DEV) LBX_BT(19, __nv_bfloat16, LBX_BF16DEV)
+      LBX_BT(27, double, LBX_F64) LBX_BT(27, float, LBX_F32) LBX_BT(27, __half, LBX_F16DEV) LBX_BT(27, __nv_bfloat16, LBX_BF16DEV)
+#undef LBX_BT
+      default: bt = 64;
+    }
+    return (a.flatEnd - a.flatBase + bt - 1) / bt;
   }
   const int k = L->kernel == 2 ? L->cellsPerThread : 1;
   const int64_t groups = (nf + k - 1) / k;
@@ -526,6 +541,8 @@ int lbx_lattice_create(int32_t q, const int32_t core[3], const int32_t periodic[
   if (e == cudaSuccess) e = cudaMalloc(&L->stats, sizeof(StatAcc));
   if (e == cudaSuccess) e = cudaMemset(L->stats, 0, sizeof(StatAcc));
   if (e == cudaSuccess) e = cudaMalloc(&L->reduceAcc, 8 * sizeof(double) + sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&L->devErr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(L->devErr, 0, sizeof(int));
   if (e != cudaSuccess) {
     const std::string msg = std::string("allocation failed: ") + cudaGetErrorString(e);
     release_columns(L);
@@ -557,6 +574,7 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->statPart);
   cudaFree(L->reduceAcc);
   cudaFree(L->reducePart);
+  cudaFree(L->devErr);
   cudaFree(L->residualSnap);
   cudaFree(L->stage);
   delete L;
@@ -932,8 +950,14 @@ int lbx_get_statistics(lbx_lattice L, double out[4], void* stream) {
   DeviceGuard guard(L->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   StatAcc h;
+  int kerr = 0;
   LBX_CUDA_TRY(cudaMemcpyAsync(&h, L->stats, sizeof(StatAcc), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaMemcpyAsync(&kerr, L->devErr, sizeof(int), cudaMemcpyDeviceToHost, s));
   LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  if (kerr) {
+    cudaMemset(L->devErr, 0, sizeof(int));
+    return fail(LBX_ERR_CUDA, "a step kernel gave up waiting for its bulk copies; results of that step are invalid");
+  }
   double mx;
   std::memcpy(&mx, &h.maxbits, sizeof(double));
   const double cnt = double(h.count);
@@ -1030,7 +1054,9 @@ int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
 int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
-  if (variant < 0 || variant > 2) return fail(LBX_ERR_INVALID, "variant must be 0, 1 or 2");
+  if (variant < 0 || variant > 3) return fail(LBX_ERR_INVALID, "variant must be 0, 1, 2 or 3");
+  if (variant == 3 && (!L->doubled || L->period >= (int64_t(1) << 31)))
+    return fail(LBX_ERR_UNSUPPORTED, "variant 3 (bulk copies) needs the doubled column mapping and fewer than 2^31 cells");
   if (variant == 2 && L->period >= (int64_t(1) << 31))
     return fail(LBX_ERR_UNSUPPORTED, "variant 2 needs a column period below 2^31 cells");
   if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2 &&
@@ -1070,6 +1096,7 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
     block_shape_for(nf, 1, bx, by);
     cands.push_back({1, bx, by, 1});
     cands.push_back({0, 256, 1, 1});
+    if (L->doubled && L->period < (int64_t(1) << 31)) cands.push_back({3, 256, 1, 1});
   }
   if (n_out) *n_out = int32_t(cands.size());
   const Cand keep{L->kernel, L->blockX, L->blockY, L->cellsPerThread};

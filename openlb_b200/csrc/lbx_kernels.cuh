@@ -445,6 +445,215 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
   if (statPart) block_partial(accRho, accUsq, accMax, double(accCount), statPart);
 }
 
+// ---- fused collide + PS stream, whole tiles moved by the TMA bulk-copy engine ------------
+// Variant 3.  A tile is BT consecutive cells of the flat padded index space.  In periodic-shift
+// storage the slots of those cells in column i are one contiguous run (no wrap with doubled
+// columns), so each tile is brought into shared memory with one 1D bulk copy per population
+// (cp.async.bulk, completion on an mbarrier), computed in place, and written back with one bulk
+// store per population for the 16-byte-aligned interior of the run plus element stores for the
+// unaligned head and tail (at most 15 bytes each), so no slot outside the tile is written.
+// Two stages per block: the next tile's copies are in flight while the current one is computed.
+// Ghost and spare cells inside a tile are written back unchanged; the periodic overlap copy
+// (k_periodic_halo) runs after this kernel and overwrites the ghost slots it owns.
+// Memory requests: 2 * Q bulk operations per tile instead of 2 * Q * BT / 32 warp accesses,
+// which is what the 16-bit forms are limited by on the SM -> L2 path.
+// Division of flat cell indices (< 2^31) by the padded strides sx and sy: round-up multiplier and
+// shift (Granlund and Montgomery, "Division by invariant integers using multiplication", 1994):
+// n / d = (umulhi(m, n) + n) >> l with l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1.
+struct FlatDiv {
+  uint32_t mx, my;
+  int32_t lx, ly;
+  static void make(uint32_t d, uint32_t& m, int32_t& l) {
+    l = 0;
+    while ((uint64_t(1) << l) < d) ++l;
+    m = uint32_t(((uint64_t(1) << 32) * ((uint64_t(1) << l) - d)) / d + 1);
+  }
+};
+
+template <int Q, typename S> struct BulkCfg {
+  static constexpr int ES = int(sizeof(S));
+  static constexpr int BT = (36864 / (Q * ES)) / 64 * 64;  // cells per tile: ~36 KB of populations
+  static constexpr int COL_BYTES = BT * ES + 32;           // one column's run + alignment slack
+  static constexpr int STAGE_BYTES = Q * COL_BYTES;
+  static constexpr int SMEM = 2 * STAGE_BYTES + 64;        // two stages + the mbarriers
+  static constexpr int THREADS = 256;
+  static constexpr int BLOCKS = 3;                          // resident blocks per SM (registers <= 85)
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_addr(src)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false (and the error flag set) if it did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it > 64) __nanosleep(64);
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
+template <int Q, typename S, int DYN>
+__global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS) k_collide_stream_bulk(
+    S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t base, int64_t nFlat, int64_t nTiles,
+    CollisionParams<typename Storage<S>::R> p, const uint8_t* __restrict__ cellDyn, double* __restrict__ statPart,
+    int* __restrict__ err, FlatDiv dv) {
+  using R = typename Storage<S>::R;
+  using C = BulkCfg<Q, S>;
+  constexpr int ES = C::ES, BT = C::BT, NT = C::THREADS, VE = 16 / ES;
+  constexpr int COL = C::COL_BYTES / ES;  // elements per column buffer
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * C::STAGE_BYTES);
+  __shared__ int sHead[2][Q];  // per stage and column: elements from the aligned run start to the tile
+  __shared__ int sAbort;
+  const int tid = threadIdx.x;
+  int issued[2] = {0, 0}, waited[2] = {0, 0};  // bulk-load phases per stage (thread 0's view)
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    sAbort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  // the bulk loads of `tile` into stage `st` (thread 0)
+  auto issue = [&](int64_t tile, int st) {
+    const int64_t t0 = base + tile * BT;
+    const int64_t cells = (t0 + BT <= nFlat) ? BT : nFlat - t0;
+    uint32_t total = 0;
+    for (int i = 0; i < Q; ++i) {
+      const int64_t first = (t0 + sh.s[i]) * ES;
+      const int64_t a0 = first & ~int64_t(15), a1 = (first + cells * ES + 15) & ~int64_t(15);
+      sHead[st][i] = int((first - a0) / ES);
+      total += uint32_t(a1 - a0);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    mbar_expect_tx(&bar[st], total);
+    unsigned char* stage = smem_raw + st * C::STAGE_BYTES;
+    for (int i = 0; i < Q; ++i) {
+      const int64_t first = (t0 + sh.s[i]) * ES;
+      const int64_t a0 = first & ~int64_t(15), a1 = (first + cells * ES + 15) & ~int64_t(15);
+      bulk_g2s(stage + i * C::COL_BYTES, reinterpret_cast<const unsigned char*>(pop + i * g.stride) + a0,
+               uint32_t(a1 - a0), &bar[st]);
+    }
+    ++issued[st];
+  };
+
+  double accRho = 0.0, accUsq = 0.0, accMax = 0.0, accCount = 0.0;
+  const int64_t stride = gridDim.x;
+  int k = 0;
+  if (tid == 0 && int64_t(blockIdx.x) < nTiles) issue(blockIdx.x, 0);
+  for (int64_t tile = blockIdx.x; tile < nTiles; tile += stride, ++k) {
+    const int st = k & 1;
+    __syncthreads();  // every thread is done with stage st ^ 1 (the previous tile)
+    if (tid == 0) {
+      asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // its bulk stores have read it
+      if (tile + stride < nTiles) issue(tile + stride, st ^ 1);
+    }
+    if (!mbar_wait_bounded(&bar[st], uint32_t((k >> 1) & 1), err)) sAbort = 1;
+    else if (tid == 0) ++waited[st];
+    __syncthreads();
+    if (sAbort) break;
+    const int64_t t0 = base + tile * BT;
+    const int cells = int((t0 + BT <= nFlat) ? BT : nFlat - t0);
+    S* stage = reinterpret_cast<S*>(smem_raw + st * C::STAGE_BYTES);
+    for (int j = tid; j < cells; j += NT) {
+      // core test of flat cell t0 + j by multiply-high division (the divisors sx, sy are fixed)
+      const uint32_t un = uint32_t(t0 + j);
+      const uint32_t px = (__umulhi(un, dv.mx) + un) >> dv.lx;
+      const uint32_t rem = un - px * uint32_t(g.sx);
+      const uint32_t py = (__umulhi(rem, dv.my) + rem) >> dv.ly;
+      const int x = int(px) - 1, y = int(py) - 1, z = int(rem - py * uint32_t(g.sy)) - g.pz;
+      if (!(x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz)) continue;
+      const uint8_t kind = cellDyn ? cellDyn[t0 + j] : uint8_t(1);
+      if (kind != 1 && kind != 2) continue;
+      R f[Q];
+      static_for<Q>([&](auto I) { f[I] = Storage<S>::load(stage + I * COL + sHead[st][I] + j); });
+      if (kind == 1) {
+        R rho, usq;
+        collide<Q, R, DYN>(f, p, rho, usq);
+        accRho += double(rho);
+        accUsq += double(usq);
+        accMax = fmax(accMax, double(usq));
+        accCount += 1.0;
+      } else {
+        revert<Q, R>(f);
+      }
+      static_for<Q>([&](auto I) { Storage<S>::store(stage + I * COL + sHead[st][I] + j, f[I]); });
+    }
+    // the new stage contents become visible to the bulk-copy (async) proxy, then go back: the
+    // 16-byte-aligned interior of each column's run by one bulk store, the unaligned head and
+    // tail (fewer than 16 bytes each) by element stores
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 0; i < Q; ++i) {
+        const int64_t first = (t0 + sh.s[i]) * ES;
+        const int64_t b0 = (first + 15) & ~int64_t(15), b1 = (first + int64_t(cells) * ES) & ~int64_t(15);
+        if (b1 > b0)
+          bulk_s2g(reinterpret_cast<unsigned char*>(pop + i * g.stride) + b0,
+                   reinterpret_cast<unsigned char*>(stage) + i * C::COL_BYTES + (b0 - (first & ~int64_t(15))),
+                   uint32_t(b1 - b0));
+      }
+      asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    }
+    for (int c = tid; c < Q * 2 * VE; c += NT) {
+      const int i = c / (2 * VE), e = c - i * (2 * VE);
+      const int64_t first = (t0 + sh.s[i]) * ES;
+      const int64_t b0 = (first + 15) & ~int64_t(15), b1 = (first + int64_t(cells) * ES) & ~int64_t(15);
+      int jj;
+      bool ok;
+      if (b1 > b0) {
+        const int head = int((b0 - first) / ES), tail = int((b1 - first) / ES);
+        jj = e < VE ? e : tail + (e - VE);
+        ok = e < VE ? jj < head : jj < cells;
+      } else {  // run shorter than 32 bytes: every element by an element store
+        jj = e;
+        ok = jj < cells;
+      }
+      if (ok) pop[i * g.stride + t0 + sh.s[i] + jj] = stage[i * COL + sHead[st][i] + jj];
+    }
+  }
+  if (tid == 0) {
+    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+    // after an abort: let the loads still in flight land before the block exits (bounded)
+    for (int st = 0; st < 2; ++st)
+      while (waited[st] < issued[st]) {
+        mbar_wait_bounded(&bar[st], uint32_t(waited[st] & 1), err);
+        ++waited[st];
+      }
+  }
+  if (statPart) block_partial(accRho, accUsq, accMax, accCount, statPart);
+}
+
 // ---- fused collide + PS stream, K consecutive cells per thread --------------------------
 // One thread owns K consecutive cells along the fastest core axis (z in 3D, y in 2D).  For
 // every population it forms ONE wrapped column index; the K values are then reached with
@@ -1185,6 +1394,7 @@ struct LaunchArgs {
   const uint8_t* fdMeta;     // normal axis, orientation, kind (FdMeta)
   const double* fdValue;     // 4 imposed values per cell
   double* fdMom;             // 7 doubles per cell of scratch (k_fd_momenta)
+  int* err;                  // device flag: a bounded wait of a step kernel gave up
 };
 
 // Blocks of 256 threads the boundary-cell collision adds to a step's statistics partials.
@@ -1270,6 +1480,34 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     k_collide_stream_tiled<Q, S, DYN><<<unsigned(grid), TILE, smem, stream>>>(pop, g, sh, a.flatBase, a.flatEnd,
                                                                                tiles, p, a.cellDyn,
                                                                                a.stats ? a.statPart : nullptr);
+    nblocks = grid;
+  } else if (a.kernel == 3) {
+    using BC = BulkCfg<Q, S>;
+    static unsigned long long configured = 0;  // one bit per device ordinal
+    static int residentBlocks[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured >> (dev & 63) & 1ull)) {
+      cudaError_t e = cudaFuncSetAttribute(k_collide_stream_bulk<Q, S, DYN>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, BC::SMEM);
+      if (e != cudaSuccess) return e;
+      int perSM = 0, sms = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_collide_stream_bulk<Q, S, DYN>, BC::THREADS, BC::SMEM);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      residentBlocks[dev & 63] = (perSM > 0 ? perSM : 1) * sms;
+      configured |= 1ull << (dev & 63);
+    }
+    if (!a.doubled) return cudaErrorInvalidValue;  // bulk runs need the doubled columns (no wrap)
+    const int64_t tiles = (a.flatEnd - a.flatBase + BC::BT - 1) / BC::BT;
+    const int64_t grid = tiles < residentBlocks[dev & 63] ? tiles : residentBlocks[dev & 63];
+    if (a.stats && grid > a.statCapacity) return cudaErrorInvalidValue;
+    FlatDiv dv;
+    FlatDiv::make(uint32_t(g.sx), dv.mx, dv.lx);
+    FlatDiv::make(uint32_t(g.sy), dv.my, dv.ly);
+    k_collide_stream_bulk<Q, S, DYN><<<unsigned(grid), BC::THREADS, BC::SMEM, stream>>>(
+        pop, g, sh, a.flatBase, a.flatEnd, tiles, p, a.cellDyn, a.stats ? a.statPart : nullptr, a.err, dv);
     nblocks = grid;
   } else if (a.kernel == 1) {
     dim3 block(a.blockX, a.blockY, 1);

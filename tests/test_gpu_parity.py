@@ -235,12 +235,13 @@ def test_invalid_parameters_raise():
                                   "porous_d2q9_trt_f64", "tgv_d3q19_bgk_f32"])
 @pytest.mark.parametrize("storage", ["f64", "f32", "f16dev", "bf16dev"])
 def test_kernel_variants_agree_bitwise(name, storage):
-    """Every step kernel variant and launch shape computes identical bits (the 16-bit forms also
-    with two cells per thread in paired 32-bit words, and four cells per thread)."""
+    """Every step kernel variant and launch shape computes identical bits (variant 3 moves whole
+    tiles with bulk copies; the 16-bit forms also with four cells per thread)."""
     fx = L.load_fixture(name)
     setup = L.case_setup(fx)
     outs = []
-    shapes = [(0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2), (2, 256, 1, 1)]
+    shapes = [(0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2), (2, 256, 1, 1),
+              (3, 256, 1, 1)]
     if storage in ("f16dev", "bf16dev"):
         shapes += [(2, 32, 4, 4), (2, 128, 1, 2)]
     for variant, bx, by, k in shapes:
