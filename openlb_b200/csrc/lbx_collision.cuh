@@ -142,10 +142,65 @@ __device__ __forceinline__ R smagorinsky_omega(const R (&f)[Q], R rho, const R (
 }
 
 // Collide one cell in place.  Returns the cell statistic {rho, |u|^2}.
+// FP32 BGK, written so that no product is ever an operand of a separate add: the sums of the
+// populations and of the momentum are plain adds, every product that meets an add does so inside
+// an explicit fused multiply-add.  The packed two-cell form (collide_bgk_x2) repeats this
+// sequence lane by lane, and since nothing here is left for the compiler to contract, the
+// two give the same bits.
+template <int Q>
+__device__ __forceinline__ void collide_bgk_f32(float (&f)[Q], float omega, float& rhoOut, float& uSqrOut) {
+  using D = Desc<Q>;
+  float rho = 0.f;
+  static_for<Q>([&](auto I) { rho = __fadd_rn(rho, f[I]); });
+  rho = __fadd_rn(rho, 1.f);
+  float j[3] = {0.f, 0.f, 0.f};
+  static_for<Q>([&](auto I) {
+    static_for<D::d>([&](auto A) {
+      constexpr int c = D::C[I][A];
+      if constexpr (c == 1) j[A] = __fadd_rn(j[A], f[I]);
+      else if constexpr (c == -1) j[A] = __fsub_rn(j[A], f[I]);
+    });
+  });
+  const float inv = 1.f / rho;
+  float u[3];
+  static_for<D::d>([&](auto A) { u[A] = __fmul_rn(j[A], inv); });
+  float uSqr = __fmul_rn(u[0], u[0]);
+  static_for<D::d - 1>([&](auto A) { uSqr = __fmaf_rn(u[A + 1], u[A + 1], uSqr); });
+  const float keep = 1.f - omega;
+  const float base = __fmaf_rn(-1.5f, uSqr, 1.f);
+  {
+    constexpr float t0 = weight<Q, float>(0);
+    f[0] = __fmaf_rn(omega, __fmaf_rn(__fmul_rn(rho, t0), base, -t0), __fmul_rn(f[0], keep));
+  }
+  static_for<Q / 2>([&](auto K) {
+    constexpr int i = K + 1;
+    constexpr int jj = D::OPP[i];
+    constexpr float t = weight<Q, float>(i);
+    float cj = 0.f;  // c_i . j over the non-zero components in axis order
+    static_for<D::d>([&](auto A) {
+      constexpr int c = D::C[i][A];
+      if constexpr (c == 1) cj = __fadd_rn(cj, j[A]);
+      else if constexpr (c == -1) cj = __fsub_rn(cj, j[A]);
+    });
+    const float cu = __fmul_rn(cj, inv);
+    const float sym = __fmaf_rn(__fmul_rn(rho, t), __fmaf_rn(__fmul_rn(4.5f, cu), cu, base), -t);
+    const float r3t = __fmul_rn(rho, 3 * t);
+    const float plus = __fmaf_rn(r3t, cu, sym), minus = __fmaf_rn(-r3t, cu, sym);
+    f[i] = __fmaf_rn(omega, plus, __fmul_rn(f[i], keep));
+    f[jj] = __fmaf_rn(omega, minus, __fmul_rn(f[jj], keep));
+  });
+  rhoOut = rho;
+  uSqrOut = uSqr;
+}
+
 template <int Q, typename R, int DYN>
 __device__ __forceinline__ void collide(R (&f)[Q], const CollisionParams<R>& p, R& rhoOut, R& uSqrOut) {
   using D = Desc<Q>;
   using T = DynTraits<DYN>;
+  if constexpr (DYN == DYN_BGK && sizeof(R) == 4) {
+    collide_bgk_f32<Q>(f, p.omega, rhoOut, uSqrOut);
+    return;
+  }
   R rho, u[3];
   moments<Q, R, T::forced>(f, p.force, rho, u);
   R uSqr = R(0);
@@ -223,6 +278,93 @@ __device__ __forceinline__ void collide(R (&f)[Q], const CollisionParams<R>& p, 
   }
   rhoOut = rho;
   uSqrOut = uSqr;
+}
+
+// ---- two cells at once: packed FP32 pairs (sm_100 f32x2 arithmetic) ------------------------
+// Each packed operation rounds every lane exactly as the scalar operation does, so a pair of
+// cells computed here gets the same bits as two calls of the scalar float path below: the
+// operation sequence of collide<Q, float, DYN_BGK> is kept step for step.
+struct F2 {
+  float x, y;
+};
+__device__ __forceinline__ F2 f2(float v) { return F2{v, v}; }
+#define LBX_F32X2_BINOP(NAME, OP)                                                                          \
+  __device__ __forceinline__ F2 NAME(F2 a, F2 b) {                                                        \
+    F2 d;                                                                                                 \
+    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2,%3};\n mov.b64 rb, {%4,%5};\n " OP " rd, ra, rb;\n" \
+        " mov.b64 {%0,%1}, rd;\n}\n"                                                                     \
+        : "=f"(d.x), "=f"(d.y)                                                                            \
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                                        \
+    return d;                                                                                             \
+  }
+LBX_F32X2_BINOP(add2, "add.rn.f32x2")
+LBX_F32X2_BINOP(sub2, "sub.rn.f32x2")
+LBX_F32X2_BINOP(mul2, "mul.rn.f32x2")
+#undef LBX_F32X2_BINOP
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+  F2 d;
+  asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2,%3};\n mov.b64 rb, {%4,%5};\n mov.b64 rc, {%6,%7};\n"
+      " fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0,%1}, rd;\n}\n"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+// BGK collision of two cells (f[k][i], k = 0, 1) in place: collide_bgk_f32 on pairs, the same
+// operation sequence (no product ever meets a separate add, so no contraction can differ).
+template <int Q>
+__device__ __forceinline__ void collide_bgk_x2(float (&f)[2][Q], float omega, float (&rhoOut)[2], float (&usqOut)[2]) {
+  using D = Desc<Q>;
+  F2 g[Q];
+  static_for<Q>([&](auto I) { g[I] = F2{f[0][I], f[1][I]}; });
+  F2 rho = f2(0.f);
+  static_for<Q>([&](auto I) { rho = add2(rho, g[I]); });
+  rho = add2(rho, f2(1.f));
+  F2 j[3] = {f2(0.f), f2(0.f), f2(0.f)};
+  static_for<Q>([&](auto I) {
+    static_for<D::d>([&](auto A) {
+      constexpr int c = D::C[I][A];
+      if constexpr (c == 1) j[A] = add2(j[A], g[I]);
+      else if constexpr (c == -1) j[A] = sub2(j[A], g[I]);
+    });
+  });
+  const F2 inv{1.f / rho.x, 1.f / rho.y};
+  F2 u[3];
+  static_for<D::d>([&](auto A) { u[A] = mul2(j[A], inv); });
+  F2 uSqr = mul2(u[0], u[0]);
+  static_for<D::d - 1>([&](auto A) { uSqr = fma2(u[A + 1], u[A + 1], uSqr); });
+  const F2 w = f2(omega);
+  const F2 keep = f2(1.f - omega);
+  const F2 base = fma2(f2(-1.5f), uSqr, f2(1.f));
+  {
+    constexpr float t0 = weight<Q, float>(0);
+    g[0] = fma2(w, fma2(mul2(rho, f2(t0)), base, f2(-t0)), mul2(g[0], keep));
+  }
+  static_for<Q / 2>([&](auto K) {
+    constexpr int i = K + 1;
+    constexpr int jj = D::OPP[i];
+    constexpr float t = weight<Q, float>(i);
+    F2 cj = f2(0.f);
+    static_for<D::d>([&](auto A) {
+      constexpr int c = D::C[i][A];
+      if constexpr (c == 1) cj = add2(cj, j[A]);
+      else if constexpr (c == -1) cj = sub2(cj, j[A]);
+    });
+    const F2 cu = mul2(cj, inv);
+    const F2 sym = fma2(mul2(rho, f2(t)), fma2(mul2(f2(4.5f), cu), cu, base), f2(-t));
+    const F2 r3t = mul2(rho, f2(3 * t));
+    const F2 plus = fma2(r3t, cu, sym), minus = fma2(F2{-r3t.x, -r3t.y}, cu, sym);
+    g[i] = fma2(w, plus, mul2(g[i], keep));
+    g[jj] = fma2(w, minus, mul2(g[jj], keep));
+  });
+  static_for<Q>([&](auto I) {
+    f[0][I] = g[I].x;
+    f[1][I] = g[I].y;
+  });
+  rhoOut[0] = rho.x;
+  rhoOut[1] = rho.y;
+  usqOut[0] = uSqr.x;
+  usqOut[1] = uSqr.y;
 }
 
 template <int Q, typename R>
