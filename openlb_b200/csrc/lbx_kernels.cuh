@@ -743,38 +743,43 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     uint8_t kinds[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) kinds[k] = (k < nvalid) ? (cellDyn ? cellDyn[n0 + k] : uint8_t(1)) : uint8_t(0);
-    // two bulk BGK cells of a 16-bit form: one packed (f32x2) collision, the same bits as two
-    // scalar ones.  The 16-bit forms are limited by instruction issue, where the packed form
-    // halves the collision's arithmetic; the FP32 form waits on HBM, and there the packed form's
-    // extra registers cost more than they save.
-    constexpr bool PACKED = K == 2 && sizeof(R) == 4 && sizeof(S) == 2 && DYN == DYN_BGK;
-    bool packedDone = false;
-    if constexpr (PACKED) {
-      if (kinds[0] == 1 && kinds[1] == 1) {
-        float rr[2], uu[2];
-        collide_bgk_x2<Q>(f, p.omega, rr, uu);
+    // pairs of bulk BGK cells of a 16-bit form: one packed (f32x2) collision per pair, the same
+    // bits as two scalar ones.  The 16-bit forms are limited by instruction issue, where the
+    // packed form halves the collision's arithmetic; the FP32 form waits on HBM, and there the
+    // packed form's extra registers cost more than they save.
+    constexpr bool PACKED = K >= 2 && sizeof(R) == 4 && sizeof(S) == 2 && DYN == DYN_BGK;
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          accRho += double(rr[k]);
-          accUsq += double(uu[k]);
-          accMax = fmax(accMax, double(uu[k]));
-          ++accCount;
+    for (int pr = 0; pr < (K + 1) / 2; ++pr) {
+      const int k0 = 2 * pr, k1 = 2 * pr + 1;
+      bool packedDone = false;
+      if constexpr (PACKED) {
+        if (k1 < K && kinds[k0] == 1 && kinds[k1] == 1) {
+          float rr[2], uu[2];
+          collide_bgk_x2<Q>(*reinterpret_cast<float(*)[2][Q]>(&f[k0]), p.omega, rr, uu);
+#pragma unroll
+          for (int k = 0; k < 2; ++k) {
+            accRho += double(rr[k]);
+            accUsq += double(uu[k]);
+            accMax = fmax(accMax, double(uu[k]));
+            ++accCount;
+          }
+          packedDone = true;
         }
-        packedDone = true;
       }
-    }
-    if (!packedDone) {
+      if (!packedDone) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        if (kinds[k] == 1) {
-          R rho, usq;
-          collide<Q, R, DYN>(f[k], p, rho, usq);
-          accRho += double(rho);
-          accUsq += double(usq);
-          accMax = fmax(accMax, double(usq));
-          ++accCount;
-        } else if (kinds[k] == 2) {
-          revert<Q, R>(f[k]);
+        for (int k = k0; k <= k1; ++k) {
+          if (k >= K) break;
+          if (kinds[k] == 1) {
+            R rho, usq;
+            collide<Q, R, DYN>(f[k], p, rho, usq);
+            accRho += double(rho);
+            accUsq += double(usq);
+            accMax = fmax(accMax, double(usq));
+            ++accCount;
+          } else if (kinds[k] == 2) {
+            revert<Q, R>(f[k]);
+          }
         }
       }
     }
