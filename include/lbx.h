@@ -294,7 +294,7 @@ int lbx_ensemble_moments(lbx_ensemble ens, int32_t slot, double* rho, double* u,
 /* Free a slot and its slab space (no effect on the others). */
 int lbx_ensemble_retire(lbx_ensemble ens, int32_t slot);
 /* Launch shape of the persistent kernel (the autotuner's knob): threads per block (multiple of
- * 32, <= 256; a tile is 256 cells whatever the block size, so results and residuals do not
+ * 32, <= 256; a tile is 512 cells whatever the block size, so results and residuals do not
  * depend on it), resident blocks per SM (0: occupancy maximum), and the residual check interval
  * in steps. */
 int lbx_ensemble_set_config(lbx_ensemble ens, int32_t threads, int32_t blocks_per_sm, int32_t check_interval);
@@ -303,6 +303,10 @@ int lbx_ensemble_set_config(lbx_ensemble ens, int32_t threads, int32_t blocks_pe
  * CUDA graph (the launch boundaries order the steps, and populations may then be read through
  * L1).  Both give identical results. */
 int lbx_ensemble_set_launch_mode(lbx_ensemble ens, int32_t mode);
+/* Cells per thread of the tile loop, 1 (default) or 2: a warp steps 32 * cells consecutive
+ * cells of a tile per round, keeping that many loads in flight per thread.  Both give identical
+ * results. */
+int lbx_ensemble_set_cells_per_thread(lbx_ensemble ens, int32_t cells);
 
 /* ---- autotuner ----------------------------------------------------------------------------
  * No reference counterpart (the reference's CUDA platform launches fixed 32-thread blocks,
@@ -317,7 +321,9 @@ int lbx_ensemble_set_launch_mode(lbx_ensemble ens, int32_t mode);
  * ms_per_step < 0 marks a shape the device or the lattice does not accept. */
 typedef struct {
   int32_t variant, block_x, block_y, cells_per_thread;  /* lbx_autotune: lbx_set_launch_config;
-                                                           lbx_ensemble_autotune: variant = launch mode */
+                                                           lbx_ensemble_autotune: variant = launch
+                                                           mode, cells_per_thread as set by
+                                                           lbx_ensemble_set_cells_per_thread */
   int32_t threads, blocks_per_sm;                       /* lbx_ensemble_autotune: set_config */
   double ms_per_step;
 } lbx_tune_entry;

@@ -3,10 +3,10 @@
 // Each admitted request owns a region of one device slab: Q population columns of period P
 // (its padded cell count rounded up to 64; the periodic-shift layout of lbx_kernels.cuh, the
 // ghost layer being the walls) and a velocity snapshot for the convergence residual.  A tile
-// is up to 2048 consecutive core cells of one lattice; the persistent kernel runs
-// `steps` steps, in each of which its blocks stride over the tile list, and two grid-wide
-// barriers per step separate the steps from the per-lattice bookkeeping done by block 0
-// (column shifts of the next step, step count, residual, state).  Lattices stop on their own
+// is up to 512 consecutive core cells of one lattice; the persistent kernel runs `steps`
+// steps, in each of which its warps claim tiles from a counter and step them, and two
+// grid-wide barriers per step separate the steps from the per-lattice bookkeeping done by
+// block 0 (column shifts of the next step, step count, residual, state).  Lattices stop on their own
 // residual and are retired by the host between runs while the others keep going, so requests
 // of different sizes and ages are stepped together.
 //
@@ -44,7 +44,7 @@ namespace {
 using namespace lbx;
 
 constexpr int kMaxQ = 27;
-constexpr int kTileCells = 2048;  // cells per tile, independent of the block size
+constexpr int kTileCells = 512;  // cells per tile, independent of the launch shape
 
 struct EnsLattice {
   void* pop;        // column 0; column i starts at element i * P
@@ -71,6 +71,7 @@ struct EnsArgs {
   const int* nTiles;
   const int2* range;       // per slot {first tile, tile count}
   double* tilePart;        // {sum |du|^2, sum |u|^2} per tile at check steps
+  int* tileCounter;        // tiles claimed so far in this step
   unsigned* barrier;       // {arrived, generation}
   int* err;
   long long* globalStep;
@@ -139,12 +140,16 @@ __device__ bool grid_barrier(unsigned* barrier, int* err) {
   return ok != 0;
 }
 
-// Resident 256-thread blocks per SM the register budget is cut for: three for the 32- and
-// 16-bit D3Q19 forms (80 registers; a few bytes spill), the compiler's choice otherwise.
-template <int Q, typename S> struct EnsOccupancy { static constexpr int blocks = 1; };
-template <> struct EnsOccupancy<19, float> { static constexpr int blocks = 3; };
-template <> struct EnsOccupancy<19, __half> { static constexpr int blocks = 3; };
-template <> struct EnsOccupancy<19, __nv_bfloat16> { static constexpr int blocks = 3; };
+// Resident 256-thread blocks per SM the register budget is cut for: one cell per thread, three
+// for the 32- and 16-bit D3Q19 forms (80 registers); two cells per thread, two blocks (128
+// registers); the compiler's choice otherwise.
+template <int Q, typename S, int K> struct EnsOccupancy { static constexpr int blocks = 1; };
+template <> struct EnsOccupancy<19, float, 1> { static constexpr int blocks = 3; };
+template <> struct EnsOccupancy<19, __half, 1> { static constexpr int blocks = 3; };
+template <> struct EnsOccupancy<19, __nv_bfloat16, 1> { static constexpr int blocks = 3; };
+template <> struct EnsOccupancy<19, float, 2> { static constexpr int blocks = 2; };
+template <> struct EnsOccupancy<19, __half, 2> { static constexpr int blocks = 2; };
+template <> struct EnsOccupancy<19, __nv_bfloat16, 2> { static constexpr int blocks = 2; };
 
 // Loads of populations inside a step: through L1 when every step is its own launch (the L1
 // starts clean at each launch), around it (ld.global.cg) in the persistent kernel, where a
@@ -156,42 +161,55 @@ template <typename S, bool CACHED> struct EnsLoad {
   }
 };
 
-// Per-block scratch of the tile loop.
-template <int Q, typename S> struct EnsShared {
-  uint32_t sShift[Q];
-  float sDelta[Q];
-  // column i's base pointer with the shift folded in, valid for every cell of the tile when
-  // sWrap == 0 (no column's cyclic wrap point falls inside the tile's index range)
-  S* sCol[Q];
-  int sWrap;
-  double red[2][kTileCells / 32];
+// Per-warp scratch of the tile loop: each warp steps whole tiles on its own.
+template <int Q, typename S> struct EnsWarp {
+  // column i's base pointer with the shift folded in, valid for every cell of the tile when no
+  // column's cyclic wrap point falls inside the tile's index range ("straight" tiles)
+  S* col[Q];
+  uint32_t shift[Q];
+  float delta[Q];
 };
+constexpr int kMaxWarps = 8;  // 256 threads
 
-// One step of every running lattice: this block's share of the tile list.
-template <int Q, typename S, bool CACHED>
-__device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nTiles, EnsShared<Q, S>& sm) {
+// Core faces a cell lies on: bit 2a for the low face of axis a, bit 2a + 1 for the high one.
+__device__ __forceinline__ int face_mask(int x, int y, int z, int nx, int ny, int nz) {
+  return int(x == 0) | (int(x == nx - 1) << 1) | (int(y == 0) << 2) | (int(y == ny - 1) << 3) | (int(z == 0) << 4) |
+         (int(z == nz - 1) << 5);
+}
+// Faces through which direction (cx, cy, cz) leaves the core from a cell lying on them.
+constexpr int leaving_faces(int cx, int cy, int cz) {
+  return (cx < 0 ? 1 : 0) | (cx > 0 ? 2 : 0) | (cy < 0 ? 4 : 0) | (cy > 0 ? 8 : 0) | (cz < 0 ? 16 : 0) |
+         (cz > 0 ? 32 : 0);
+}
+
+// One step of every running lattice.  Each warp claims tiles from a shared counter until the
+// list is exhausted and steps each claimed tile alone (no block-wide barrier): its lanes read
+// the lattice's column shifts into the warp's scratch, then the warp walks the tile in 32-cell
+// slots, K consecutive slots per round, lane l holding cell l of each, so every load and store
+// instruction covers 32 consecutive cells.  Each slot's residual terms are reduced by a fixed
+// shuffle tree and summed over the tile in slot order: neither the populations nor the residual
+// depend on the launch shape, K or which warp stepped which tile.
+template <int Q, typename S, bool CACHED, int K>
+__device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nTiles, EnsWarp<Q, S>& w) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
-  uint32_t* sShift = sm.sShift;
-  float* sDelta = sm.sDelta;
-  S** sCol = sm.sCol;
-  int& sWrap = sm.sWrap;
-  double (*red)[kTileCells / 32] = sm.red;
-  const int tid = threadIdx.x;
-  for (int tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tileCounter, 1);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= nTiles) break;
     const int2 t = a.tiles[tile];
     EnsLattice* L = a.lat + t.x;
-    const int state = __ldcg(&L->state);
-    if (state != LBX_SLOT_RUNNING) continue;  // uniform over the block
+    if (__ldcg(&L->state) != LBX_SLOT_RUNNING) continue;  // uniform over the warp
     const int64_t steps = __ldcg(reinterpret_cast<const long long*>(&L->steps));
     const bool check = ((steps + 1) % a.check) == 0;
-    __syncthreads();  // the previous tile's readers of sShift/sDelta are done
-    if (tid == 0) sWrap = 0;
-    __syncthreads();
-    if (tid < Q) {
-      const uint32_t sh = __ldcg(&L->shift[par][tid]);
-      sShift[tid] = sh;
-      sDelta[tid] = __ldcg(&L->delta[tid]);
+    __syncwarp();  // the previous tile's readers of the scratch are done
+    bool wraps = false;
+    if (lane < Q) {
+      const uint32_t sh = __ldcg(&L->shift[par][lane]);
+      w.shift[lane] = sh;
+      w.delta[lane] = __ldcg(&L->delta[lane]);
       // padded index range of the tile's cells: rows of the first and the last cell
       const int c0 = t.y, c1 = min(t.y + kTileCells, L->ncore) - 1;
       const uint32_t q0 = FastDiv::div(uint32_t(c0), L->mz, L->lz), q1 = FastDiv::div(uint32_t(c1), L->mz, L->lz);
@@ -203,15 +221,15 @@ __device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nT
       const uint32_t P = L->P;
       // the bounce-back stores reach one padded row beyond the tile's range on either side
       const uint32_t span = uint32_t(L->sx) + uint32_t(L->sy) + 1;
-      const int64_t a = int64_t(lo) - span + sh, b = int64_t(hi) + span + sh;
-      int64_t off;
-      if (b < int64_t(P) && a >= 0) off = sh;
-      else if (a >= int64_t(P)) off = int64_t(sh) - int64_t(P);
-      else { off = 0; atomicOr(&sWrap, 1); }
-      sCol[tid] = static_cast<S*>(L->pop) + int64_t(tid) * int64_t(P) + off;
+      const int64_t a0 = int64_t(lo) - span + sh, b0 = int64_t(hi) + span + sh;
+      int64_t off = 0;
+      if (b0 < int64_t(P) && a0 >= 0) off = sh;
+      else if (a0 >= int64_t(P)) off = int64_t(sh) - int64_t(P);
+      else wraps = true;
+      w.col[lane] = static_cast<S*>(L->pop) + int64_t(lane) * int64_t(P) + off;
     }
-    __syncthreads();
-    const bool straight = sWrap == 0;  // uniform over the block
+    const bool straight = !__any_sync(0xffffffffu, wraps);
+    __syncwarp();
     const uint32_t P = L->P;
     const int nx = L->nx, ny = L->ny, nz = L->nz, sx = L->sx, sy = L->sy;
     const uint32_t mz = L->mz, my = L->my;
@@ -225,143 +243,191 @@ __device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nT
     cp.smagorinsky = R(0);
     cp.force[0] = cp.force[1] = cp.force[2] = R(0);
     const int dyn = L->dynamics;
-    // The block walks the tile's cells in rounds of blockDim.x; each warp's 32 consecutive
-    // cells form one residual slot, reduced by the same shuffle tree whatever the block size,
-    // so the residual does not depend on the launch shape.
-    const int rounds = (last + 31) / 32 * 32;
-    for (int cl = tid; cl < rounds; cl += blockDim.x) {
-      double du2 = 0.0, u2 = 0.0;
-      const int c = t.y + cl;
-      if (cl < last) {
-        const uint32_t xy = FastDiv::div(uint32_t(c), mz, lz);
-        const int z = c - int(xy) * nz;
-        const int x = int(FastDiv::div(xy, my, ly));
-        const int y = int(xy) - x * ny;
-        const uint32_t n = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
-        R f[Q];
-        if (straight) static_for<Q>([&](auto I) { f[I] = EnsLoad<S, CACHED>::ld(sCol[I] + n); });
-        else static_for<Q>([&](auto I) { f[I] = EnsLoad<S, CACHED>::ld(pop + I * int64_t(P) + wrap32(n + sShift[I], P)); });
+    const int slots = (last + 31) / 32;
+    double tileDu2 = 0.0, tileU2 = 0.0;  // the tile's sums, slot by slot
+    for (int g = 0; g < slots; g += K) {
+      uint32_t n[K];
+      int fm[K];  // face mask of the lane's cell in slot g + k; -1: no cell
+      double du2[K], u2[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        du2[k] = 0.0;
+        u2[k] = 0.0;
+        n[k] = 0;
+        fm[k] = -1;
+        const int cl = (g + k) * 32 + lane;
+        if (cl < last) {
+          const int c = t.y + cl;
+          const uint32_t xy = FastDiv::div(uint32_t(c), mz, lz);
+          const int z = c - int(xy) * nz;
+          const int x = int(FastDiv::div(xy, my, ly));
+          const int y = int(xy) - x * ny;
+          n[k] = uint32_t((x + 1) * sx + (y + 1) * sy + z + 1);
+          fm[k] = face_mask(x, y, z, nx, ny, nz);
+        }
+      }
+      R f[K][Q];
+      if (straight) {
+        static_for<Q>([&](auto I) {
+          const S* col = w.col[I];
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (fm[k] >= 0) f[k][I] = EnsLoad<S, CACHED>::ld(col + n[k]);
+        });
+      } else {
+        static_for<Q>([&](auto I) {
+          const uint32_t sh = w.shift[I];
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (fm[k] >= 0) f[k][I] = EnsLoad<S, CACHED>::ld(pop + I * int64_t(P) + wrap32(n[k] + sh, P));
+        });
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (fm[k] < 0) continue;
         if (check) {
           R rho, u[3];
-          moments<Q, R, false>(f, nullptr, rho, u);
+          moments<Q, R, false>(f[k], nullptr, rho, u);
           float* snap = L->snap;
+          const int c = t.y + (g + k) * 32 + lane;
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
             const double cur = double(u[d]);
             const double dd = cur - double(__ldcg(snap + int64_t(d) * ncore + c));
-            du2 += dd * dd;
-            u2 += cur * cur;
+            du2[k] += dd * dd;
+            u2[k] += cur * cur;
             snap[int64_t(d) * ncore + c] = float(cur);
           }
         }
         R rho, usq;
-        if (dyn == LBX_TRT) collide<Q, R, DYN_TRT>(f, cp, rho, usq);
-        else collide<Q, R, DYN_BGK>(f, cp, rho, usq);
-        if (!(usq == usq) || usq > R(1)) du2 = __longlong_as_double(0x7ff8000000000000ll);  // NaN flags divergence
-        // store addresses recomputed from shared memory (volatile: not kept live in registers
-        // across the collision, which would cost two registers per population)
-        if (straight) {
-          static_for<Q>([&](auto I) { Storage<S>::store(*reinterpret_cast<S* volatile*>(&sCol[I]) + n, f[I]); });
-        } else {
-          static_for<Q>([&](auto I) {
-            const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&sShift[I]);
-            Storage<S>::store(pop + I * int64_t(P) + wrap32(n + sh, P), f[I]);
-          });
-        }
-        // Halfway bounce-back of the links that leave the core: the population sent into the
-        // wall comes back as the opposite one, written where the next step's load of this
-        // cell finds it (the slot of ghost cell x + c_K in column opp(K) at this step's shift).
-        if (x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || z == 0 || z == nz - 1) {
-          static_for<Q>([&](auto K) {
-            constexpr int cx = D::C[K][0], cy = D::C[K][1], cz = D::C[K][2];
-            if constexpr (cx != 0 || cy != 0 || cz != 0) {
-              const int tx = x + cx, ty = y + cy, tz = z + cz;
-              if (tx < 0 || tx >= nx || ty < 0 || ty >= ny || tz < 0 || tz >= nz) {
-                constexpr int O = D::OPP[K];
-                const uint32_t gh = uint32_t(int(n) + cx * sx + cy * sy + cz);
-                const R v = f[K] - (ty == ny ? R(sDelta[K]) : R(0));
-                if (straight) {
-                  Storage<S>::store(*reinterpret_cast<S* volatile*>(&sCol[O]) + gh, v);
-                } else {
-                  const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&sShift[O]);
-                  Storage<S>::store(pop + O * int64_t(P) + wrap32(gh + sh, P), v);
-                }
+        if (dyn == LBX_TRT) collide<Q, R, DYN_TRT>(f[k], cp, rho, usq);
+        else collide<Q, R, DYN_BGK>(f[k], cp, rho, usq);
+        if (!(usq == usq) || usq > R(1)) du2[k] = __longlong_as_double(0x7ff8000000000000ll);  // NaN flags divergence
+      }
+      // store addresses re-read from shared memory (volatile: not kept live in registers
+      // across the collision, which would cost two registers per population)
+      if (straight) {
+        static_for<Q>([&](auto I) {
+          S* col = *reinterpret_cast<S* volatile*>(&w.col[I]);
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (fm[k] >= 0) Storage<S>::store(col + n[k], f[k][I]);
+        });
+      } else {
+        static_for<Q>([&](auto I) {
+          const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&w.shift[I]);
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            if (fm[k] >= 0) Storage<S>::store(pop + I * int64_t(P) + wrap32(n[k] + sh, P), f[k][I]);
+        });
+      }
+      // Halfway bounce-back of the links that leave the core: the population sent into the
+      // wall comes back as the opposite one, written where the next step's load of this cell
+      // finds it (the slot of ghost cell x + c_J in column opp(J) at this step's shift).
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (fm[k] <= 0) continue;
+        static_for<Q>([&](auto J) {
+          constexpr int cx = D::C[J][0], cy = D::C[J][1], cz = D::C[J][2];
+          constexpr int leaves = leaving_faces(cx, cy, cz);
+          if constexpr (leaves != 0) {
+            if (fm[k] & leaves) {
+              constexpr int O = D::OPP[J];
+              const uint32_t gh = uint32_t(int(n[k]) + cx * sx + cy * sy + cz);
+              // through the +y face: the moving lid
+              const R v = f[k][J] - ((cy > 0 && (fm[k] & 8)) ? R(w.delta[J]) : R(0));
+              if (straight) {
+                Storage<S>::store(*reinterpret_cast<S* volatile*>(&w.col[O]) + gh, v);
+              } else {
+                const uint32_t sh = *reinterpret_cast<volatile uint32_t*>(&w.shift[O]);
+                Storage<S>::store(pop + O * int64_t(P) + wrap32(gh + sh, P), v);
               }
             }
-          });
-        }
+          }
+        });
       }
       if (check) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          du2 += __shfl_xor_sync(0xffffffffu, du2, o);
-          u2 += __shfl_xor_sync(0xffffffffu, u2, o);
-        }
-        if ((tid & 31) == 0) {
-          red[0][cl >> 5] = du2;
-          red[1][cl >> 5] = u2;
+        for (int k = 0; k < K; ++k) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            du2[k] += __shfl_xor_sync(0xffffffffu, du2[k], o);
+            u2[k] += __shfl_xor_sync(0xffffffffu, u2[k], o);
+          }
+          if (g + k < slots) {
+            tileDu2 += du2[k];
+            tileU2 += u2[k];
+          }
         }
       }
     }
-    if (check) {
-      __syncthreads();
-      if (tid == 0) {
-        double s0 = 0, s1 = 0;
-        for (int w = 0; w < (last + 31) / 32; ++w) {
-          s0 += red[0][w];
-          s1 += red[1][w];
-        }
-        a.tilePart[2 * int64_t(tile)] = s0;
-        a.tilePart[2 * int64_t(tile) + 1] = s1;
-      }
+    if (check && lane == 0) {
+      a.tilePart[2 * int64_t(tile)] = tileDu2;
+      a.tilePart[2 * int64_t(tile) + 1] = tileU2;
     }
   }
 }
 
-// Per-lattice bookkeeping after a step (one block): step count, the next step's column shifts,
-// and at check steps the residual (tile partials summed in tile order) and the state.
+// Per-lattice bookkeeping after a step (one block, a warp per lattice): step count, the next
+// step's column shifts, and at check steps the residual and the state.  The residual sums the
+// lattice's tile partials in a fixed order (lane l takes tiles l, l + 32, ..., then a shuffle
+// tree), which depends on neither the block size nor the launch mode.  Thread 0 also resets the
+// tile counter for the next step.
 template <int Q>
 __device__ __forceinline__ void ensemble_book(const EnsArgs& a, int par) {
   using D = Desc<Q>;
-  for (int s = threadIdx.x; s < a.maxLattices; s += blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) *a.tileCounter = 0;
+  for (int s = threadIdx.x >> 5; s < a.maxLattices; s += blockDim.x >> 5) {
     EnsLattice* L = a.lat + s;
-    if (__ldcg(&L->state) != LBX_SLOT_RUNNING) continue;
+    if (__ldcg(&L->state) != LBX_SLOT_RUNNING) continue;  // uniform over the warp
     const int64_t steps = __ldcg(reinterpret_cast<const long long*>(&L->steps));
     const bool check = ((steps + 1) % a.check) == 0;
-    L->steps = steps + 1;
     const uint32_t P = L->P;
     const int sx = L->sx, sy = L->sy;
     static_for<Q>([&](auto I) {
-      const int64_t off = D::C[I][0] * int64_t(sx) + D::C[I][1] * int64_t(sy) + D::C[I][2];
-      int64_t ns = (int64_t(__ldcg(&L->shift[par][I])) - off) % int64_t(P);
-      if (ns < 0) ns += P;
-      L->shift[par ^ 1][I] = uint32_t(ns);
+      if (lane == I) {
+        const int64_t off = D::C[I][0] * int64_t(sx) + D::C[I][1] * int64_t(sy) + D::C[I][2];
+        int64_t ns = (int64_t(__ldcg(&L->shift[par][I])) - off) % int64_t(P);
+        if (ns < 0) ns += P;
+        L->shift[par ^ 1][I] = uint32_t(ns);
+      }
     });
     int state = LBX_SLOT_RUNNING;
+    double res = 0.0;
     if (check) {
       const int2 r = a.range[s];
       double s0 = 0, s1 = 0;
-      for (int k = 0; k < r.y; ++k) {
+      for (int k = lane; k < r.y; k += 32) {
         s0 += __ldcg(a.tilePart + 2 * int64_t(r.x + k));
         s1 += __ldcg(a.tilePart + 2 * int64_t(r.x + k) + 1);
       }
-      const double res = s1 > 0 ? sqrt(s0 / s1) : (s0 > 0 ? INFINITY : 0.0);
-      L->residual = res;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      }
+      res = s1 > 0 ? sqrt(s0 / s1) : (s0 > 0 ? INFINITY : 0.0);
       if (!(res == res) || !(s1 == s1) || isinf(s1)) state = LBX_SLOT_DIVERGED;
       else if (res < L->tol) state = LBX_SLOT_CONVERGED;
     }
     if (state == LBX_SLOT_RUNNING && steps + 1 >= L->maxSteps) state = LBX_SLOT_MAX_STEPS;
-    if (state != LBX_SLOT_RUNNING) L->state = state;
+    __syncwarp();  // every lane has read the step count and the state
+    if (lane == 0) {
+      L->steps = steps + 1;
+      if (check) L->residual = res;
+      if (state != LBX_SLOT_RUNNING) L->state = state;
+    }
   }
 }
 
-template <int Q, typename S>
-__global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble(EnsArgs a) {
-  __shared__ EnsShared<Q, S> sm;
+template <int Q, typename S, int K>
+__global__ void __launch_bounds__(256, EnsOccupancy<Q, S, K>::blocks) k_ensemble(EnsArgs a) {
+  __shared__ EnsWarp<Q, S> scratch[kMaxWarps];
   for (int step = 0; step < a.steps; ++step) {
     const long long g = *reinterpret_cast<volatile long long*>(a.globalStep);
     const int par = int(g & 1);
-    ensemble_tiles<Q, S, false>(a, par, *a.nTiles, sm);
+    ensemble_tiles<Q, S, false, K>(a, par, *a.nTiles, scratch[threadIdx.x >> 5]);
     if (!grid_barrier(a.barrier, a.err)) return;
     if (blockIdx.x == 0) {
       ensemble_book<Q>(a, par);
@@ -373,11 +439,11 @@ __global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble(En
 
 // The same step as one ordinary launch (launch mode 1: a CUDA graph chains step and
 // bookkeeping launches; the launch boundaries order the blocks, so no grid barrier is needed).
-template <int Q, typename S>
-__global__ void __launch_bounds__(256, EnsOccupancy<Q, S>::blocks) k_ensemble_step(EnsArgs a) {
-  __shared__ EnsShared<Q, S> sm;
+template <int Q, typename S, int K>
+__global__ void __launch_bounds__(256, EnsOccupancy<Q, S, K>::blocks) k_ensemble_step(EnsArgs a) {
+  __shared__ EnsWarp<Q, S> scratch[kMaxWarps];
   const long long g = *a.globalStep;
-  ensemble_tiles<Q, S, true>(a, int(g & 1), *a.nTiles, sm);
+  ensemble_tiles<Q, S, true, K>(a, int(g & 1), *a.nTiles, scratch[threadIdx.x >> 5]);
 }
 
 template <int Q>
@@ -460,25 +526,36 @@ using MomentsFn = void (*)(const EnsLattice*, const long long*, double*, double*
 using InitFn = void (*)(const EnsLattice*);
 using BookFn = void (*)(EnsArgs);
 
+// Kernels of one (Q, storage) pair; persistent[k] and step[k] take k + 1 cells per thread.
+struct EnsKernels {
+  KernelFn persistent[2] = {nullptr, nullptr};
+  KernelFn step[2] = {nullptr, nullptr};
+  MomentsFn moments = nullptr;
+  InitFn init = nullptr;
+  BookFn book = nullptr;
+};
+
 template <int Q, typename S>
-void pick(KernelFn& k, MomentsFn& m, InitFn& i, KernelFn& step, BookFn& book) {
-  k = k_ensemble<Q, S>;
-  m = k_ensemble_moments<Q, S>;
-  i = k_ensemble_init_links<Q, S>;
-  step = k_ensemble_step<Q, S>;
-  book = k_ensemble_book<Q>;
+void pick(EnsKernels& k) {
+  k.persistent[0] = k_ensemble<Q, S, 1>;
+  k.persistent[1] = k_ensemble<Q, S, 2>;
+  k.step[0] = k_ensemble_step<Q, S, 1>;
+  k.step[1] = k_ensemble_step<Q, S, 2>;
+  k.moments = k_ensemble_moments<Q, S>;
+  k.init = k_ensemble_init_links<Q, S>;
+  k.book = k_ensemble_book<Q>;
 }
 
-bool kernels_for(int q, int storage, KernelFn& k, MomentsFn& m, InitFn& i, KernelFn& step, BookFn& book) {
+bool kernels_for(int q, int storage, EnsKernels& k) {
   switch (q * 4 + storage) {
-  case 19 * 4 + LBX_F64: pick<19, double>(k, m, i, step, book); return true;
-  case 19 * 4 + LBX_F32: pick<19, float>(k, m, i, step, book); return true;
-  case 19 * 4 + LBX_F16DEV: pick<19, __half>(k, m, i, step, book); return true;
-  case 19 * 4 + LBX_BF16DEV: pick<19, __nv_bfloat16>(k, m, i, step, book); return true;
-  case 27 * 4 + LBX_F64: pick<27, double>(k, m, i, step, book); return true;
-  case 27 * 4 + LBX_F32: pick<27, float>(k, m, i, step, book); return true;
-  case 27 * 4 + LBX_F16DEV: pick<27, __half>(k, m, i, step, book); return true;
-  case 27 * 4 + LBX_BF16DEV: pick<27, __nv_bfloat16>(k, m, i, step, book); return true;
+  case 19 * 4 + LBX_F64: pick<19, double>(k); return true;
+  case 19 * 4 + LBX_F32: pick<19, float>(k); return true;
+  case 19 * 4 + LBX_F16DEV: pick<19, __half>(k); return true;
+  case 19 * 4 + LBX_BF16DEV: pick<19, __nv_bfloat16>(k); return true;
+  case 27 * 4 + LBX_F64: pick<27, double>(k); return true;
+  case 27 * 4 + LBX_F32: pick<27, float>(k); return true;
+  case 27 * 4 + LBX_F16DEV: pick<27, __half>(k); return true;
+  case 27 * 4 + LBX_BF16DEV: pick<27, __nv_bfloat16>(k); return true;
   default: return false;
   }
 }
@@ -516,6 +593,7 @@ struct lbx_ensemble_s {
   int2* dTiles = nullptr;
   int2* dRange = nullptr;
   int* dNTiles = nullptr;
+  int* dTileCounter = nullptr;
   double* dTilePart = nullptr;
   int tileCapacity = 0;
   unsigned* dBarrier = nullptr;
@@ -524,12 +602,10 @@ struct lbx_ensemble_s {
   bool dirty = true;
   int threads = 256, blocksPerSM = 0, check = 100;
   int grid = 0;
-  KernelFn kernel = nullptr;
-  MomentsFn momentsKernel = nullptr;
-  InitFn initKernel = nullptr;
-  KernelFn stepKernel = nullptr;  // launch mode 1: one launch per step ...
-  BookFn bookKernel = nullptr;    // ... and one bookkeeping launch, chained in a CUDA graph
-  int mode = 0;                   // 0: persistent cooperative kernel, 1: per-step launches
+  EnsKernels kern;
+  int mode = 0;   // 0: persistent cooperative kernel, 1: per-step launches and a bookkeeping
+                  // launch each, chained in a CUDA graph
+  int cells = 1;  // cells per thread of the tile loop (1 or 2)
   std::map<int, cudaGraphExec_t> graphs;
   cudaGraph_t graphTemplate = nullptr;
 };
@@ -569,10 +645,14 @@ void drop_graphs(lbx_ensemble_s* E) {
   E->graphs.clear();
 }
 
+KernelFn launch_kernel(const lbx_ensemble_s* E) {
+  return E->mode ? E->kern.step[E->cells - 1] : E->kern.persistent[E->cells - 1];
+}
+
 int ensure_grid(lbx_ensemble_s* E) {
   if (E->grid > 0) return LBX_OK;
   int perSM = 0, sms = 0;
-  ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, E->mode ? E->stepKernel : E->kernel, E->threads, 0));
+  ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, launch_kernel(E), E->threads, 0));
   ENS_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device));
   if (E->blocksPerSM > 0) perSM = std::min(perSM, E->blocksPerSM);
   if (perSM < 1) return lbx::set_error(LBX_ERR_UNSUPPORTED, "ensemble kernel does not fit on an SM");
@@ -647,13 +727,15 @@ int lbx_ensemble_create(int32_t q, int32_t storage, int64_t slab_bytes, int32_t 
   E->slotBytes.assign(size_t(max_lattices), 0);
   E->slotUsed.assign(size_t(max_lattices), 0);
   E->slotCells.assign(size_t(max_lattices), 0);
-  kernels_for(q, storage, E->kernel, E->momentsKernel, E->initKernel, E->stepKernel, E->bookKernel);
+  kernels_for(q, storage, E->kern);
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&E->slab), size_t(E->slabBytes));
   if (e == cudaSuccess) e = cudaMalloc(&E->dLat, size_t(max_lattices) * sizeof(EnsLattice));
   if (e == cudaSuccess) e = cudaMemset(E->dLat, 0, size_t(max_lattices) * sizeof(EnsLattice));
   if (e == cudaSuccess) e = cudaMalloc(&E->dRange, size_t(max_lattices) * sizeof(int2));
   if (e == cudaSuccess) e = cudaMalloc(&E->dNTiles, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(E->dNTiles, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&E->dTileCounter, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(E->dTileCounter, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&E->dBarrier, 2 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(E->dBarrier, 0, 2 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc(&E->dErr, sizeof(int));
@@ -680,6 +762,7 @@ int lbx_ensemble_destroy(lbx_ensemble E) {
   cudaFree(E->dTiles);
   cudaFree(E->dRange);
   cudaFree(E->dNTiles);
+  cudaFree(E->dTileCounter);
   cudaFree(E->dTilePart);
   cudaFree(E->dBarrier);
   cudaFree(E->dErr);
@@ -714,6 +797,17 @@ int lbx_ensemble_set_launch_mode(lbx_ensemble E, int32_t mode) {
   return LBX_OK;
 }
 
+int lbx_ensemble_set_cells_per_thread(lbx_ensemble E, int32_t cells) {
+  if (!E) return lbx::set_error(LBX_ERR_INVALID, "null ensemble");
+  if (cells != 1 && cells != 2) return lbx::set_error(LBX_ERR_INVALID, "cells per thread must be 1 or 2");
+  DeviceScope scope(E->device);
+  cudaDeviceSynchronize();
+  E->cells = cells;
+  E->grid = 0;
+  drop_graphs(E);
+  return LBX_OK;
+}
+
 int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, int32_t capacity, int32_t* n_out,
                           void* stream) {
   if (!E) return lbx::set_error(LBX_ERR_INVALID, "null ensemble");
@@ -724,19 +818,22 @@ int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, in
   if (hi == 0) return lbx::set_error(LBX_ERR_STATE, "autotune needs at least one admitted lattice");
   DeviceScope scope(E->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // Candidates: block sizes 64..256, resident blocks per SM from 1 to the occupancy maximum
-  // (the grid, and with it the cost of each grid barrier, grows with both).
-  struct Cand { int mode, threads, perSM; };
+  // Candidates: both launch modes, one or two cells per thread, block sizes 64..256, resident
+  // blocks per SM from 1 to the occupancy maximum (the grid, and with it the cost of each grid
+  // barrier, grows with both).
+  struct Cand { int mode, cells, threads, perSM; };
   std::vector<Cand> cands;
   for (int mode = 0; mode <= 1; ++mode)
-    for (int threads = 64; threads <= 256; threads *= 2) {
-      int maxPerSM = 0;
-      ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxPerSM, mode ? E->stepKernel : E->kernel, threads, 0));
-      for (int b = 1; b <= std::min(maxPerSM, 8); b *= 2) cands.push_back({mode, threads, b});
-      if (maxPerSM > 8) cands.push_back({mode, threads, maxPerSM});
-    }
+    for (int cells = 1; cells <= 2; ++cells)
+      for (int threads = 64; threads <= 256; threads *= 2) {
+        int maxPerSM = 0;
+        KernelFn fn = mode ? E->kern.step[cells - 1] : E->kern.persistent[cells - 1];
+        ENS_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&maxPerSM, fn, threads, 0));
+        for (int b = 1; b <= std::min(maxPerSM, 8); b *= 2) cands.push_back({mode, cells, threads, b});
+        if (maxPerSM > 8) cands.push_back({mode, cells, threads, maxPerSM});
+      }
   if (n_out) *n_out = int32_t(cands.size());
-  const Cand keep{E->mode, E->threads, E->blocksPerSM};
+  const Cand keep{E->mode, E->cells, E->threads, E->blocksPerSM};
   const size_t latBytes = size_t(E->maxLattices) * sizeof(EnsLattice);
   char* saved = nullptr;
   cudaError_t e = cudaMalloc(&saved, size_t(hi) + latBytes + sizeof(long long));
@@ -766,6 +863,7 @@ int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, in
   float bestMs = 0.f;
   auto apply = [&](const Cand& c) {
     E->mode = c.mode;
+    E->cells = c.cells;
     E->threads = c.threads;
     E->blocksPerSM = c.perSM;
     E->grid = 0;
@@ -796,7 +894,7 @@ int lbx_ensemble_autotune(lbx_ensemble E, int32_t steps, lbx_tune_entry* out, in
     } else if (kerr != 0) {
       ms = -1.f;
     }
-    if (out && int32_t(i) < capacity) out[i] = lbx_tune_entry{c.mode, 0, 0, 0, c.threads, c.perSM, double(ms)};
+    if (out && int32_t(i) < capacity) out[i] = lbx_tune_entry{c.mode, 0, 0, c.cells, c.threads, c.perSM, double(ms)};
   }
   const std::string err = rc != LBX_OK ? std::string(lbx_last_error()) : std::string();
   cudaError_t e2 = cudaStreamSynchronize(s);
@@ -864,7 +962,7 @@ int lbx_ensemble_admit(lbx_ensemble E, const lbx_ensemble_request* req, int32_t*
   if (e == cudaSuccess) e = cudaMemcpy(E->dLat + s, &L, sizeof(L), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
     const int lid = L.nx * L.nz;
-    E->initKernel<<<(lid + 255) / 256, 256>>>(E->dLat + s);
+    E->kern.init<<<(lid + 255) / 256, 256>>>(E->dLat + s);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -911,6 +1009,7 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
     a.nTiles = E->dNTiles;
     a.range = E->dRange;
     a.tilePart = E->dTilePart;
+    a.tileCounter = E->dTileCounter;
     a.barrier = E->dBarrier;
     a.err = E->dErr;
     a.globalStep = E->dGlobalStep;
@@ -934,12 +1033,13 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaMemsetAsync(E->dErr, 0, sizeof(int), cap);
+    if (e == cudaSuccess) e = cudaMemsetAsync(E->dTileCounter, 0, sizeof(int), cap);
     if (E->mode == 0) {
-      if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, E->kernel, a);
+      if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, launch_kernel(E), a);
     } else {
       for (int k = 0; k < steps && e == cudaSuccess; ++k) {
-        E->stepKernel<<<unsigned(E->grid), unsigned(E->threads), 0, cap>>>(a);
-        E->bookKernel<<<1, 256, 0, cap>>>(a);
+        launch_kernel(E)<<<unsigned(E->grid), unsigned(E->threads), 0, cap>>>(a);
+        E->kern.book<<<1, 256, 0, cap>>>(a);
         e = cudaGetLastError();
       }
     }
@@ -954,12 +1054,13 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
       cudaGetLastError();
       cfg.stream = s;
       ENS_TRY(cudaMemsetAsync(E->dErr, 0, sizeof(int), s));
+      ENS_TRY(cudaMemsetAsync(E->dTileCounter, 0, sizeof(int), s));
       if (E->mode == 0) {
-        ENS_TRY(cudaLaunchKernelEx(&cfg, E->kernel, a));
+        ENS_TRY(cudaLaunchKernelEx(&cfg, launch_kernel(E), a));
       } else {
         for (int k = 0; k < steps; ++k) {
-          E->stepKernel<<<unsigned(E->grid), unsigned(E->threads), 0, s>>>(a);
-          E->bookKernel<<<1, 256, 0, s>>>(a);
+          launch_kernel(E)<<<unsigned(E->grid), unsigned(E->threads), 0, s>>>(a);
+          E->kern.book<<<1, 256, 0, s>>>(a);
         }
         ENS_TRY(cudaGetLastError());
       }
@@ -1002,7 +1103,7 @@ int lbx_ensemble_moments(lbx_ensemble E, int32_t slot, double* rho, double* u, v
   const int64_t n = E->slotCells[size_t(slot)];
   double* dev = nullptr;
   ENS_TRY(cudaMalloc(&dev, size_t(n) * 4 * sizeof(double)));
-  E->momentsKernel<<<unsigned((n + 255) / 256), 256, 0, s>>>(E->dLat + slot, E->dGlobalStep, dev, dev + n);
+  E->kern.moments<<<unsigned((n + 255) / 256), 256, 0, s>>>(E->dLat + slot, E->dGlobalStep, dev, dev + n);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && rho) e = cudaMemcpyAsync(rho, dev, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && u) e = cudaMemcpyAsync(u, dev + n, size_t(n) * 3 * sizeof(double), cudaMemcpyDeviceToHost, s);

@@ -60,7 +60,7 @@ class TuneEntry(C.Structure):
 
 
 def _tune(fn, handle, steps: int, stream, where: str) -> list[dict]:
-    cap = 64
+    cap = 128
     arr = (TuneEntry * cap)()
     n = C.c_int32()
     check(fn(handle, steps, arr, cap, C.byref(n), _stream_ptr(stream)), where)
@@ -103,6 +103,7 @@ def _load() -> C.CDLL:
         "lbx_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_set_launch_mode": ([VP, I32], C.c_int),
+        "lbx_ensemble_set_cells_per_thread": ([VP, I32], C.c_int),
         "lbx_ensemble_footprint": ([I32, I32, P(EnsembleRequest), P(I64)], C.c_int),
         "lbx_ensemble_create": ([I32, I32, I64, I32, I32, P(VP)], C.c_int),
         "lbx_ensemble_destroy": ([VP], C.c_int),
@@ -479,6 +480,10 @@ class Ensemble:
     def set_launch_mode(self, mode: int) -> None:
         """0: one persistent kernel per run; 1: one launch per step, chained in a CUDA graph."""
         check(lib.lbx_ensemble_set_launch_mode(self._h, mode), "lbx_ensemble_set_launch_mode")
+
+    def set_cells_per_thread(self, cells: int) -> None:
+        """1 or 2 cells per thread in the tile loop (identical results)."""
+        check(lib.lbx_ensemble_set_cells_per_thread(self._h, cells), "lbx_ensemble_set_cells_per_thread")
 
     def set_config(self, threads: int = 256, blocks_per_sm: int = 0, check_interval: int = 100) -> None:
         check(lib.lbx_ensemble_set_config(self._h, threads, blocks_per_sm, check_interval), "lbx_ensemble_set_config")

@@ -75,6 +75,7 @@ def test_ensemble_autotune_keeps_every_lattice_state():
         assert any(e["ms_per_step"] > 0 for e in entries)
         assert {e["threads"] for e in entries} == {64, 128, 256}
         assert {e["variant"] for e in entries} == {0, 1}  # both launch modes tried
+        assert {e["cells_per_thread"] for e in entries} == {1, 2}
         assert tuned.statuses() == before
         for s, (r0, u0) in zip(st, m_before):
             r1, u1 = tuned.moments(s)
@@ -88,15 +89,19 @@ def test_ensemble_autotune_keeps_every_lattice_state():
             assert np.array_equal(ra, rb) and np.array_equal(ua, ub)
 
 
-@pytest.mark.parametrize("threads,blocks,mode", [(64, 0, 0), (128, 2, 0), (256, 1, 0), (256, 0, 1), (64, 3, 1)])
-def test_ensemble_results_do_not_depend_on_the_launch_shape(threads, blocks, mode):
-    """Launch shape and launch mode (one persistent kernel, or one launch per step in a graph)
-    give identical populations, step counts, states and residuals."""
-    with lbx.Ensemble(19, "f32", slab_bytes=64 << 20, max_lattices=8) as a, \
-            lbx.Ensemble(19, "f32", slab_bytes=64 << 20, max_lattices=8) as b:
+@pytest.mark.parametrize("threads,blocks,mode,cells,storage", [
+    (64, 0, 0, 1, "f32"), (128, 2, 0, 1, "f32"), (256, 1, 0, 1, "f32"), (256, 0, 1, 1, "f32"), (64, 3, 1, 1, "f32"),
+    (256, 0, 0, 2, "f32"), (128, 0, 1, 2, "f32"), (64, 5, 1, 2, "f32"), (256, 0, 1, 2, "f16dev"),
+    (96, 0, 0, 2, "bf16dev"), (128, 0, 1, 2, "f64")])
+def test_ensemble_results_do_not_depend_on_the_launch_shape(threads, blocks, mode, cells, storage):
+    """Launch shape, launch mode (one persistent kernel, or one launch per step in a graph) and
+    cells per thread give identical populations, step counts, states and residuals."""
+    with lbx.Ensemble(19, storage, slab_bytes=64 << 20, max_lattices=8) as a, \
+            lbx.Ensemble(19, storage, slab_bytes=64 << 20, max_lattices=8) as b:
         a.set_config(threads=256, blocks_per_sm=0, check_interval=40)
         b.set_config(threads=threads, blocks_per_sm=blocks, check_interval=40)
         b.set_launch_mode(mode)
+        b.set_cells_per_thread(cells)
         sa, sb = _mix(a), _mix(b)
         a.run(200)
         b.run(200)
