@@ -204,3 +204,51 @@ def summarise(records: list[Record], wall_seconds: float) -> dict:
             "mlups": round(updates / wall_seconds / 1e6, 1),
             "p50_s": round(float(np.percentile(lat, 50)), 4), "p99_s": round(float(np.percentile(lat, 99)), 4),
             "lattice_updates": updates, "states": states}
+
+
+def time_ensemble(edges, steps: int, storage: str = "f32", mode: int = 1, cells: int = 2, threads: int = 256,
+                  blocks_per_sm: int = 2, device: int = 0) -> dict:
+    """Steps a fixed set of cavities (edge lengths `edges`, Re 100, no convergence stop) with one
+    launch shape and returns the device-timed rate of the engine alone: one untimed run of
+    `steps` steps (graph capture), then one timed run of `steps` steps."""
+    import torch
+
+    with lbx.Ensemble(19, storage, slab_bytes=8 << 30, max_lattices=max(8, len(edges)), device=device) as ens:
+        ens.set_config(threads=threads, blocks_per_sm=blocks_per_sm, check_interval=100)
+        ens.set_launch_mode(mode)
+        ens.set_cells_per_thread(cells)
+        for i, e in enumerate(edges):
+            ens.admit(CavityRequest(i, e, 100.0, tolerance=0.0, max_steps=10 ** 9).engine_request())
+        ens.run(steps)
+        torch.cuda.synchronize(device)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        ens.run(steps)
+        t1.record()
+        torch.cuda.synchronize(device)
+        ms = t0.elapsed_time(t1) / steps
+    n = sum(e ** 3 for e in edges)
+    return {"edges": list(edges), "storage": storage, "mode": mode, "cells_per_thread": cells, "threads": threads,
+            "blocks_per_sm": blocks_per_sm, "ms_per_step": ms, "mlups": n / ms / 1e3}
+
+
+def main(argv=None) -> int:
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="Time the ensemble engine on a fixed set of cavities.")
+    ap.add_argument("--edges", default="192,128,96,64,48,32,128,96", help="comma-separated cavity edge lengths")
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--storage", default="f32", choices=["f32", "f64", "f16dev", "bf16dev"])
+    ap.add_argument("--mode", type=int, default=1, help="0: persistent kernel, 1: graph of step launches")
+    ap.add_argument("--cells", type=int, default=2, help="cells per thread (1 or 2)")
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--blocks-per-sm", type=int, default=2)
+    a = ap.parse_args(argv)
+    edges = [int(v) for v in a.edges.split(",")]
+    print(json.dumps(time_ensemble(edges, a.steps, a.storage, a.mode, a.cells, a.threads, a.blocks_per_sm)))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
