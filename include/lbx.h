@@ -175,6 +175,22 @@ int lbx_build_bouzidi_links(int32_t q, const int32_t core[3], const int32_t peri
 int lbx_upload_populations(lbx_lattice lattice, const void* host, int32_t host_type, void* stream);
 int lbx_download_populations(lbx_lattice lattice, void* host, int32_t host_type, void* stream);
 
+/* Checkpoint and resume (SuperLattice::save / load into a buffer, core/serializer.h:77-79 and
+ * 187-189; a CUDA column serialises its data with its periodic-shift offset,
+ * gpu/cuda/column.hh:305-321).  A checkpoint is a host buffer of lbx_checkpoint_bytes bytes: a
+ * 128-byte header (format tag, descriptor, storage form, core extent, periodic axes, the
+ * statistics of the last statistics step) followed by the core cells' populations in the
+ * layout of lbx_download_populations, FP64 for the FP64 form and FP32 for the others, which is
+ * exact for every form.  The shift is not stored: populations are written in logical order and
+ * load into a lattice at any shift, and the steps after a load give the same bits as steps
+ * that were never interrupted.  Dynamics, boundaries and launch shape are set-up rather than
+ * state: the caller applies them to the lattice it loads into, as an application re-runs its
+ * set-up before SuperLattice::load.  A load checks that descriptor, storage, extent and
+ * periodicity match (LBX_ERR_INVALID otherwise).  Both calls synchronise the stream. */
+int lbx_checkpoint_bytes(lbx_lattice lattice, int64_t* bytes);
+int lbx_save_checkpoint(lbx_lattice lattice, void* host, int64_t bytes, void* stream);
+int lbx_load_checkpoint(lbx_lattice lattice, const void* host, int64_t bytes, void* stream);
+
 /* Equilibrium initialisation from moment fields (BlockLattice::iniEquilibrium,
  * core/blockLattice.hh:201-219): rho [core cells], u [d][core cells], doubles. */
 int lbx_ini_equilibrium(lbx_lattice lattice, const double* rho, const double* u, void* stream);

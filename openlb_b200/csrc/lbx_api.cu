@@ -853,6 +853,79 @@ int lbx_download_populations(lbx_lattice L, void* host, int32_t host_type, void*
   return LBX_OK;
 }
 
+// ---- checkpoint / resume ------------------------------------------------------------------
+// Header of a checkpoint buffer (128 bytes, host byte order), then [q][core cells] populations
+// of the exchange layout: FP64 for the FP64 form, FP32 for the others (exact for every form).
+struct CheckpointHeader {
+  char magic[8];          // "LBXCKPT1"
+  int32_t version;        // 1
+  int32_t q, d, storage;
+  int32_t core[3], periodic[3];
+  int64_t ncore;
+  StatAcc stats;          // accumulator of the last statistics step (lbx_get_statistics)
+  int32_t valueBytes;     // 8 or 4
+  int32_t pad[9];
+};
+static_assert(sizeof(CheckpointHeader) == 128, "checkpoint header is 128 bytes");
+
+static int64_t checkpoint_value_bytes(const lbx_lattice_s* L) { return L->storage == LBX_F64 ? 8 : 4; }
+
+int lbx_checkpoint_bytes(lbx_lattice L, int64_t* bytes) {
+  if (!L || !bytes) return fail(LBX_ERR_INVALID, "null argument");
+  *bytes = int64_t(sizeof(CheckpointHeader)) + int64_t(L->q) * L->ncore * checkpoint_value_bytes(L);
+  return LBX_OK;
+}
+
+int lbx_save_checkpoint(lbx_lattice L, void* host, int64_t bytes, void* stream) {
+  if (!L || !host) return fail(LBX_ERR_INVALID, "null argument");
+  int64_t need = 0;
+  lbx_checkpoint_bytes(L, &need);
+  if (bytes < need) return fail(LBX_ERR_INVALID, "checkpoint buffer holds " + std::to_string(bytes) +
+                                                     " bytes, the lattice needs " + std::to_string(need));
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CheckpointHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, "LBXCKPT1", 8);
+  h.version = 1;
+  h.q = L->q;
+  h.d = L->d;
+  h.storage = L->storage;
+  for (int a = 0; a < 3; ++a) {
+    h.core[a] = L->core[a];
+    h.periodic[a] = L->periodic[a];
+  }
+  h.ncore = L->ncore;
+  h.valueBytes = int32_t(checkpoint_value_bytes(L));
+  LBX_CUDA_TRY(cudaMemcpyAsync(&h.stats, L->stats, sizeof(StatAcc), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  std::memcpy(host, &h, sizeof(h));
+  return lbx_download_populations(L, static_cast<char*>(host) + sizeof(h), h.valueBytes == 8 ? 0 : 1, stream);
+}
+
+int lbx_load_checkpoint(lbx_lattice L, const void* host, int64_t bytes, void* stream) {
+  if (!L || !host) return fail(LBX_ERR_INVALID, "null argument");
+  if (bytes < int64_t(sizeof(CheckpointHeader))) return fail(LBX_ERR_INVALID, "checkpoint shorter than its header");
+  CheckpointHeader h;
+  std::memcpy(&h, host, sizeof(h));
+  if (std::memcmp(h.magic, "LBXCKPT1", 8) != 0 || h.version != 1) return fail(LBX_ERR_INVALID, "not a checkpoint of this format");
+  bool same = h.q == L->q && h.d == L->d && h.storage == L->storage && h.ncore == L->ncore &&
+              h.valueBytes == checkpoint_value_bytes(L);
+  for (int a = 0; a < 3; ++a) same = same && h.core[a] == L->core[a] && h.periodic[a] == L->periodic[a];
+  if (!same) return fail(LBX_ERR_INVALID, "checkpoint was taken from a lattice of another descriptor, storage, extent or periodicity");
+  int64_t need = 0;
+  lbx_checkpoint_bytes(L, &need);
+  if (bytes < need) return fail(LBX_ERR_INVALID, "checkpoint truncated");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (int rc = lbx_upload_populations(L, static_cast<const char*>(host) + sizeof(h), h.valueBytes == 8 ? 0 : 1, stream))
+    return rc;
+  StatAcc st = h.stats;
+  LBX_CUDA_TRY(cudaMemcpyAsync(L->stats, &st, sizeof(StatAcc), cudaMemcpyHostToDevice, s));
+  LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  return LBX_OK;
+}
+
 int lbx_ini_equilibrium(lbx_lattice L, const double* rho, const double* u, void* stream) {
   if (!L || !rho || !u) return fail(LBX_ERR_INVALID, "null argument");
   DeviceGuard guard(L->device);

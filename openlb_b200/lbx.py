@@ -89,6 +89,9 @@ def _load() -> C.CDLL:
         "lbx_build_bouzidi_links": ([I32, P(I32), P(I32), VP, I32, I32, VP, VP, I64, VP, VP, VP, P(I64)], C.c_int),
         "lbx_upload_populations": ([VP, VP, I32, VP], C.c_int),
         "lbx_download_populations": ([VP, VP, I32, VP], C.c_int),
+        "lbx_checkpoint_bytes": ([VP, P(I64)], C.c_int),
+        "lbx_save_checkpoint": ([VP, VP, I64, VP], C.c_int),
+        "lbx_load_checkpoint": ([VP, VP, I64, VP], C.c_int),
         "lbx_ini_equilibrium": ([VP, VP, VP, VP], C.c_int),
         "lbx_collide_and_stream": ([VP, I64, U32, VP], C.c_int),
         "lbx_get_statistics": ([VP, P(D), VP], C.c_int),
@@ -336,6 +339,21 @@ class BlockLattice:
         check(lib.lbx_download_populations(self._h, _ptr(a), 0 if a.dtype == np.float64 else 1, _stream_ptr(stream)),
               "lbx_download_populations")
         return a
+
+    def save_checkpoint(self, stream=None) -> bytes:
+        """The lattice state as a byte string (SuperLattice::save): populations of the core cells
+        in logical order and the last statistics, behind a header naming the lattice's shape."""
+        n = C.c_int64()
+        check(lib.lbx_checkpoint_bytes(self._h, C.byref(n)), "lbx_checkpoint_bytes")
+        buf = np.empty(n.value, dtype=np.uint8)
+        check(lib.lbx_save_checkpoint(self._h, _ptr(buf), n.value, _stream_ptr(stream)), "lbx_save_checkpoint")
+        return buf.tobytes()
+
+    def load_checkpoint(self, data: bytes, stream=None) -> None:
+        """Restores a checkpoint of a lattice with the same descriptor, storage, extent and
+        periodicity (SuperLattice::load); dynamics and boundaries are the caller's set-up."""
+        buf = np.frombuffer(data, dtype=np.uint8)
+        check(lib.lbx_load_checkpoint(self._h, _ptr(buf), buf.size, _stream_ptr(stream)), "lbx_load_checkpoint")
 
     def ini_equilibrium(self, rho: np.ndarray, u: np.ndarray, stream=None) -> None:
         r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)

@@ -201,6 +201,17 @@ class BlockLattice {
     check(lbx_download_populations(h_, f.data(), 0, stream), "lbx_download_populations");
     return f;
   }
+  // SuperLattice::save / load, into and from a byte buffer (Serializer::save(buffer) / load)
+  std::vector<uint8_t> save(void* stream = nullptr) const {
+    int64_t n = 0;
+    check(lbx_checkpoint_bytes(h_, &n), "lbx_checkpoint_bytes");
+    std::vector<uint8_t> buf(static_cast<size_t>(n));
+    check(lbx_save_checkpoint(h_, buf.data(), n, stream), "lbx_save_checkpoint");
+    return buf;
+  }
+  void load(const std::vector<uint8_t>& buf, void* stream = nullptr) {
+    check(lbx_load_checkpoint(h_, buf.data(), int64_t(buf.size()), stream), "lbx_load_checkpoint");
+  }
   // SuperLatticeDensity / SuperLatticeVelocity: rho [cells], u [d][cells]
   std::pair<std::vector<double>, std::vector<double>> computeRhoU(void* stream = nullptr) const {
     std::vector<double> rho(static_cast<size_t>(coreCells())), u(static_cast<size_t>(d * coreCells()));
