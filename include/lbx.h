@@ -56,7 +56,11 @@ typedef enum {
   LBX_TRT = 2,                   /* TRTdynamics            dynamics/dynamics.h:529-536 */
   LBX_SMAGORINSKY_BGK = 3,       /* SmagorinskyBGKdynamics smagorinskyBGKdynamics.h:39-44 */
   LBX_FORCED_BGK = 4,            /* ForcedBGKdynamics      dynamics/dynamics.h:223-230 */
-  LBX_SMAGORINSKY_FORCED_BGK = 5 /* SmagorinskyForcedBGKdynamics smagorinskyBGKdynamics.h:67-73 */
+  LBX_SMAGORINSKY_FORCED_BGK = 5, /* SmagorinskyForcedBGKdynamics smagorinskyBGKdynamics.h:67-73 */
+  LBX_CONST_RHO_BGK = 6          /* ConstRhoBGKdynamics    dynamics/dynamics.h:209-215,
+                                    collision.h:322-351; AVERAGE_RHO is the previous step's
+                                    average density (superLattice.hh:675-677), 1 before the
+                                    first step, and statistics are kept on every step */
 } lbx_dynamics;
 
 /* Per-cell dynamics ids (the role of BlockDynamicsMap, core/blockDynamicsMap.h:264-416). */

@@ -155,6 +155,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   for (int k = 0; k < 3; ++k) a.force[k] = L->params.force[k];
   a.cellDyn = L->cellDyn;
   a.stats = nullptr;
+  a.avgSrc = L->dynamics == LBX_CONST_RHO_BGK ? L->stats : nullptr;
   a.blockX = L->blockX;
   a.blockY = L->blockY;
   a.kernel = L->kernel;
@@ -604,7 +605,7 @@ int lbx_get_info(lbx_lattice L, lbx_info* info) {
 
 int lbx_set_dynamics(lbx_lattice L, int32_t dynamics, const lbx_params* params) {
   if (!L || !params) return fail(LBX_ERR_INVALID, "null argument");
-  if (dynamics < LBX_BGK || dynamics > LBX_SMAGORINSKY_FORCED_BGK) return fail(LBX_ERR_UNSUPPORTED, "unknown dynamics");
+  if (dynamics < LBX_BGK || dynamics > LBX_CONST_RHO_BGK) return fail(LBX_ERR_UNSUPPORTED, "unknown dynamics");
   if (!(params->omega > 0.0 && params->omega < 2.0)) return fail(LBX_ERR_INVALID, "omega must lie in (0, 2)");
   if (dynamics == LBX_TRT && !(params->magic > 0.0)) return fail(LBX_ERR_INVALID, "TRT magic parameter must be > 0");
   if ((dynamics == LBX_SMAGORINSKY_BGK || dynamics == LBX_SMAGORINSKY_FORCED_BGK) && !(params->smagorinsky >= 0.0))
@@ -948,9 +949,12 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
   if (steps < 0) return fail(LBX_ERR_INVALID, "steps must be >= 0");
   DeviceGuard guard(L->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // ConstRhoBGK reads the previous step's average density, so its statistics are kept on
+  // every step, as the reference keeps them whenever statistics are enabled (its default)
+  const bool everyStep = L->dynamics == LBX_CONST_RHO_BGK;
   for (int64_t k = 0; k < steps; ++k) {
     LaunchArgs a = args_of(L);
-    if ((flags & LBX_STEP_STATISTICS) && k == steps - 1) {
+    if (((flags & LBX_STEP_STATISTICS) && k == steps - 1) || everyStep) {
       if (int rc = ensure_stat_capacity(L)) return rc;
       a.stats = L->stats;
       a.statPart = L->statPart;
@@ -1185,12 +1189,22 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
   }
   int64_t shift0[27];
   std::memcpy(shift0, L->shift, sizeof(shift0));
+  // the statistics too: ConstRhoBGK reads the last step's average density from them
+  StatAcc stats0;
+  cudaError_t estat = cudaMemcpyAsync(&stats0, L->stats, sizeof(StatAcc), cudaMemcpyDeviceToHost, s);
+  if (estat == cudaSuccess) estat = cudaStreamSynchronize(s);
+  if (estat != cudaSuccess) {
+    cudaFree(saved);
+    return fail(LBX_ERR_CUDA, std::string("autotune state copy: ") + cudaGetErrorString(estat));
+  }
   const bool timing0 = L->timing;
   if (timing0) drain_timing(L);
   L->timing = false;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   auto restore = [&]() -> cudaError_t {
     std::memcpy(L->shift, shift0, sizeof(shift0));
+    cudaError_t r = cudaMemcpyAsync(L->stats, &stats0, sizeof(StatAcc), cudaMemcpyHostToDevice, s);
+    if (r != cudaSuccess) return r;
     return cudaMemcpy2DAsync(L->pop, pitch, saved, colBytes, colBytes, size_t(L->q), cudaMemcpyDeviceToDevice, s);
   };
   e = cudaMemcpy2DAsync(saved, colBytes, L->pop, pitch, colBytes, size_t(L->q), cudaMemcpyDeviceToDevice, s);

@@ -15,6 +15,7 @@
 //   Guo forcing      forcing::PlainGuo / forcing::Guo         src/dynamics/forcing.h:35-65, 115-151
 //                    lbm<>::addExternalForce                   src/dynamics/lbm.h:568-588
 //   bounce-back      collision::Revert                        src/dynamics/collision.h:465-484
+//   ConstRhoBGK      collision::ConstRhoBGK::apply            src/dynamics/collision.h:322-351
 #pragma once
 
 #include "lbx_desc.cuh"
@@ -26,7 +27,15 @@ enum Dyn : int {
   DYN_TRT = 2,
   DYN_SMAGORINSKY = 3,
   DYN_FORCED_BGK = 4,
-  DYN_FORCED_SMAGORINSKY = 5
+  DYN_FORCED_SMAGORINSKY = 5,
+  DYN_CONST_RHO = 6
+};
+
+// Statistics accumulator: {sum rho, sum |u|^2} in FP64, {count, max |u|^2 bits}.
+struct StatAcc {
+  double sum[2];
+  unsigned long long count;
+  unsigned long long maxbits;
 };
 
 template <typename R>
@@ -35,6 +44,9 @@ struct CollisionParams {
   R magic;
   R smagorinsky;
   R force[3];
+  // ConstRhoBGK: the statistics of the previous step, whose average density is the
+  // AVERAGE_RHO parameter (1 while no step has been counted)
+  const StatAcc* avgSrc;
 };
 
 template <int DYN> struct DynTraits {
@@ -208,6 +220,29 @@ __device__ __forceinline__ void collide(R (&f)[Q], const CollisionParams<R>& p, 
 
   R omega = p.omega;
   if constexpr (T::smagorinsky) omega = smagorinsky_omega<Q, R, T::forced>(f, rho, u, p);
+
+  if constexpr (DYN == DYN_CONST_RHO) {
+    // collision::ConstRhoBGK::apply (src/dynamics/collision.h:336-349): the equilibrium part
+    // is rescaled by 1 + (1 - <rho>) / rho, which pulls the lattice's average density back to
+    // 1; the cell reports rho + (1 - <rho>) to the statistics.
+    double avg = 1.0;
+    if (p.avgSrc) {
+      const unsigned long long cnt = p.avgSrc->count;
+      if (cnt) avg = p.avgSrc->sum[0] / double(cnt);
+    }
+    const R deltaRho = R(1) - R(avg);
+    const R ratioRho = R(1) + deltaRho / rho;
+    const R keep = R(1) - omega;
+    static_for<Q>([&](auto I) {
+      constexpr R t = weight<Q, R>(I);
+      const R feq = equilibrium<Q, I>(rho, u, uSqr);
+      if constexpr (sizeof(R) == 8) f[I] = ratioRho * (feq + t) - t + keep * (f[I] - feq);
+      else f[I] = __fmaf_rn(keep, f[I] - feq, __fmaf_rn(ratioRho, feq + t, -t));
+    });
+    rhoOut = rho + deltaRho;
+    uSqrOut = uSqr;
+    return;
+  }
 
   if constexpr (T::trt) {
     const R omega2 = R(1) / (p.magic / (R(1) / omega - R(0.5)) + R(0.5));

@@ -242,6 +242,7 @@ __device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nT
     cp.magic = R(L->magic);
     cp.smagorinsky = R(0);
     cp.force[0] = cp.force[1] = cp.force[2] = R(0);
+    cp.avgSrc = nullptr;
     const int dyn = L->dynamics;
     const int slots = (last + 31) / 32;
     double tileDu2 = 0.0, tileU2 = 0.0;  // the tile's sums, slot by slot

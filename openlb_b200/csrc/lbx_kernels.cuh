@@ -67,12 +67,6 @@ __device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t s, int64_t n) {
   return r >= n ? r - n : r;
 }
 
-// Statistics accumulator: {sum rho, sum |u|^2} in FP64, {count, max |u|^2 bits}.
-struct StatAcc {
-  double sum[2];
-  unsigned long long count;
-  unsigned long long maxbits;
-};
 
 // Block partial of the lattice statistics {sum rho, sum |u|^2, max |u|^2, count}: a warp
 // butterfly, then the warps in index order, written to part[4 * block] without atomics.  With
@@ -1410,6 +1404,7 @@ struct LaunchArgs {
   double omega, magic, smagorinsky, force[3];
   const uint8_t* cellDyn;
   StatAcc* stats;       // statistics of this step requested: totals land here
+  const StatAcc* avgSrc;  // ConstRhoBGK: statistics of the previous step (average density)
   double* statPart;     // block partials of the statistics (4 doubles per block)
   int64_t statCapacity; // blocks statPart can hold
   int blockX, blockY;
@@ -1470,6 +1465,7 @@ inline CollisionParams<R> params_of(const LaunchArgs& a) {
   p.magic = R(a.magic);
   p.smagorinsky = R(a.smagorinsky);
   for (int k = 0; k < 3; ++k) p.force[k] = R(a.force[k]);
+  p.avgSrc = a.avgSrc;
   return p;
 }
 
@@ -1635,6 +1631,7 @@ cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream) {
   case DYN_SMAGORINSKY: return launch_step_dyn<Q, S, DYN_SMAGORINSKY>(a, stream);
   case DYN_FORCED_BGK: return launch_step_dyn<Q, S, DYN_FORCED_BGK>(a, stream);
   case DYN_FORCED_SMAGORINSKY: return launch_step_dyn<Q, S, DYN_FORCED_SMAGORINSKY>(a, stream);
+  case DYN_CONST_RHO: return launch_step_dyn<Q, S, DYN_CONST_RHO>(a, stream);
   default: return cudaErrorInvalidValue;
   }
 }

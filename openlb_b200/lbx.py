@@ -26,7 +26,8 @@ LIB_PATH = Path(os.environ.get("LBX_LIBRARY", Path(__file__).resolve().parent / 
 LBX_OK = 0
 STORAGE = {"f64": 0, "f32": 1, "f16dev": 2, "bf16dev": 3}
 STORAGE_BYTES = {"f64": 8, "f32": 4, "f16dev": 2, "bf16dev": 2}
-DYNAMICS = {"bgk": 1, "trt": 2, "smagorinsky_bgk": 3, "forced_bgk": 4, "smagorinsky_forced_bgk": 5}
+DYNAMICS = {"bgk": 1, "trt": 2, "smagorinsky_bgk": 3, "forced_bgk": 4, "smagorinsky_forced_bgk": 5,
+            "const_rho_bgk": 6}
 CELL_NONE, CELL_BULK, CELL_BOUNCE_BACK = 0, 1, 2
 STEP_STATISTICS = 1
 REDUCE_MASS_MOMENTUM, REDUCE_DRAG, REDUCE_RESIDUAL = 1, 2, 3

@@ -54,6 +54,7 @@ struct TRTdynamics { static constexpr int id = LBX_TRT; };
 struct SmagorinskyBGKdynamics { static constexpr int id = LBX_SMAGORINSKY_BGK; };
 struct ForcedBGKdynamics { static constexpr int id = LBX_FORCED_BGK; };
 struct SmagorinskyForcedBGKdynamics { static constexpr int id = LBX_SMAGORINSKY_FORCED_BGK; };
+struct ConstRhoBGKdynamics { static constexpr int id = LBX_CONST_RHO_BGK; };
 
 // ---- parameters (descriptors::OMEGA, collision::TRT::MAGIC, collision::LES::SMAGORINSKY) ------
 struct OMEGA {};

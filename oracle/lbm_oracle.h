@@ -25,7 +25,8 @@ enum lbo_dynamics {
   LBO_TRT = 1,        /* TRTdynamics                 src/dynamics/dynamics.h:529-536 */
   LBO_SMAGORINSKY = 2,/* SmagorinskyBGKdynamics      src/dynamics/smagorinskyBGKdynamics.h:39-44 */
   LBO_FORCED_BGK = 3, /* ForcedBGKdynamics (Guo)     src/dynamics/dynamics.h:223-230 */
-  LBO_FORCED_SMAGORINSKY = 4 /* SmagorinskyForcedBGKdynamics smagorinskyBGKdynamics.h:67-73 */
+  LBO_FORCED_SMAGORINSKY = 4, /* SmagorinskyForcedBGKdynamics smagorinskyBGKdynamics.h:67-73 */
+  LBO_CONST_RHO_BGK = 5       /* ConstRhoBGKdynamics dynamics.h:209-215, collision.h:322-351 */
 };
 
 enum lbo_material {

@@ -4,7 +4,7 @@
 
 /* Collision of one fluid cell in place on g[0..q-1] (values f_i - w_i).
  * Returns the cell statistic {rho, |u|^2} through rho_out/usq_out. */
-static void FN(collide)(const lbo_desc* d, const lbo_case* c, REAL* g, REAL* rho_out, REAL* usq_out)
+static void FN(collide)(const lbo_desc* d, const lbo_case* c, REAL* g, REAL avg_rho, REAL* rho_out, REAL* usq_out)
 {
   const int q = d->q, dim = d->d;
   const REAL invCs2 = (REAL)3;
@@ -85,6 +85,17 @@ static void FN(collide)(const lbo_desc* d, const lbo_case* c, REAL* g, REAL* rho
     const REAL magic = (REAL)c->magic;
     const REAL omega2 = (REAL)1 / (magic / ((REAL)1 / omega - (REAL)0.5) + (REAL)0.5);
     for (int i = 0; i < q; ++i) g[i] -= omega * (fp[i] - ep[i]) + omega2 * (fm[i] - em[i]);
+  } else if (c->dynamics == LBO_CONST_RHO_BGK) {
+    /* collision::ConstRhoBGK::apply (src/dynamics/collision.h:336-349): the equilibrium is
+     * rescaled so that the lattice's average density returns to 1; avg_rho is the
+     * AVERAGE_RHO parameter, the statistics' average density of the previous step. */
+    const REAL deltaRho = (REAL)1 - avg_rho;
+    const REAL ratioRho = (REAL)1 + deltaRho / rho;
+    for (int i = 0; i < q; ++i)
+      g[i] = ratioRho * (feq[i] + t[i]) - t[i] + ((REAL)1 - omega) * (g[i] - feq[i]);
+    *rho_out = rho + deltaRho;
+    *usq_out = uSqr;
+    return;
   } else {
     /* collision::BGK::apply (src/dynamics/collision.h:68-78) */
     for (int i = 0; i < q; ++i) {
@@ -307,6 +318,10 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
   for (int64_t x = 0; x < n; ++x) fdIndex[x] = -1;
   for (int64_t b = 0; b < c->n_fd; ++b) fdIndex[c->fd_cell[b]] = b;
 
+  /* AVERAGE_RHO: the superlattice statistics' average density, 1 before the first step
+   * (latticeStatistics.hh:137), set before every collision (superLattice.hh:675-677) */
+  REAL avgRho = (REAL)1;
+  const int constRho = c->dynamics == LBO_CONST_RHO_BGK;
   for (int64_t s = 0; s < steps; ++s) {
     /* collide (ConcreteBlockCollisionO<..CPU_SISD..>::apply, cpu/sisd/operator.h:143-228) */
 #pragma omp parallel for schedule(static) if (n > 200000)
@@ -317,7 +332,7 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
       if (m == LBO_FLUID) {
         REAL g[27];
         for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
-        FN(collide)(d, c, g, &cellRho[x], &cellUsq[x]);
+        FN(collide)(d, c, g, avgRho, &cellRho[x], &cellUsq[x]);
         for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);
       } else if (m == LBO_FD_BOUNDARY && fdIndex[x] >= 0) {
         /* BGKdynamics with the boundary momenta exchanged in (collision::BGK::apply,
@@ -338,7 +353,7 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
       }
     }
     /* statistics, accumulated in cell order (latticeStatistics.hh:183-192, 60-90) */
-    if (stats) {
+    if (stats || constRho) {
       double sr = 0, se = 0, mx = 0;
       int64_t cnt = 0;
       REAL sumR = 0, sumE = 0, maxE = 0;
@@ -351,9 +366,18 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
         }
       }
       sr = (double)sumR; se = (double)sumE; mx = (double)maxE;
-      stats[3 * s + 0] = cnt ? sr / (double)cnt : 1.0;
-      stats[3 * s + 1] = cnt ? 0.5 * se / (double)cnt : 1.0;
-      stats[3 * s + 2] = sqrt(mx);
+      if (stats) {
+        stats[3 * s + 0] = cnt ? sr / (double)cnt : 1.0;
+        stats[3 * s + 1] = cnt ? 0.5 * se / (double)cnt : 1.0;
+        stats[3 * s + 2] = sqrt(mx);
+      }
+      if (cnt) {
+        /* the block average, then the superlattice's cell-count-weighted mean of the block
+         * averages (superLattice.hh:61-106; one block of spacing 1: weight = cell count) */
+        const REAL w = (REAL)cnt;
+        const REAL avgBlock = sumR / w;
+        avgRho = avgBlock * w / w;
+      }
     }
     /* stream: f_i(x) <- f_i(x - c_i).  This is what the reference's periodic-shift rotation
      * (ConcreteBlockLattice::stream, core/blockLattice.hh:316-338) plus the periodic overlap

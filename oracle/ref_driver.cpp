@@ -10,6 +10,7 @@
  *    defineDynamics<...>                      src/core/superLattice.h (BlockLattice::defineDynamics blockLattice.hh:274)
  *    BGKdynamics / TRTdynamics / ForcedBGK    src/dynamics/dynamics.h:89,223,529
  *    SmagorinskyBGK / SmagorinskyForcedBGK    src/dynamics/smagorinskyBGKdynamics.h:39,67
+ *    ConstRhoBGKdynamics                      src/dynamics/dynamics.h:209-215
  *    BounceBack (Revert) / NoDynamics         src/dynamics/dynamics.h:51,557
  *    setBouzidiBoundary / setBouzidiVelocity  src/boundary/setBouzidiBoundary.h:193-420
  *    boundary::set<InterpolatedVelocity/Pressure>  src/boundary/setBoundary.h:80-160,
@@ -21,7 +22,7 @@
  *  without the FORCE field; used by the timing build of plain BGK).
  *
  *  Usage:
- *    lbref <periodic|cavity|porous|channel> [--n NX NY [NZ]] [--dyn bgk|trt|smag|fbgk|fsmag]
+ *    lbref <periodic|cavity|porous|channel> [--n NX NY [NZ]] [--dyn bgk|trt|smag|fbgk|fsmag|constrho]
  *          [--omega W] [--magic L] [--cs C] [--force FX FY [FZ]] [--steps S]
  *          [--init tgv|random|rest] [--u0 U] [--amp A] [--seed K] [--ulid U]
  *          [--walls bouzidi|bounceback] [--solid-frac P] [--out PREFIX]
@@ -257,6 +258,7 @@ int main(int argc, char** argv) {
   if (o.dyn == "bgk") defineFluid<BGKdynamics<T,DESCRIPTOR>>(lat, geo);
   else if (o.dyn == "trt") defineFluid<TRTdynamics<T,DESCRIPTOR>>(lat, geo);
   else if (o.dyn == "smag") defineFluid<SmagorinskyBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "constrho") defineFluid<ConstRhoBGKdynamics<T,DESCRIPTOR>>(lat, geo);
 #ifndef REF_NO_FORCE
   else if (o.dyn == "fbgk") defineFluid<ForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);
   else if (o.dyn == "fsmag") defineFluid<SmagorinskyForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);

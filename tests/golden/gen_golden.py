@@ -86,6 +86,16 @@ CASES.update({
                                                                    "--omega", str(1.0 / (3 * 0.128 + 0.5)),
                                                                    "--ulid", "0.1", "--init", "rest",
                                                                    "--steps", "20000"]),
+    # ConstRhoBGK (the bulk dynamics of the cavity2d example): a periodic lattice whose random
+    # initial density averages below 1, which the dynamics pulls back to 1, and a cavity
+    "periodic_d2q9_constrho_f64": ("d2q9_f64_nocse", "periodic", [*P2, "--dyn", "constrho", "--omega", "1.7", *RND,
+                                                                  "--steps", "20", "--seed", "9"]),
+    "periodic_d2q9_constrho_f32": ("d2q9_f32", "periodic", [*P2, "--dyn", "constrho", "--omega", "1.7", *RND,
+                                                            "--steps", "20", "--seed", "9"]),
+    "periodic_d3q19_constrho_f64": ("d3q19_f64_nocse", "periodic", [*P3, "--dyn", "constrho", "--omega", "1.5",
+                                                                    *RND, "--steps", "20", "--seed", "19"]),
+    "cavity_d2q9_constrho_f64": ("d2q9_f64_nocse", "cavity", ["--n", "16", "14", "--dyn", "constrho", "--omega", "1.2",
+                                                              "--ulid", "0.1", "--init", "rest", "--steps", "150"]),
     # Taylor-Green vortex (the benchmark's initial condition), small
     "tgv_d3q19_bgk_f64": ("d3q19_f64_nocse", "periodic", ["--n", "16", "16", "16", "--dyn", "bgk",
                                                            "--omega", str(1.0 / (3 * 0.01 + 0.5)), "--init", "tgv",

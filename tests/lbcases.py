@@ -30,9 +30,9 @@ VEL = {9: np.array(C9), 19: np.array(C19), 27: np.array(C27)}
 W = {9: np.array([4 / 9] + [1 / 36, 1 / 9] * 4),
      19: np.array([1 / 3] + [1 / 18] * 3 + [1 / 36] * 6 + [1 / 18] * 3 + [1 / 36] * 6),
      27: np.array([8 / 27] + [2 / 27] * 3 + [1 / 54] * 6 + [1 / 216] * 4 + [2 / 27] * 3 + [1 / 54] * 6 + [1 / 216] * 4)}
-DYN_CODE = {"bgk": 0, "trt": 1, "smag": 2, "fbgk": 3, "fsmag": 4}
+DYN_CODE = {"bgk": 0, "trt": 1, "smag": 2, "fbgk": 3, "fsmag": 4, "constrho": 5}
 GPU_DYN = {"bgk": "bgk", "trt": "trt", "smag": "smagorinsky_bgk", "fbgk": "forced_bgk",
-           "fsmag": "smagorinsky_forced_bgk"}
+           "fsmag": "smagorinsky_forced_bgk", "constrho": "const_rho_bgk"}
 
 
 def opposite(q: int) -> np.ndarray:
