@@ -313,6 +313,17 @@ int lbx_ensemble_statuses(lbx_ensemble ens, lbx_ensemble_status* out, int32_t n,
 int lbx_ensemble_moments(lbx_ensemble ens, int32_t slot, double* rho, double* u, void* stream);
 /* Free a slot and its slab space (no effect on the others). */
 int lbx_ensemble_retire(lbx_ensemble ens, int32_t slot);
+/* Pre-emption: a running (or finished) slot saved to a host buffer and restored later, in this
+ * or another ensemble of the same descriptor and storage, as a newly admitted slot that
+ * continues exactly where it stopped: populations at their shifts, velocity snapshot, step
+ * count, residual and state (the ensemble form of SuperLattice::save / load,
+ * core/serializer.h:77-79).  The buffer holds a header and the slot's slab region;
+ * lbx_ensemble_checkpoint_bytes gives its size.  Saving synchronises the stream and leaves the
+ * slot admitted: retire it to free its memory.  Restoring admits by footprint like
+ * lbx_ensemble_admit (LBX_ERR_OUT_OF_MEMORY when it does not fit yet). */
+int lbx_ensemble_checkpoint_bytes(lbx_ensemble ens, int32_t slot, int64_t* bytes);
+int lbx_ensemble_save_slot(lbx_ensemble ens, int32_t slot, void* host, int64_t bytes, void* stream);
+int lbx_ensemble_restore_slot(lbx_ensemble ens, const void* host, int64_t bytes, int32_t* slot, void* stream);
 /* Launch shape of the persistent kernel (the autotuner's knob): threads per block (multiple of
  * 32, <= 256; a tile is 512 cells whatever the block size, so results and residuals do not
  * depend on it), resident blocks per SM (0: occupancy maximum), and the residual check interval

@@ -590,6 +590,7 @@ struct lbx_ensemble_s {
   std::vector<int64_t> slotOffset, slotBytes;
   std::vector<int> slotUsed;
   std::vector<int32_t> slotCells;
+  std::vector<double> slotLid;  // lid velocity of each admitted request (for its checkpoint)
   EnsLattice* dLat = nullptr;
   int2* dTiles = nullptr;
   int2* dRange = nullptr;
@@ -728,6 +729,7 @@ int lbx_ensemble_create(int32_t q, int32_t storage, int64_t slab_bytes, int32_t 
   E->slotBytes.assign(size_t(max_lattices), 0);
   E->slotUsed.assign(size_t(max_lattices), 0);
   E->slotCells.assign(size_t(max_lattices), 0);
+  E->slotLid.assign(size_t(max_lattices), 0.0);
   kernels_for(q, storage, E->kern);
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&E->slab), size_t(E->slabBytes));
   if (e == cudaSuccess) e = cudaMalloc(&E->dLat, size_t(max_lattices) * sizeof(EnsLattice));
@@ -975,6 +977,7 @@ int lbx_ensemble_admit(lbx_ensemble E, const lbx_ensemble_request* req, int32_t*
   E->slotOffset[size_t(s)] = off;
   E->slotBytes[size_t(s)] = bytes;
   E->slotCells[size_t(s)] = L.ncore;
+  E->slotLid[size_t(s)] = req->lid_velocity;
   E->dirty = true;
   *slot = s;
   return LBX_OK;
@@ -992,6 +995,127 @@ int lbx_ensemble_retire(lbx_ensemble E, int32_t slot) {
   E->slotUsed[size_t(slot)] = 0;
   E->slotOffset[size_t(slot)] = -1;
   E->dirty = true;
+  return LBX_OK;
+}
+
+// ---- checkpoint of one slot (pre-emption) ---------------------------------------------------
+// Header, then the slot's raw population columns (q columns of period P at the saved shifts)
+// and its velocity snapshot.  The request is re-admitted on restore and its state written over
+// the fresh region, so the resumed lattice continues bit for bit.
+struct EnsCheckpointHeader {
+  char magic[8];  // "LBXENS01"
+  int32_t q, storage;
+  int32_t core[3];
+  int32_t dynamics, state, pad;
+  int64_t steps, maxSteps;
+  double tol, residual, lid, omega, magicParam;
+  uint32_t P;
+  uint32_t shift[kMaxQ];  // the column shifts the next step reads
+  int64_t popBytes, snapBytes;
+};
+
+namespace {
+int64_t slot_pop_bytes(const lbx_ensemble_s* E, uint32_t P) { return int64_t(E->q) * int64_t(P) * int64_t(elem_bytes(E->storage)); }
+int64_t slot_snap_bytes(int64_t ncore) { return 3 * ncore * int64_t(sizeof(float)); }
+}  // namespace
+
+int lbx_ensemble_checkpoint_bytes(lbx_ensemble E, int32_t slot, int64_t* bytes) {
+  if (!E || !bytes || slot < 0 || slot >= E->maxLattices || !E->slotUsed[size_t(slot)])
+    return lbx::set_error(LBX_ERR_INVALID, "not an admitted slot");
+  DeviceScope scope(E->device);
+  EnsLattice L;
+  ENS_TRY(cudaMemcpy(&L, E->dLat + slot, sizeof(L), cudaMemcpyDeviceToHost));
+  *bytes = int64_t(sizeof(EnsCheckpointHeader)) + slot_pop_bytes(E, L.P) + slot_snap_bytes(L.ncore);
+  return LBX_OK;
+}
+
+int lbx_ensemble_save_slot(lbx_ensemble E, int32_t slot, void* host, int64_t bytes, void* stream) {
+  if (!E || !host || slot < 0 || slot >= E->maxLattices || !E->slotUsed[size_t(slot)])
+    return lbx::set_error(LBX_ERR_INVALID, "not an admitted slot");
+  DeviceScope scope(E->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  ENS_TRY(cudaStreamSynchronize(s));
+  EnsLattice L;
+  long long g = 0;
+  ENS_TRY(cudaMemcpy(&L, E->dLat + slot, sizeof(L), cudaMemcpyDeviceToHost));
+  ENS_TRY(cudaMemcpy(&g, E->dGlobalStep, sizeof(g), cudaMemcpyDeviceToHost));
+  EnsCheckpointHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, "LBXENS01", 8);
+  h.q = E->q;
+  h.storage = E->storage;
+  h.core[0] = L.nx;
+  h.core[1] = L.ny;
+  h.core[2] = L.nz;
+  h.dynamics = L.dynamics;
+  h.state = L.state;
+  h.steps = L.steps;
+  h.maxSteps = L.maxSteps;
+  h.tol = L.tol;
+  h.residual = L.residual;
+  h.omega = L.omega;
+  h.magicParam = L.magic;
+  h.lid = E->slotLid[size_t(slot)];
+  h.P = L.P;
+  for (int k = 0; k < E->q; ++k) h.shift[k] = L.shift[g & 1][k];
+  h.popBytes = slot_pop_bytes(E, L.P);
+  h.snapBytes = slot_snap_bytes(L.ncore);
+  const int64_t need = int64_t(sizeof(h)) + h.popBytes + h.snapBytes;
+  if (bytes < need) return lbx::set_error(LBX_ERR_INVALID, "checkpoint buffer holds " + std::to_string(bytes) +
+                                                            " bytes, the slot needs " + std::to_string(need));
+  char* out = static_cast<char*>(host);
+  std::memcpy(out, &h, sizeof(h));
+  ENS_TRY(cudaMemcpyAsync(out + sizeof(h), L.pop, size_t(h.popBytes), cudaMemcpyDeviceToHost, s));
+  ENS_TRY(cudaMemcpyAsync(out + sizeof(h) + h.popBytes, L.snap, size_t(h.snapBytes), cudaMemcpyDeviceToHost, s));
+  ENS_TRY(cudaStreamSynchronize(s));
+  return LBX_OK;
+}
+
+int lbx_ensemble_restore_slot(lbx_ensemble E, const void* host, int64_t bytes, int32_t* slot, void* stream) {
+  if (!E || !host || !slot) return lbx::set_error(LBX_ERR_INVALID, "null argument");
+  if (bytes < int64_t(sizeof(EnsCheckpointHeader))) return lbx::set_error(LBX_ERR_INVALID, "checkpoint shorter than its header");
+  EnsCheckpointHeader h;
+  std::memcpy(&h, host, sizeof(h));
+  if (std::memcmp(h.magic, "LBXENS01", 8) != 0) return lbx::set_error(LBX_ERR_INVALID, "not an ensemble slot checkpoint");
+  if (h.q != E->q || h.storage != E->storage)
+    return lbx::set_error(LBX_ERR_INVALID, "checkpoint was taken from an ensemble of another descriptor or storage");
+  if (bytes < int64_t(sizeof(h)) + h.popBytes + h.snapBytes) return lbx::set_error(LBX_ERR_INVALID, "checkpoint truncated");
+  lbx_ensemble_request req;
+  std::memset(&req, 0, sizeof(req));
+  for (int a = 0; a < 3; ++a) req.core[a] = h.core[a];
+  req.dynamics = h.dynamics;
+  req.params.omega = h.omega;
+  req.params.magic = h.magicParam;
+  req.lid_velocity = h.lid;
+  req.tolerance = h.tol;
+  req.max_steps = h.maxSteps;
+  int32_t s0 = -1;
+  if (int rc = lbx_ensemble_admit(E, &req, &s0)) return rc;
+  DeviceScope scope(E->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  EnsLattice L;
+  cudaError_t e = cudaMemcpy(&L, E->dLat + s0, sizeof(L), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && (L.P != h.P || slot_pop_bytes(E, L.P) != h.popBytes || slot_snap_bytes(L.ncore) != h.snapBytes)) {
+    lbx_ensemble_retire(E, s0);
+    return lbx::set_error(LBX_ERR_INVALID, "checkpoint does not match the lattice its request describes");
+  }
+  const char* in = static_cast<const char*>(host) + sizeof(h);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(L.pop, in, size_t(h.popBytes), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(L.snap, in + h.popBytes, size_t(h.snapBytes), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    L.state = h.state;
+    L.steps = h.steps;
+    L.residual = h.residual;
+    // both parities: whichever this ensemble's next step reads
+    for (int k = 0; k < E->q; ++k) L.shift[0][k] = L.shift[1][k] = h.shift[k];
+    e = cudaMemcpyAsync(E->dLat + s0, &L, sizeof(L), cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    lbx_ensemble_retire(E, s0);
+    return lbx::set_error(LBX_ERR_CUDA, std::string("restore failed: ") + cudaGetErrorString(e));
+  }
+  *slot = s0;
   return LBX_OK;
 }
 

@@ -108,6 +108,9 @@ def _load() -> C.CDLL:
         "lbx_ensemble_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_set_launch_mode": ([VP, I32], C.c_int),
         "lbx_ensemble_set_cells_per_thread": ([VP, I32], C.c_int),
+        "lbx_ensemble_checkpoint_bytes": ([VP, I32, P(I64)], C.c_int),
+        "lbx_ensemble_save_slot": ([VP, I32, VP, I64, VP], C.c_int),
+        "lbx_ensemble_restore_slot": ([VP, VP, I64, P(I32), VP], C.c_int),
         "lbx_ensemble_footprint": ([I32, I32, P(EnsembleRequest), P(I64)], C.c_int),
         "lbx_ensemble_create": ([I32, I32, I64, I32, I32, P(VP)], C.c_int),
         "lbx_ensemble_destroy": ([VP], C.c_int),
@@ -499,6 +502,24 @@ class Ensemble:
     def set_launch_mode(self, mode: int) -> None:
         """0: one persistent kernel per run; 1: one launch per step, chained in a CUDA graph."""
         check(lib.lbx_ensemble_set_launch_mode(self._h, mode), "lbx_ensemble_set_launch_mode")
+
+    def save_slot(self, slot: int, stream=None) -> bytes:
+        """A slot's full state as bytes (pre-emption); the slot stays admitted."""
+        n = C.c_int64()
+        check(lib.lbx_ensemble_checkpoint_bytes(self._h, slot, C.byref(n)), "lbx_ensemble_checkpoint_bytes")
+        buf = np.empty(n.value, dtype=np.uint8)
+        check(lib.lbx_ensemble_save_slot(self._h, slot, _ptr(buf), n.value, _stream_ptr(stream)), "lbx_ensemble_save_slot")
+        return buf.tobytes()
+
+    def restore_slot(self, data: bytes, stream=None) -> int:
+        """Admits a saved slot, which continues where it stopped; returns its new slot."""
+        buf = np.frombuffer(data, dtype=np.uint8)
+        slot = C.c_int32(-1)
+        check(lib.lbx_ensemble_restore_slot(self._h, _ptr(buf), buf.size, C.byref(slot), _stream_ptr(stream)),
+              "lbx_ensemble_restore_slot")
+        core = np.frombuffer(data, dtype=np.int32, count=3, offset=16)  # the header's core extent
+        self.cells[slot.value] = int(core[0]) * int(core[1]) * int(core[2])
+        return slot.value
 
     def set_cells_per_thread(self, cells: int) -> None:
         """1 or 2 cells per thread in the tile loop (identical results)."""

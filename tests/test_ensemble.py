@@ -135,3 +135,36 @@ def test_invalid_requests_are_refused():
                     lbx.make_request((0, 8, 8), 1.5, 0.05)):
             with pytest.raises(lbx.LbxError):
                 ens.admit(req)
+
+
+def test_preempted_slot_resumes_exactly():
+    """Pre-emption: a slot saved mid-run and restored into another ensemble (whose global step
+    parity differs) continues bit for bit: populations, step count, residual and state."""
+    r1 = lbx.make_request((16, 14, 12), 1.2, 0.05, tolerance=0.0, max_steps=10 ** 9)
+    r2 = lbx.make_request((20, 18, 16), 1.7, 0.08, tolerance=1e-9, max_steps=10 ** 9, dynamics="trt")
+    with lbx.Ensemble(19, "f32", slab_bytes=256 << 20, max_lattices=8) as a, \
+            lbx.Ensemble(19, "f32", slab_bytes=256 << 20, max_lattices=8) as b:
+        a.set_config(threads=128, blocks_per_sm=0, check_interval=50)
+        b.set_config(threads=256, blocks_per_sm=0, check_interval=50)
+        a.admit(r1)
+        s2 = a.admit(r2)
+        a.run(150)
+        ckpt = a.save_slot(s2)
+        a.run(120)
+        want_status = a.statuses()[s2]
+        want = a.moments(s2)
+        other = b.admit(lbx.make_request((10, 10, 10), 1.5, 0.05, tolerance=0.0, max_steps=10 ** 9))
+        b.run(37)
+        s = b.restore_slot(ckpt)
+        assert s != other
+        assert b.statuses()[s][1] == 150
+        b.run(120)
+        assert b.statuses()[s] == want_status
+        got = b.moments(s)
+        assert all(np.array_equal(x, y) for x, y in zip(got, want))
+        assert b.statuses()[other][1] == 157
+        with pytest.raises(lbx.LbxError, match="checkpoint"):
+            b.restore_slot(ckpt[:100])
+    with lbx.Ensemble(19, "f64", slab_bytes=64 << 20, max_lattices=2) as c:
+        with pytest.raises(lbx.LbxError, match="checkpoint"):
+            c.restore_slot(ckpt)  # another storage form
