@@ -662,11 +662,16 @@ struct ColumnBases {
 };
 
 // Resident blocks per SM the step kernel is compiled for: the 16-bit forms move half the
-// bytes per request, so they need more warps in flight to keep HBM busy.
-// (D3Q27 keeps the compiler's choice: at 6 blocks its 27 values spill.)
+// bytes per request, so they need more warps in flight to keep HBM busy.  D3Q27 at one cell
+// per thread (16-bit and FP32): four blocks (64 registers, no spills; for the 16-bit forms
+// 24-38 % faster than the compiler's 96-142 registers for TRT and Smagorinsky-forced BGK); at
+// six blocks its 27 values spill.
 template <int Q, typename S, int K> struct StepOccupancy { static constexpr int blocks = 1; };
 template <> struct StepOccupancy<19, __half, 1> { static constexpr int blocks = 6; };
 template <> struct StepOccupancy<19, __nv_bfloat16, 1> { static constexpr int blocks = 6; };
+template <> struct StepOccupancy<27, float, 1> { static constexpr int blocks = 4; };
+template <> struct StepOccupancy<27, __half, 1> { static constexpr int blocks = 4; };
+template <> struct StepOccupancy<27, __nv_bfloat16, 1> { static constexpr int blocks = 4; };
 template <> struct StepOccupancy<9, __half, 1> { static constexpr int blocks = 6; };
 template <> struct StepOccupancy<9, __nv_bfloat16, 1> { static constexpr int blocks = 6; };
 // two cells per thread (the packed two-cell collision): 80 registers (three blocks); at four
