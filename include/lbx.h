@@ -139,15 +139,82 @@ int lbx_set_cell_dynamics(lbx_lattice lattice, const uint8_t* ids);
  * its populations as f^eq(rho, u) + f^neq(Pi) with Pi from finite-difference velocity gradients.
  * cells: core cell indices; kinds: lbx_fd_kind; dirs: normal axis; orients: +1 or -1, the
  * direction of the outward normal along that axis; values[4 * i ...]: the imposed velocity
- * (velocity cells) or {rho, tangential velocity} (pressure cells).  Flat faces only: every
- * cell needs two cells inward along its normal, and its neighbours along the face must be on
- * the face or across a periodic axis (edges and corners are rejected with
- * LBX_ERR_UNSUPPORTED).  The cells become LBX_CELL_FD_BOUNDARY in the cell dynamics map and
- * keep that id through later lbx_set_cell_dynamics calls; n = 0 removes the list.  A neighbour
- * reached across a periodic face contributes its j / rho, as the reference's overlap copy of
- * that cell does (it carries bulk dynamics). */
+ * (velocity cells) or {rho, tangential velocity} (pressure cells).  Every cell needs two cells
+ * inward along its normal inside the core.  Its neighbours along the face contribute the
+ * velocity their own dynamics give (computeU): a boundary cell of the list its momenta, a bulk
+ * cell j / rho, a cell without dynamics or with plain bounce-back (and a padding cell beyond a
+ * non-periodic face) zero.  Edges and corners take lbx_set_boundary_cells.  The cells become
+ * LBX_CELL_FD_BOUNDARY in the cell dynamics map and keep that id through later
+ * lbx_set_cell_dynamics calls; n = 0 removes the list.  A neighbour reached across a periodic
+ * face contributes its j / rho, as the reference's overlap copy of that cell does (it carries
+ * bulk dynamics). */
 int lbx_set_fd_boundaries(lbx_lattice lattice, int64_t n, const int64_t* cells, const int32_t* kinds,
                           const int32_t* dirs, const int32_t* orients, const double* values);
+
+/* Discrete normal types of a boundary cell (DiscreteNormalType, geometry/discreteNormals.h:33-39). */
+typedef enum {
+  LBX_NORMAL_FLAT = 0,
+  LBX_NORMAL_EXTERNAL_CORNER = 1,
+  LBX_NORMAL_INTERNAL_CORNER = 2,
+  LBX_NORMAL_EXTERNAL_EDGE = 3,   /* 3D only */
+  LBX_NORMAL_INTERNAL_EDGE = 4    /* 3D only */
+} lbx_normal_type;
+
+/* Discrete normal of every core cell of material `boundary` (computeBoundaryTypeAndNormal,
+ * geometry/discreteNormals.hh:31-172 in 2D and 176-1191 in 3D, as boundary::set calls it,
+ * boundary/setBoundary.h:80-99): a cell that is neither fluid nor outside is classified from
+ * the fluid / outside state of its neighbours; the outward normal points away from the fluid.
+ * A fluid cell is one whose material is in fluid[0..n_fluid), an outside cell one whose
+ * material is in outside[0..n_outside); cells beyond a non-periodic face of the block count as
+ * material 0, across a periodic face the partner cell is read.  A cell that matches no pattern
+ * comes back as LBX_NORMAL_FLAT with a zero normal.  Returns the number of boundary-material
+ * cells through n_out and, up to `cap` of them in ascending core-cell order, their core index,
+ * type and normal (normals[3 * k + a]; arrays may be NULL to count only).  Host only. */
+int lbx_discrete_normals(int32_t q, const int32_t core[3], const int32_t periodic[3], const int32_t* material,
+                         int32_t boundary, int32_t n_fluid, const int32_t* fluid, int32_t n_outside,
+                         const int32_t* outside, int64_t cap, int64_t* cells, int32_t* types, int32_t* normals,
+                         int64_t* n_out);
+
+/* Velocity / pressure boundary cells with their discrete normals: flat faces, external edges
+ * and external corners, what boundary::set<InterpolatedVelocity> / <InterpolatedPressure>
+ * install for each normal type (boundary/interpolatedVelocity3D.h:45-90,
+ * interpolatedVelocity2D.h:45-80, interpolatedPressure3D.h:48-90):
+ *   flat, velocity or pressure: as lbx_set_fd_boundaries (PlaneFdBoundaryProcessor3D /
+ *     StraightFdBoundaryProcessor2D);
+ *   external edge (3D), velocity: BGKdynamics with momenta::FixedVelocityBoundaryTuple
+ *     (rho = sum f + 1, u imposed; dynamics/momenta/aliases.h:215-220) and after each stream
+ *     OuterVelocityEdgeProcessor3D (boundary/boundaryPostProcessors3D.hh:164-238);
+ *   external corner, velocity: the same momenta and OuterVelocityCornerProcessor3D
+ *     (boundaryPostProcessors3D.hh:240-294) / OuterVelocityCornerProcessor2D
+ *     (boundaryPostProcessors2D.hh:278-323), run after the flat and edge processors as their
+ *     priority 1 orders them.
+ * kinds: lbx_fd_kind; types: lbx_normal_type; normals[3 * i + a]: outward normal components in
+ * {-1, 0, 1} (a flat cell has one non-zero component, an edge two, a corner d); values[4 * i]:
+ * the imposed velocity, or {rho, tangential velocity} of a pressure cell.  Every cell needs the
+ * two cells inward along each non-zero normal component inside the core, and no normal
+ * component may lie along a periodic axis.  Internal corners and edges, and pressure cells that
+ * are not flat, return LBX_ERR_UNSUPPORTED.  A neighbour that carries no dynamics or plain
+ * bounce-back (and a padding cell beyond a non-periodic face, the reference's NoDynamics
+ * overlap) reads as u = 0, rho = 1 in the finite differences, as their momenta
+ * (momenta::ZeroMomentum, OneDensity / FixedDensity) give it.  Replaces the boundary list of
+ * lbx_set_fd_boundaries; n = 0 removes it. */
+int lbx_set_boundary_cells(lbx_lattice lattice, int64_t n, const int64_t* cells, const int32_t* kinds,
+                           const int32_t* types, const int32_t* normals, const double* values);
+
+/* boundary::set<InterpolatedVelocity> (kind LBX_FD_VELOCITY) or <InterpolatedPressure>
+ * (LBX_FD_PRESSURE) over the core cells of material `boundary`, with the given fluid and outside
+ * material lists, or (n_fluid = 0, n_outside = 0) those of the reference's default overload
+ * (boundary/setBoundary.h:112-121: fluid 1, outside 0), followed by the values the application
+ * would give them with
+ * momenta::setVelocity / defineU or defineRho: values[4 * c ...] for core cell c (only the
+ * entries of the boundary cells are read).  Pressure cells that are not flat are left out, as
+ * the reference installs neither dynamics nor post-processor there; a velocity cell with no
+ * discrete normal fails as the reference's "Could not set Boundary." does
+ * (boundary/setBoundary3D.h:204-226).  The cells are added to those already set (a cell set
+ * twice takes the later call). */
+int lbx_set_interpolated_boundary(lbx_lattice lattice, int32_t kind, const int32_t* material, int32_t boundary,
+                                  int32_t n_fluid, const int32_t* fluid, int32_t n_outside, const int32_t* outside,
+                                  const double* values);
 
 /* Halfway bounce-back links: BouzidiVelocityPostProcessor with q = 1/2
  * (boundary/setBouzidiBoundary.h:129-162), applied after streaming.  Link l acts on core
@@ -226,8 +293,8 @@ int lbx_compute_moments(lbx_lattice lattice, double* rho, double* u, void* strea
 /* FP64 device reductions over the cells with bulk dynamics (SuperLatticeFieldReductionO,
  * core/superLatticeFieldReductionO.h; host functors SuperLpNorm3D, SuperLatticePhysDrag3D):
  *   LBX_REDUCE_MASS_MOMENTUM  out = {sum rho, sum j_x, sum j_y, sum j_z}
- *   LBX_REDUCE_DRAG           out = {F_x, F_y, F_z} momentum exchange over the links
- *                             (BlockLatticePhysBoundaryForce3D, latticePhysBoundaryForce3D.hh:88-116)
+ *   LBX_REDUCE_DRAG           out = {F_x, F_y, F_z} momentum exchange over all links, in the
+ *                             convention of lbx_boundary_force
  *   LBX_REDUCE_RESIDUAL       out = {||u - u_prev||_2, ||u||_2, max |u - u_prev|} against
  *                             the velocity snapshot of the previous RESIDUAL call, then
  *                             refreshes the snapshot (ValueTracer-style convergence). */
@@ -235,6 +302,17 @@ int lbx_compute_moments(lbx_lattice lattice, double* rho, double* u, void* strea
 #define LBX_REDUCE_DRAG 2
 #define LBX_REDUCE_RESIDUAL 3
 int lbx_reduce(lbx_lattice lattice, int32_t what, double* out, void* stream);
+
+/* Force on the solid behind a group of halfway bounce-back links, lattice units, FP64: the sum of
+ * the reference's boundary-force functor over that solid (SuperLatticePhysBoundaryForce3D summed
+ * by SuperSum3D; BlockLatticePhysBoundaryForce3D::operator(), functors/lattice/
+ * latticePhysBoundaryForce3D.hh:85-113): for every solid cell x_s and direction k towards a fluid
+ * cell, F -= c_k (f_k(x_s + c_k) + f_opp(k)(x_s)) on the stored values f - w, read after the last
+ * step's post-processing.  group: the index in `solid` of lbx_set_bouzidi_from_materials of the
+ * material whose force is wanted (links set by lbx_set_bouzidi_links are group 0), -1 for every
+ * link.  The drag coefficient of SuperLatticePhysDrag3D is 2 F / (rho U^2 A) of this force.
+ * Synchronises the stream. */
+int lbx_boundary_force(lbx_lattice lattice, int32_t group, double out[3], void* stream);
 
 /* Periodic-shift bookkeeping for a platform that keeps the reference's split collide /
  * stream calls: the device base of population column i at the current shift

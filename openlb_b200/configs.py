@@ -1,9 +1,9 @@
 """The larger benchmark configurations as runnable set-ups (the GPU path only).
 
-Channel past a sphere (default 512 x 128 x 128, D3Q27, TRT with magic 1/4): a sphere of
-diameter 24 at (128, 64, 64) with halfway bounce-back, uniform inflow 0.04 through a flat
-InterpolatedVelocity face at x = 0, an InterpolatedPressure face at the far end, periodic across
-the section, Re = U d / nu = 50.
+Channel past a sphere (default 512 x 128 x 128, D3Q27, TRT with magic 1/4): a duct with
+bounce-back side walls, a sphere of diameter 24 at (128, 64, 64) with halfway bounce-back,
+a parabolic inflow (RectanglePoiseuille3D, peak 0.04) through an InterpolatedVelocity face at
+x = 0 and an InterpolatedPressure face at the far end; Re = U_peak d / nu = 50.
 
 Porous medium (default 384^3, D3Q27, Smagorinsky-forced BGK with C_s = 0.12): non-overlapping
 spheres of diameter U[8, 20] placed by seeded random sequential addition towards porosity 0.6,
@@ -22,36 +22,81 @@ import numpy as np
 from . import lbx
 
 
-def channel_sphere(storage: str = "f16dev", extent=(512, 128, 128), u_in: float = 0.04, d: int = 24,
-                   re: float = 50.0) -> lbx.BlockLattice:
-    """The channel lattice, initialised at the inflow velocity and post-processed once."""
+def channel_materials(extent=(512, 128, 128), center=(128, 64, 64), d: float = 24) -> np.ndarray:
+    """Material map of the channel past a sphere: walls (2) on the outer layer of the box, the
+    inlet (3) and the outlet (4) on the interior of the x = 0 and x = end faces, the sphere (5):
+    the fluid cells within d / 2 of `center`, fluid (1) elsewhere."""
+    mat = np.full(extent, 2, np.int32)
+    mat[1:-1, 1:-1, 1:-1] = 1
+    mat[0, 1:-1, 1:-1] = 3
+    mat[-1, 1:-1, 1:-1] = 4
+    cx, cy, cz = center
+    r2 = (d / 2) ** 2
+    x = (np.arange(extent[0]) - cx)[:, None, None] ** 2
+    y = (np.arange(extent[1]) - cy)[None, :, None] ** 2
+    z = (np.arange(extent[2]) - cz)[None, None, :] ** 2
+    mat[(x + y + z <= r2) & (mat == 1)] = 5
+    return mat
+
+
+def poiseuille_inlet(material: np.ndarray, inlet: int, peak: float) -> np.ndarray:
+    """The inlet profile of RectanglePoiseuille3D over the cells of material `inlet` (functors/
+    analytical/frameChangeF3D.hh:449-553): the zero-velocity planes lie half a cell outside the
+    inlet's extent across the flow, and u = peak * 16 (d0/l0)(d1/l0)(d2/l1)(d3/l1) along the face
+    normal, d0, d1 (d2, d3) the distances to the two planes of the first (second) cross axis and
+    l0 = d0 + d1, l1 = d2 + d3.  Returns u[..., 3] over the whole map (zero off the inlet)."""
+    cells = np.argwhere(material == inlet)
+    lo, hi = cells.min(axis=0), cells.max(axis=0)
+    normal = int(np.nonzero(lo == hi)[0][0])
+    a1, a2 = [a for a in range(3) if a != normal]
+    s1, e1 = lo[a1] - 0.5, hi[a1] + 0.5
+    s2, e2 = lo[a2] - 0.5, hi[a2] + 0.5
+    d0 = cells[:, a1] - s1
+    d1 = e1 - cells[:, a1]
+    d2 = cells[:, a2] - s2
+    d3 = e2 - cells[:, a2]
+    l0 = d0 + d1
+    l1 = d2 + d3
+    factor = 16.0 * d0 / l0 * d1 / l0 * d2 / l1 * d3 / l1
+    u = np.zeros(material.shape + (3,))
+    u[tuple(cells.T) + (np.zeros(len(cells), int),)] = peak * factor
+    return u
+
+
+def channel_sphere(storage: str = "f16dev", extent=(512, 128, 128), u_peak: float = 0.04, d: float = 24,
+                   re: float = 50.0, center=None, rho_out: float = 1.0):
+    """The channel lattice at rest, post-processed once as SuperLattice::initialize does.
+    D3Q27 TRT with magic 1/4, nu = u_peak d / Re; no-slip side walls of BounceBack dynamics
+    (collision::Revert), halfway bounce-back on the sphere (link group 0);
+    boundary::set<InterpolatedVelocity> on the inlet with the RectanglePoiseuille3D
+    profile of peak u_peak along x, <InterpolatedPressure> with rho_out on the outlet.  Returns
+    (lattice, material map)."""
     nx, ny, nz = extent
-    nu = u_in * d / re
+    if center is None:
+        center = (nx // 4, ny // 2, nz // 2)
+    nu = u_peak * d / re
     omega = 1.0 / (3 * nu + 0.5)
-    cx, cy, cz = nx // 4, ny // 2, nz // 2
-    x, y, z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
-    solid = (x - cx) ** 2 + (y - cy) ** 2 + (z - cz) ** 2 <= (d / 2) ** 2
-    del x, y, z
-    mat = np.where(solid, 2, 1).astype(np.int32)
-    mat[0] = 3
-    mat[-1] = 4
-    lat = lbx.BlockLattice(27, (nx, ny, nz), (0, 1, 1), storage)
+    mat = channel_materials(extent, center, d)
+    lat = lbx.BlockLattice(27, extent, (0, 0, 0), storage)
     lat.define_dynamics("trt", omega=omega, magic=0.25)
-    lat.set_cell_dynamics(np.where(mat == 2, 0, 1).astype(np.uint8).reshape(-1))
-    lat.set_bouzidi_boundary(mat, 1, (2,))
-    n_face = ny * nz
-    inlet = np.arange(n_face, dtype=np.int64)
-    outlet = (nx - 1) * n_face + np.arange(n_face, dtype=np.int64)
-    values = np.zeros((2 * n_face, 4))
-    values[:n_face, 0] = u_in
-    values[n_face:, 0] = 1.0
-    lat.set_fd_boundaries(np.concatenate([inlet, outlet]), np.r_[np.ones(n_face), np.full(n_face, 2)],
-                          np.zeros(2 * n_face), np.r_[-np.ones(n_face), np.ones(n_face)], values)
-    u = np.zeros((3, nx * ny * nz))
-    u[0] = np.where(mat.reshape(-1) == 2, 0.0, u_in)
-    lat.ini_equilibrium(np.ones(nx * ny * nz), u)
+    cell = np.zeros(mat.shape, np.uint8)
+    cell[mat == 1] = lbx.CELL_BULK
+    cell[mat == 2] = lbx.CELL_BOUNCE_BACK
+    lat.set_cell_dynamics(cell.reshape(-1))
+    lat.set_bouzidi_boundary(mat, 1, (5,))
+    vals = np.zeros(mat.shape + (4,))
+    vals[..., :3] = poiseuille_inlet(mat, 3, u_peak)
+    vals[mat == 4, 0] = rho_out
+    vals = vals.reshape(-1, 4)
+    lat.set_interpolated_boundary(lbx.FD_VELOCITY, mat, 3, vals)
+    lat.set_interpolated_boundary(lbx.FD_PRESSURE, mat, 4, vals)
     lat.post_process()
-    return lat
+    return lat, mat
+
+
+def drag_coefficient(force_x: float, u: float, d: float, rho: float = 1.0) -> float:
+    """2 F_x / (rho u^2 A) with A = pi d^2 / 4, the frontal area of the sphere."""
+    return 2.0 * force_x / (rho * u * u * math.pi * d * d / 4.0)
 
 
 def porous_spheres(n: int, seed: int = 7, porosity: float = 0.6, batches: int = 400, batch: int = 1000) -> np.ndarray:
@@ -133,7 +178,7 @@ def main(argv=None) -> int:
     ap.add_argument("--no-autotune", action="store_true")
     a = ap.parse_args(argv)
     if a.case == "channel":
-        lat = channel_sphere(a.storage, tuple(a.size) if a.size else (512, 128, 128))
+        lat, _ = channel_sphere(a.storage, tuple(a.size) if a.size else (512, 128, 128))
     else:
         lat = porous_medium(porous_spheres(a.size[0] if a.size else 384), a.storage)
     if not a.no_autotune:

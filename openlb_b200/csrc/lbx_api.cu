@@ -79,7 +79,20 @@ double weight_of(int q, int i) {
 
 namespace lbx {
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
+// lbx_normals.cu
+int discrete_normals(int q, const int32_t core[3], const int32_t periodic[3], const int32_t* material,
+                     int32_t boundary, int32_t n_fluid, const int32_t* fluid, int32_t n_outside,
+                     const int32_t* outside, std::vector<int64_t>& cells, std::vector<int32_t>& types,
+                     std::vector<int32_t>& normals);
 }  // namespace lbx
+
+// A velocity / pressure boundary cell as set through the ABI.
+struct FdHostCell {
+  int64_t core = 0;
+  int32_t kind = 0, type = 0;
+  int32_t n[3] = {0, 0, 0};
+  double v[4] = {0, 0, 0, 0};
+};
 
 struct lbx_lattice_s {
   int q = 0, d = 0, storage = 0, device = 0;
@@ -96,6 +109,7 @@ struct lbx_lattice_s {
   uint32_t* linkCell = nullptr;
   uint8_t* linkDir = nullptr;
   void* linkDelta = nullptr;
+  uint8_t* linkGroup = nullptr;             // per link: index of the solid it faces
   int64_t nLinks = 0;
   // flat-face velocity / pressure boundary cells (lbx_set_fd_boundaries)
   int64_t nFd = 0;
@@ -104,6 +118,8 @@ struct lbx_lattice_s {
   double* fdValue = nullptr;
   double* fdMom = nullptr;
   std::vector<uint32_t> fdHostCells;  // padded indices, to re-mark after lbx_set_cell_dynamics
+  std::vector<FdHostCell> fdHost;     // the list as set (core cells ascending)
+  int64_t nFdCorners = 0;             // corner cells among them (second regularisation pass)
   StatAcc* stats = nullptr;
   double* statPart = nullptr;        // per-block statistics partials
   int64_t statCapacity = 0;          // blocks statPart holds
@@ -171,6 +187,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.fdMeta = L->fdMeta;
   a.fdValue = L->fdValue;
   a.fdMom = L->fdMom;
+  a.nFdCorners = L->nFdCorners;
   a.err = L->devErr;
   return a;
 }
@@ -480,6 +497,175 @@ bool device_ok(int device, std::string& why) {
   return true;
 }
 
+
+// Validates a boundary list, sorts it by cell and uploads it (lbx_set_fd_boundaries,
+// lbx_set_boundary_cells, lbx_set_interpolated_boundary).  The listed cells become
+// LBX_CELL_FD_BOUNDARY in the cell map; cells of the previous list that are not listed again
+// become bulk.
+int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
+  DeviceGuard guard(L->device);
+  const int64_t n = int64_t(list.size());
+  for (const FdHostCell& c : list) {
+    if (c.core < 0 || c.core >= L->ncore) return fail(LBX_ERR_INVALID, "boundary cell out of range");
+    if (c.kind != LBX_FD_VELOCITY && c.kind != LBX_FD_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+    if (c.type == LBX_NORMAL_INTERNAL_CORNER || c.type == LBX_NORMAL_INTERNAL_EDGE)
+      return fail(LBX_ERR_UNSUPPORTED, "internal corners and edges (concave boundaries) are not provided");
+    if (c.type != LBX_NORMAL_FLAT && c.type != LBX_NORMAL_EXTERNAL_CORNER && c.type != LBX_NORMAL_EXTERNAL_EDGE)
+      return fail(LBX_ERR_INVALID, "unknown normal type");
+    if (c.type == LBX_NORMAL_EXTERNAL_EDGE && L->d != 3) return fail(LBX_ERR_INVALID, "edges exist in 3D only");
+    if (c.kind == LBX_FD_PRESSURE && c.type != LBX_NORMAL_FLAT)
+      return fail(LBX_ERR_UNSUPPORTED, "pressure boundaries are provided on flat faces only");
+    int nonzero = 0;
+    for (int a = 0; a < 3; ++a) {
+      if (c.n[a] < -1 || c.n[a] > 1 || (a >= L->d && c.n[a] != 0)) return fail(LBX_ERR_INVALID, "normal components must be -1, 0 or 1");
+      nonzero += c.n[a] != 0;
+    }
+    const int want = c.type == LBX_NORMAL_FLAT ? 1 : (c.type == LBX_NORMAL_EXTERNAL_EDGE ? 2 : L->d);
+    if (nonzero != want) return fail(LBX_ERR_INVALID, "the normal does not match the normal type");
+    const int64_t ny = L->core[1], nz = (L->d == 3) ? L->core[2] : 1;
+    const int p[3] = {int(c.core / (ny * nz)), int((c.core / nz) % ny), int(c.core % nz)};
+    for (int a = 0; a < L->d; ++a) {
+      if (c.n[a] == 0) continue;
+      if (L->periodic[a]) return fail(LBX_ERR_INVALID, "a boundary normal cannot lie along a periodic axis");
+      const int in2 = p[a] - 2 * c.n[a];
+      if (in2 < 0 || in2 >= L->core[a])
+        return fail(LBX_ERR_INVALID, "a boundary cell needs two cells inward along each normal component");
+    }
+    for (int k = 0; k < 4; ++k)
+      if (!std::isfinite(c.v[k])) return fail(LBX_ERR_INVALID, "boundary values must be finite");
+    if (c.kind == LBX_FD_PRESSURE && !(c.v[0] > 0)) return fail(LBX_ERR_INVALID, "boundary density must be > 0");
+  }
+  std::sort(list.begin(), list.end(), [](const FdHostCell& x, const FdHostCell& y) { return x.core < y.core; });
+  for (int64_t i = 1; i < n; ++i)
+    if (list[size_t(i)].core == list[size_t(i - 1)].core) return fail(LBX_ERR_INVALID, "duplicate boundary cell");
+  std::vector<uint32_t> hc(static_cast<size_t>(n));
+  std::vector<uint8_t> hm(static_cast<size_t>(n));
+  std::vector<double> hv(static_cast<size_t>(4 * n));
+  int64_t corners = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    const FdHostCell& c = list[size_t(k)];
+    hc[size_t(k)] = uint32_t(core_index_to_padded(L, c.core));
+    int t = FD_FLAT_VELOCITY;
+    if (c.type == LBX_NORMAL_FLAT) t = c.kind == LBX_FD_PRESSURE ? FD_FLAT_PRESSURE : FD_FLAT_VELOCITY;
+    else if (c.type == LBX_NORMAL_EXTERNAL_EDGE) t = FD_EDGE_VELOCITY;
+    else t = FD_CORNER_VELOCITY;
+    corners += t == FD_CORNER_VELOCITY;
+    hm[size_t(k)] = FdMeta::encode(t, c.n);
+    for (int v = 0; v < 4; ++v) hv[size_t(4 * k + v)] = c.v[v];
+  }
+  cudaDeviceSynchronize();
+  cudaFree(L->fdCell);
+  cudaFree(L->fdMeta);
+  cudaFree(L->fdValue);
+  cudaFree(L->fdMom);
+  L->fdCell = nullptr;
+  L->fdMeta = nullptr;
+  L->fdValue = nullptr;
+  L->fdMom = nullptr;
+  L->nFd = 0;
+  L->nFdCorners = 0;
+  // cell map: the listed cells become LBX_CELL_FD_BOUNDARY, the ones of an old list bulk
+  std::vector<uint8_t> map(static_cast<size_t>(L->n), 0);
+  if (L->cellDyn) {
+    LBX_CUDA_TRY(cudaMemcpy(map.data(), L->cellDyn, size_t(L->n), cudaMemcpyDeviceToHost));
+  } else {
+    for (int64_t c = 0; c < L->ncore; ++c) map[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
+    LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
+  }
+  for (uint32_t old : L->fdHostCells) map[old] = LBX_CELL_BULK;
+  for (uint32_t c : hc) map[c] = LBX_CELL_FD_BOUNDARY;
+  L->fdHostCells = hc;
+  L->fdHost = list;
+  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, map.data(), size_t(L->n), cudaMemcpyHostToDevice));
+  if (n == 0) return LBX_OK;
+  LBX_CUDA_TRY(cudaMalloc(&L->fdCell, size_t(n) * sizeof(uint32_t)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdMeta, size_t(n)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdValue, size_t(4 * n) * sizeof(double)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdMom, size_t(7 * n) * sizeof(double)));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdMeta, hm.data(), size_t(n), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdValue, hv.data(), size_t(4 * n) * sizeof(double), cudaMemcpyHostToDevice));
+  L->nFd = n;
+  L->nFdCorners = corners;
+  return LBX_OK;
+}
+// Installs a link list (lbx_set_bouzidi_links, lbx_set_bouzidi_from_materials); groups[l] tags
+// link l with the solid it faces (NULL: every link in group 0).
+int set_links_impl(lbx_lattice_s* L, int64_t n, const int64_t* cells, const int32_t* dirs, const double* wall,
+                   const uint8_t* groups) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (n < 0 || (n > 0 && (!cells || !dirs))) return fail(LBX_ERR_INVALID, "bad link arrays");
+  DeviceGuard guard(L->device);
+  cudaFree(L->linkCell);
+  cudaFree(L->linkDir);
+  cudaFree(L->linkDelta);
+  cudaFree(L->linkGroup);
+  L->linkGroup = nullptr;
+  L->linkCell = nullptr;
+  L->linkDir = nullptr;
+  L->linkDelta = nullptr;
+  L->nLinks = 0;
+  if (n == 0) return LBX_OK;
+  std::vector<uint32_t> hc(static_cast<size_t>(n));
+  std::vector<uint8_t> hd(static_cast<size_t>(n));
+  std::vector<double> delta(static_cast<size_t>(n));
+  std::vector<uint8_t> hg(static_cast<size_t>(n), 0);
+  bool anyWall = false;
+  for (int64_t l = 0; l < n; ++l) {
+    if (cells[l] < 0 || cells[l] >= L->ncore) return fail(LBX_ERR_INVALID, "link cell out of range");
+    if (dirs[l] < 1 || dirs[l] >= L->q) return fail(LBX_ERR_INVALID, "link direction out of range");
+    hc[size_t(l)] = uint32_t(core_index_to_padded(L, cells[l]));
+    hd[size_t(l)] = uint8_t(dirs[l]);
+    if (groups) hg[size_t(l)] = groups[l];
+    // 2 * veloTerm, veloTerm = (c_k . u_w) * t_k * invCs2 (setBouzidiBoundary.h:146)
+    delta[size_t(l)] = wall ? 2.0 * (wall[l] * weight_of(L->q, dirs[l]) * 3.0) : 0.0;
+    if (delta[size_t(l)] != 0.0) anyWall = true;
+  }
+  // Links ordered by direction, then cell: neighbouring threads of the link kernel then read
+  // and write the same population column at nearby cells and share DRAM sectors, instead of
+  // touching q different columns for one cell.  Every link reads and writes its own slots, so
+  // the order does not change any result.
+  {
+    std::vector<int64_t> order(static_cast<size_t>(n));
+    for (int64_t l = 0; l < n; ++l) order[size_t(l)] = l;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+      return hd[size_t(a)] != hd[size_t(b)] ? hd[size_t(a)] < hd[size_t(b)] : hc[size_t(a)] < hc[size_t(b)];
+    });
+    std::vector<uint32_t> sc(hc.size());
+    std::vector<uint8_t> sd(hd.size());
+    std::vector<double> sdelta(delta.size());
+    std::vector<uint8_t> sg(hg.size());
+    for (size_t i = 0; i < order.size(); ++i) {
+      sc[i] = hc[size_t(order[i])];
+      sd[i] = hd[size_t(order[i])];
+      sdelta[i] = delta[size_t(order[i])];
+      sg[i] = hg[size_t(order[i])];
+    }
+    hc.swap(sc);
+    hd.swap(sd);
+    delta.swap(sdelta);
+    hg.swap(sg);
+  }
+  LBX_CUDA_TRY(cudaMalloc(&L->linkCell, size_t(n) * sizeof(uint32_t)));
+  LBX_CUDA_TRY(cudaMalloc(&L->linkDir, size_t(n)));
+  LBX_CUDA_TRY(cudaMemcpy(L->linkCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->linkDir, hd.data(), size_t(n), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMalloc(&L->linkGroup, size_t(n)));
+  LBX_CUDA_TRY(cudaMemcpy(L->linkGroup, hg.data(), size_t(n), cudaMemcpyHostToDevice));
+  if (anyWall) {
+    if (L->storage == LBX_F64) {
+      LBX_CUDA_TRY(cudaMalloc(&L->linkDelta, size_t(n) * sizeof(double)));
+      LBX_CUDA_TRY(cudaMemcpy(L->linkDelta, delta.data(), size_t(n) * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> df(delta.begin(), delta.end());
+      LBX_CUDA_TRY(cudaMalloc(&L->linkDelta, size_t(n) * sizeof(float)));
+      LBX_CUDA_TRY(cudaMemcpy(L->linkDelta, df.data(), size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  }
+  L->nLinks = n;
+  return LBX_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -567,6 +753,7 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->linkCell);
   cudaFree(L->linkDir);
   cudaFree(L->linkDelta);
+  cudaFree(L->linkGroup);
   cudaFree(L->fdCell);
   cudaFree(L->fdMeta);
   cudaFree(L->fdValue);
@@ -641,142 +828,91 @@ int lbx_set_fd_boundaries(lbx_lattice L, int64_t n, const int64_t* cells, const 
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   if (n < 0 || (n > 0 && (!cells || !kinds || !dirs || !orients || !values)))
     return fail(LBX_ERR_INVALID, "bad boundary arrays");
-  DeviceGuard guard(L->device);
-  // validate and sort by cell (the kernels binary-search the list)
-  std::vector<int64_t> order(static_cast<size_t>(n));
+  std::vector<FdHostCell> list(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
-    order[size_t(i)] = i;
-    if (cells[i] < 0 || cells[i] >= L->ncore) return fail(LBX_ERR_INVALID, "boundary cell out of range");
-    if (kinds[i] != LBX_FD_VELOCITY && kinds[i] != LBX_FD_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+    FdHostCell& c = list[size_t(i)];
+    c.core = cells[i];
+    c.kind = kinds[i];
+    c.type = LBX_NORMAL_FLAT;
     if (dirs[i] < 0 || dirs[i] >= L->d) return fail(LBX_ERR_INVALID, "normal axis out of range");
     if (orients[i] != 1 && orients[i] != -1) return fail(LBX_ERR_INVALID, "orientation must be +1 or -1");
-    if (L->periodic[dirs[i]]) return fail(LBX_ERR_INVALID, "a boundary normal cannot lie along a periodic axis");
-    for (int k = 0; k < 4; ++k)
-      if (!std::isfinite(values[4 * i + k])) return fail(LBX_ERR_INVALID, "boundary values must be finite");
-    if (kinds[i] == LBX_FD_PRESSURE && !(values[4 * i] > 0)) return fail(LBX_ERR_INVALID, "boundary density must be > 0");
+    c.n[dirs[i]] = orients[i];
+    for (int k = 0; k < 4; ++k) c.v[k] = values[4 * i + k];
   }
-  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cells[a] < cells[b]; });
-  for (int64_t i = 1; i < n; ++i)
-    if (cells[order[size_t(i)]] == cells[order[size_t(i - 1)]]) return fail(LBX_ERR_INVALID, "duplicate boundary cell");
-  // Flat faces only: the two cells inward along the normal must lie in the core, and along
-  // every other axis the face must continue (or the axis be periodic).
+  return install_boundary_list(L, std::move(list));
+}
+
+int lbx_set_boundary_cells(lbx_lattice L, int64_t n, const int64_t* cells, const int32_t* kinds, const int32_t* types,
+                           const int32_t* normals, const double* values) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (n < 0 || (n > 0 && (!cells || !kinds || !types || !normals || !values)))
+    return fail(LBX_ERR_INVALID, "bad boundary arrays");
+  std::vector<FdHostCell> list(static_cast<size_t>(n));
   for (int64_t i = 0; i < n; ++i) {
-    int64_t c = cells[i];
-    const int64_t ny = L->core[1], nz = L->core[2];
-    const int p[3] = {int(c / (ny * nz)), int((c / nz) % ny), int(c % nz)};
-    const int a = dirs[i];
-    const int in2 = p[a] - 2 * orients[i];
-    if (in2 < 0 || in2 >= L->core[a]) return fail(LBX_ERR_INVALID, "a boundary cell needs two cells inward along its normal");
-    for (int b = 0; b < L->d; ++b)
-      if (b != a && !L->periodic[b] && (p[b] == 0 || p[b] == L->core[b] - 1))
-        return fail(LBX_ERR_UNSUPPORTED, "boundary cell on an edge or corner (flat faces only)");
+    FdHostCell& c = list[size_t(i)];
+    c.core = cells[i];
+    c.kind = kinds[i];
+    c.type = types[i];
+    for (int a = 0; a < 3; ++a) c.n[a] = normals[3 * i + a];
+    for (int k = 0; k < 4; ++k) c.v[k] = values[4 * i + k];
   }
-  std::vector<uint32_t> hc(static_cast<size_t>(n));
-  std::vector<uint8_t> hm(static_cast<size_t>(n));
-  std::vector<double> hv(static_cast<size_t>(4 * n));
-  for (int64_t k = 0; k < n; ++k) {
-    const int64_t i = order[size_t(k)];
-    hc[size_t(k)] = uint32_t(core_index_to_padded(L, cells[i]));
-    hm[size_t(k)] = uint8_t(dirs[i] | (orients[i] > 0 ? 4 : 0) | (kinds[i] == LBX_FD_PRESSURE ? 8 : 0));
-    for (int v = 0; v < 4; ++v) hv[size_t(4 * k + v)] = values[4 * i + v];
+  return install_boundary_list(L, std::move(list));
+}
+
+int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* material, int32_t boundary,
+                                  int32_t n_fluid, const int32_t* fluid, int32_t n_outside, const int32_t* outside,
+                                  const double* values) {
+  if (!L || !material || !values) return fail(LBX_ERR_INVALID, "null argument");
+  if (kind != LBX_FD_VELOCITY && kind != LBX_FD_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+  const int32_t defFluid = 1, defOutside = 0;
+  if (n_fluid == 0) {
+    fluid = &defFluid;
+    n_fluid = 1;
   }
-  cudaDeviceSynchronize();
-  cudaFree(L->fdCell);
-  cudaFree(L->fdMeta);
-  cudaFree(L->fdValue);
-  cudaFree(L->fdMom);
-  L->fdCell = nullptr;
-  L->fdMeta = nullptr;
-  L->fdValue = nullptr;
-  L->fdMom = nullptr;
-  L->nFd = 0;
-  // cell map: the listed cells become LBX_CELL_FD_BOUNDARY, the ones of an old list bulk
-  std::vector<uint8_t> map(static_cast<size_t>(L->n), 0);
-  if (L->cellDyn) {
-    LBX_CUDA_TRY(cudaMemcpy(map.data(), L->cellDyn, size_t(L->n), cudaMemcpyDeviceToHost));
-  } else {
-    for (int64_t c = 0; c < L->ncore; ++c) map[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
-    LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
+  if (n_outside == 0) {
+    outside = &defOutside;
+    n_outside = 1;
   }
-  for (uint32_t old : L->fdHostCells) map[old] = LBX_CELL_BULK;
-  for (uint32_t c : hc) map[c] = LBX_CELL_FD_BOUNDARY;
-  L->fdHostCells = hc;
-  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, map.data(), size_t(L->n), cudaMemcpyHostToDevice));
-  if (n == 0) return LBX_OK;
-  LBX_CUDA_TRY(cudaMalloc(&L->fdCell, size_t(n) * sizeof(uint32_t)));
-  LBX_CUDA_TRY(cudaMalloc(&L->fdMeta, size_t(n)));
-  LBX_CUDA_TRY(cudaMalloc(&L->fdValue, size_t(4 * n) * sizeof(double)));
-  LBX_CUDA_TRY(cudaMalloc(&L->fdMom, size_t(7 * n) * sizeof(double)));
-  LBX_CUDA_TRY(cudaMemcpy(L->fdCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  LBX_CUDA_TRY(cudaMemcpy(L->fdMeta, hm.data(), size_t(n), cudaMemcpyHostToDevice));
-  LBX_CUDA_TRY(cudaMemcpy(L->fdValue, hv.data(), size_t(4 * n) * sizeof(double), cudaMemcpyHostToDevice));
-  L->nFd = n;
-  return LBX_OK;
+  std::vector<int64_t> cells;
+  std::vector<int32_t> types, normals;
+  if (int rc = discrete_normals(L->q, L->core, L->periodic, material, boundary, n_fluid, fluid, n_outside, outside,
+                                cells, types, normals))
+    return rc;
+  std::vector<FdHostCell> add;
+  for (size_t k = 0; k < cells.size(); ++k) {
+    const int t = types[k];
+    const int* nn = &normals[3 * k];
+    if (t < 0) return fail(LBX_ERR_INVALID, "the boundary material is also a fluid or outside material");
+    const bool zero = nn[0] == 0 && nn[1] == 0 && nn[2] == 0;
+    if (kind == LBX_FD_PRESSURE && (t != LBX_NORMAL_FLAT || zero)) {
+      if (zero) return fail(LBX_ERR_UNSUPPORTED, "could not set boundary: a pressure cell has no discrete normal");
+      continue;  // InterpolatedPressure installs nothing on edges and corners
+    }
+    if (zero) return fail(LBX_ERR_UNSUPPORTED, "could not set boundary: a velocity cell has no discrete normal");
+    if (t == LBX_NORMAL_INTERNAL_CORNER || t == LBX_NORMAL_INTERNAL_EDGE)
+      return fail(LBX_ERR_UNSUPPORTED, "internal corners and edges (concave boundaries) are not provided");
+    FdHostCell c;
+    c.core = cells[k];
+    c.kind = kind;
+    c.type = t;
+    for (int a = 0; a < 3; ++a) c.n[a] = nn[a];
+    for (int v = 0; v < 4; ++v) c.v[v] = values[4 * cells[k] + v];
+    add.push_back(c);
+  }
+  // merge with the cells already set: a cell set again takes the new entry
+  std::vector<FdHostCell> list;
+  {
+    std::vector<char> taken(static_cast<size_t>(L->ncore), 0);
+    for (const FdHostCell& c : add) taken[size_t(c.core)] = 1;
+    for (const FdHostCell& c : L->fdHost)
+      if (!taken[size_t(c.core)]) list.push_back(c);
+    list.insert(list.end(), add.begin(), add.end());
+  }
+  return install_boundary_list(L, std::move(list));
 }
 
 int lbx_set_bouzidi_links(lbx_lattice L, int64_t n, const int64_t* cells, const int32_t* dirs, const double* wall) {
-  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
-  if (n < 0 || (n > 0 && (!cells || !dirs))) return fail(LBX_ERR_INVALID, "bad link arrays");
-  DeviceGuard guard(L->device);
-  cudaFree(L->linkCell);
-  cudaFree(L->linkDir);
-  cudaFree(L->linkDelta);
-  L->linkCell = nullptr;
-  L->linkDir = nullptr;
-  L->linkDelta = nullptr;
-  L->nLinks = 0;
-  if (n == 0) return LBX_OK;
-  std::vector<uint32_t> hc(static_cast<size_t>(n));
-  std::vector<uint8_t> hd(static_cast<size_t>(n));
-  std::vector<double> delta(static_cast<size_t>(n));
-  bool anyWall = false;
-  for (int64_t l = 0; l < n; ++l) {
-    if (cells[l] < 0 || cells[l] >= L->ncore) return fail(LBX_ERR_INVALID, "link cell out of range");
-    if (dirs[l] < 1 || dirs[l] >= L->q) return fail(LBX_ERR_INVALID, "link direction out of range");
-    hc[size_t(l)] = uint32_t(core_index_to_padded(L, cells[l]));
-    hd[size_t(l)] = uint8_t(dirs[l]);
-    // 2 * veloTerm, veloTerm = (c_k . u_w) * t_k * invCs2 (setBouzidiBoundary.h:146)
-    delta[size_t(l)] = wall ? 2.0 * (wall[l] * weight_of(L->q, dirs[l]) * 3.0) : 0.0;
-    if (delta[size_t(l)] != 0.0) anyWall = true;
-  }
-  // Links ordered by direction, then cell: neighbouring threads of the link kernel then read
-  // and write the same population column at nearby cells and share DRAM sectors, instead of
-  // touching q different columns for one cell.  Every link reads and writes its own slots, so
-  // the order does not change any result.
-  {
-    std::vector<int64_t> order(static_cast<size_t>(n));
-    for (int64_t l = 0; l < n; ++l) order[size_t(l)] = l;
-    std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
-      return hd[size_t(a)] != hd[size_t(b)] ? hd[size_t(a)] < hd[size_t(b)] : hc[size_t(a)] < hc[size_t(b)];
-    });
-    std::vector<uint32_t> sc(hc.size());
-    std::vector<uint8_t> sd(hd.size());
-    std::vector<double> sdelta(delta.size());
-    for (size_t i = 0; i < order.size(); ++i) {
-      sc[i] = hc[size_t(order[i])];
-      sd[i] = hd[size_t(order[i])];
-      sdelta[i] = delta[size_t(order[i])];
-    }
-    hc.swap(sc);
-    hd.swap(sd);
-    delta.swap(sdelta);
-  }
-  LBX_CUDA_TRY(cudaMalloc(&L->linkCell, size_t(n) * sizeof(uint32_t)));
-  LBX_CUDA_TRY(cudaMalloc(&L->linkDir, size_t(n)));
-  LBX_CUDA_TRY(cudaMemcpy(L->linkCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  LBX_CUDA_TRY(cudaMemcpy(L->linkDir, hd.data(), size_t(n), cudaMemcpyHostToDevice));
-  if (anyWall) {
-    if (L->storage == LBX_F64) {
-      LBX_CUDA_TRY(cudaMalloc(&L->linkDelta, size_t(n) * sizeof(double)));
-      LBX_CUDA_TRY(cudaMemcpy(L->linkDelta, delta.data(), size_t(n) * sizeof(double), cudaMemcpyHostToDevice));
-    } else {
-      std::vector<float> df(delta.begin(), delta.end());
-      LBX_CUDA_TRY(cudaMalloc(&L->linkDelta, size_t(n) * sizeof(float)));
-      LBX_CUDA_TRY(cudaMemcpy(L->linkDelta, df.data(), size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
-    }
-  }
-  L->nLinks = n;
-  return LBX_OK;
+  return set_links_impl(L, n, cells, dirs, wall, nullptr);
 }
 
 int lbx_build_bouzidi_links(int32_t q, const int32_t core[3], const int32_t periodic[3], const int32_t* material,
@@ -840,7 +976,25 @@ int lbx_set_bouzidi_from_materials(lbx_lattice L, const int32_t* material, int32
   rc = lbx_build_bouzidi_links(L->q, L->core, L->periodic, material, fluid, n_solid, solid, wall_velocity, n,
                                cells.data(), dirs.data(), wall.data(), &n);
   if (rc != LBX_OK) return rc;
-  return lbx_set_bouzidi_links(L, n, cells.data(), dirs.data(), wall_velocity ? wall.data() : nullptr);
+  if (n_solid > 255) return fail(LBX_ERR_INVALID, "at most 255 solid materials");
+  // group of each link: the index in `solid` of the material of the solid neighbour
+  std::vector<uint8_t> groups(static_cast<size_t>(n), 0);
+  {
+    const int64_t ny = L->core[1], nz = (L->d == 3) ? L->core[2] : 1;
+    for (int64_t l = 0; l < n; ++l) {
+      const int* c = velocity(L->q, dirs[size_t(l)]);
+      int64_t p[3] = {cells[size_t(l)] / (ny * nz), (cells[size_t(l)] / nz) % ny, cells[size_t(l)] % nz};
+      const int64_t ext[3] = {L->core[0], ny, nz};
+      for (int a = 0; a < L->d; ++a) p[a] = ((p[a] + c[a]) % ext[a] + ext[a]) % ext[a];
+      const int32_t m = material[(p[0] * ny + p[1]) * nz + p[2]];
+      for (int32_t j = 0; j < n_solid; ++j)
+        if (solid[j] == m) {
+          groups[size_t(l)] = uint8_t(j);
+          break;
+        }
+    }
+  }
+  return set_links_impl(L, n, cells.data(), dirs.data(), wall_velocity ? wall.data() : nullptr, groups.data());
 }
 
 int lbx_upload_populations(lbx_lattice L, const void* host, int32_t host_type, void* stream) {
@@ -1107,8 +1261,8 @@ int lbx_reduce(lbx_lattice L, int32_t what, double* out, void* stream) {
     LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_mass_momentum<Q, S>(a, L->reducePart, L->reduceAcc, s))));
     break;
   case LBX_REDUCE_DRAG:
-    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_link_force<Q, S>(a, L->linkCell, L->linkDir, L->nLinks, L->reducePart,
-                                                          L->reduceAcc, s))));
+    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_link_force<Q, S>(a, L->linkCell, L->linkDir, L->linkGroup, -1, L->nLinks,
+                                                          L->reducePart, L->reduceAcc, s))));
     break;
   default:
     if (!L->residualSnap) {
@@ -1131,6 +1285,29 @@ int lbx_reduce(lbx_lattice L, int32_t what, double* out, void* stream) {
     out[1] = std::sqrt(h[1]);
     out[2] = h[2];
   }
+  return LBX_OK;
+}
+
+int lbx_boundary_force(lbx_lattice L, int32_t group, double out[3], void* stream) {
+  if (!L || !out) return fail(LBX_ERR_INVALID, "null argument");
+  if (group < -1 || group > 254) return fail(LBX_ERR_INVALID, "group must be -1 (all links) or a solid index");
+  DeviceGuard guard(L->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const LaunchArgs a = args_of(L);
+  const int64_t need = reduce_blocks(std::max<int64_t>(L->ncore, L->nLinks)) + 1;
+  if (need > L->reducePartCapacity) {
+    cudaFree(L->reducePart);
+    L->reducePart = nullptr;
+    L->reducePartCapacity = 0;
+    LBX_CUDA_TRY(cudaMalloc(&L->reducePart, size_t(need) * 4 * sizeof(double)));
+    L->reducePartCapacity = need;
+  }
+  double h[4] = {};
+  LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_link_force<Q, S>(a, L->linkCell, L->linkDir, L->linkGroup, group, L->nLinks,
+                                                        L->reducePart, L->reduceAcc, s))));
+  LBX_CUDA_TRY(cudaMemcpyAsync(h, L->reduceAcc, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  LBX_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int k = 0; k < 3; ++k) out[k] = h[k];
   return LBX_OK;
 }
 

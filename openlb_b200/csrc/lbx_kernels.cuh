@@ -962,27 +962,65 @@ __global__ void __launch_bounds__(256) k_bouzidi(S* __restrict__ pop, Geometry g
                     v - (delta ? delta[l] : R(0)));
 }
 
-// ---- flat-face velocity / pressure boundaries (InterpolatedVelocity / InterpolatedPressure)
-// A boundary cell carries a meta byte: bits 0-1 the normal axis d, bit 2 set for an outward
-// normal along +d (orientation +1, else -1), bit 3 set for a pressure cell (else velocity), and
+// ---- velocity / pressure boundaries (InterpolatedVelocity / InterpolatedPressure) ---------
+// A boundary cell carries a meta byte: bits 0-1 the cell type (0 flat velocity, 1 flat
+// pressure, 2 external edge (3D) with imposed velocity, 3 external corner with imposed
+// velocity), bits 2-7 the outward discrete normal, two bits per axis (0: 0, 1: +1, 2: -1), and
 // four values: the imposed velocity, or {rho, tangential velocity}.  Reference: the boundary
-// momenta momenta::BasicDirichletVelocityBoundaryTuple / BasicDirichletPressureBoundaryTuple
-// (dynamics/momenta/aliases.h:173-198) mixed into BGKdynamics for the collision, and the
-// post-stream PlaneFdBoundaryProcessor3D / StraightFdBoundaryProcessor2D
-// (boundary/boundaryPostProcessors3D.hh:39-93, boundaryPostProcessors2D.hh:39-76).
+// momenta mixed into BGKdynamics for the collision (momenta::BasicDirichletVelocityBoundaryTuple
+// / BasicDirichletPressureBoundaryTuple on flat faces, FixedVelocityBoundaryTuple on edges and
+// corners, dynamics/momenta/aliases.h:173-220), and the post-stream processors
+// PlaneFdBoundaryProcessor3D / StraightFdBoundaryProcessor2D (boundary/boundaryPostProcessors3D.hh:
+// 39-93, boundaryPostProcessors2D.hh:39-76), OuterVelocityEdgeProcessor3D (3D.hh:164-238) and
+// OuterVelocityCornerProcessor3D / 2D (3D.hh:240-294, 2D.hh:276-323).
+enum FdType { FD_FLAT_VELOCITY = 0, FD_FLAT_PRESSURE = 1, FD_EDGE_VELOCITY = 2, FD_CORNER_VELOCITY = 3 };
+
 struct FdMeta {
-  int dir, orient, pressure;
-  __device__ __forceinline__ explicit FdMeta(uint8_t m)
-      : dir(m & 3), orient((m & 4) ? 1 : -1), pressure((m >> 3) & 1) {}
+  int type;
+  int n[3];         // outward normal
+  int dir, orient;  // flat cells: the normal axis and its sign
+  int pressure;
+  __host__ __device__ __forceinline__ explicit FdMeta(uint8_t m) : type(m & 3), dir(0), orient(0), pressure((m & 3) == 1) {
+    for (int a = 0; a < 3; ++a) {
+      const int code = (m >> (2 + 2 * a)) & 3;
+      n[a] = code == 1 ? 1 : (code == 2 ? -1 : 0);
+    }
+    for (int a = 2; a >= 0; --a)
+      if (n[a] != 0) {
+        dir = a;
+        orient = n[a];
+      }
+  }
+  static __host__ __device__ __forceinline__ uint8_t encode(int type, const int* normal) {
+    unsigned m = unsigned(type & 3);
+    for (int a = 0; a < 3; ++a) m |= unsigned(normal[a] == 1 ? 1 : (normal[a] == -1 ? 2 : 0)) << (2 + 2 * a);
+    return uint8_t(m);
+  }
 };
 
-// rho and u of a boundary cell from its momenta (velocityBMRho, dynamics/momenta/elements.h:54-71;
-// FixedPressureMomentum::computeU, elements.h:653-690): rho_onWall sums the populations with
-// c_d = 0, rho_normal those with c_d = orientation, each in index order.
+// Plain rho = sum f + 1 (lbm::computeRho, dynamics/lbm.h:289-297: BulkDensity).
+template <int Q, typename R>
+__device__ __forceinline__ R bulk_rho(const R (&f)[Q]) {
+  R rho = R(0);
+  static_for<Q>([&](auto I) { rho += f[I]; });
+  return rho + R(1);
+}
+
+// rho and u of a boundary cell from its momenta.  Flat velocity: u imposed, rho = velocityBMRho
+// (dynamics/momenta/elements.h:54-71) with rho_onWall summing the populations with c_d = 0 and
+// rho_normal those with c_d = orientation, each in index order.  Flat pressure: rho imposed,
+// the tangential velocity imposed and u_d from the populations (FixedPressureMomentum::computeU,
+// elements.h:653-690).  Edge and corner: u imposed, rho = sum f + 1 (BulkDensity).
 template <int Q, typename R>
 __device__ __forceinline__ void fd_momenta(const R (&f)[Q], FdMeta m, const double* __restrict__ v, R& rho,
                                            R (&u)[3]) {
   using D = Desc<Q>;
+  u[0] = u[1] = u[2] = R(0);
+  if (m.type >= FD_EDGE_VELOCITY) {
+    static_for<D::d>([&](auto A) { u[A] = R(v[A]); });
+    rho = bulk_rho<Q, R>(f);
+    return;
+  }
   R onWall = R(0), normal = R(0);
   static_for<Q>([&](auto I) {
     constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
@@ -994,7 +1032,6 @@ __device__ __forceinline__ void fd_momenta(const R (&f)[Q], FdMeta m, const doub
     const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
     if (c == m.orient) normal += f[I];
   });
-  u[0] = u[1] = u[2] = R(0);
   if (!m.pressure) {
     static_for<D::d>([&](auto A) { u[A] = R(v[A]); });
     rho = (R(2) * normal + onWall + R(1)) / (R(1) + R(m.orient) * u[m.dir]);
@@ -1014,13 +1051,13 @@ __device__ __forceinline__ R equilibrium_plain(R rho, const R (&u)[3], R uSqr) {
   return rho * t * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * uSqr) - t;
 }
 
-// Plain j / rho of a cell (BulkMomentum::computeU, dynamics/momenta/elements.h:500-508).
+// u of a bulk cell through its momenta: j / rho (BulkMomentum::computeU, dynamics/momenta/
+// elements.h:500-508), plus F / 2 for the forced dynamics (ForcedMomentum, elements.h:1600-1608;
+// halfF is zero otherwise).
 template <int Q, typename R>
-__device__ __forceinline__ void bulk_velocity(const R (&f)[Q], R (&u)[3]) {
+__device__ __forceinline__ void bulk_velocity(const R (&f)[Q], const R (&halfF)[3], R (&u)[3]) {
   using D = Desc<Q>;
-  R rho = R(0);
-  static_for<Q>([&](auto I) { rho += f[I]; });
-  rho += R(1);
+  const R rho = bulk_rho<Q, R>(f);
   u[0] = u[1] = u[2] = R(0);
   static_for<Q>([&](auto I) {
     static_for<D::d>([&](auto A) {
@@ -1029,7 +1066,10 @@ __device__ __forceinline__ void bulk_velocity(const R (&f)[Q], R (&u)[3]) {
       else if constexpr (c == -1) u[A] -= f[I];
     });
   });
-  static_for<D::d>([&](auto A) { u[A] /= rho; });
+  static_for<D::d>([&](auto A) {
+    u[A] /= rho;
+    u[A] += halfF[A];
+  });
 }
 
 __device__ __forceinline__ void fd_decode(const Geometry& g, int64_t n, int& x, int& y, int& z) {
@@ -1093,14 +1133,16 @@ __global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometr
   if (statPart) block_partial(aR, aU, aU, aC, statPart);
 }
 
-// Post-stream pass 1: every boundary cell's velocity from its momenta, its plain j / rho (what a
-// neighbour reached across a periodic face sees: the reference's overlap copy of the cell,
-// which carries bulk dynamics) and its rho, from the populations before any cell is rewritten.
+// Post-stream pass 1: every boundary cell's velocity and density from its momenta, and its
+// bulk velocity (what a neighbour reached across a periodic face sees: the reference's overlap
+// copy of the cell, which carries bulk dynamics), from the populations before any cell is
+// rewritten.  fdMom[7 b ...] = {u, u_bulk, rho}.
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_fd_momenta(const S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t nFd,
                                                     const uint32_t* __restrict__ fdCell,
                                                     const uint8_t* __restrict__ fdMeta,
-                                                    const double* __restrict__ fdValue, double* __restrict__ fdMom) {
+                                                    const double* __restrict__ fdValue, double hfx, double hfy,
+                                                    double hfz, double* __restrict__ fdMom) {
   using R = typename Storage<S>::R;
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (b >= nFd) return;
@@ -1108,8 +1150,9 @@ __global__ void __launch_bounds__(256) k_fd_momenta(const S* __restrict__ pop, G
   R f[Q];
   static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
   R rho, u[3], ub[3];
+  const R halfF[3] = {R(hfx), R(hfy), R(hfz)};
   fd_momenta<Q, R>(f, FdMeta(fdMeta[b]), fdValue + 4 * b, rho, u);
-  bulk_velocity<Q, R>(f, ub);
+  bulk_velocity<Q, R>(f, halfF, ub);
   double* out = fdMom + 7 * b;
   for (int a = 0; a < 3; ++a) {
     out[a] = double(u[a]);
@@ -1131,65 +1174,135 @@ __device__ __forceinline__ int64_t fd_find(const uint32_t* __restrict__ fdCell, 
   return -1;
 }
 
-// Post-stream pass 2: the regularised populations of every boundary cell
-// (PlaneFdBoundaryProcessor3D::apply / StraightFdBoundaryProcessor2D::apply): velocity gradients
-// by fd::DirectedGradients (utilities/finiteDifference3D.h:74-210) -- along the normal the
-// one-sided -o (-3 u0 + 4 u1 - u2) / 2 from the cell and the two cells inward, along the face
-// the central (u(+1) - u(-1)) / 2 --, Pi = -rho / (c_s^-2 omega) (grad u + grad u^T) and
-// f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270).  Neighbours' velocities
-// come from pass 1 (boundary cells) or their populations (bulk cells, not written here), so
-// the result does not depend on the order the cells are processed in.
+// Post-stream passes 2 and 3: the regularised populations f_i = f_i^eq(rho, u) +
+// fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270) with Pi = -rho / (c_s^-2 omega) (grad u + grad u^T)
+// of every boundary cell.  Velocity gradients by fd::DirectedGradients (utilities/
+// finiteDifference3D.h:74-210, finiteDifference2D.h): along a non-zero normal component n_a the
+// one-sided -n_a (-3 u0 + 4 u1 - u2) / 2 from the cell and the two cells inward, along the other
+// axes the central (u(+1) - u(-1)) / 2.  rho: a flat cell's own (momenta); an edge extrapolates
+// 2/3 (rho_B1 + rho_A1) - 1/6 (rho_B2 + rho_A2) from the cells one and two steps inward along its
+// two normal axes A < B in the cyclic order after the edge axis (OuterVelocityEdgeProcessor3D::
+// getNeighborRho), a 2D corner the same with A = x, B = y, a 3D corner
+// 4/9 (rho_z1 + rho_y1 + rho_x1) - 1/9 (rho_z2 + rho_y2 + rho_x2).
+// Pass 2 (`corners` = 0) rebuilds the flat and edge cells, whose processors have priority 0;
+// pass 3 (`corners` = 1) the corners, priority 1, after them, as the reference orders the
+// post-processors of a stage.  Neighbour velocities come from pass 1 (boundary cells: their
+// momenta; the imposed velocity of velocity cells does not depend on the order) or from the
+// populations (bulk cells, never rewritten here); cells without dynamics or with plain
+// bounce-back, and padding cells, read u = 0, rho = 1 (ZeroMomentum with OneDensity /
+// FixedDensity).  Neighbour densities in pass 2 come from pass 1; in pass 3 from the current
+// populations, i.e. those the priority-0 processors left, as the reference's corner processor
+// reads them.
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geometry g, Shifts<Q> sh, double omega,
                                                        int64_t nFd, const uint32_t* __restrict__ fdCell,
                                                        const uint8_t* __restrict__ fdMeta,
-                                                       const double* __restrict__ fdMom) {
+                                                       const double* __restrict__ fdValue,
+                                                       const uint8_t* __restrict__ cellDyn, double hfx, double hfy,
+                                                       double hfz, const double* __restrict__ fdMom, int corners) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (b >= nFd) return;
-  const int64_t n = fdCell[b];
   const FdMeta m(fdMeta[b]);
+  if ((m.type == FD_CORNER_VELOCITY) != (corners != 0)) return;
+  const int64_t n = fdCell[b];
   int pos[3];
   fd_decode(g, n, pos[0], pos[1], pos[2]);
   const int ext[3] = {g.nx, g.ny, g.nz};
+  const R halfF[3] = {R(hfx), R(hfy), R(hfz)};
   const double* own = fdMom + 7 * b;
-  const R rho = R(own[6]);
   R u[3] = {R(own[0]), R(own[1]), R(own[2])};
-  auto velocity_at = [&](int px, int py, int pz, bool wrapped, R (&v)[3]) {
-    const int64_t nn = int64_t(px + 1) * g.sx + int64_t(py + 1) * g.sy + (pz + g.pz);
+  auto padded_of = [&](const int (&p)[3]) -> int64_t {
+    return int64_t(p[0] + 1) * g.sx + int64_t(p[1] + 1) * g.sy + (p[2] + g.pz);
+  };
+  auto load_cell = [&](int64_t nn, R (&f)[Q]) {
+    static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(nn, sh.s[I], g.n)); });
+  };
+  auto velocity_at = [&](const int (&p)[3], bool wrapped, R (&v)[3]) {
+    const int64_t nn = padded_of(p);
     const int64_t j = fd_find(fdCell, nFd, uint32_t(nn));
     if (j >= 0) {
       const double* mm = fdMom + 7 * j + (wrapped ? 3 : 0);
       v[0] = R(mm[0]);
       v[1] = R(mm[1]);
       v[2] = R(mm[2]);
-    } else {
+      return;
+    }
+    const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
+    if (kind == 1) {
       R f[Q];
-      static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(nn, sh.s[I], g.n)); });
-      bulk_velocity<Q, R>(f, v);
+      load_cell(nn, f);
+      bulk_velocity<Q, R>(f, halfF, v);
+    } else {
+      v[0] = v[1] = v[2] = R(0);
     }
   };
+  auto rho_at = [&](const int (&p)[3]) -> R {
+    const int64_t nn = padded_of(p);
+    const int64_t j = fd_find(fdCell, nFd, uint32_t(nn));
+    if (j >= 0) {
+      if (!corners) return R(fdMom[7 * j + 6]);
+      R f[Q], r, v[3];
+      load_cell(nn, f);
+      fd_momenta<Q, R>(f, FdMeta(fdMeta[j]), fdValue + 4 * j, r, v);
+      return r;
+    }
+    const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
+    if (kind != 1) return R(1);
+    R f[Q];
+    load_cell(nn, f);
+    return bulk_rho<Q, R>(f);
+  };
+  // density at the cell `step` cells inward along axis a
+  auto rho_in = [&](int a, int step) -> R {
+    int p[3] = {pos[0], pos[1], pos[2]};
+    p[a] -= step * m.n[a];
+    return rho_at(p);
+  };
+  R rho;
+  if (m.type == FD_FLAT_VELOCITY || m.type == FD_FLAT_PRESSURE) {
+    rho = R(own[6]);
+  } else if (m.type == FD_EDGE_VELOCITY || D::d == 2) {
+    int A = 0, B = 1;
+    if (D::d == 3) {
+      int plane = 0;
+      for (int a = 0; a < 3; ++a)
+        if (m.n[a] == 0) plane = a;
+      A = (plane + 1) % 3;
+      B = (plane + 2) % 3;
+    }
+    const R r10 = rho_in(A, 1), r01 = rho_in(B, 1), r20 = rho_in(A, 2), r02 = rho_in(B, 2);
+    rho = R(2) / R(3) * (r01 + r10) - R(1) / R(6) * (r02 + r20);
+  } else {
+    const R r100 = rho_in(0, 1), r010 = rho_in(1, 1), r001 = rho_in(2, 1);
+    const R r200 = rho_in(0, 2), r020 = rho_in(1, 2), r002 = rho_in(2, 2);
+    rho = R(4) / R(9) * (r001 + r010 + r100) - R(1) / R(9) * (r002 + r020 + r200);
+  }
   R grad[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
   for (int a = 0; a < D::d; ++a) {
     R ua[3] = {R(0), R(0), R(0)}, ub[3] = {R(0), R(0), R(0)};
-    if (a == m.dir) {
+    if (m.n[a] != 0) {
+      const int o = m.n[a];
       int p1[3] = {pos[0], pos[1], pos[2]}, p2[3] = {pos[0], pos[1], pos[2]};
-      p1[a] -= m.orient;
-      p2[a] -= 2 * m.orient;
-      velocity_at(p1[0], p1[1], p1[2], false, ua);
-      velocity_at(p2[0], p2[1], p2[2], false, ub);
+      p1[a] -= o;
+      p2[a] -= 2 * o;
+      velocity_at(p1, false, ua);
+      velocity_at(p2, false, ub);
       for (int iD = 0; iD < D::d; ++iD)
-        grad[a][iD] = R(-m.orient) * (((R(-3) * u[iD] + R(4) * ua[iD]) - R(1) * ub[iD]) / R(2));
+        grad[a][iD] = R(-o) * (((R(-3) * u[iD] + R(4) * ua[iD]) - R(1) * ub[iD]) / R(2));
     } else {
       int pp[3] = {pos[0], pos[1], pos[2]}, pm[3] = {pos[0], pos[1], pos[2]};
       pp[a] += 1;
       pm[a] -= 1;
-      const bool wp = pp[a] >= ext[a], wm = pm[a] < 0;  // across a periodic face (flat faces only)
+      // across a periodic face the partner cell is read (its overlap copy carries bulk
+      // dynamics); across a non-periodic one the padding cell, which has none
+      const bool per = (g.pmask >> a) & 1;
+      const bool wp = per && pp[a] >= ext[a], wm = per && pm[a] < 0;
       if (wp) pp[a] -= ext[a];
       if (wm) pm[a] += ext[a];
-      velocity_at(pp[0], pp[1], pp[2], wp, ua);
-      velocity_at(pm[0], pm[1], pm[2], wm, ub);
+      velocity_at(pp, wp, ua);
+      velocity_at(pm, wm, ub);
       for (int iD = 0; iD < D::d; ++iD) grad[a][iD] = (ua[iD] - ub[iD]) / R(2);
     }
   }
@@ -1333,35 +1446,38 @@ __global__ void __launch_bounds__(256) k_mass_momentum(const S* __restrict__ pop
   block_partial4<0>(v[0], v[1], v[2], v[3], part);
 }
 
-// Momentum exchange over the bounce-back links after the PostStream step:
-// F = sum_links c_k (f~_k(x_b) + f_opp(k)(x_b)), f~_k(x_b) = the post-collision population
-// that streamed into the solid neighbour (now held there).  Full populations (f - w + w).
+// Momentum exchange over the bounce-back links after the PostStream step, in the convention of
+// the reference's boundary-force functor (BlockLatticePhysBoundaryForce3D::operator(),
+// functors/lattice/latticePhysBoundaryForce3D.hh:85-113): for every solid cell x_s and direction
+// k towards a fluid cell x_f = x_s + c_k, F -= c_k (f_k(x_f) + f_opp(k)(x_s)) on the stored values
+// f - w.  A link (x_b, j) with x_b + c_j = x_s is that pair with k = opp(j), x_f = x_b, so it
+// contributes c_j (f_opp(j)(x_b) + f_j(x_s)): the population the link kernel wrote back and the
+// one that streamed into the solid cell.  Links whose group is not `want` (want >= 0) are skipped.
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_link_force(const S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                     const uint32_t* __restrict__ cell,
-                                                    const uint8_t* __restrict__ dir, int64_t nLinks,
+                                                    const uint8_t* __restrict__ dir,
+                                                    const uint8_t* __restrict__ group, int want, int64_t nLinks,
                                                     double* __restrict__ part) {
-  using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double fx = 0, fy = 0, fz = 0;
-  if (l < nLinks) {
+  if (l < nLinks && (want < 0 || (group && int(group[l]) == want) || (!group && want == 0))) {
     const int64_t xb = cell[l];
     const int k = dir[l];
     int64_t off = 0;
     int kopp = 0;
-    double cx = 0, cy = 0, cz = 0, w = 0;
+    double cx = 0, cy = 0, cz = 0;
     static_for<Q>([&](auto I) {
       if (I == k) {
         off = D::C[I][0] * g.sx + D::C[I][1] * g.sy + D::C[I][2];
         kopp = D::OPP[I];
         cx = D::C[I][0]; cy = D::C[I][1]; cz = D::C[I][2];
-        w = weight<Q, double>(I);
       }
     });
-    const double fin = double(Storage<S>::load(pop + int64_t(k) * g.stride + wrap_add(xb + off, sh.s[k], g.n))) + w;
-    const double fout = double(Storage<S>::load(pop + int64_t(kopp) * g.stride + wrap_add(xb, sh.s[kopp], g.n))) + w;
-    const double s = fin + fout;
+    const double fb = double(Storage<S>::load(pop + int64_t(kopp) * g.stride + wrap_add(xb, sh.s[kopp], g.n)));
+    const double fs = double(Storage<S>::load(pop + int64_t(k) * g.stride + wrap_add(xb + off, sh.s[k], g.n)));
+    const double s = fb + fs;
     fx = cx * s; fy = cy * s; fz = cz * s;
   }
   block_partial4<0>(fx, fy, fz, 0.0, part);
@@ -1421,11 +1537,12 @@ struct LaunchArgs {
   int doubled;         // columns mapped twice back to back: index n + shift needs no wrap
   int64_t flatBase;    // first tile start (multiple of 8) and end of the flat cell range
   int64_t flatEnd;
-  int64_t nFd;               // flat-face velocity/pressure boundary cells
+  int64_t nFd;               // velocity/pressure boundary cells
   const uint32_t* fdCell;    // their padded indices, ascending
-  const uint8_t* fdMeta;     // normal axis, orientation, kind (FdMeta)
+  const uint8_t* fdMeta;     // type and outward normal (FdMeta)
   const double* fdValue;     // 4 imposed values per cell
   double* fdMom;             // 7 doubles per cell of scratch (k_fd_momenta)
+  int64_t nFdCorners;        // how many of them are corners (regularised in a second pass)
   int* err;                  // device flag: a bounded wait of a step kernel gave up
 };
 
@@ -1454,8 +1571,8 @@ inline int64_t reduce_blocks(int64_t items) { return (items + 255) / 256; }
 template <int Q, typename S>
 cudaError_t launch_mass_momentum(const LaunchArgs& a, double* part, double* out, cudaStream_t stream);
 template <int Q, typename S>
-cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir, int64_t nLinks,
-                              double* part, double* out, cudaStream_t stream);
+cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir, const uint8_t* group,
+                              int want, int64_t nLinks, double* part, double* out, cudaStream_t stream);
 template <int Q, typename S>
 cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, double* out, cudaStream_t stream);
 
@@ -1600,18 +1717,28 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
   k_stats_finalize<<<1, kFinalizeThreads, 0, stream>>>(a.statPart, nblocks + fdb, a.stats);
   return cudaGetLastError();
 }
-// Post-stream regularisation of the flat-face boundary cells (two passes, see k_fd_regularize).
+// Post-stream regularisation of the boundary cells: momenta, then flat faces and edges, then
+// corners (see k_fd_regularize).
 template <int Q, typename S>
 cudaError_t launch_fd_boundary(const LaunchArgs& a, cudaStream_t stream) {
   if (a.nFd <= 0) return cudaSuccess;
   const unsigned blocks = unsigned(fd_blocks(a.nFd));
   S* pop = static_cast<S*>(a.pop);
   const auto sh = shifts_of<Q>(a);
-  k_fd_momenta<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.nFd, a.fdCell, a.fdMeta, a.fdValue, a.fdMom);
+  // forced bulk neighbours report j / rho + F / 2 (ForcedMomentum)
+  const bool forced = a.dynamics == DYN_FORCED_BGK || a.dynamics == DYN_FORCED_SMAGORINSKY;
+  const double hf[3] = {forced ? 0.5 * a.force[0] : 0.0, forced ? 0.5 * a.force[1] : 0.0, forced ? 0.5 * a.force[2] : 0.0};
+  k_fd_momenta<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.nFd, a.fdCell, a.fdMeta, a.fdValue, hf[0], hf[1],
+                                                 hf[2], a.fdMom);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_fd_regularize<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.omega, a.nFd, a.fdCell, a.fdMeta, a.fdMom);
-  return cudaGetLastError();
+  for (int corners = 0; corners < (a.nFdCorners > 0 ? 2 : 1); ++corners) {
+    k_fd_regularize<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.omega, a.nFd, a.fdCell, a.fdMeta, a.fdValue,
+                                                      a.cellDyn, hf[0], hf[1], hf[2], a.fdMom, corners);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 // Periodic overlap copy after the collision (no launch for a lattice without periodic axes).
 template <int Q, typename S>
@@ -1694,12 +1821,12 @@ cudaError_t launch_mass_momentum(const LaunchArgs& a, double* part, double* out,
   return cudaGetLastError();
 }
 template <int Q, typename S>
-cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir,
-                                    int64_t nLinks, double* part, double* out, cudaStream_t stream) {
+cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const uint8_t* dir, const uint8_t* group,
+                              int want, int64_t nLinks, double* part, double* out, cudaStream_t stream) {
   const int64_t blocks = reduce_blocks(nLinks);
   if (nLinks > 0) {
     k_link_force<Q, S><<<unsigned(blocks), 256, 0, stream>>>(static_cast<const S*>(a.pop), a.g, shifts_of<Q>(a), cell,
-                                                             dir, nLinks, part);
+                                                             dir, group, want, nLinks, part);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -1730,7 +1857,8 @@ cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, doub
   template cudaError_t launch_moments<Q, S>(const LaunchArgs&, double*, double*, cudaStream_t);       \
   template cudaError_t launch_mass_momentum<Q, S>(const LaunchArgs&, double*, double*, cudaStream_t); \
   template cudaError_t launch_link_force<Q, S>(const LaunchArgs&, const uint32_t*, const uint8_t*,    \
-                                               int64_t, double*, double*, cudaStream_t);              \
+                                               const uint8_t*, int, int64_t, double*, double*,         \
+                                               cudaStream_t);                                          \
   template cudaError_t launch_residual<Q, S>(const LaunchArgs&, float*, double*, double*, cudaStream_t);
 #endif  // LBX_KERNEL_TU
 

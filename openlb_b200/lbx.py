@@ -98,12 +98,17 @@ def _load() -> C.CDLL:
         "lbx_get_statistics": ([VP, P(D), VP], C.c_int),
         "lbx_compute_moments": ([VP, VP, VP, VP], C.c_int),
         "lbx_reduce": ([VP, I32, P(D), VP], C.c_int),
+        "lbx_boundary_force": ([VP, I32, P(D), VP], C.c_int),
         "lbx_population_shift": ([VP, I32, P(I64)], C.c_int),
         "lbx_rotate": ([VP, I32, I64], C.c_int),
         "lbx_set_launch_config": ([VP, I32, I32, I32, I32], C.c_int),
         "lbx_set_kernel_timing": ([VP, I32], C.c_int),
         "lbx_post_process": ([VP, VP], C.c_int),
         "lbx_set_fd_boundaries": ([VP, I64, VP, VP, VP, VP, VP], C.c_int),
+        "lbx_set_boundary_cells": ([VP, I64, VP, VP, VP, VP, VP], C.c_int),
+        "lbx_set_interpolated_boundary": ([VP, I32, VP, I32, I32, VP, I32, VP, VP], C.c_int),
+        "lbx_discrete_normals": ([I32, P(I32), P(I32), VP, I32, I32, VP, I32, VP, I64, VP, VP, VP, P(I64)],
+                                 C.c_int),
         "lbx_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_autotune": ([VP, I32, VP, I32, P(I32), VP], C.c_int),
         "lbx_ensemble_set_launch_mode": ([VP, I32], C.c_int),
@@ -187,46 +192,43 @@ def build_bouzidi_links(q: int, core, material: np.ndarray, fluid: int = 1, soli
 FD_VELOCITY, FD_PRESSURE = 1, 2
 
 
+NORMAL_FLAT, NORMAL_EXTERNAL_CORNER, NORMAL_INTERNAL_CORNER, NORMAL_EXTERNAL_EDGE, NORMAL_INTERNAL_EDGE = 0, 1, 2, 3, 4
+
+
+def discrete_normals(material: np.ndarray, boundary: int, fluid=(1,), outside=(0,),
+                     periodic=(False, False, False)):
+    """computeBoundaryTypeAndNormal (geometry/discreteNormals.hh) for every cell of material
+    `boundary`, through lbx_discrete_normals: returns (cells, types, normals[n, 3]) in ascending
+    core-cell order; a cell matching no pattern has type NORMAL_FLAT and a zero normal."""
+    mat = np.ascontiguousarray(material, dtype=np.int32)
+    d = mat.ndim
+    q = 9 if d == 2 else 19
+    core = list(mat.shape) + [1] * (3 - d)
+    fl = np.ascontiguousarray(fluid, dtype=np.int32)
+    ou = np.ascontiguousarray(outside, dtype=np.int32)
+    per = [int(bool(p)) for p in periodic] + [0] * (3 - len(periodic))
+    n = C.c_int64()
+    args = (q, _i32x3(core), _i32x3(per[:3]), _ptr(mat), int(boundary), len(fl), _ptr(fl), len(ou), _ptr(ou))
+    check(lib.lbx_discrete_normals(*args, 0, None, None, None, C.byref(n)), "lbx_discrete_normals")
+    cells = np.empty(n.value, np.int64)
+    types = np.empty(n.value, np.int32)
+    normals = np.empty((n.value, 3), np.int32)
+    check(lib.lbx_discrete_normals(*args, n.value, _ptr(cells), _ptr(types), _ptr(normals), C.byref(n)),
+          "lbx_discrete_normals")
+    return cells, types, normals
+
+
 def fd_boundaries_from_materials(material: np.ndarray, boundary: int, fluid=(1,), outside=(0,),
                                  periodic=(False, False, False)):
-    """Flat-face cells of material `boundary` with their discrete normal, as boundary::set
-    classifies them (geometry/discreteNormals.h): the normal points to the one axis direction
-    whose neighbour is outside (a material in `outside`, or past a non-periodic domain edge)
-    while the opposite neighbour is fluid.  Returns (cells, dirs, orients) for the cells with
-    exactly one such direction; other cells of the material (edges, corners) are left out."""
-    mat = np.asarray(material)
-    d = mat.ndim
-    fluid_m = np.isin(mat, fluid)
-    outside_m = np.isin(mat, outside)
-    cells, dirs, orients = [], [], []
-
-    def look(pt, a, mask):
-        if 0 <= pt[a] < mat.shape[a]:
-            return bool(mask[tuple(pt)])
-        if periodic[a]:
-            pt = list(pt)
-            pt[a] %= mat.shape[a]
-            return bool(mask[tuple(pt)])
-        return mask is outside_m  # past a non-periodic edge: outside
-
-    for idx in zip(*np.nonzero(mat == boundary)):
-        open_sides = []  # (axis, orientation) of every outside neighbour along the axes
-        for a in range(d):
-            for o in (-1, 1):
-                p = list(idx)
-                p[a] += o
-                if look(p, a, outside_m):
-                    open_sides.append((a, o))
-        if len(open_sides) != 1:
-            continue  # interior of the material, or an edge / corner
-        a, o = open_sides[0]
-        q = list(idx)
-        q[a] -= o
-        if look(q, a, fluid_m):
-            cells.append(int(np.ravel_multi_index(idx, mat.shape)))
-            dirs.append(a)
-            orients.append(o)
-    return np.array(cells, np.int64), np.array(dirs, np.int32), np.array(orients, np.int32)
+    """The flat-face cells of material `boundary` as boundary::set classifies them
+    (discrete_normals): returns (cells, dirs, orients) of the cells whose discrete normal is flat;
+    edges and corners are left out."""
+    cells, types, normals = discrete_normals(material, boundary, fluid, outside, periodic)
+    keep = (types == NORMAL_FLAT) & (np.abs(normals).sum(axis=1) == 1)
+    cells, normals = cells[keep], normals[keep]
+    dirs = np.argmax(np.abs(normals), axis=1).astype(np.int32)
+    orients = normals[np.arange(len(cells)), dirs].astype(np.int32)
+    return cells, dirs, orients
 
 
 class BlockLattice:
@@ -323,6 +325,33 @@ class BlockLattice:
         check(lib.lbx_set_fd_boundaries(self._h, len(c), _ptr(c), _ptr(k), _ptr(d), _ptr(o), _ptr(v)),
               "lbx_set_fd_boundaries")
 
+    def set_boundary_cells(self, cells, kinds, types, normals, values) -> None:
+        """Velocity / pressure boundary cells with their discrete normal type (flat, external
+        edge, external corner) and outward normal [n, 3]: lbx_set_boundary_cells."""
+        c = np.ascontiguousarray(cells, dtype=np.int64)
+        k = np.ascontiguousarray(kinds, dtype=np.int32)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        nn = np.ascontiguousarray(normals, dtype=np.int32).reshape(-1, 3)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1, 4)
+        if not (len(c) == len(k) == len(t) == len(nn) == len(v)):
+            raise ValueError("boundary arrays differ in length")
+        check(lib.lbx_set_boundary_cells(self._h, len(c), _ptr(c), _ptr(k), _ptr(t), _ptr(nn), _ptr(v)),
+              "lbx_set_boundary_cells")
+
+    def set_interpolated_boundary(self, kind: int, material: np.ndarray, boundary: int, values: np.ndarray,
+                                  fluid=(1,), outside=(0,)) -> None:
+        """boundary::set<InterpolatedVelocity> (kind FD_VELOCITY) or <InterpolatedPressure>
+        (FD_PRESSURE) over the cells of material `boundary`; values [core cells, 4] hold the
+        imposed velocity, or {rho, tangential velocity}, of each boundary cell."""
+        mat = np.ascontiguousarray(material, dtype=np.int32).reshape(-1)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if mat.size != self.n_core or v.size != 4 * self.n_core:
+            raise ValueError("material [core cells] and values [core cells, 4] expected")
+        fl = np.ascontiguousarray(fluid, dtype=np.int32)
+        ou = np.ascontiguousarray(outside, dtype=np.int32)
+        check(lib.lbx_set_interpolated_boundary(self._h, int(kind), _ptr(mat), int(boundary), len(fl), _ptr(fl),
+                                                len(ou), _ptr(ou), _ptr(v)), "lbx_set_interpolated_boundary")
+
     def set_bouzidi_boundary(self, material: np.ndarray, fluid: int = 1, solid=(2,), wall_velocity=None) -> None:
         mat = np.ascontiguousarray(material, dtype=np.int32).reshape(-1)
         sol = np.ascontiguousarray(solid, dtype=np.int32)
@@ -389,6 +418,14 @@ class BlockLattice:
         check(lib.lbx_reduce(self._h, what, out, _stream_ptr(stream)), "lbx_reduce")
         n = {REDUCE_MASS_MOMENTUM: 4, REDUCE_DRAG: 3, REDUCE_RESIDUAL: 3}[what]
         return np.array(out[:n])
+
+    def boundary_force(self, group: int = -1, stream=None) -> np.ndarray:
+        """Force on the solid behind link group `group` (the index of its material in the
+        `solid` list of set_bouzidi_boundary; -1: all links), lattice units, in the convention of
+        the reference's SuperLatticePhysBoundaryForce3D summed over that solid."""
+        out = (C.c_double * 3)()
+        check(lib.lbx_boundary_force(self._h, int(group), out, _stream_ptr(stream)), "lbx_boundary_force")
+        return np.array(out[:])
 
     def set_launch_config(self, variant: int, block_x: int = 256, block_y: int = 1,
                           cells_per_thread: int = 1) -> None:

@@ -33,7 +33,7 @@ enum lbo_material {
   LBO_SOLID = 0,      /* NoDynamics: left untouched (dynamics.h:51-63) */
   LBO_FLUID = 1,      /* the case's bulk dynamics */
   LBO_BOUNCE_BACK = 4,/* BounceBack = collision::Revert (collision.h:465-484) */
-  LBO_FD_BOUNDARY = 5 /* flat-face Dirichlet cell: BGK with boundary momenta (fd_* below) */
+  LBO_FD_BOUNDARY = 5 /* velocity / pressure boundary cell: BGK with boundary momenta (fd_* below) */
 };
 
 typedef struct {
@@ -57,6 +57,12 @@ typedef struct {
   const int32_t* fd_dir;     /* normal axis */
   const int32_t* fd_orient;  /* outward normal sign, -1 or +1 */
   const double* fd_value;    /* 4 per cell: the velocity, or {rho, tangential velocity} */
+  /* Optional (NULL: every cell flat with the normal of fd_dir / fd_orient): the discrete normal
+   * type (0 flat, 1 external corner, 3 external edge; geometry/discreteNormals.h:33-39) and the
+   * outward normal, 3 per cell.  Edges and corners carry an imposed velocity
+   * (boundary/interpolatedVelocity3D.h:45-90, interpolatedVelocity2D.h:45-80). */
+  const int32_t* fd_type;
+  const int32_t* fd_normal;
 } lbo_case;
 
 /* Run `steps` collide-and-stream steps in place.  stats (may be NULL) receives per step

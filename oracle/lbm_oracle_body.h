@@ -123,19 +123,44 @@ static void FN(collide)(const lbo_desc* d, const lbo_case* c, REAL* g, REAL avg_
   *usq_out = uSqr;
 }
 
-/* Density and velocity of a flat-face boundary cell from its momenta
- * (momenta::BasicDirichletVelocityBoundaryTuple / BasicDirichletPressureBoundaryTuple,
- * src/dynamics/momenta/aliases.h:173-198):
- *  velocity: u = imposed (FixedVelocityMomentumGeneric, elements.h:603-630), rho from
- *            velocityBMRho (elements.h:54-71) = (2 rho_normal + rho_onWall + 1) / (1 + o u_d);
- *  pressure: rho = imposed (FixedDensity, elements.h:270-280), u = imposed tangential
- *            velocity with u_d = o ((2 rho_normal + rho_onWall + 1) / rho - 1)
- *            (FixedPressureMomentum::computeU, elements.h:653-690).
+/* Type and outward normal of boundary cell b (see lbo_case). */
+static void FN(fd_meta)(const lbo_case* c, int64_t b, int* type, int n[3])
+{
+  n[0] = n[1] = n[2] = 0;
+  if (c->fd_normal) {
+    *type = c->fd_type ? c->fd_type[b] : 0;
+    for (int a = 0; a < 3; ++a) n[a] = c->fd_normal[3 * b + a];
+  } else {
+    *type = 0;
+    n[c->fd_dir[b]] = c->fd_orient[b];
+  }
+}
+
+/* Density and velocity of a boundary cell from its momenta
+ * (src/dynamics/momenta/aliases.h:173-220):
+ *  flat velocity (BasicDirichletVelocityBoundaryTuple): u = imposed (FixedVelocityMomentumGeneric,
+ *            elements.h:603-630), rho from velocityBMRho (elements.h:54-71)
+ *            = (2 rho_normal + rho_onWall + 1) / (1 + o u_d);
+ *  flat pressure (BasicDirichletPressureBoundaryTuple): rho = imposed (FixedDensity,
+ *            elements.h:270-280), u = imposed tangential velocity with
+ *            u_d = o ((2 rho_normal + rho_onWall + 1) / rho - 1) (FixedPressureMomentum::computeU,
+ *            elements.h:653-690);
+ *  external edge / corner (FixedVelocityBoundaryTuple): u = imposed, rho = sum f + 1 (BulkDensity).
  * rho_onWall sums the populations with c_d = 0, rho_normal those with c_d = o, in index order. */
-static void FN(fd_momenta)(const lbo_desc* d, const REAL* g, int kind, int dir, int orient,
+static void FN(fd_momenta)(const lbo_desc* d, const REAL* g, int kind, int type, const int* nrm,
                            const double* value, REAL* rho, REAL* u)
 {
   const int q = d->q, dim = d->d;
+  if (type != 0) {
+    REAL r = 0;
+    for (int i = 0; i < q; ++i) r += g[i];
+    *rho = r + (REAL)1;
+    for (int a = 0; a < dim; ++a) u[a] = (REAL)value[a];
+    return;
+  }
+  int dir = 0, orient = 0;
+  for (int a = dim - 1; a >= 0; --a)
+    if (nrm[a] != 0) { dir = a; orient = nrm[a]; }
   REAL onWall = 0, normal = 0;
   for (int i = 0; i < q; ++i)
     if (d->c[i][dir] == 0) onWall += g[i];
@@ -170,8 +195,9 @@ static REAL FN(bgk_with)(const lbo_desc* d, REAL omega, REAL rho, const REAL* u,
   return uSqr;
 }
 
-/* u of a bulk cell: BulkMomentum::computeU (elements.h:500-508) = j / rho. */
-static void FN(bulk_u)(const lbo_desc* d, const REAL* g, REAL* u)
+/* u of a bulk cell: BulkMomentum::computeU (elements.h:500-508) = j / rho, plus F / 2 for the
+ * forced dynamics (ForcedMomentum, elements.h:1600-1608). */
+static void FN(bulk_u)(const lbo_desc* d, const lbo_case* c, const REAL* g, REAL* u)
 {
   const int q = d->q, dim = d->d;
   for (int a = 0; a < dim; ++a) u[a] = 0;
@@ -180,121 +206,205 @@ static void FN(bulk_u)(const lbo_desc* d, const REAL* g, REAL* u)
   REAL rho = 0;
   for (int i = 0; i < q; ++i) rho += g[i];
   rho += (REAL)1;
-  for (int a = 0; a < dim; ++a) u[a] /= rho;
+  const int forced = (c->dynamics == LBO_FORCED_BGK || c->dynamics == LBO_FORCED_SMAGORINSKY);
+  for (int a = 0; a < dim; ++a) {
+    u[a] /= rho;
+    if (forced) u[a] += (REAL)c->force[a] * (REAL)0.5;
+  }
 }
 
-/* Velocity u of the cell a finite difference reads (cell.computeU through its dynamics):
- * a boundary cell of the list uses its momenta on the current (in-place updated) populations;
- * a bulk cell j / rho.  A neighbour reached across a periodic face is the overlap copy of the
- * partner cell, which the post-stream communication filled with the partner's populations
- * before any post-processor ran (core/superLattice.hh:800-820, boundary/setBoundary3D.h:56-110)
- * and which carries bulk dynamics (boundary::set skips the overlap, setBoundary.h:83-86). */
+/* Cell index of p, -1 beyond a non-periodic face; *wrapped set when a periodic face was crossed. */
+static int64_t FN(fd_index)(const lbo_case* c, int64_t p0, int64_t p1, int64_t p2, int* wrapped)
+{
+  const int64_t ext[3] = {c->nx, c->ny, c->nz};
+  int64_t p[3] = {p0, p1, p2};
+  *wrapped = 0;
+  for (int a = 0; a < 3; ++a) {
+    if (p[a] >= 0 && p[a] < ext[a]) continue;
+    if (!((c->periodic >> a) & 1)) return -1;
+    p[a] = (p[a] + ext[a]) % ext[a];
+    *wrapped = 1;
+  }
+  return (p[0] * ext[1] + p[1]) * ext[2] + p[2];
+}
+
+/* Velocity the finite differences read at cell m (cell.computeU through its dynamics): a
+ * boundary cell of the list its momenta on the current (in-place updated) populations, a bulk
+ * cell j / rho, a cell without dynamics or with plain bounce-back zero (ZeroMomentum), and so a
+ * cell beyond a non-periodic face (the reference's overlap carries NoDynamics there).  A
+ * neighbour reached across a periodic face is the overlap copy of the partner cell, which the
+ * post-stream communication filled with the partner's populations before any post-processor ran
+ * (core/superLattice.hh:800-820, boundary/setBoundary3D.h:56-110) and which carries the
+ * partner's dynamics as defined before boundary::set (boundary::set skips the overlap,
+ * setBoundary.h:83-86): bulk for a boundary cell. */
 static void FN(fd_u_of)(const lbo_desc* d, const lbo_case* c, const STORE_T* f, const STORE_T* pre,
                         const int64_t* fdIndex, int64_t m, int wrapped, REAL* u)
 {
   const int q = d->q;
   const int64_t n = (int64_t)c->nx * c->ny * c->nz;
   REAL g[27];
+  u[0] = u[1] = u[2] = 0;
+  if (m < 0) return;
+  const int mat = c->material ? c->material[m] : LBO_FLUID;
+  if (mat == LBO_SOLID || mat == LBO_BOUNCE_BACK) return;
   if (wrapped) {
     for (int i = 0; i < q; ++i) g[i] = LOAD(pre[i * n + m]);
-    FN(bulk_u)(d, g, u);
+    FN(bulk_u)(d, c, g, u);
     return;
   }
   for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + m]);
   const int64_t b = fdIndex[m];
   if (b >= 0) {
     REAL rho;
-    FN(fd_momenta)(d, g, c->fd_kind[b], c->fd_dir[b], c->fd_orient[b], c->fd_value + 4 * b, &rho, u);
+    int type, nrm[3];
+    FN(fd_meta)(c, b, &type, nrm);
+    FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
   } else {
-    FN(bulk_u)(d, g, u);
+    FN(bulk_u)(d, c, g, u);
   }
 }
 
-/* PlaneFdBoundaryProcessor3D::apply (src/boundary/boundaryPostProcessors3D.hh:39-93) and
- * StraightFdBoundaryProcessor2D::apply (boundaryPostProcessors2D.hh:39-76), one cell after the
- * other in ascending cell order and in place, as the CPU post-processor loop runs them
- * (core/platform/cpu/sisd/operator.h:368-385): velocity gradients by
- * fd::DirectedGradients (utilities/finiteDifference3D.h:74-210: one-sided second order along
- * the normal, central along the face), Pi = -rho / (c_s^-2 omega) (grad u + grad u^T), and
- * f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270). */
+/* Density at cell m (cell.computeRho through its dynamics), on the current populations. */
+static REAL FN(fd_rho_of)(const lbo_desc* d, const lbo_case* c, const STORE_T* f, const int64_t* fdIndex, int64_t m)
+{
+  const int q = d->q;
+  const int64_t n = (int64_t)c->nx * c->ny * c->nz;
+  if (m < 0) return (REAL)1;
+  const int mat = c->material ? c->material[m] : LBO_FLUID;
+  if (mat == LBO_SOLID || mat == LBO_BOUNCE_BACK) return (REAL)1;
+  REAL g[27];
+  for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + m]);
+  const int64_t b = fdIndex[m];
+  if (b >= 0) {
+    REAL rho, u[3] = {0, 0, 0};
+    int type, nrm[3];
+    FN(fd_meta)(c, b, &type, nrm);
+    FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
+    return rho;
+  }
+  REAL r = 0;
+  for (int i = 0; i < q; ++i) r += g[i];
+  return r + (REAL)1;
+}
+
+/* The post-stream boundary processors, one cell after the other in ascending cell order and in
+ * place, as the CPU post-processor loop runs them (core/platform/cpu/sisd/operator.h:368-385),
+ * by priority: the flat faces (PlaneFdBoundaryProcessor3D::apply, src/boundary/
+ * boundaryPostProcessors3D.hh:39-93; StraightFdBoundaryProcessor2D::apply,
+ * boundaryPostProcessors2D.hh:39-76) and the external edges (OuterVelocityEdgeProcessor3D,
+ * boundaryPostProcessors3D.hh:164-238) at priority 0, then the external corners
+ * (OuterVelocityCornerProcessor3D / 2D, 3D.hh:240-294, 2D.hh:276-323) at priority 1.  Velocity
+ * gradients by fd::DirectedGradients (utilities/finiteDifference3D.h:74-210: one-sided second
+ * order along each non-zero normal component, central along the other axes); rho: the cell's
+ * momenta on a flat face, 2/3 (rho_01 + rho_10) - 1/6 (rho_02 + rho_20) on an edge or a 2D corner
+ * (the cells one and two steps inward along its normal axes), 4/9 (rho_001 + rho_010 + rho_100)
+ * - 1/9 (rho_002 + rho_020 + rho_200) on a 3D corner; Pi = -rho / (c_s^-2 omega)
+ * (grad u + grad u^T), and f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270). */
 static void FN(fd_postprocess)(const lbo_desc* d, const lbo_case* c, STORE_T* f, const STORE_T* pre,
                                const int64_t* fdIndex)
 {
   const int q = d->q, dim = d->d;
-  const int64_t nx = c->nx, ny = c->ny, nz = c->nz, n = nx * ny * nz;
-  const int64_t ext[3] = {nx, ny, nz};
+  const int64_t ny = c->ny, nz = c->nz, n = (int64_t)c->nx * ny * nz;
   const REAL invCs2 = (REAL)3;
   const REAL omega = (REAL)c->omega;
-  for (int64_t b = 0; b < c->n_fd; ++b) {
-    const int64_t cell = c->fd_cell[b];
-    const int dir = c->fd_dir[b], orient = c->fd_orient[b];
-    const int64_t pos[3] = {cell / (ny * nz), (cell / nz) % ny, cell % nz};
-    REAL g[27], rho, u[3] = {0, 0, 0};
-    for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + cell]);
-    FN(fd_momenta)(d, g, c->fd_kind[b], dir, orient, c->fd_value + 4 * b, &rho, u);
-    REAL grad[3][3] = {{0}};  /* grad[a][iD] = d u_iD / d x_a */
-    for (int a = 0; a < dim; ++a) {
-      /* neighbour at offset s along axis a: index and whether it wrapped periodically */
-      REAL ua[3] = {0, 0, 0}, ub[3] = {0, 0, 0};
-      if (a == dir) {
-        for (int k = 1; k <= 2; ++k) {
-          int64_t p[3] = {pos[0], pos[1], pos[2]};
-          p[a] -= k * orient;
-          const int64_t m = (p[0] * ny + p[1]) * nz + p[2];
-          FN(fd_u_of)(d, c, f, pre, fdIndex, m, 0, k == 1 ? ua : ub);
-        }
-        for (int iD = 0; iD < dim; ++iD)
-          grad[a][iD] = (REAL)(-orient) * (((REAL)-3 * u[iD] + (REAL)4 * ua[iD]) - (REAL)1 * ub[iD]) / (REAL)2;
-      } else {
-        for (int k = 0; k < 2; ++k) {
-          int64_t p[3] = {pos[0], pos[1], pos[2]};
-          p[a] += k == 0 ? 1 : -1;
-          int wrapped = 0;
-          if (p[a] < 0 || p[a] >= ext[a]) {
-            p[a] = (p[a] + ext[a]) % ext[a];
-            wrapped = 1;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int64_t b = 0; b < c->n_fd; ++b) {
+      int type, nrm[3];
+      FN(fd_meta)(c, b, &type, nrm);
+      if ((type == 1) != (pass == 1)) continue;
+      const int64_t cell = c->fd_cell[b];
+      const int64_t pos[3] = {cell / (ny * nz), (cell / nz) % ny, cell % nz};
+      REAL g[27], rho, u[3] = {0, 0, 0};
+      for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + cell]);
+      FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
+      if (type != 0) {
+        /* densities of the cells one (r1) and two (r2) steps inward along each normal axis */
+        REAL r1[3] = {0, 0, 0}, r2[3] = {0, 0, 0};
+        for (int a = 0; a < dim; ++a) {
+          if (nrm[a] == 0) continue;
+          for (int k = 1; k <= 2; ++k) {
+            int64_t p[3] = {pos[0], pos[1], pos[2]};
+            p[a] -= k * nrm[a];
+            int w;
+            const REAL r = FN(fd_rho_of)(d, c, f, fdIndex, FN(fd_index)(c, p[0], p[1], p[2], &w));
+            if (k == 1) r1[a] = r; else r2[a] = r;
           }
-          const int64_t m = (p[0] * ny + p[1]) * nz + p[2];
-          FN(fd_u_of)(d, c, f, pre, fdIndex, m, wrapped, k == 0 ? ua : ub);
         }
-        for (int iD = 0; iD < dim; ++iD) grad[a][iD] = (ua[iD] - ub[iD]) / (REAL)2;
-      }
-    }
-    const REAL sToPi = -rho / invCs2 / omega;
-    REAL pi[6];
-    if (dim == 3) {
-      pi[0] = (REAL)2 * grad[0][0] * sToPi;             /* xx */
-      pi[3] = (REAL)2 * grad[1][1] * sToPi;             /* yy */
-      pi[5] = (REAL)2 * grad[2][2] * sToPi;             /* zz */
-      pi[1] = (grad[0][1] + grad[1][0]) * sToPi;        /* xy */
-      pi[2] = (grad[0][2] + grad[2][0]) * sToPi;        /* xz */
-      pi[4] = (grad[1][2] + grad[2][1]) * sToPi;        /* yz */
-    } else {
-      pi[0] = (REAL)2 * grad[0][0] * sToPi;             /* xx */
-      pi[2] = (REAL)2 * grad[1][1] * sToPi;             /* yy */
-      pi[1] = (grad[0][1] + grad[1][0]) * sToPi;        /* xy */
-    }
-    REAL uSqr = 0;
-    for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
-    for (int i = 0; i < q; ++i) {
-      const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
-      REAL cu = 0;
-      for (int a = 0; a < dim; ++a) cu += (REAL)d->c[i][a] * u[a];
-      const REAL feq = rho * t * ((REAL)1 + invCs2 * cu + invCs2 * invCs2 * (REAL)0.5 * cu * cu
-                                  - invCs2 * (REAL)0.5 * uSqr) - t;
-      REAL fneq = 0;
-      int ip = 0;
-      for (int al = 0; al < dim; ++al) {
-        for (int be = al; be < dim; ++be) {
-          REAL add = (REAL)d->c[i][al] * (REAL)d->c[i][be];
-          if (al == be) add -= (REAL)1 / invCs2;
-          else add *= (REAL)2;
-          add *= pi[ip++];
-          fneq += add;
+        if (dim == 3 && type == 1) {
+          rho = (REAL)4 / (REAL)9 * (r1[2] + r1[1] + r1[0]) - (REAL)1 / (REAL)9 * (r2[2] + r2[1] + r2[0]);
+        } else {
+          int A = 0, B = 1;
+          if (dim == 3) {
+            int plane = 0;
+            for (int a = 0; a < 3; ++a)
+              if (nrm[a] == 0) plane = a;
+            A = (plane + 1) % 3;
+            B = (plane + 2) % 3;
+          }
+          rho = (REAL)2 / (REAL)3 * (r1[B] + r1[A]) - (REAL)1 / (REAL)6 * (r2[B] + r2[A]);
         }
       }
-      fneq *= t * invCs2 * invCs2 / (REAL)2;
-      f[i * n + cell] = STORE(feq + fneq);
+      REAL grad[3][3] = {{0}};  /* grad[a][iD] = d u_iD / d x_a */
+      for (int a = 0; a < dim; ++a) {
+        REAL ua[3] = {0, 0, 0}, ub[3] = {0, 0, 0};
+        if (nrm[a] != 0) {
+          const int o = nrm[a];
+          for (int k = 1; k <= 2; ++k) {
+            int64_t p[3] = {pos[0], pos[1], pos[2]};
+            p[a] -= k * o;
+            int w;
+            const int64_t m = FN(fd_index)(c, p[0], p[1], p[2], &w);
+            FN(fd_u_of)(d, c, f, pre, fdIndex, m, 0, k == 1 ? ua : ub);
+          }
+          for (int iD = 0; iD < dim; ++iD)
+            grad[a][iD] = (REAL)(-o) * (((REAL)-3 * u[iD] + (REAL)4 * ua[iD]) - (REAL)1 * ub[iD]) / (REAL)2;
+        } else {
+          for (int k = 0; k < 2; ++k) {
+            int64_t p[3] = {pos[0], pos[1], pos[2]};
+            p[a] += k == 0 ? 1 : -1;
+            int wrapped;
+            const int64_t m = FN(fd_index)(c, p[0], p[1], p[2], &wrapped);
+            FN(fd_u_of)(d, c, f, pre, fdIndex, m, wrapped, k == 0 ? ua : ub);
+          }
+          for (int iD = 0; iD < dim; ++iD) grad[a][iD] = (ua[iD] - ub[iD]) / (REAL)2;
+        }
+      }
+      const REAL sToPi = -rho / invCs2 / omega;
+      REAL pi[6];
+      if (dim == 3) {
+        pi[0] = (REAL)2 * grad[0][0] * sToPi;             /* xx */
+        pi[3] = (REAL)2 * grad[1][1] * sToPi;             /* yy */
+        pi[5] = (REAL)2 * grad[2][2] * sToPi;             /* zz */
+        pi[1] = (grad[0][1] + grad[1][0]) * sToPi;        /* xy */
+        pi[2] = (grad[0][2] + grad[2][0]) * sToPi;        /* xz */
+        pi[4] = (grad[1][2] + grad[2][1]) * sToPi;        /* yz */
+      } else {
+        pi[0] = (REAL)2 * grad[0][0] * sToPi;             /* xx */
+        pi[2] = (REAL)2 * grad[1][1] * sToPi;             /* yy */
+        pi[1] = (grad[0][1] + grad[1][0]) * sToPi;        /* xy */
+      }
+      REAL uSqr = 0;
+      for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+      for (int i = 0; i < q; ++i) {
+        const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+        REAL cu = 0;
+        for (int a = 0; a < dim; ++a) cu += (REAL)d->c[i][a] * u[a];
+        const REAL feq = rho * t * ((REAL)1 + invCs2 * cu + invCs2 * invCs2 * (REAL)0.5 * cu * cu
+                                    - invCs2 * (REAL)0.5 * uSqr) - t;
+        REAL fneq = 0;
+        int ip = 0;
+        for (int al = 0; al < dim; ++al) {
+          for (int be = al; be < dim; ++be) {
+            REAL add = (REAL)d->c[i][al] * (REAL)d->c[i][be];
+            if (al == be) add -= (REAL)1 / invCs2;
+            else add *= (REAL)2;
+            add *= pi[ip++];
+            fneq += add;
+          }
+        }
+        fneq *= t * invCs2 * invCs2 / (REAL)2;
+        f[i * n + cell] = STORE(feq + fneq);
+      }
     }
   }
 }
@@ -339,8 +449,10 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
          * collision.h:68-78, with MOMENTA::computeRhoU of the tuple above) */
         const int64_t b = fdIndex[x];
         REAL g[27], rho, u[3] = {0, 0, 0};
+        int type, nrm[3];
+        FN(fd_meta)(c, b, &type, nrm);
         for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
-        FN(fd_momenta)(d, g, c->fd_kind[b], c->fd_dir[b], c->fd_orient[b], c->fd_value + 4 * b, &rho, u);
+        FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
         cellUsq[x] = FN(bgk_with)(d, (REAL)c->omega, rho, u, g);
         cellRho[x] = rho;
         for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);

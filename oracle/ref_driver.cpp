@@ -27,6 +27,29 @@
  *          [--init tgv|random|rest] [--u0 U] [--amp A] [--seed K] [--ulid U]
  *          [--walls bouzidi|bounceback] [--solid-frac P] [--out PREFIX]
  *          [--time W K] [--stats]
+ *    lbref geo --mat FILE --n NX NY [NZ] [--periodic PX PY [PZ]] [--dyn ...] [--omega W] ...
+ *          [--bouzidi M,...] [--lid M --ulid U] [--bounceback M,...] [--outside M,...]
+ *          [--ivel M,... (--poiseuille UMAX | --uconst UX UY [UZ])] [--ivel-lid M] [--ipres M --rho R]
+ *          [--classify M] [--classify-only] [--force-mat M --force-every K] [--moments]
+ *          [--no-pops] [--steps S] [--out PREFIX]
+ *  The geo case reads the int32 materials of the core cells from FILE (x slowest, z fastest)
+ *  and sets the lattice up through the reference's own setters: bulk dynamics on material 1,
+ *  NoDynamics elsewhere; setBouzidiBoundary (q = 1/2) from fluid 1 towards the --bouzidi and
+ *  --lid materials, setBouzidiVelocity (x velocity U) on the lid; BounceBack dynamics on the
+ *  --bounceback materials; boundary::set<InterpolatedVelocity> / <InterpolatedPressure> on the
+ *  --ivel / --ivel-lid / --ipres materials with fluid 1 and outside {0, --outside...}, which
+ *  classifies every cell with computeBoundaryTypeAndNormal itself.  The imposed velocity of an
+ *  --ivel material is RectanglePoiseuille3D over it (one --ivel material) with the zero-velocity
+ *  planes half a cell outside it (peak UMAX along +x), or a constant; the --ivel-lid material
+ *  moves with (--ulid, 0, 0).  Populations start at rest (all zero) or random (--init random).
+ *  --classify M writes PREFIX.normals.bin (int32 {core cell, type, n0, n1, n2} per cell of
+ *  material M, fluid 1, outside {0, --outside...}); --classify-only stops there.
+ *  --force-mat M writes PREFIX.force.txt: "step Fx Fy Fz" every K steps, the sum of
+ *  SuperLatticePhysBoundaryForce3D over material M (lattice units).  --moments writes
+ *  PREFIX.mom.bin (double rho, u [1 + d][ext...] from each cell's own computeRhoU) after the
+ *  run; --no-pops skips the population dumps.  PREFIX.bclass.bin holds, for every cell the
+ *  velocity / pressure setters equipped, int32 {core cell, kind (1 velocity, 2 pressure), normal
+ *  type, n0, n1, n2} as computeBoundaryTypeAndNormal gave them.
  *  Output (with --out): PREFIX.f0.bin / PREFIX.fS.bin  raw T populations [Q][ext...] of the
  *  core cells after initialize() and after S steps; PREFIX.mat.bin int32 materials [ext...];
  *  PREFIX.stats.txt per-step "avgRho avgEnergy maxU"; PREFIX.json the case description.
@@ -43,7 +66,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <fstream>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -102,7 +127,29 @@ struct Options {
   long timeWarm = -1;
   long timeSteps = 0;
   bool stats = false;
+  // geo case
+  std::string matFile;
+  int periodicFlags[3] = {0, 0, 0};
+  std::vector<int> bouzidiMats, bouncebackMats, outsideMats;
+  std::vector<int> ivelMats;
+  int lidMat = -1, ivelLidMat = -1, ipresMat = -1, classifyMat = -1, forceMat = -1;
+  long forceEvery = 0;
+  double poiseuille = -1.0, uconst[3] = {0, 0, 0}, rhoOut = 1.0;
+  bool classifyOnly = false, moments = false, noPops = false;
 };
+
+std::vector<int> parseList(const char* s) {
+  std::vector<int> out;
+  std::string t(s);
+  std::size_t p = 0;
+  while (p < t.size()) {
+    std::size_t q = t.find(',', p);
+    if (q == std::string::npos) q = t.size();
+    out.push_back(std::atoi(t.substr(p, q - p).c_str()));
+    p = q + 1;
+  }
+  return out;
+}
 
 /// splitmix64: deterministic per-(cell, population) values shared with the Python tests.
 std::uint64_t mix(std::uint64_t x) {
@@ -169,6 +216,24 @@ Options parse(int argc, char** argv) {
     else if (a == "--out") o.out = next();
     else if (a == "--time") { o.timeWarm = std::atol(next()); o.timeSteps = std::atol(next()); }
     else if (a == "--stats") o.stats = true;
+    else if (a == "--mat") o.matFile = next();
+    else if (a == "--periodic") { for (int d = 0; d < D; ++d) o.periodicFlags[d] = std::atoi(next()); }
+    else if (a == "--bouzidi") o.bouzidiMats = parseList(next());
+    else if (a == "--bounceback") o.bouncebackMats = parseList(next());
+    else if (a == "--outside") o.outsideMats = parseList(next());
+    else if (a == "--lid") o.lidMat = std::atoi(next());
+    else if (a == "--ivel") o.ivelMats = parseList(next());
+    else if (a == "--ivel-lid") o.ivelLidMat = std::atoi(next());
+    else if (a == "--ipres") o.ipresMat = std::atoi(next());
+    else if (a == "--poiseuille") o.poiseuille = std::atof(next());
+    else if (a == "--uconst") { for (int d = 0; d < D; ++d) o.uconst[d] = std::atof(next()); }
+    else if (a == "--rho") o.rhoOut = std::atof(next());
+    else if (a == "--classify") o.classifyMat = std::atoi(next());
+    else if (a == "--classify-only") o.classifyOnly = true;
+    else if (a == "--force-mat") o.forceMat = std::atoi(next());
+    else if (a == "--force-every") o.forceEvery = std::atol(next());
+    else if (a == "--moments") o.moments = true;
+    else if (a == "--no-pops") o.noPops = true;
     else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); std::exit(2); }
   }
   return o;
@@ -193,12 +258,273 @@ void dumpPopulations(SuperLattice<T,DESCRIPTOR>& lat, const int ext[3], const st
   f.write(reinterpret_cast<const char*>(buf.data()), buf.size() * sizeof(T));
 }
 
+
+/// The geo case (see the usage note at the top of this file).
+int runGeo(const Options& o) {
+  int ext[3] = {1, 1, 1};
+  for (int d = 0; d < D; ++d) ext[d] = o.n[d];
+  const std::size_t nCore = std::size_t(ext[0]) * ext[1] * ext[2];
+  std::vector<std::int32_t> mat(nCore);
+  {
+    std::ifstream f(o.matFile, std::ios::binary);
+    f.read(reinterpret_cast<char*>(mat.data()), mat.size() * sizeof(std::int32_t));
+    if (!f) { std::fprintf(stderr, "cannot read %zu materials from %s\n", nCore, o.matFile.c_str()); return 2; }
+  }
+  Vector<T,D> origin(T(0));
+  Vector<int,D> extent;
+  for (int d = 0; d < D; ++d) extent[d] = ext[d];
+  CuboidDecomposition<T,D> cuboids(origin, T(1), extent, 1);
+  {
+    Vector<bool,D> per;
+    for (int d = 0; d < D; ++d) per[d] = o.periodicFlags[d] != 0;
+    cuboids.setPeriodicity(per);
+  }
+  HeuristicLoadBalancer<T> balancer(cuboids);
+  SuperGeometry<T,D> geo(cuboids, balancer, 2);
+  {
+    auto& bg = geo.getBlockGeometry(0);
+    std::size_t c = 0;
+    forCore(ext, [&](int x, int y, int z) { bg.set(loc(x, y, z), mat[c++]); });
+    geo.rename(1000, 1001);
+    geo.communicate();
+  }
+  std::vector<int> outside{0};
+  outside.insert(outside.end(), o.outsideMats.begin(), o.outsideMats.end());
+
+  if (o.classifyMat >= 0) {
+    auto fluidI = geo.getMaterialIndicator(1);
+    auto outsideI = geo.getMaterialIndicator(std::vector<int>(outside));
+    auto& fb = fluidI->getBlockIndicatorF(0);
+    auto& ob = outsideI->getBlockIndicatorF(0);
+    std::vector<std::int32_t> rows;
+    std::size_t c = 0;
+    forCore(ext, [&](int x, int y, int z) {
+      if (mat[c] == o.classifyMat) {
+        auto [type, n] = computeBoundaryTypeAndNormal(fb, ob, loc(x, y, z));
+        rows.push_back(std::int32_t(c));
+        rows.push_back(std::int32_t(static_cast<int>(type)));
+        for (int d = 0; d < 3; ++d) rows.push_back(d < D ? std::int32_t(n[d]) : 0);
+      }
+      ++c;
+    });
+    std::ofstream f(o.out + ".normals.bin", std::ios::binary);
+    f.write(reinterpret_cast<const char*>(rows.data()), rows.size() * sizeof(std::int32_t));
+    if (o.classifyOnly) return 0;
+  }
+
+  SuperLattice<T,DESCRIPTOR> lat(geo);
+  const T nu = (T(1) / T(o.omega) - T(0.5)) / T(3);
+  const UnitConverter<T,DESCRIPTOR> converter(T(1), T(1), T(1), T(1), nu, T(1));
+  lat.setUnitConverter(converter);
+  {
+    std::vector<int> seen;
+    for (std::int32_t m : mat)
+      if (m != 1 && std::find(seen.begin(), seen.end(), m) == seen.end()) seen.push_back(m);
+    lat.template defineDynamics<NoDynamics>(geo, 0);
+    for (int m : seen) lat.template defineDynamics<NoDynamics>(geo, m);
+  }
+  if (o.dyn == "bgk") defineFluid<BGKdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "trt") defineFluid<TRTdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "smag") defineFluid<SmagorinskyBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "constrho") defineFluid<ConstRhoBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+#ifndef REF_NO_FORCE
+  else if (o.dyn == "fbgk") defineFluid<ForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+  else if (o.dyn == "fsmag") defineFluid<SmagorinskyForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);
+#endif
+  else { std::fprintf(stderr, "unsupported --dyn %s\n", o.dyn.c_str()); return 2; }
+
+  Nowhere<D> nowhere;
+  if (o.lidMat >= 0) {
+    std::vector<int> walls = o.bouzidiMats;
+    walls.push_back(o.lidMat);
+    setBouzidiBoundary<T,DESCRIPTOR,BouzidiVelocityPostProcessor>(
+      lat, geo.getMaterialIndicator(std::vector<int>(walls)), geo.getMaterialIndicator({1}), nowhere);
+    Vector<T,D> uw(T(0));
+    uw[0] = T(o.ulid);
+    AnalyticalConst<D,T,T> lidU(uw);
+    setBouzidiVelocity<T,DESCRIPTOR>(lat, geo.getMaterialIndicator({o.lidMat}), geo.getMaterialIndicator({1}), lidU);
+  } else if (!o.bouzidiMats.empty()) {
+    setBouzidiBoundary<T,DESCRIPTOR,BouzidiPostProcessor>(
+      lat, geo.getMaterialIndicator(std::vector<int>(o.bouzidiMats)), geo.getMaterialIndicator({1}), nowhere);
+  }
+  for (int m : o.bouncebackMats) lat.template defineDynamics<BounceBack>(geo, m);
+  std::vector<int> ivelAll = o.ivelMats;
+  if (o.ivelLidMat >= 0) ivelAll.push_back(o.ivelLidMat);
+  for (int m : ivelAll)
+    boundary::set<T, DESCRIPTOR, boundary::InterpolatedVelocity<T,DESCRIPTOR>>(
+      lat, geo.getMaterialIndicator({m}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+  auto isIvel = [&](int m) { return std::find(ivelAll.begin(), ivelAll.end(), m) != ivelAll.end(); };
+  if (o.ipresMat >= 0)
+    boundary::set<T, DESCRIPTOR, boundary::InterpolatedPressure<T,DESCRIPTOR>>(
+      lat, geo.getMaterialIndicator({o.ipresMat}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+
+  // the classification boundary::set gave every cell it set up: rows {cell, kind (1 velocity,
+  // 2 pressure), type, n0, n1, n2}; pressure cells only where the reference installs a condition
+  // (flat faces)
+  std::vector<std::int32_t> bclass;
+  {
+    auto fluidI = geo.getMaterialIndicator(1);
+    auto outsideI = geo.getMaterialIndicator(std::vector<int>(outside));
+    auto& fb = fluidI->getBlockIndicatorF(0);
+    auto& ob = outsideI->getBlockIndicatorF(0);
+    std::size_t c = 0;
+    forCore(ext, [&](int x, int y, int z) {
+      const bool vel = isIvel(mat[c]), pres = mat[c] == o.ipresMat;
+      if (vel || pres) {
+        auto [type, n] = computeBoundaryTypeAndNormal(fb, ob, loc(x, y, z));
+        if (vel || static_cast<int>(type) == 0) {
+          bclass.push_back(std::int32_t(c));
+          bclass.push_back(vel ? 1 : 2);
+          bclass.push_back(std::int32_t(static_cast<int>(type)));
+          for (int d = 0; d < 3; ++d) bclass.push_back(d < D ? std::int32_t(n[d]) : 0);
+        }
+      }
+      ++c;
+    });
+  }
+
+  lat.template setParameter<descriptors::OMEGA>(T(o.omega));
+  if (o.dyn == "trt") lat.template setParameter<collision::TRT::MAGIC>(T(o.magic));
+  if (o.dyn == "smag" || o.dyn == "fsmag") lat.template setParameter<collision::LES::SMAGORINSKY>(T(o.cs));
+
+  // imposed values: values[4 * c ...] = velocity (inlet) or {rho, 0, 0, 0} (outlet)
+  std::vector<double> vals(4 * nCore, 0.0);
+#if REF_Q != 9
+  std::unique_ptr<RectanglePoiseuille3D<T>> profile;
+  std::vector<T> umax{T(o.poiseuille), T(0), T(0)};
+  if (o.ivelMats.size() == 1 && o.poiseuille >= 0)
+    profile.reset(new RectanglePoiseuille3D<T>(geo, o.ivelMats[0], umax, T(0.5), T(0.5), T(0.5)));
+#endif
+  {
+    auto& block = lat.getBlock(0);
+    std::size_t c = 0;
+    forCore(ext, [&](int x, int y, int z) {
+      auto cell = block.get(loc(x, y, z));
+      for (int i = 0; i < Q; ++i) cell[i] = T(0);
+#ifndef REF_NO_FORCE
+      if (mat[c] == 1) {
+        Vector<T,D> fv;
+        for (int d = 0; d < D; ++d) fv[d] = T(o.force[d]);
+        cell.template setField<FORCE>(fv);
+      }
+#endif
+      if (o.init == "random" && (mat[c] == 1 || isIvel(mat[c]) || mat[c] == o.ipresMat)) {
+        T rho = T(1.0 + o.amp * (unit(o.seed, c, 60) - 0.5));
+        T u[D] = {};
+        for (int d = 0; d < D; ++d) u[d] = T(o.u0 * (unit(o.seed, c, 61 + d) - 0.5));
+        cell.iniEquilibrium(rho, u);
+        for (int i = 0; i < Q; ++i) cell[i] += T(o.amp * descriptors::t<double,DESCRIPTOR>(i) * (unit(o.seed, c, i) - 0.5));
+      }
+      if (isIvel(mat[c])) {
+        T u[3] = {T(o.uconst[0]), T(o.uconst[1]), T(o.uconst[2])};
+        if (mat[c] == o.ivelLidMat) {
+          u[0] = T(o.ulid);
+          u[1] = u[2] = T(0);
+        }
+#if REF_Q != 9
+        if (profile && mat[c] != o.ivelLidMat) {
+          const T at[3] = {T(x), T(y), T(z)};
+          (*profile)(u, at);
+        }
+#endif
+        Vector<T,D> uv;
+        for (int d = 0; d < D; ++d) {
+          uv[d] = u[d];
+          vals[4 * c + d] = double(u[d]);
+        }
+        cell.defineU(uv.data());
+      } else if (mat[c] == o.ipresMat) {
+        cell.defineRho(T(o.rhoOut));
+        vals[4 * c] = double(T(o.rhoOut));
+      }
+      ++c;
+    });
+  }
+  lat.initialize();
+
+  std::FILE* statsFile = nullptr;
+  std::FILE* forceFile = nullptr;
+#if REF_Q != 9
+  std::unique_ptr<SuperLatticePhysBoundaryForce3D<T,DESCRIPTOR>> forceF;
+  std::unique_ptr<SuperSum3D<T,T>> sumF;
+  if (o.forceMat >= 0) {
+    forceF.reset(new SuperLatticePhysBoundaryForce3D<T,DESCRIPTOR>(lat, geo.getMaterialIndicator(o.forceMat), converter));
+    sumF.reset(new SuperSum3D<T,T>(*forceF, geo.getMaterialIndicator(o.forceMat)));
+  }
+#endif
+  if (!o.out.empty()) {
+    if (!o.noPops) dumpPopulations(lat, ext, o.out + ".f0.bin");
+    std::ofstream m(o.out + ".mat.bin", std::ios::binary);
+    m.write(reinterpret_cast<const char*>(mat.data()), mat.size() * sizeof(std::int32_t));
+    std::ofstream v(o.out + ".vals.bin", std::ios::binary);
+    v.write(reinterpret_cast<const char*>(vals.data()), vals.size() * sizeof(double));
+    std::ofstream bc(o.out + ".bclass.bin", std::ios::binary);
+    bc.write(reinterpret_cast<const char*>(bclass.data()), bclass.size() * sizeof(std::int32_t));
+    statsFile = std::fopen((o.out + ".stats.txt").c_str(), "w");
+    if (o.forceMat >= 0) forceFile = std::fopen((o.out + ".force.txt").c_str(), "w");
+  }
+  auto writeForce = [&](long step) {
+#if REF_Q != 9
+    if (!forceFile || !sumF) return;
+    T sum[4] = {};
+    int in[1] = {0};
+    (*sumF)(sum, in);
+    std::fprintf(forceFile, "%ld %.17g %.17g %.17g\n", step, double(sum[0]), double(sum[1]), double(sum[2]));
+    std::fflush(forceFile);
+#else
+    (void)step;
+#endif
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+  for (long s = 0; s < o.steps; ++s) {
+    lat.collideAndStream();
+    if (statsFile) {
+      auto& st = lat.getStatistics();
+      std::fprintf(statsFile, "%.17g %.17g %.17g\n", double(st.getAverageRho()), double(st.getAverageEnergy()), double(st.getMaxU()));
+    }
+    if (o.forceEvery > 0 && (s + 1) % o.forceEvery == 0) writeForce(s + 1);
+  }
+  const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (o.forceEvery <= 0) writeForce(o.steps);
+  if (!o.out.empty()) {
+    std::fclose(statsFile);
+    if (forceFile) std::fclose(forceFile);
+    if (!o.noPops) dumpPopulations(lat, ext, o.out + ".fS.bin");
+    if (o.moments) {
+      auto& block = lat.getBlock(0);
+      std::vector<double> mom(std::size_t(1 + D) * nCore);
+      std::size_t c = 0;
+      forCore(ext, [&](int x, int y, int z) {
+        auto cell = block.get(loc(x, y, z));
+        T rho, u[D];
+        cell.computeRhoU(rho, u);
+        mom[c] = double(rho);
+        for (int d = 0; d < D; ++d) mom[(1 + d) * nCore + c] = double(u[d]);
+        ++c;
+      });
+      std::ofstream f(o.out + ".mom.bin", std::ios::binary);
+      f.write(reinterpret_cast<const char*>(mom.data()), mom.size() * sizeof(double));
+    }
+    std::ofstream j(o.out + ".json");
+    j.precision(17);
+    j << "{\"case\": \"geo\", \"q\": " << Q << ", \"d\": " << D << ", \"ext\": [" << ext[0] << ", " << ext[1] << ", "
+      << ext[2] << "], \"periodic\": [" << o.periodicFlags[0] << ", " << o.periodicFlags[1] << ", "
+      << o.periodicFlags[2] << "], \"dyn\": \"" << o.dyn << "\", \"omega\": " << o.omega << ", \"magic\": " << o.magic
+      << ", \"cs\": " << o.cs << ", \"force\": [" << o.force[0] << ", " << o.force[1] << ", " << o.force[2] << "]"
+      << ", \"steps\": " << o.steps << ", \"init\": \"" << o.init << "\", \"ulid\": " << o.ulid
+      << ", \"poiseuille\": " << o.poiseuille << ", \"rho_out\": " << o.rhoOut << ", \"seconds\": " << sec
+      << ", \"bytes\": " << sizeof(T) << "}\n";
+  }
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   olb::initialize(&argc, &argv);
   Options o = parse(argc, argv);
   OstreamManager clout(std::cout, "lbref");
+  if (o.kase == "geo") return runGeo(o);
 
   const bool periodic = (o.kase == "periodic" || o.kase == "porous");
   const bool channel = o.kase == "channel";

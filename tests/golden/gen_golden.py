@@ -9,6 +9,11 @@ are committed and are all the tests need.
 
     python tests/golden/gen_golden.py            # all cases
     python tests/golden/gen_golden.py NAME ...   # selected cases
+
+The "geo" cases write their material map (geo_box, geo_channel) to a file the driver reads, and
+keep the imposed boundary values (vals [cells, 4]), the reference's classification of every
+boundary cell it set up (bclass rows {cell, kind, normal type, n0, n1, n2}) and the boundary
+force on the sphere over time (force rows {step, Fx, Fy, Fz}) beside the populations.
 """
 from __future__ import annotations
 
@@ -106,6 +111,84 @@ CASES.update({
 })
 
 
+
+# ---- material maps of the "geo" cases (materials from a file, the reference's own setters) ----
+def geo_box(shape, lid=True):
+    """A closed box: the outer layer is material 2, the top layer along y (edges and corners
+    included) material 3 when `lid`, the inside fluid (1)."""
+    mat = np.full(shape, 2, np.int32)
+    inner = tuple(slice(1, s - 1) for s in shape)
+    mat[inner] = 1
+    if lid:
+        mat[:, -1, ...] = 3
+    return mat
+
+
+def geo_channel(shape, sphere):
+    """The channel past a sphere of the full-size configuration (openlb_b200.configs.
+    channel_materials) at a reduced size: sphere = (centre x, y, z, radius)."""
+    sys.path.insert(0, str(HERE.parent.parent))
+    from openlb_b200.configs import channel_materials
+    cx, cy, cz, r = sphere
+    return channel_materials(tuple(shape), (cx, cy, cz), 2 * r)
+
+
+GEO = {
+    # cavity2d's setup: InterpolatedVelocity on every wall (flat faces and external corners),
+    # the lid the top row including its corners
+    "geo_cavity_d2q9_ivel_bgk_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
+                                                                  "--ivel-lid", "3", "--ulid", "0.1", "--steps", "150"]),
+    "geo_cavity_d2q9_ivel_bgk_f32": ("d2q9_f32", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
+                                                            "--ivel-lid", "3", "--ulid", "0.1", "--steps", "150"]),
+    "geo_cavity_d2q9_ivel_constrho_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "constrho", "--omega", "1.3",
+                                                                       "--ivel", "2", "--ivel-lid", "3", "--ulid",
+                                                                       "0.1", "--steps", "150"]),
+    "geo_cavity_d2q9_ivel_rnd_f64": ("d2q9_f64_nocse", (13, 11), ["--dyn", "trt", "--omega", "1.5", "--magic", "0.25",
+                                                                  "--ivel", "2", "--ivel-lid", "3", "--ulid", "0.08",
+                                                                  *RND, "--steps", "80"]),
+    # a 3D cavity with InterpolatedVelocity on every wall: flat faces, external edges and corners
+    "geo_cavity_d3q19_ivel_bgk_f64": ("d3q19_f64_nocse", (9, 8, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                      "--ivel-lid", "3", "--ulid", "0.05", *RND,
+                                                                      "--steps", "60"]),
+    "geo_cavity_d3q27_ivel_trt_f64": ("d3q27_f64_nocse", (8, 9, 7), ["--dyn", "trt", "--omega", "1.6", "--magic",
+                                                                     "0.25", "--ivel", "2", "--ivel-lid", "3",
+                                                                     "--ulid", "0.05", "--steps", "80"]),
+    "geo_cavity_d3q19_ivel_bgk_f32": ("d3q19_f32", (9, 8, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                "--ivel-lid", "3", "--ulid", "0.05", "--steps", "60"]),
+    # the channel past a sphere at reduced size: D3Q27 TRT (magic 1/4), RectanglePoiseuille3D inlet
+    # (peak 0.04), pressure outlet, bounce-back side walls, halfway bounce-back sphere, force on the
+    # sphere.  The side walls carry BounceBack dynamics: with no dynamics on the wall cells, the
+    # populations the wall cells pass on to the inlet and outlet cells along the faces come from
+    # the block's padding, whose content in the reference is whatever the periodic-shift storage
+    # rotates into it, so the result would depend on the padding layout.
+    "geo_channel_d3q27_trt_f64": ("d3q27_f64_nocse", (26, 14, 14), ["--dyn", "trt", "--omega", "1.6", "--magic",
+                                                                    "0.25", "--ivel", "3", "--poiseuille", "0.04",
+                                                                    "--ipres", "4", "--rho", "1", "--bounceback", "2",
+                                                                    "--bouzidi", "5", "--force-mat", "5",
+                                                                    "--force-every", "10",
+                                                                    "--steps", "120"]),
+    "geo_channel_d3q27_trt_f32": ("d3q27_f32", (26, 14, 14), ["--dyn", "trt", "--omega", "1.6", "--magic", "0.25",
+                                                              "--ivel", "3", "--poiseuille", "0.04", "--ipres", "4",
+                                                              "--rho", "1", "--bounceback", "2", "--bouzidi", "5",
+                                                              "--force-mat", "5",
+                                                              "--force-every", "10", "--steps", "120"]),
+    "geo_channel_d3q19_bgk_rnd_f64": ("d3q19_f64_nocse", (20, 12, 11), ["--dyn", "bgk", "--omega", "1.3", "--ivel",
+                                                                        "3", "--poiseuille", "0.05", "--ipres", "4",
+                                                                        "--rho", "0.99", "--bounceback", "2", "--bouzidi", "5",
+                                                                        "--force-mat", "5", "--force-every", "5",
+                                                                        *RND, "--steps", "60"]),
+}
+GEO_SPHERE = {"geo_channel_d3q27_trt_f64": (8, 7, 7, 3), "geo_channel_d3q27_trt_f32": (8, 7, 7, 3),
+              "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5)}
+
+
+def geo_material(name: str) -> np.ndarray:
+    shape = GEO[name][1]
+    if name in GEO_SPHERE:
+        return geo_channel(shape, GEO_SPHERE[name])
+    return geo_box(shape)
+
+
 STATS_EVERY = {"full_cavity_d2q9_bgk_128_f64": 100}
 
 
@@ -115,12 +198,19 @@ def select_stats(stats: np.ndarray, every: int) -> np.ndarray:
 
 
 def generate(name: str) -> Path:
-    binary, case, args = CASES[name]
+    if name in GEO:
+        binary, shape, geo_args = GEO[name]
+        case, args = "geo", ["--n", *map(str, shape), *geo_args]
+    else:
+        binary, case, args = CASES[name]
     exe = REF / f"lbref_{binary}"
     if not exe.exists():
         raise SystemExit(f"{exe} missing: build it with `make -C oracle ref`")
     with tempfile.TemporaryDirectory() as tmp:
         prefix = str(Path(tmp) / "c")
+        if case == "geo":
+            geo_material(name).tofile(prefix + ".in.mat")
+            args = [*args, "--mat", prefix + ".in.mat"]
         subprocess.run([str(exe), case, *args, "--out", prefix], check=True, timeout=600, cwd=tmp,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         meta = json.loads(Path(prefix + ".json").read_text())
@@ -133,18 +223,27 @@ def generate(name: str) -> Path:
         stats = np.loadtxt(prefix + ".stats.txt", ndmin=2)
         bnd = Path(prefix + ".bnd.bin")
         extra = {"bnd": np.fromfile(bnd, dtype=np.float64).reshape(-1, 8)} if bnd.exists() else {}
+        vals = Path(prefix + ".vals.bin")
+        if vals.exists():
+            extra["vals"] = np.fromfile(vals, dtype=np.float64).reshape(-1, 4)
+        bclass = Path(prefix + ".bclass.bin")
+        if bclass.exists():
+            extra["bclass"] = np.fromfile(bclass, dtype=np.int32).reshape(-1, 6)
+        force = Path(prefix + ".force.txt")
+        if force.exists():
+            extra["force"] = np.loadtxt(force, ndmin=2)
     every = STATS_EVERY.get(name, 1)
     stats = select_stats(stats, every)
     meta["stats_every"] = every
     meta["binary"] = binary
-    meta["args"] = [case, *args]
+    meta["args"] = [case, *[a for a in args if not a.endswith(".in.mat")]]
     out = HERE / f"{name}.npz"
     np.savez_compressed(out, f0=f0, fS=fS, mat=mat, stats=stats, meta=json.dumps(meta), **extra)
     return out
 
 
 def main(argv: list[str]) -> int:
-    names = argv or list(CASES)
+    names = argv or [*CASES, *GEO]
     for name in names:
         print(generate(name))
     return 0

@@ -49,8 +49,9 @@ def load_fixture(name: str) -> dict:
     z = np.load(GOLDEN / f"{name}.npz")
     meta = json.loads(str(z["meta"]))
     fx = {k: z[k] for k in ("f0", "fS", "mat", "stats")}
-    if "bnd" in z.files:
-        fx["bnd"] = z["bnd"]
+    for k in ("bnd", "vals", "bclass", "force"):
+        if k in z.files:
+            fx[k] = z[k]
     fx["meta"] = meta
     fx["name"] = name
     return fx
@@ -62,6 +63,8 @@ def core_of(meta: dict) -> tuple[int, int, int]:
 
 
 def periodic_of(meta: dict) -> tuple[int, int, int]:
+    if meta["case"] == "geo":
+        return tuple(int(v) for v in meta["periodic"])
     if meta["case"] == "channel":  # inlet/outlet along x, periodic across
         return (0, 1, 1 if meta["d"] == 3 else 0)
     p = 1 if meta["case"] in ("periodic", "porous") else 0
@@ -129,12 +132,50 @@ def case_setup(fx: dict) -> dict:
         else:
             setup["cell_dyn"] = np.where(mat == 1, 1, 0).astype(np.uint8)
             setup["links"] = bouzidi_links(q, core, mat, 1, (2,), None, per)
+    elif meta["case"] == "geo":
+        a = geo_args(meta)
+        mat3 = mat.reshape(core)
+        cd = np.zeros(mat.shape, np.uint8)
+        cd[mat == 1] = 1
+        for m in a["bounceback"]:
+            cd[mat == m] = 2
+        solid = list(a["bouzidi"])
+        walls = [(0.0, 0.0, 0.0)] * len(solid)
+        if a["lid"] is not None:
+            solid.append(a["lid"])
+            walls.append((meta["ulid"], 0.0, 0.0))
+        if solid:
+            setup["links"] = bouzidi_links(q, core, mat3, 1, solid, walls if a["lid"] is not None else None, per)
+        bc = fx["bclass"]
+        cd[bc[:, 0]] = 3
+        setup["cell_dyn"] = cd
+        setup["fd"] = {"cells": bc[:, 0].astype(np.int64), "kinds": bc[:, 1].astype(np.int32),
+                       "types": bc[:, 2].astype(np.int32), "normals": np.ascontiguousarray(bc[:, 3:6], np.int32),
+                       "values": np.ascontiguousarray(fx["vals"][bc[:, 0]])}
     elif meta["case"] == "channel":
         # bulk dynamics on 1, bounce-back on the layers behind the open faces (2), BGK with
         # the boundary momenta on the inlet (3) and outlet (4) faces
         setup["cell_dyn"] = np.select([mat == 1, mat == 2], [1, 2], 3).astype(np.uint8)
         setup["fd"] = fd_boundaries(fx["bnd"])
     return setup
+
+
+def geo_args(meta: dict) -> dict:
+    """The boundary set-up of a "geo" fixture, read back from the driver arguments it was made
+    with (oracle/ref_driver.cpp, geo case)."""
+    args = meta["args"]
+
+    def value(flag):
+        return args[args.index(flag) + 1] if flag in args else None
+
+    def ints(flag):
+        v = value(flag)
+        return [int(x) for x in v.split(",")] if v else []
+
+    lid = value("--lid")
+    return {"bouzidi": ints("--bouzidi"), "bounceback": ints("--bounceback"), "ivel": ints("--ivel"),
+            "ivel_lid": ints("--ivel-lid"), "ipres": ints("--ipres"), "lid": int(lid) if lid else None,
+            "force_mat": ints("--force-mat")}
 
 
 def fd_boundaries(bnd: np.ndarray) -> dict:
@@ -154,7 +195,7 @@ class _Case(C.Structure):
                 ("n_links", C.c_int64), ("link_cell", C.c_void_p), ("link_dir", C.c_void_p),
                 ("link_wall", C.c_void_p), ("n_fd", C.c_int64), ("fd_cell", C.c_void_p),
                 ("fd_kind", C.c_void_p), ("fd_dir", C.c_void_p), ("fd_orient", C.c_void_p),
-                ("fd_value", C.c_void_p)]
+                ("fd_value", C.c_void_p), ("fd_type", C.c_void_p), ("fd_normal", C.c_void_p)]
 
 
 _oracle = None
@@ -202,10 +243,16 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
         c.material = m.ctypes.data
     if setup.get("fd") is not None:
         fd = setup["fd"]
-        arrs = [np.ascontiguousarray(fd[k]) for k in ("cells", "kinds", "dirs", "orients", "values")]
-        keep += arrs
-        c.n_fd = len(arrs[0])
-        c.fd_cell, c.fd_kind, c.fd_dir, c.fd_orient, c.fd_value = (a.ctypes.data for a in arrs)
+        if "normals" in fd:
+            arrs = [np.ascontiguousarray(fd[k]) for k in ("cells", "kinds", "values", "types", "normals")]
+            keep += arrs
+            c.n_fd = len(arrs[0])
+            c.fd_cell, c.fd_kind, c.fd_value, c.fd_type, c.fd_normal = (a.ctypes.data for a in arrs)
+        else:
+            arrs = [np.ascontiguousarray(fd[k]) for k in ("cells", "kinds", "dirs", "orients", "values")]
+            keep += arrs
+            c.n_fd = len(arrs[0])
+            c.fd_cell, c.fd_kind, c.fd_dir, c.fd_orient, c.fd_value = (a.ctypes.data for a in arrs)
     if setup["links"] is not None:
         cells, dirs, wall = (np.ascontiguousarray(a) for a in setup["links"])
         keep += [cells, dirs, wall]
@@ -262,4 +309,8 @@ def fluid_mask(fx: dict) -> np.ndarray:
     inlet and outlet faces (materials 3 and 4; in the cavity those numbers are walls)."""
     if fx["meta"]["case"] == "channel":
         return np.isin(fx["mat"], (1, 3, 4))
+    if fx["meta"]["case"] == "geo":
+        m = fx["mat"] == 1
+        m[fx["bclass"][:, 0]] = True
+        return m
     return fx["mat"] == 1

@@ -36,9 +36,12 @@ def test_normals_from_materials_match_the_reference_list(name):
 def test_corner_cells_are_not_flat():
     mat = np.ones((6, 5), np.int32)
     mat[0, :] = 3
+    mat[:, 0] = 3
     cells, dirs, orients = lbx.fd_boundaries_from_materials(mat, 3, outside=(0,), periodic=(False, False))
-    # (0,0) and (0,4) touch two open sides: corners, left out
-    assert sorted(cells.tolist()) == [1, 2, 3] and set(dirs.tolist()) == {0} and set(orients.tolist()) == {-1}
+    # the x = 0 row and the y = 0 column meet at (0, 0), an external corner: left out
+    assert sorted(cells.tolist()) == [1, 2, 3, 5, 10, 15, 20]  # the far ends of each side have no normal
+    _, types, normals = lbx.discrete_normals(mat, 3, outside=(0,), periodic=(False, False))
+    assert types[0] == lbx.NORMAL_EXTERNAL_CORNER and normals[0].tolist() == [-1, -1, 0]
 
 
 @pytest.mark.gpu
@@ -54,9 +57,10 @@ def test_fd_boundary_arguments_are_checked():
     with pytest.raises(lbx.LbxError):  # duplicate cell
         lat.set_fd_boundaries([0, 0], [1, 1], [0, 0], [-1, -1], np.zeros((2, 4)))
     lat.close()
+    # a flat cell at the end of a face: its neighbour along y is a padding cell, which carries no
+    # dynamics (u = 0), as the reference's overlap does
     walls = lbx.BlockLattice(19, (8, 6, 5), (0, 0, 1), "f64")
-    with pytest.raises(lbx.LbxError, match="edge or corner"):
-        walls.set_fd_boundaries([0], [1], [0], [-1], v)  # (0, 0, 0): y is a wall
+    walls.set_fd_boundaries([0], [1], [0], [-1], v)
     walls.close()
 
 

@@ -33,7 +33,10 @@ def make_lattice(setup: dict, storage: str) -> lbx.BlockLattice:
         lat.set_bouzidi_links(*setup["links"])
     if setup.get("fd") is not None:
         fd = setup["fd"]
-        lat.set_fd_boundaries(fd["cells"], fd["kinds"], fd["dirs"], fd["orients"], fd["values"])
+        if "normals" in fd:
+            lat.set_boundary_cells(fd["cells"], fd["kinds"], fd["types"], fd["normals"], fd["values"])
+        else:
+            lat.set_fd_boundaries(fd["cells"], fd["kinds"], fd["dirs"], fd["orients"], fd["values"])
     return lat
 
 
