@@ -6,8 +6,9 @@ a parabolic inflow (RectanglePoiseuille3D, peak 0.04) through an InterpolatedVel
 x = 0 and an InterpolatedPressure face at the far end; Re = U_peak d / nu = 50.
 
 Porous medium (default 384^3, D3Q27, Smagorinsky-forced BGK with C_s = 0.12): non-overlapping
-spheres of diameter U[8, 20] placed by seeded random sequential addition towards porosity 0.6,
-periodic, body force F_x = 1e-6, nu = 0.05, halfway bounce-back on the sphere surfaces.
+spheres of diameter U[8, 20] placed by seeded random sequential addition (largest first) to
+porosity 0.6, periodic, body force F_x = 1e-6, nu = 0.05, halfway bounce-back on the sphere
+surfaces.
 
     python -m openlb_b200.configs channel --storage f16dev --steps 100
     python -m openlb_b200.configs porous --size 192 --steps 100
@@ -99,57 +100,68 @@ def drag_coefficient(force_x: float, u: float, d: float, rho: float = 1.0) -> fl
     return 2.0 * force_x / (rho * u * u * math.pi * d * d / 4.0)
 
 
-def porous_spheres(n: int, seed: int = 7, porosity: float = 0.6, batches: int = 400, batch: int = 1000) -> np.ndarray:
-    """Seeded random sequential addition of non-overlapping periodic spheres, d ~ U[8, 20]:
-    candidates are drawn in batches and taken in order if they overlap neither an accepted
-    sphere nor an earlier candidate of the batch (periodic distances), until the solid volume
-    reaches 1 - porosity or the batches run out (the packing jams short of 0.6)."""
+def porous_spheres(n: int, seed: int = 7, porosity: float = 0.6, d_min: float = 8.0, d_max: float = 20.0,
+                   tries: int = 64, batch: int = 32) -> np.ndarray:
+    """Seeded random sequential addition of non-overlapping spheres in a periodic n^3 box.
+
+    Diameters are drawn uniformly from [d_min, d_max] until their volume is 1.3 times the solid
+    volume wanted, then placed largest first: each sphere tries up to `tries` batches of `batch`
+    uniform random centres and takes the first centre whose periodic distance to every placed
+    sphere is at least the sum of the radii (a sphere that finds none is skipped).  Placing the
+    large spheres first leaves the gaps to the small ones, which lets the addition pass the
+    jamming point of drawing sizes in random order.  The solid cells are those whose centre lies
+    in a sphere; the addition stops once they make up 1 - porosity of the box.  Returns the
+    boolean solid map."""
     from scipy.spatial import cKDTree
     rng = np.random.default_rng(seed)
     target = (1 - porosity) * n ** 3
+    diameters = []
+    vol = 0.0
+    while vol < 1.3 * target:
+        d = rng.uniform(d_min, d_max)
+        diameters.append(d)
+        vol += math.pi * d ** 3 / 6
+    diameters = np.sort(np.array(diameters))[::-1]
     cen = np.zeros((0, 3))
     rad = np.zeros(0)
-    filled = 0.0
-    for _ in range(batches):
-        if filled >= target:
-            break
-        c = rng.uniform(0, n, (batch, 3))
-        r = rng.uniform(4, 10, batch)
-        ok = np.ones(batch, bool)
-        if len(cen):
-            tree = cKDTree(cen, boxsize=n)
-            for i, nbrs in enumerate(tree.query_ball_point(c, 20.0)):
-                if nbrs:
-                    dd = np.abs(cen[nbrs] - c[i])
-                    dd = np.minimum(dd, n - dd)
-                    if np.any((dd ** 2).sum(axis=1) < (rad[nbrs] + r[i]) ** 2):
-                        ok[i] = False
-        keep = []
-        own = cKDTree(c, boxsize=n)
-        for i in np.nonzero(ok)[0]:
-            clash = False
-            for j in own.query_ball_point(c[i], 20.0):
-                if j in keep:
-                    dd = np.abs(c[j] - c[i])
-                    dd = np.minimum(dd, n - dd)
-                    if (dd ** 2).sum() < (r[j] + r[i]) ** 2:
-                        clash = True
-                        break
-            if not clash:
-                keep.append(i)
-                filled += 4 / 3 * math.pi * r[i] ** 3
-                if filled >= target:
-                    break
-        cen = np.vstack([cen, c[keep]])
-        rad = np.concatenate([rad, r[keep]])
+    tree, in_tree = None, 0
     solid = np.zeros((n, n, n), bool)
-    for c, r in zip(cen, rad):
-        lo = np.floor(c - r).astype(int)
-        hi = np.ceil(c + r).astype(int) + 1
-        ix, iy, iz = (np.arange(lo[a], hi[a]) for a in range(3))
-        X, Y, Z = np.meshgrid(ix, iy, iz, indexing="ij")
-        inside = (X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2 <= r ** 2
-        solid[np.ix_(ix % n, iy % n, iz % n)] |= inside
+    count = 0
+    for d in diameters:
+        r = d / 2
+        for _ in range(tries):
+            c = rng.uniform(0, n, (batch, 3))
+            ok = np.ones(batch, bool)
+            if tree is not None:  # spheres in the tree, within reach of a candidate
+                for i, nb in enumerate(tree.query_ball_point(c, r + d_max / 2)):
+                    if nb:
+                        dd = np.abs(cen[nb] - c[i])
+                        dd = np.minimum(dd, n - dd)
+                        if np.any((dd ** 2).sum(axis=1) < (rad[nb] + r) ** 2):
+                            ok[i] = False
+            if in_tree < len(cen):  # spheres placed since the tree was built
+                dd = np.abs(cen[None, in_tree:] - c[:, None])
+                dd = np.minimum(dd, n - dd)
+                ok &= ~np.any((dd ** 2).sum(axis=2) < (rad[None, in_tree:] + r) ** 2, axis=1)
+            hit = np.nonzero(ok)[0]
+            if len(hit) == 0:
+                continue
+            cc = c[hit[0]]
+            cen = np.vstack([cen, cc])
+            rad = np.append(rad, r)
+            lo = np.floor(cc - r).astype(int)
+            hi = np.ceil(cc + r).astype(int) + 1
+            ix, iy, iz = (np.arange(lo[a], hi[a]) for a in range(3))
+            inside = ((ix[:, None, None] - cc[0]) ** 2 + (iy[None, :, None] - cc[1]) ** 2
+                      + (iz[None, None, :] - cc[2]) ** 2) <= r * r
+            box = np.ix_(ix % n, iy % n, iz % n)
+            count += int((inside & ~solid[box]).sum())
+            solid[box] |= inside
+            break
+        if len(cen) - in_tree >= 256:
+            tree, in_tree = cKDTree(cen, boxsize=n), len(cen)
+        if count >= target:
+            break
     return solid
 
 

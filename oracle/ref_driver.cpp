@@ -68,6 +68,9 @@
 #include <cstring>
 #include <algorithm>
 #include <fstream>
+#ifdef PARALLEL_MODE_OMP
+#include <omp.h>
+#endif
 #include <memory>
 #include <string>
 #include <vector>
@@ -312,6 +315,12 @@ int runGeo(const Options& o) {
     if (o.classifyOnly) return 0;
   }
 
+  // The set-up runs on one thread: with several, the OpenMP build's setBouzidiBoundary gives
+  // results that vary from run to run (a race in the set-up, not in the steps).
+#ifdef PARALLEL_MODE_OMP
+  const int stepThreads = omp_get_max_threads();
+  omp_set_num_threads(1);
+#endif
   SuperLattice<T,DESCRIPTOR> lat(geo);
   const T nu = (T(1) / T(o.omega) - T(0.5)) / T(3);
   const UnitConverter<T,DESCRIPTOR> converter(T(1), T(1), T(1), T(1), nu, T(1));
@@ -441,6 +450,9 @@ int runGeo(const Options& o) {
     });
   }
   lat.initialize();
+#ifdef PARALLEL_MODE_OMP
+  omp_set_num_threads(stepThreads);
+#endif
 
   std::FILE* statsFile = nullptr;
   std::FILE* forceFile = nullptr;

@@ -1,20 +1,20 @@
 """The larger benchmark configurations at full size, run on the GPU path with their own physics
-checks.  A reference oracle run of these sizes does not fit a test; the checks are stability,
-conservation and the expected sign and order of the flow response.
+checks (their accuracy against the reference's FP64 runs is recorded by
+openlb_b200/full_size.py).
 
 Channel past a sphere (512 x 128 x 128, D3Q27, TRT with magic 1/4):
-  - a sphere of diameter 24 at (128, 64, 64), halfway bounce-back;
-  - uniform inflow 0.04 through a flat InterpolatedVelocity face at x = 0, an InterpolatedPressure
-    face at x = 511, periodic across the section;
-  - Re = U d / nu = 50, so nu = 0.0192;
+  - a duct with bounce-back side walls and a sphere of diameter 24 at (128, 64, 64) with halfway
+    bounce-back;
+  - a RectanglePoiseuille3D inflow of peak 0.04 through the x = 0 face (InterpolatedVelocity), an
+    InterpolatedPressure face at x = 511;
+  - Re = U_peak d / nu = 50, so nu = 0.0192;
   - FP16 and BF16 deviation storage.
-  The reference's own setup has walls around the section, which needs the edge processors this
-  build does not provide yet. The drag must be positive and finite, and the populations must stay
-  finite.
+  The drag on the sphere must be positive and its cross components small, and the populations
+  must stay finite.
 
 Porous medium (384^3, D3Q27, Smagorinsky-forced BGK with C_s = 0.12, FP16):
   - non-overlapping spheres of diameter U[8, 20], placed by seeded random sequential addition
-    towards porosity 0.6 (the addition jams near 0.70, which is what the test runs);
+    (largest first) to porosity 0.6;
   - periodic, body force F_x = 1e-6, nu = 0.05 (the value this build records for the case);
   - halfway bounce-back on the sphere surfaces.
   Mass must be conserved and the mean x velocity must be positive, giving a finite permeability
@@ -32,7 +32,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _channel_sphere(storage, steps):
-    lat = configs.channel_sphere(storage)
+    lat, _ = configs.channel_sphere(storage)
     lat.collide_and_stream(1)
     lat.autotune(steps=3)
     import torch
@@ -41,7 +41,7 @@ def _channel_sphere(storage, steps):
     lat.collide_and_stream(steps, statistics=True)
     st = lat.get_statistics()
     sec = time.perf_counter() - t0
-    drag = lat.reduce(lbx.REDUCE_DRAG)
+    drag = lat.boundary_force(0)  # link group 0: the sphere
     lat.close()
     return st, drag, 512 * 128 * 128 * steps / sec / 1e6
 
@@ -75,6 +75,6 @@ def test_porous_medium_at_full_size():
     perm = nu * ux * porosity / force
     print(f"porous 384^3 D3Q27 Smagorinsky-forced FP16: porosity {porosity:.3f}, "
           f"{n ** 3 * steps / sec / 1e6:.0f} MLUPS, <u_x> {ux:.3e}, k = {perm:.3f}")
-    assert 0.55 < porosity < 0.75
+    assert 0.595 < porosity <= 0.6
     assert abs(m1[0] - m0[0]) <= 1e-4 * m0[0]  # 16-bit storage: mass to the rounding of the form
     assert ux > 0 and math.isfinite(perm) and st["max_u"] < 0.1
