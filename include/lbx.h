@@ -319,6 +319,15 @@ int lbx_boundary_force(lbx_lattice lattice, int32_t group, double out[3], void* 
  * (CyclicColumn::operator[] / deviceData, gpu/cuda/column.h:100-171) and a column rotation
  * by `offset` cells (CyclicColumn::rotate, gpu/cuda/column.h:144-154). */
 int lbx_population_shift(lbx_lattice lattice, int32_t pop, int64_t* shift);
+/* Device address of population column `pop` for code outside this library that works on the
+ * populations in place (ConcreteBlockLattice::getPopulationPointers, core/blockLattice.h:134,
+ * 676-681; CyclicColumn::deviceData, gpu/cuda/column.h:100-171).  Population i of padded cell n
+ * (n = (x + 1) * padded[1] * padded[2] + (y + 1) * padded[2] + z + 1 in 3D, see lbx_info) is at
+ * ((S*)*ptr)[(n + *shift) % column_period], S the storage type.  With the columns mapped twice
+ * (the default layout) *shift is 0 and the index needs no wrap; a plain layout returns the
+ * column start and its shift.  The address stays valid until the lattice is destroyed; the
+ * shift changes with every step (lbx_collide_and_stream, lbx_rotate). */
+int lbx_population_ptr(lbx_lattice lattice, int32_t pop, void** ptr, int64_t* shift);
 int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
 
 /* Launch configuration of the step kernel, the knob the autotuner turns (no reference
@@ -454,9 +463,10 @@ int lbx_ensemble_autotune(lbx_ensemble ens, int32_t steps, lbx_tune_entry* out, 
  *                i * column_stride, n_cells cells per column, values f_i - w_i of `storage`;
  *   out          host array {sum rho, sum j_x, sum j_y, sum j_z} (rho = sum_i f_i + 1), FP64;
  *   n_cells      at most LBX_NOALLOC_MAX_CELLS, otherwise LBX_ERR_INVALID before any device work.
- * Runs on the current device and `stream`, and synchronises the stream.  The first call on a
- * device looks up the scratch's device address; make it before any stream capture.  All calls
- * share the one scratch array: calls that overlap on the GPU race, so serialise them. */
+ * Runs on the current device and `stream`; every call looks up the scratch's device address on
+ * the current device and synchronises the stream, so it must not be called while that stream is
+ * being captured.  All calls share the one scratch array: calls that overlap on the GPU race, so
+ * serialise them. */
 #define LBX_NOALLOC_MAX_BLOCKS 8192
 #define LBX_NOALLOC_CELLS_PER_BLOCK 4096
 #define LBX_NOALLOC_MAX_CELLS ((int64_t)LBX_NOALLOC_MAX_BLOCKS * LBX_NOALLOC_CELLS_PER_BLOCK)

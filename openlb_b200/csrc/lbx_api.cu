@@ -111,6 +111,19 @@ struct lbx_lattice_s {
   void* linkDelta = nullptr;
   uint8_t* linkGroup = nullptr;             // per link: index of the solid it faces
   int64_t nLinks = 0;
+  // host copies: the cell map as set (public ids incl. the boundary list's marks; empty = bulk
+  // everywhere) and the links (padded cell, direction, wall term) in their device order
+  std::vector<uint8_t> hostMap;
+  std::vector<uint32_t> linkHostCell;
+  std::vector<uint8_t> linkHostDir;
+  std::vector<double> linkHostDelta;
+  // resting links fused into the K-cells step kernel (one direction bit per padded cell) and the
+  // links the link kernel still applies after that kernel (moving walls, unusual neighbours)
+  uint32_t* linkMask = nullptr;
+  uint32_t* restCell = nullptr;
+  uint8_t* restDir = nullptr;
+  void* restDelta = nullptr;
+  int64_t nRest = 0;
   // flat-face velocity / pressure boundary cells (lbx_set_fd_boundaries)
   int64_t nFd = 0;
   uint32_t* fdCell = nullptr;
@@ -188,6 +201,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.fdValue = L->fdValue;
   a.fdMom = L->fdMom;
   a.nFdCorners = L->nFdCorners;
+  a.linkMask = L->kernel == 2 ? L->linkMask : nullptr;
   a.err = L->devErr;
   return a;
 }
@@ -498,6 +512,105 @@ bool device_ok(int device, std::string& why) {
 }
 
 
+// Composes the device cell map from the map as set and the links, and splits the links: a link
+// from a bulk cell (x_b, k) towards a cell without dynamics, at rest (no wall term), is fused
+// into the K-cells step kernel (bit k of linkMask[x_b], x_b marked kCellBulkLinked); every other
+// link stays with the link kernel, which with the other kernel variants applies all links.
+int refresh_cell_map(lbx_lattice_s* L) {
+  const bool need = !L->hostMap.empty() || L->nLinks > 0;
+  cudaFree(L->linkMask);
+  cudaFree(L->restCell);
+  cudaFree(L->restDir);
+  cudaFree(L->restDelta);
+  L->linkMask = nullptr;
+  L->restCell = nullptr;
+  L->restDir = nullptr;
+  L->restDelta = nullptr;
+  L->nRest = 0;
+  if (!need) {
+    cudaFree(L->cellDyn);
+    L->cellDyn = nullptr;
+    return LBX_OK;
+  }
+  std::vector<uint8_t> map = L->hostMap;
+  if (map.empty()) {
+    map.assign(static_cast<size_t>(L->n), 0);
+    for (int64_t c = 0; c < L->ncore; ++c) map[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
+  }
+  std::vector<uint32_t> mask;
+  std::vector<uint32_t> rc;
+  std::vector<uint8_t> rd;
+  std::vector<double> rdelta;
+  bool restWall = false;
+  if (L->nLinks > 0) {
+    mask.assign(static_cast<size_t>(L->n), 0u);
+    const Geometry g = geometry_of(L);
+    const int64_t ext[3] = {g.nx, g.ny, g.nz};
+    for (size_t l = 0; l < L->linkHostCell.size(); ++l) {
+      const uint32_t src = L->linkHostCell[l];
+      const int k = L->linkHostDir[l];
+      // core coordinates of the solid neighbour, across a periodic face to its image
+      int64_t p[3];
+      p[0] = int64_t(src) / g.sx - 1;
+      const int64_t r = int64_t(src) - (p[0] + 1) * g.sx;
+      p[1] = r / g.sy - 1;
+      p[2] = r - (p[1] + 1) * g.sy - g.pz;
+      const int* c = velocity(L->q, k);
+      bool inside = true;
+      for (int a = 0; a < L->d; ++a) {
+        p[a] += c[a];
+        if (p[a] < 0 || p[a] >= ext[a]) {
+          if (L->periodic[a]) p[a] = (p[a] + ext[a]) % ext[a];
+          else inside = false;
+        }
+      }
+      const int64_t tgt = inside ? (p[0] + 1) * g.sx + (p[1] + 1) * g.sy + (p[2] + g.pz) : -1;
+      const bool fuse = L->linkHostDelta[l] == 0.0 && map[src] == LBX_CELL_BULK && tgt >= 0 &&
+                        map[size_t(tgt)] == LBX_CELL_NONE;
+      if (fuse) {
+        mask[src] |= 1u << k;
+      } else {
+        rc.push_back(src);
+        rd.push_back(uint8_t(k));
+        rdelta.push_back(L->linkHostDelta[l]);
+        restWall = restWall || L->linkHostDelta[l] != 0.0;
+      }
+    }
+    bool any = false;
+    for (size_t n = 0; n < mask.size(); ++n)
+      if (mask[n]) {
+        map[n] = kCellBulkLinked;
+        any = true;
+      }
+    if (any) {
+      LBX_CUDA_TRY(cudaMalloc(&L->linkMask, mask.size() * sizeof(uint32_t)));
+      LBX_CUDA_TRY(cudaMemcpy(L->linkMask, mask.data(), mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    // the links the link kernel applies after the K-cells kernel
+    const int64_t nr = int64_t(rc.size());
+    if (nr > 0) {
+      LBX_CUDA_TRY(cudaMalloc(&L->restCell, size_t(nr) * sizeof(uint32_t)));
+      LBX_CUDA_TRY(cudaMalloc(&L->restDir, size_t(nr)));
+      LBX_CUDA_TRY(cudaMemcpy(L->restCell, rc.data(), size_t(nr) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+      LBX_CUDA_TRY(cudaMemcpy(L->restDir, rd.data(), size_t(nr), cudaMemcpyHostToDevice));
+      if (restWall) {
+        if (L->storage == LBX_F64) {
+          LBX_CUDA_TRY(cudaMalloc(&L->restDelta, size_t(nr) * sizeof(double)));
+          LBX_CUDA_TRY(cudaMemcpy(L->restDelta, rdelta.data(), size_t(nr) * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+          std::vector<float> df(rdelta.begin(), rdelta.end());
+          LBX_CUDA_TRY(cudaMalloc(&L->restDelta, size_t(nr) * sizeof(float)));
+          LBX_CUDA_TRY(cudaMemcpy(L->restDelta, df.data(), size_t(nr) * sizeof(float), cudaMemcpyHostToDevice));
+        }
+      }
+      L->nRest = nr;
+    }
+  }
+  if (!L->cellDyn) LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
+  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, map.data(), size_t(L->n), cudaMemcpyHostToDevice));
+  return LBX_OK;
+}
+
 // Validates a boundary list, sorts it by cell and uploads it (lbx_set_fd_boundaries,
 // lbx_set_boundary_cells, lbx_set_interpolated_boundary).  The listed cells become
 // LBX_CELL_FD_BOUNDARY in the cell map; cells of the previous list that are not listed again
@@ -565,18 +678,15 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
   L->nFd = 0;
   L->nFdCorners = 0;
   // cell map: the listed cells become LBX_CELL_FD_BOUNDARY, the ones of an old list bulk
-  std::vector<uint8_t> map(static_cast<size_t>(L->n), 0);
-  if (L->cellDyn) {
-    LBX_CUDA_TRY(cudaMemcpy(map.data(), L->cellDyn, size_t(L->n), cudaMemcpyDeviceToHost));
-  } else {
-    for (int64_t c = 0; c < L->ncore; ++c) map[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
-    LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
+  if (L->hostMap.empty()) {
+    L->hostMap.assign(static_cast<size_t>(L->n), 0);
+    for (int64_t c = 0; c < L->ncore; ++c) L->hostMap[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
   }
-  for (uint32_t old : L->fdHostCells) map[old] = LBX_CELL_BULK;
-  for (uint32_t c : hc) map[c] = LBX_CELL_FD_BOUNDARY;
+  for (uint32_t old : L->fdHostCells) L->hostMap[old] = LBX_CELL_BULK;
+  for (uint32_t c : hc) L->hostMap[c] = LBX_CELL_FD_BOUNDARY;
   L->fdHostCells = hc;
   L->fdHost = list;
-  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, map.data(), size_t(L->n), cudaMemcpyHostToDevice));
+  if (int rc = refresh_cell_map(L)) return rc;
   if (n == 0) return LBX_OK;
   LBX_CUDA_TRY(cudaMalloc(&L->fdCell, size_t(n) * sizeof(uint32_t)));
   LBX_CUDA_TRY(cudaMalloc(&L->fdMeta, size_t(n)));
@@ -605,7 +715,10 @@ int set_links_impl(lbx_lattice_s* L, int64_t n, const int64_t* cells, const int3
   L->linkDir = nullptr;
   L->linkDelta = nullptr;
   L->nLinks = 0;
-  if (n == 0) return LBX_OK;
+  L->linkHostCell.clear();
+  L->linkHostDir.clear();
+  L->linkHostDelta.clear();
+  if (n == 0) return refresh_cell_map(L);
   std::vector<uint32_t> hc(static_cast<size_t>(n));
   std::vector<uint8_t> hd(static_cast<size_t>(n));
   std::vector<double> delta(static_cast<size_t>(n));
@@ -663,7 +776,10 @@ int set_links_impl(lbx_lattice_s* L, int64_t n, const int64_t* cells, const int3
     }
   }
   L->nLinks = n;
-  return LBX_OK;
+  L->linkHostCell = hc;
+  L->linkHostDir = hd;
+  L->linkHostDelta = delta;
+  return refresh_cell_map(L);
 }
 
 }  // namespace
@@ -754,6 +870,10 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->linkDir);
   cudaFree(L->linkDelta);
   cudaFree(L->linkGroup);
+  cudaFree(L->linkMask);
+  cudaFree(L->restCell);
+  cudaFree(L->restDir);
+  cudaFree(L->restDelta);
   cudaFree(L->fdCell);
   cudaFree(L->fdMeta);
   cudaFree(L->fdValue);
@@ -807,20 +927,17 @@ int lbx_set_dynamics(lbx_lattice L, int32_t dynamics, const lbx_params* params) 
 int lbx_set_cell_dynamics(lbx_lattice L, const uint8_t* ids) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   DeviceGuard guard(L->device);
-  if (!ids) {
-    cudaFree(L->cellDyn);
-    L->cellDyn = nullptr;
-    return LBX_OK;
-  }
   std::vector<uint8_t> padded(static_cast<size_t>(L->n), 0);
   for (int64_t c = 0; c < L->ncore; ++c) {
-    if (ids[c] > LBX_CELL_FD_BOUNDARY) return fail(LBX_ERR_INVALID, "cell dynamics id out of range");
-    padded[size_t(core_index_to_padded(L, c))] = ids[c];
+    const uint8_t id = ids ? ids[c] : uint8_t(LBX_CELL_BULK);
+    if (id > LBX_CELL_FD_BOUNDARY) return fail(LBX_ERR_INVALID, "cell dynamics id out of range");
+    padded[size_t(core_index_to_padded(L, c))] = id;
   }
   for (uint32_t n : L->fdHostCells) padded[n] = LBX_CELL_FD_BOUNDARY;  // the boundary list wins
-  if (!L->cellDyn) LBX_CUDA_TRY(cudaMalloc(&L->cellDyn, size_t(L->n)));
-  LBX_CUDA_TRY(cudaMemcpy(L->cellDyn, padded.data(), size_t(L->n), cudaMemcpyHostToDevice));
-  return LBX_OK;
+  if (!ids && L->fdHostCells.empty()) padded.clear();  // bulk everywhere: no map
+  L->hostMap.swap(padded);
+  cudaDeviceSynchronize();
+  return refresh_cell_map(L);
 }
 
 int lbx_set_fd_boundaries(lbx_lattice L, int64_t n, const int64_t* cells, const int32_t* kinds,
@@ -1149,8 +1266,14 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
     rotate_all(L);
     if (L->nLinks > 0 || L->nFd > 0) {
       const LaunchArgs b = args_of(L);
-      if (L->nLinks > 0)
+      // the K-cells kernel applied the resting links itself (linkMask); the link kernel does
+      // the rest, or all of them after the other kernel variants
+      if (b.linkMask) {
+        if (L->nRest > 0)
+          LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->restCell, L->restDir, L->restDelta, L->nRest, s))));
+      } else if (L->nLinks > 0) {
         LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
+      }
       if (L->nFd > 0) LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_fd_boundary<Q, S>(b, s))));
     }
     if (ev[3]) {
@@ -1315,6 +1438,20 @@ int lbx_population_shift(lbx_lattice L, int32_t pop, int64_t* shift) {
   if (!L || !shift) return fail(LBX_ERR_INVALID, "null argument");
   if (pop < 0 || pop >= L->q) return fail(LBX_ERR_INVALID, "population index out of range");
   *shift = L->shift[pop];
+  return LBX_OK;
+}
+
+int lbx_population_ptr(lbx_lattice L, int32_t pop, void** ptr, int64_t* shift) {
+  if (!L || !ptr || !shift) return fail(LBX_ERR_INVALID, "null argument");
+  if (pop < 0 || pop >= L->q) return fail(LBX_ERR_INVALID, "population index out of range");
+  char* column = static_cast<char*>(L->pop) + size_t(pop) * size_t(L->stride) * storage_bytes(L->storage);
+  if (L->doubled) {  // the second mapping makes [shift, shift + period) one contiguous run
+    *ptr = column + size_t(L->shift[pop]) * storage_bytes(L->storage);
+    *shift = 0;
+  } else {
+    *ptr = column;
+    *shift = L->shift[pop];
+  }
   return LBX_OK;
 }
 

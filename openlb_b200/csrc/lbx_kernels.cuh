@@ -67,6 +67,13 @@ __device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t s, int64_t n) {
   return r >= n ? r - n : r;
 }
 
+// Cell kinds of the device cell map: the public ids (0 no dynamics, 1 bulk, 2 bounce-back,
+// 3 velocity / pressure boundary) plus 4, a bulk cell some of whose populations leave towards a
+// resting halfway bounce-back wall; the K-cells step kernel writes those populations back into the
+// cell's opposite slots itself (see k_collide_stream_groups), the other kernels treat 4 as 1.
+constexpr uint8_t kCellBulkLinked = 4;
+__device__ __forceinline__ bool bulk_kind(uint8_t k) { return k == 1 || k == kCellBulkLinked; }
+
 
 // Block partial of the lattice statistics {sum rho, sum |u|^2, max |u|^2, count}: a warp
 // butterfly, then the warps in index order, written to part[4 * block] without atomics.  With
@@ -240,7 +247,7 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
     if (needPops) {
       static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
     }
-    if (kind == 1) {
+    if (bulk_kind(kind)) {
       collide<Q, R, DYN>(f, p, rho, usq);
       valid = true;
     } else if (kind == 2) {
@@ -392,7 +399,7 @@ __global__ void __launch_bounds__(TILE) k_collide_stream_tiled(S* __restrict__ p
       const uint8_t kind = cellDyn ? cellDyn[n] : uint8_t(1);
       R f[Q];
       static_for<Q>([&](auto I) { f[I] = Storage<S>::load(stage + I * SPAN + sR[I] + tid); });
-      if (kind == 1) {
+      if (bulk_kind(kind)) {
         R rho, usq;
         collide<Q, R, DYN>(f, p, rho, usq);
         accRho += double(rho);
@@ -588,10 +595,10 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
       const int x = int(px) - 1, y = int(py) - 1, z = int(rem - py * uint32_t(g.sy)) - g.pz;
       if (!(x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz)) continue;
       const uint8_t kind = cellDyn ? cellDyn[t0 + j] : uint8_t(1);
-      if (kind != 1 && kind != 2) continue;
+      if (!bulk_kind(kind) && kind != 2) continue;
       R f[Q];
       static_for<Q>([&](auto I) { f[I] = Storage<S>::load(stage + I * COL + sHead[st][I] + j); });
-      if (kind == 1) {
+      if (bulk_kind(kind)) {
         R rho, usq;
         collide<Q, R, DYN>(f, p, rho, usq);
         accRho += double(rho);
@@ -693,6 +700,7 @@ template <int Q, typename S, int DYN, int K, bool DOUBLED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
+                                                               const uint32_t* __restrict__ linkMask,
                                                                double* __restrict__ statPart) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
@@ -718,7 +726,12 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     // 3D: (x+1)*sx + (y+1)*sy + z0 + 1; 2D: the fast axis is y (sy = 1), z absent
     const uint32_t n0 = (D::d == 3) ? uint32_t((x + 1) * g.sx + (y + 1) * g.sy + z0 + 1)
                                     : uint32_t((x + 1) * g.sx + z0 + 1);
-    // raw loads first, all in straight-line code (the wrap is a select, not a branch), so every
+    // the cell kinds first: a cell without dynamics is neither loaded nor stored, so the solid
+    // part of a porous medium costs no population traffic
+    uint8_t kinds[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) kinds[k] = (k < nvalid) ? (cellDyn ? cellDyn[n0 + k] : uint8_t(1)) : uint8_t(0);
+    // raw loads next, all in straight-line code (the wrap is a select, not a branch), so every
     // load of the thread is in flight before the first value is used
     S raw[K][Q];
     static_for<Q>([&](auto I) {
@@ -726,7 +739,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       if constexpr (DOUBLED) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (k < nvalid) raw[k][I] = col[n0 + k];
+          if (kinds[k] != 0) raw[k][I] = col[n0 + k];
       } else {
         uint32_t idx = n0 + cols.s[I];
         idx = idx >= P ? idx - P : idx;
@@ -734,17 +747,14 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
         for (int k = 0; k < K; ++k) {
           uint32_t ik = idx + k;
           if (k > 0) ik = ik >= P ? ik - P : ik;
-          if (k < nvalid) raw[k][I] = col[ik];
+          if (kinds[k] != 0) raw[k][I] = col[ik];
         }
       }
     });
     R f[K][Q];
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      static_for<Q>([&](auto I) { f[k][I] = (k < nvalid) ? Storage<S>::load(&raw[k][I]) : R(0); });
-    uint8_t kinds[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) kinds[k] = (k < nvalid) ? (cellDyn ? cellDyn[n0 + k] : uint8_t(1)) : uint8_t(0);
+      static_for<Q>([&](auto I) { f[k][I] = (kinds[k] != 0) ? Storage<S>::load(&raw[k][I]) : R(0); });
     // pairs of bulk BGK cells of a 16-bit form: one packed (f32x2) collision per pair, the same
     // bits as two scalar ones.  The 16-bit forms are limited by instruction issue, where the
     // packed form halves the collision's arithmetic; the FP32 form waits on HBM, and there the
@@ -755,7 +765,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       const int k0 = 2 * pr, k1 = 2 * pr + 1;
       bool packedDone = false;
       if constexpr (PACKED) {
-        if (k1 < K && kinds[k0] == 1 && kinds[k1] == 1) {
+        if (k1 < K && bulk_kind(kinds[k0]) && bulk_kind(kinds[k1])) {
           float rr[2], uu[2];
           collide_bgk_x2<Q>(*reinterpret_cast<float(*)[2][Q]>(&f[k0]), p.omega, rr, uu);
 #pragma unroll
@@ -772,7 +782,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
 #pragma unroll
         for (int k = k0; k <= k1; ++k) {
           if (k >= K) break;
-          if (kinds[k] == 1) {
+          if (bulk_kind(kinds[k])) {
             R rho, usq;
             collide<Q, R, DYN>(f[k], p, rho, usq);
             accRho += double(rho);
@@ -806,7 +816,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     if (slowFace) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        if (k >= nvalid) continue;
+        if (kinds[k] == 0) continue;  // no dynamics: nothing to carry across (see linkMask)
         const int cz0 = D::d == 3 ? z0 + k : 0;
         const int cy0 = D::d == 3 ? y : z0 + k;
         static_for<Q>([&](auto I) {
@@ -828,7 +838,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const int fk = z0 + k;
-        if (k >= nvalid || (fk != 0 && fk != nf - 1)) continue;
+        if (kinds[k] == 0 || (fk != 0 && fk != nf - 1)) continue;
         static_for<Q>([&](auto I) {
           constexpr int cf = D::d == 3 ? D::C[I][2] : D::C[I][1];
           if constexpr (cf != 0) {
@@ -837,6 +847,34 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
               bool inside = x + cx >= 0 && x + cx < g.nx;
               if constexpr (D::d == 3) inside = inside && y + cy >= 0 && y + cy < g.ny;
               if (inside) ghost_store(I, k, n0 + k - uint32_t(cf * nf));
+            }
+          }
+        });
+      }
+    }
+    // resting halfway bounce-back (BouzidiPostProcessor with q = 1/2 and a wall at rest,
+    // boundary/setBouzidiBoundary.h:48-77), fused into the store: a population f_k that leaves the
+    // cell towards a solid neighbour x_s = x_b + c_k is also written into the slot of x_s's
+    // opposite population, which the rotation of this step carries into f_opp(k)(x_b) -- the value
+    // the link kernel would copy there after the stream.  The solid cell has no dynamics, so no
+    // other thread writes that slot (cells without dynamics make no stores, ghost ones included).
+    if (linkMask) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (kinds[k] != kCellBulkLinked) continue;
+        const uint32_t mk = linkMask[n0 + k];
+        static_for<Q>([&](auto I) {
+          if ((mk >> int(I)) & 1u) {
+            constexpr int O = D::OPP[I];
+            const int32_t off = int32_t(D::C[I][0] * g.sx + D::C[I][1] * g.sy + D::C[I][2]);
+            S* col = static_cast<S*>(cols.base[O]);
+            const uint32_t slot = n0 + k + uint32_t(off);
+            if constexpr (DOUBLED) {
+              Storage<S>::store(col + slot, f[k][I]);
+            } else {
+              uint32_t idx = slot + cols.s[O];
+              idx = idx >= P ? idx - P : idx;
+              Storage<S>::store(col + idx, f[k][I]);
             }
           }
         });
@@ -1230,7 +1268,7 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
       return;
     }
     const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
-    if (kind == 1) {
+    if (bulk_kind(kind)) {
       R f[Q];
       load_cell(nn, f);
       bulk_velocity<Q, R>(f, halfF, v);
@@ -1249,7 +1287,7 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
       return r;
     }
     const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
-    if (kind != 1) return R(1);
+    if (!bulk_kind(kind)) return R(1);
     R f[Q];
     load_cell(nn, f);
     return bulk_rho<Q, R>(f);
@@ -1430,7 +1468,7 @@ __global__ void __launch_bounds__(256) k_mass_momentum(const S* __restrict__ pop
     const int y = int((c / g.nz) % g.ny);
     const int x = int(c / (int64_t(g.nz) * g.ny));
     const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
-    if (!cellDyn || cellDyn[n] == 1) {
+    if (!cellDyn || bulk_kind(cellDyn[n])) {
       double r = 1.0;
       static_for<Q>([&](auto I) {
         const double fi = double(Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)));
@@ -1500,7 +1538,7 @@ __global__ void __launch_bounds__(256) k_residual(const S* __restrict__ pop, Geo
     const int y = int((c / g.nz) % g.ny);
     const int x = int(c / (int64_t(g.nz) * g.ny));
     const int64_t n = int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
-    if (!cellDyn || cellDyn[n] == 1) {
+    if (!cellDyn || bulk_kind(cellDyn[n])) {
       R f[Q];
       static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
       R r, uu[3];
@@ -1543,6 +1581,7 @@ struct LaunchArgs {
   const double* fdValue;     // 4 imposed values per cell
   double* fdMom;             // 7 doubles per cell of scratch (k_fd_momenta)
   int64_t nFdCorners;        // how many of them are corners (regularised in a second pass)
+  const uint32_t* linkMask;  // per padded cell: directions of resting bounce-back links (kind 4 cells)
   int* err;                  // device flag: a bounded wait of a step kernel gave up
 };
 
@@ -1685,17 +1724,17 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
     double* part = a.stats ? a.statPart : nullptr;
     switch (sel) {
-    case 2: k_collide_stream_groups<Q, S, DYN, 1, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
-    case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
-    case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
-    case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part); break;
+    case 2: k_collide_stream_groups<Q, S, DYN, 1, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
+    case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
+    case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
+    case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
     case 8:
     case 9:
       // four cells per thread: the 16-bit forms only (their per-cell arithmetic, not HBM, is
       // what limits them; four cells share one thread's index and address work)
       if constexpr (sizeof(S) == 2) {
-        if (sel == 8) k_collide_stream_groups<Q, S, DYN, 4, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part);
-        else k_collide_stream_groups<Q, S, DYN, 4, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, part);
+        if (sel == 8) k_collide_stream_groups<Q, S, DYN, 4, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part);
+        else k_collide_stream_groups<Q, S, DYN, 4, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part);
         break;
       }
       return cudaErrorInvalidValue;

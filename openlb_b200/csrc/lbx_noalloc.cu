@@ -17,8 +17,9 @@
 //   - every call uses the same array, so calls whose kernels overlap on the GPU (different
 //     streams, or different host threads on one device) race and must be serialised by the
 //     caller; each call writes every partial it later reads, so nothing needs clearing;
-//   - the first call on a device looks up the device address of g_partials (see
-//     partials_address); make that first call before any stream capture.
+//   - every call looks up the device address of g_partials on the current device (see
+//     partials_address) and synchronises the stream, so it must not be called while the stream
+//     is being captured into a graph.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -48,17 +49,13 @@ int noalloc_fail(int code, const std::string& msg) { return lbx::set_error(code,
 
 // Device address of g_partials on the current device.  In host code the name g_partials only
 // stands for the symbol; a kernel given &g_partials would touch host memory.  The address is
-// looked up once per device, with that device current, and cached.
-cudaError_t partials_address(int device, double** out) {
-  static double* cached[64] = {};
-  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
-  if (!cached[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
-    if (e != cudaSuccess) return e;
-    cached[device] = static_cast<double*>(p);
-  }
-  *out = cached[device];
+// looked up on every call, with the caller's device current: nothing is cached, so the call
+// stays correct after a device reset and needs no locking between host threads.
+cudaError_t partials_address(double** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<double*>(p);
   return cudaSuccess;
 }
 
@@ -132,10 +129,8 @@ extern "C" int lbx_mass_momentum_noalloc(int32_t q, int32_t storage, const void*
                                              std::to_string(int64_t(LBX_NOALLOC_MAX_CELLS)) + " cells per call");
   if (column_stride < n_cells) return noalloc_fail(LBX_ERR_INVALID, "column_stride must be >= n_cells");
   if (!populations) return noalloc_fail(LBX_ERR_INVALID, "populations is null");
-  int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
   double* partials = nullptr;
-  if (e == cudaSuccess) e = partials_address(device, &partials);
+  cudaError_t e = partials_address(&partials);
   if (e != cudaSuccess) return noalloc_fail(LBX_ERR_CUDA, std::string("scratch set-up failed: ") + cudaGetErrorString(e));
   const int blocks = int((n_cells + LBX_NOALLOC_CELLS_PER_BLOCK - 1) / LBX_NOALLOC_CELLS_PER_BLOCK);
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -101,6 +101,7 @@ def _load() -> C.CDLL:
         "lbx_boundary_force": ([VP, I32, P(D), VP], C.c_int),
         "lbx_population_shift": ([VP, I32, P(I64)], C.c_int),
         "lbx_rotate": ([VP, I32, I64], C.c_int),
+        "lbx_population_ptr": ([VP, I32, P(VP), P(I64)], C.c_int),
         "lbx_set_launch_config": ([VP, I32, I32, I32, I32], C.c_int),
         "lbx_set_kernel_timing": ([VP, I32], C.c_int),
         "lbx_post_process": ([VP, VP], C.c_int),
@@ -446,6 +447,13 @@ class BlockLattice:
         """Time every launch shape of the step kernel on this lattice's data, keep the fastest;
         the populations are left as they were.  Returns the candidates with their ms/step."""
         return _tune(lib.lbx_autotune, self._h, steps, stream, "lbx_autotune")
+
+    def population_ptr(self, pop: int) -> tuple[int, int]:
+        """(device address, shift) of population column `pop` (lbx_population_ptr)."""
+        ptr = C.c_void_p()
+        sh = C.c_int64()
+        check(lib.lbx_population_ptr(self._h, int(pop), C.byref(ptr), C.byref(sh)), "lbx_population_ptr")
+        return int(ptr.value or 0), sh.value
 
     def population_shift(self, pop: int) -> int:
         s = C.c_int64()

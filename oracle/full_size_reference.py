@@ -3,7 +3,7 @@ configurations -- TEST INFRASTRUCTURE ONLY (records for tests/full_size_accuracy
 
 Runs the sequential FP64 reference driver (oracle/_ref/lbref_d3q27_f64_nocse, CPU_SISD with the
 generic dynamics templates, see oracle/Makefile) on the same material maps the GPU runs use
-(openlb_b200.configs), and writes compact records into oracle/_ref/records/:
+(openlb_b200.configs), and writes compact records into oracle/_ref/full/:
 
     <case>_ref_<steps>.npz   the boundary-force history on the sphere (channel), the statistics of
                              the last step, and the moment fields (rho, u) on probe sets: every
@@ -33,7 +33,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF = HERE / "_ref"
-RECORDS = REF / "records"
+RECORDS = REF / "full"      # finished records
+SCRATCH = HERE.parent / "_scratch"  # the runs' working files (large; neither committed nor sent to a GPU box)
 sys.path.insert(0, str(HERE.parent))
 
 from openlb_b200 import configs  # noqa: E402  (material maps and profiles only; no GPU work)
@@ -79,10 +80,11 @@ def run(case: str, steps: int, threads: int | None = None) -> Path:
     mat, args = channel_args(steps) if case == "channel" else porous_args(steps)
     exe = REF / "lbref_d3q27_f64_nocse"
     RECORDS.mkdir(parents=True, exist_ok=True)
+    SCRATCH.mkdir(parents=True, exist_ok=True)
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
-    with tempfile.TemporaryDirectory(dir=RECORDS) as tmp:
+    with tempfile.TemporaryDirectory(dir=SCRATCH) as tmp:
         prefix = str(Path(tmp) / "r")
         mat.tofile(prefix + ".in.mat")
         t0 = time.time()

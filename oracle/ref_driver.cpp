@@ -47,7 +47,7 @@
  *  --force-mat M writes PREFIX.force.txt: "step Fx Fy Fz" every K steps, the sum of
  *  SuperLatticePhysBoundaryForce3D over material M (lattice units).  --moments writes
  *  PREFIX.mom.bin (double rho, u [1 + d][ext...] from each cell's own computeRhoU) after the
- *  run; --no-pops skips the population dumps.  PREFIX.bclass.bin holds, for every cell the
+ *  run; --no-pops skips the population and boundary-value dumps.  PREFIX.bclass.bin holds, for every cell the
  *  velocity / pressure setters equipped, int32 {core cell, kind (1 velocity, 2 pressure), normal
  *  type, n0, n1, n2} as computeBoundaryTypeAndNormal gave them.
  *  Output (with --out): PREFIX.f0.bin / PREFIX.fS.bin  raw T populations [Q][ext...] of the
@@ -468,8 +468,10 @@ int runGeo(const Options& o) {
     if (!o.noPops) dumpPopulations(lat, ext, o.out + ".f0.bin");
     std::ofstream m(o.out + ".mat.bin", std::ios::binary);
     m.write(reinterpret_cast<const char*>(mat.data()), mat.size() * sizeof(std::int32_t));
-    std::ofstream v(o.out + ".vals.bin", std::ios::binary);
-    v.write(reinterpret_cast<const char*>(vals.data()), vals.size() * sizeof(double));
+    if (!o.noPops) {  // the large runs need neither the values nor the populations
+      std::ofstream v(o.out + ".vals.bin", std::ios::binary);
+      v.write(reinterpret_cast<const char*>(vals.data()), vals.size() * sizeof(double));
+    }
     std::ofstream bc(o.out + ".bclass.bin", std::ios::binary);
     bc.write(reinterpret_cast<const char*>(bclass.data()), bclass.size() * sizeof(std::int32_t));
     statsFile = std::fopen((o.out + ".stats.txt").c_str(), "w");

@@ -6,7 +6,7 @@ against the reference's own FP64 run and between the storage forms -- TEST INFRA
     python tests/full_size_accuracy.py porous  [--steps 10000] [--ref-steps 1000]
 
 1. FP64 on the GPU is run to the step count of the reference record
-   (oracle/_ref/records/<case>_ref_<ref-steps>.npz, made by oracle/full_size_reference.py) and
+   (oracle/_ref/full/<case>_ref_<ref-steps>.npz, made by oracle/full_size_reference.py) and
    compared with it on the record's probe cells (fluid cells only: rho and u of a fluid cell are
    sum f + 1 and j / rho on both sides; the forced dynamics add F / 2) and, for the channel,
    through the boundary force on the sphere every 500 steps.
@@ -34,7 +34,7 @@ sys.path.insert(0, str(ROOT / "oracle"))
 
 from openlb_b200 import configs, lbx  # noqa: E402
 
-RECORDS = ROOT / "oracle" / "_ref" / "records"
+RECORDS = ROOT / "oracle" / "_ref" / "full"
 
 
 def build(case: str, storage: str):
