@@ -68,7 +68,8 @@ typedef enum {
   LBX_CELL_NONE = 0,        /* NoDynamics (dynamics.h:51-63) */
   LBX_CELL_BULK = 1,        /* the lattice's bulk dynamics */
   LBX_CELL_BOUNCE_BACK = 2, /* BounceBack = collision::Revert (collision.h:465-484) */
-  LBX_CELL_FD_BOUNDARY = 3  /* a cell of the lbx_set_fd_boundaries list (set by that call) */
+  LBX_CELL_FD_BOUNDARY = 3, /* a cell of the lbx_set_fd_boundaries list (set by that call) */
+  LBX_CELL_BOUNCE_BACK_VELOCITY = 4 /* BounceBackVelocity (set by lbx_set_bounce_back_velocity) */
 } lbx_cell_dynamics;
 
 /* Kinds of flat-face boundary cells (lbx_set_fd_boundaries). */
@@ -215,6 +216,18 @@ int lbx_set_boundary_cells(lbx_lattice lattice, int64_t n, const int64_t* cells,
 int lbx_set_interpolated_boundary(lbx_lattice lattice, int32_t kind, const int32_t* material, int32_t boundary,
                                   int32_t n_fluid, const int32_t* fluid, int32_t n_outside, const int32_t* outside,
                                   const double* values);
+
+/* Bounce-back cells with a wall velocity: BounceBackVelocity (dynamics/dynamics.h:629-637), the
+ * populations swapped (collision::Revert, collision.h:465-484) and then corrected by Nguyen-Ladd,
+ * f_i += 2 rho u . c_i t_i / c_s^2 (NguyenLaddCorrection, collision.h:495-521), with the cell's
+ * fixed density rho[i] (NULL: 1, FixedDensity's initial value) and velocity u[3 * i ...]
+ * (momenta::ExternalVelocityFixedDensityTuple, dynamics/momenta/aliases.h:86-91; defineU).  The
+ * cells count in the statistics with {rho, |u|^2} and become LBX_CELL_BOUNCE_BACK_VELOCITY in the
+ * cell map, keeping that id through later lbx_set_cell_dynamics calls; cells of an earlier list
+ * that are not listed again become cells without dynamics.  n = 0 removes the list.  A velocity /
+ * pressure boundary cell reads such a neighbour's fixed velocity and density. */
+int lbx_set_bounce_back_velocity(lbx_lattice lattice, int64_t n, const int64_t* cells, const double* rho,
+                                 const double* u);
 
 /* Halfway bounce-back links: BouzidiVelocityPostProcessor with q = 1/2
  * (boundary/setBouzidiBoundary.h:129-162), applied after streaming.  Link l acts on core

@@ -119,6 +119,12 @@ struct lbx_lattice_s {
   std::vector<double> linkHostDelta;
   // resting links fused into the K-cells step kernel (one direction bit per padded cell) and the
   // links the link kernel still applies after that kernel (moving walls, unusual neighbours)
+  // bounce-back cells with a wall velocity (lbx_set_bounce_back_velocity): padded cells ascending
+  // and {rho, u} per cell
+  int64_t nBbv = 0;
+  uint32_t* bbvCell = nullptr;
+  double* bbvValue = nullptr;
+  std::vector<uint32_t> bbvHostCells;
   uint32_t* linkMask = nullptr;
   uint32_t* restCell = nullptr;
   uint8_t* restDir = nullptr;
@@ -202,6 +208,9 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.fdMom = L->fdMom;
   a.nFdCorners = L->nFdCorners;
   a.linkMask = L->kernel == 2 ? L->linkMask : nullptr;
+  a.nBbv = L->nBbv;
+  a.bbvCell = L->bbvCell;
+  a.bbvValue = L->bbvValue;
   a.err = L->devErr;
   return a;
 }
@@ -293,7 +302,7 @@ int64_t step_blocks(const lbx_lattice_s* L) {
 }
 
 int ensure_stat_capacity(lbx_lattice_s* L) {
-  const int64_t need = step_blocks(L) + fd_blocks(L->nFd);
+  const int64_t need = step_blocks(L) + fd_blocks(L->nFd) + fd_blocks(L->nBbv);
   if (need > L->statCapacity) {
     cudaFree(L->statPart);
     L->statPart = nullptr;
@@ -874,6 +883,8 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->restCell);
   cudaFree(L->restDir);
   cudaFree(L->restDelta);
+  cudaFree(L->bbvCell);
+  cudaFree(L->bbvValue);
   cudaFree(L->fdCell);
   cudaFree(L->fdMeta);
   cudaFree(L->fdValue);
@@ -930,11 +941,13 @@ int lbx_set_cell_dynamics(lbx_lattice L, const uint8_t* ids) {
   std::vector<uint8_t> padded(static_cast<size_t>(L->n), 0);
   for (int64_t c = 0; c < L->ncore; ++c) {
     const uint8_t id = ids ? ids[c] : uint8_t(LBX_CELL_BULK);
-    if (id > LBX_CELL_FD_BOUNDARY) return fail(LBX_ERR_INVALID, "cell dynamics id out of range");
+    if (id > LBX_CELL_FD_BOUNDARY)
+      return fail(LBX_ERR_INVALID, "cell dynamics id out of range (boundary cells are set by their own calls)");
     padded[size_t(core_index_to_padded(L, c))] = id;
   }
-  for (uint32_t n : L->fdHostCells) padded[n] = LBX_CELL_FD_BOUNDARY;  // the boundary list wins
-  if (!ids && L->fdHostCells.empty()) padded.clear();  // bulk everywhere: no map
+  for (uint32_t n : L->fdHostCells) padded[n] = LBX_CELL_FD_BOUNDARY;  // the boundary lists win
+  for (uint32_t n : L->bbvHostCells) padded[n] = LBX_CELL_BOUNCE_BACK_VELOCITY;
+  if (!ids && L->fdHostCells.empty() && L->bbvHostCells.empty()) padded.clear();  // bulk everywhere: no map
   L->hostMap.swap(padded);
   cudaDeviceSynchronize();
   return refresh_cell_map(L);
@@ -1026,6 +1039,55 @@ int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* ma
     list.insert(list.end(), add.begin(), add.end());
   }
   return install_boundary_list(L, std::move(list));
+}
+
+int lbx_set_bounce_back_velocity(lbx_lattice L, int64_t n, const int64_t* cells, const double* rho, const double* u) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (n < 0 || (n > 0 && (!cells || !u))) return fail(LBX_ERR_INVALID, "bad bounce-back arrays");
+  DeviceGuard guard(L->device);
+  std::vector<int64_t> order(static_cast<size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    order[size_t(i)] = i;
+    if (cells[i] < 0 || cells[i] >= L->ncore) return fail(LBX_ERR_INVALID, "bounce-back cell out of range");
+    const double r = rho ? rho[i] : 1.0;
+    if (!(r > 0) || !std::isfinite(r)) return fail(LBX_ERR_INVALID, "bounce-back density must be finite and > 0");
+    for (int a = 0; a < 3; ++a)
+      if (!std::isfinite(u[3 * i + a])) return fail(LBX_ERR_INVALID, "bounce-back velocity must be finite");
+  }
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cells[a] < cells[b]; });
+  std::vector<uint32_t> hc(static_cast<size_t>(n));
+  std::vector<double> hv(static_cast<size_t>(4 * n));
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t i = order[size_t(k)];
+    if (k > 0 && cells[i] == cells[order[size_t(k - 1)]]) return fail(LBX_ERR_INVALID, "duplicate bounce-back cell");
+    hc[size_t(k)] = uint32_t(core_index_to_padded(L, cells[i]));
+    hv[size_t(4 * k)] = rho ? rho[i] : 1.0;
+    for (int a = 0; a < 3; ++a) hv[size_t(4 * k + 1 + a)] = (a < L->d) ? u[3 * i + a] : 0.0;
+  }
+  for (uint32_t c : hc)
+    for (uint32_t f : L->fdHostCells)
+      if (c == f) return fail(LBX_ERR_INVALID, "a cell cannot be a velocity / pressure boundary and a bounce-back cell");
+  cudaDeviceSynchronize();
+  cudaFree(L->bbvCell);
+  cudaFree(L->bbvValue);
+  L->bbvCell = nullptr;
+  L->bbvValue = nullptr;
+  L->nBbv = 0;
+  if (L->hostMap.empty()) {
+    L->hostMap.assign(static_cast<size_t>(L->n), 0);
+    for (int64_t c = 0; c < L->ncore; ++c) L->hostMap[size_t(core_index_to_padded(L, c))] = LBX_CELL_BULK;
+  }
+  for (uint32_t old : L->bbvHostCells) L->hostMap[old] = LBX_CELL_NONE;
+  for (uint32_t c : hc) L->hostMap[c] = LBX_CELL_BOUNCE_BACK_VELOCITY;
+  L->bbvHostCells = hc;
+  if (n > 0) {
+    LBX_CUDA_TRY(cudaMalloc(&L->bbvCell, size_t(n) * sizeof(uint32_t)));
+    LBX_CUDA_TRY(cudaMalloc(&L->bbvValue, size_t(4 * n) * sizeof(double)));
+    LBX_CUDA_TRY(cudaMemcpy(L->bbvCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    LBX_CUDA_TRY(cudaMemcpy(L->bbvValue, hv.data(), size_t(4 * n) * sizeof(double), cudaMemcpyHostToDevice));
+    L->nBbv = n;
+  }
+  return refresh_cell_map(L);
 }
 
 int lbx_set_bouzidi_links(lbx_lattice L, int64_t n, const int64_t* cells, const int32_t* dirs, const double* wall) {

@@ -68,11 +68,16 @@ __device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t s, int64_t n) {
 }
 
 // Cell kinds of the device cell map: the public ids (0 no dynamics, 1 bulk, 2 bounce-back,
-// 3 velocity / pressure boundary) plus 4, a bulk cell some of whose populations leave towards a
-// resting halfway bounce-back wall; the K-cells step kernel writes those populations back into the
-// cell's opposite slots itself (see k_collide_stream_groups), the other kernels treat 4 as 1.
-constexpr uint8_t kCellBulkLinked = 4;
+// 3 velocity / pressure boundary, 4 bounce-back with a wall velocity) plus 7, a bulk cell some of
+// whose populations leave towards a resting halfway bounce-back wall; the K-cells step kernel
+// writes those populations back into the cell's opposite slots itself (see
+// k_collide_stream_groups), the other kernels treat 7 as 1.  Kinds 3 and 4 are collided by their
+// own kernels after the bulk kernel, which neither loads nor stores them.
+constexpr uint8_t kCellBulkLinked = 7;
+constexpr uint8_t kCellBounceBackVelocity = 4;
 __device__ __forceinline__ bool bulk_kind(uint8_t k) { return k == 1 || k == kCellBulkLinked; }
+// the kinds the K-cells step kernel loads, collides and stores itself
+__device__ __forceinline__ bool stepped_kind(uint8_t k) { return bulk_kind(k) || k == 2; }
 
 
 // Block partial of the lattice statistics {sum rho, sum |u|^2, max |u|^2, count}: a warp
@@ -727,7 +732,8 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     const uint32_t n0 = (D::d == 3) ? uint32_t((x + 1) * g.sx + (y + 1) * g.sy + z0 + 1)
                                     : uint32_t((x + 1) * g.sx + z0 + 1);
     // the cell kinds first: a cell without dynamics is neither loaded nor stored, so the solid
-    // part of a porous medium costs no population traffic
+    // part of a porous medium costs no population traffic (boundary cells of kinds 3 and 4 are
+    // loaded and stored by their own kernels)
     uint8_t kinds[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) kinds[k] = (k < nvalid) ? (cellDyn ? cellDyn[n0 + k] : uint8_t(1)) : uint8_t(0);
@@ -739,7 +745,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       if constexpr (DOUBLED) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (kinds[k] != 0) raw[k][I] = col[n0 + k];
+          if (stepped_kind(kinds[k])) raw[k][I] = col[n0 + k];
       } else {
         uint32_t idx = n0 + cols.s[I];
         idx = idx >= P ? idx - P : idx;
@@ -747,14 +753,14 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
         for (int k = 0; k < K; ++k) {
           uint32_t ik = idx + k;
           if (k > 0) ik = ik >= P ? ik - P : ik;
-          if (kinds[k] != 0) raw[k][I] = col[ik];
+          if (stepped_kind(kinds[k])) raw[k][I] = col[ik];
         }
       }
     });
     R f[K][Q];
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      static_for<Q>([&](auto I) { f[k][I] = (kinds[k] != 0) ? Storage<S>::load(&raw[k][I]) : R(0); });
+      static_for<Q>([&](auto I) { f[k][I] = stepped_kind(kinds[k]) ? Storage<S>::load(&raw[k][I]) : R(0); });
     // pairs of bulk BGK cells of a 16-bit form: one packed (f32x2) collision per pair, the same
     // bits as two scalar ones.  The 16-bit forms are limited by instruction issue, where the
     // packed form halves the collision's arithmetic; the FP32 form waits on HBM, and there the
@@ -816,7 +822,8 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     if (slowFace) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        if (kinds[k] == 0) continue;  // no dynamics: nothing to carry across (see linkMask)
+        // no dynamics: nothing to carry across (see linkMask); boundary cells: their own kernels
+        if (!stepped_kind(kinds[k])) continue;
         const int cz0 = D::d == 3 ? z0 + k : 0;
         const int cy0 = D::d == 3 ? y : z0 + k;
         static_for<Q>([&](auto I) {
@@ -838,7 +845,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const int fk = z0 + k;
-        if (kinds[k] == 0 || (fk != 0 && fk != nf - 1)) continue;
+        if (!stepped_kind(kinds[k]) || (fk != 0 && fk != nf - 1)) continue;
         static_for<Q>([&](auto I) {
           constexpr int cf = D::d == 3 ? D::C[I][2] : D::C[I][1];
           if constexpr (cf != 0) {
@@ -885,7 +892,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       if constexpr (DOUBLED) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (kinds[k] != 0) Storage<S>::store(col + n0 + k, f[k][I]);
+          if (stepped_kind(kinds[k])) Storage<S>::store(col + n0 + k, f[k][I]);
       } else {
         uint32_t idx = n0 + cols.s[I];
         idx = idx >= P ? idx - P : idx;
@@ -893,7 +900,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
         for (int k = 0; k < K; ++k) {
           uint32_t ik = idx + k;
           if (k > 0) ik = ik >= P ? ik - P : ik;
-          if (kinds[k] != 0) Storage<S>::store(col + ik, f[k][I]);
+          if (stepped_kind(kinds[k])) Storage<S>::store(col + ik, f[k][I]);
         }
       }
     });
@@ -1171,6 +1178,64 @@ __global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometr
   if (statPart) block_partial(aR, aU, aU, aC, statPart);
 }
 
+// BounceBack with a wall velocity (BounceBackVelocity, dynamics/dynamics.h:629-637): the
+// populations swapped (collision::Revert, collision.h:465-484), then the Nguyen-Ladd correction
+// (NguyenLaddCorrection, collision.h:495-521) f_i += 2 rho u_a c_ia t_i c_s^-2 for i >= 1, one axis
+// after the other, with the cell's fixed density and velocity (momenta::
+// ExternalVelocityFixedDensityTuple, dynamics/momenta/aliases.h:86-91); the cell counts in the
+// statistics with {rho, |u|^2}.  In place at the current shifts after the bulk step kernel, with
+// the ghost slots of a cell on a periodic face refreshed as k_fd_collide does; value[4 b ...] =
+// {rho, u}.  Statistics partials go after the boundary kernel's.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_bbv_collide(S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t nB,
+                                                     const uint32_t* __restrict__ bCell,
+                                                     const double* __restrict__ bValue, double* __restrict__ statPart) {
+  using R = typename Storage<S>::R;
+  using D = Desc<Q>;
+  const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double aR = 0.0, aU = 0.0, aC = 0.0;
+  if (b < nB) {
+    const int64_t n = bCell[b];
+    R f[Q];
+    static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
+    revert<Q, R>(f);
+    const R rho = R(bValue[4 * b]);
+    R u[3] = {R(0), R(0), R(0)};
+    static_for<D::d>([&](auto A) { u[A] = R(bValue[4 * b + 1 + A]); });
+    static_for<Q>([&](auto I) {
+      if constexpr (I >= 1) {
+        constexpr R t = weight<Q, R>(I);
+        static_for<D::d>([&](auto A) { f[I] += R(2) * rho * u[A] * R(D::C[I][A]) * t * R(3); });
+      }
+    });
+    static_for<Q>([&](auto I) { Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), f[I]); });
+    if (g.pmask) {
+      int x, y, z;
+      fd_decode(g, n, x, y, z);
+      static_for<Q>([&](auto I) {
+        constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
+        int tx = x + cx, ty = y + cy, tz = z + cz;
+        bool crossed = false, lost = false;
+        if (tx < 0 || tx >= g.nx) { if (g.pmask & 1) { tx = tx < 0 ? tx + g.nx : tx - g.nx; crossed = true; } else lost = true; }
+        if (ty < 0 || ty >= g.ny) { if (g.pmask & 2) { ty = ty < 0 ? ty + g.ny : ty - g.ny; crossed = true; } else lost = true; }
+        if constexpr (D::d == 3) {
+          if (tz < 0 || tz >= g.nz) { if (g.pmask & 4) { tz = tz < 0 ? tz + g.nz : tz - g.nz; crossed = true; } else lost = true; }
+        }
+        if (crossed && !lost) {
+          const int64_t gn = int64_t(tx - cx + 1) * g.sx + int64_t(ty - cy + 1) * g.sy + (tz - cz + g.pz);
+          Storage<S>::store(pop + I * g.stride + wrap_add(gn, sh.s[I], g.n), f[I]);
+        }
+      });
+    }
+    R uSqr = R(0);
+    static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+    aR = double(rho);
+    aU = double(uSqr);
+    aC = 1.0;
+  }
+  if (statPart) block_partial(aR, aU, aU, aC, statPart);
+}
+
 // Post-stream pass 1: every boundary cell's velocity and density from its momenta, and its
 // bulk velocity (what a neighbour reached across a periodic face sees: the reference's overlap
 // copy of the cell, which carries bulk dynamics), from the populations before any cell is
@@ -1228,7 +1293,7 @@ __device__ __forceinline__ int64_t fd_find(const uint32_t* __restrict__ fdCell, 
 // momenta; the imposed velocity of velocity cells does not depend on the order) or from the
 // populations (bulk cells, never rewritten here); cells without dynamics or with plain
 // bounce-back, and padding cells, read u = 0, rho = 1 (ZeroMomentum with OneDensity /
-// FixedDensity).  Neighbour densities in pass 2 come from pass 1; in pass 3 from the current
+// FixedDensity), bounce-back cells with a wall velocity their fixed velocity and density.  Neighbour densities in pass 2 come from pass 1; in pass 3 from the current
 // populations, i.e. those the priority-0 processors left, as the reference's corner processor
 // reads them.
 template <int Q, typename S>
@@ -1237,7 +1302,9 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
                                                        const uint8_t* __restrict__ fdMeta,
                                                        const double* __restrict__ fdValue,
                                                        const uint8_t* __restrict__ cellDyn, double hfx, double hfy,
-                                                       double hfz, const double* __restrict__ fdMom, int corners) {
+                                                       double hfz, const double* __restrict__ fdMom, int corners,
+                                                       int64_t nBbv, const uint32_t* __restrict__ bbvCell,
+                                                       const double* __restrict__ bbvValue) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1272,6 +1339,11 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
       R f[Q];
       load_cell(nn, f);
       bulk_velocity<Q, R>(f, halfF, v);
+    } else if (kind == kCellBounceBackVelocity) {  // FixedVelocityMomentum: the wall velocity
+      const int64_t jb = fd_find(bbvCell, nBbv, uint32_t(nn));
+      v[0] = v[1] = v[2] = R(0);
+      if (jb >= 0)
+        for (int a = 0; a < D::d; ++a) v[a] = R(bbvValue[4 * jb + 1 + a]);
     } else {
       v[0] = v[1] = v[2] = R(0);
     }
@@ -1287,6 +1359,10 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
       return r;
     }
     const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
+    if (kind == kCellBounceBackVelocity) {  // FixedDensity
+      const int64_t jb = fd_find(bbvCell, nBbv, uint32_t(nn));
+      return jb >= 0 ? R(bbvValue[4 * jb]) : R(1);
+    }
     if (!bulk_kind(kind)) return R(1);
     R f[Q];
     load_cell(nn, f);
@@ -1581,7 +1657,10 @@ struct LaunchArgs {
   const double* fdValue;     // 4 imposed values per cell
   double* fdMom;             // 7 doubles per cell of scratch (k_fd_momenta)
   int64_t nFdCorners;        // how many of them are corners (regularised in a second pass)
-  const uint32_t* linkMask;  // per padded cell: directions of resting bounce-back links (kind 4 cells)
+  const uint32_t* linkMask;  // per padded cell: directions of resting bounce-back links (kind 7 cells)
+  int64_t nBbv;              // bounce-back cells with a wall velocity
+  const uint32_t* bbvCell;   // their padded indices
+  const double* bbvValue;    // {rho, u} per cell
   int* err;                  // device flag: a bounded wait of a step kernel gave up
 };
 
@@ -1752,8 +1831,17 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+  int64_t bbb = 0;
+  if (a.nBbv > 0) {
+    bbb = fd_blocks(a.nBbv);
+    if (a.stats && nblocks + fdb + bbb > a.statCapacity) return cudaErrorInvalidValue;
+    k_bbv_collide<Q, S><<<unsigned(bbb), 256, 0, stream>>>(pop, g, sh, a.nBbv, a.bbvCell, a.bbvValue,
+                                                           a.stats ? a.statPart + 4 * (nblocks + fdb) : nullptr);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   if (!a.stats) return cudaSuccess;
-  k_stats_finalize<<<1, kFinalizeThreads, 0, stream>>>(a.statPart, nblocks + fdb, a.stats);
+  k_stats_finalize<<<1, kFinalizeThreads, 0, stream>>>(a.statPart, nblocks + fdb + bbb, a.stats);
   return cudaGetLastError();
 }
 // Post-stream regularisation of the boundary cells: momenta, then flat faces and edges, then
@@ -1773,7 +1861,8 @@ cudaError_t launch_fd_boundary(const LaunchArgs& a, cudaStream_t stream) {
   if (e != cudaSuccess) return e;
   for (int corners = 0; corners < (a.nFdCorners > 0 ? 2 : 1); ++corners) {
     k_fd_regularize<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.omega, a.nFd, a.fdCell, a.fdMeta, a.fdValue,
-                                                      a.cellDyn, hf[0], hf[1], hf[2], a.fdMom, corners);
+                                                      a.cellDyn, hf[0], hf[1], hf[2], a.fdMom, corners, a.nBbv,
+                                                      a.bbvCell, a.bbvValue);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

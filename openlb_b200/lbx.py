@@ -28,7 +28,7 @@ STORAGE = {"f64": 0, "f32": 1, "f16dev": 2, "bf16dev": 3}
 STORAGE_BYTES = {"f64": 8, "f32": 4, "f16dev": 2, "bf16dev": 2}
 DYNAMICS = {"bgk": 1, "trt": 2, "smagorinsky_bgk": 3, "forced_bgk": 4, "smagorinsky_forced_bgk": 5,
             "const_rho_bgk": 6}
-CELL_NONE, CELL_BULK, CELL_BOUNCE_BACK = 0, 1, 2
+CELL_NONE, CELL_BULK, CELL_BOUNCE_BACK, CELL_FD_BOUNDARY, CELL_BOUNCE_BACK_VELOCITY = 0, 1, 2, 3, 4
 STEP_STATISTICS = 1
 REDUCE_MASS_MOMENTUM, REDUCE_DRAG, REDUCE_RESIDUAL = 1, 2, 3
 
@@ -107,6 +107,7 @@ def _load() -> C.CDLL:
         "lbx_post_process": ([VP, VP], C.c_int),
         "lbx_set_fd_boundaries": ([VP, I64, VP, VP, VP, VP, VP], C.c_int),
         "lbx_set_boundary_cells": ([VP, I64, VP, VP, VP, VP, VP], C.c_int),
+        "lbx_set_bounce_back_velocity": ([VP, I64, VP, VP, VP], C.c_int),
         "lbx_set_interpolated_boundary": ([VP, I32, VP, I32, I32, VP, I32, VP, VP], C.c_int),
         "lbx_discrete_normals": ([I32, P(I32), P(I32), VP, I32, I32, VP, I32, VP, I64, VP, VP, VP, P(I64)],
                                  C.c_int),
@@ -338,6 +339,16 @@ class BlockLattice:
             raise ValueError("boundary arrays differ in length")
         check(lib.lbx_set_boundary_cells(self._h, len(c), _ptr(c), _ptr(k), _ptr(t), _ptr(nn), _ptr(v)),
               "lbx_set_boundary_cells")
+
+    def set_bounce_back_velocity(self, cells, rho, u) -> None:
+        """BounceBackVelocity cells (lbx_set_bounce_back_velocity): rho [n] (None: 1), u [n, 3]."""
+        c = np.ascontiguousarray(cells, dtype=np.int64)
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+        uu = np.ascontiguousarray(u, dtype=np.float64).reshape(-1, 3)
+        if len(uu) != len(c) or (r is not None and len(r) != len(c)):
+            raise ValueError("bounce-back arrays differ in length")
+        check(lib.lbx_set_bounce_back_velocity(self._h, len(c), _ptr(c), _ptr(r), _ptr(uu)),
+              "lbx_set_bounce_back_velocity")
 
     def set_interpolated_boundary(self, kind: int, material: np.ndarray, boundary: int, values: np.ndarray,
                                   fluid=(1,), outside=(0,)) -> None:

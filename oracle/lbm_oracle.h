@@ -33,7 +33,8 @@ enum lbo_material {
   LBO_SOLID = 0,      /* NoDynamics: left untouched (dynamics.h:51-63) */
   LBO_FLUID = 1,      /* the case's bulk dynamics */
   LBO_BOUNCE_BACK = 4,/* BounceBack = collision::Revert (collision.h:465-484) */
-  LBO_FD_BOUNDARY = 5 /* velocity / pressure boundary cell: BGK with boundary momenta (fd_* below) */
+  LBO_FD_BOUNDARY = 5, /* velocity / pressure boundary cell: BGK with boundary momenta (fd_* below) */
+  LBO_BOUNCE_BACK_VELOCITY = 6 /* BounceBackVelocity (dynamics.h:629-637): bbv_value below */
 };
 
 typedef struct {
@@ -63,6 +64,8 @@ typedef struct {
    * (boundary/interpolatedVelocity3D.h:45-90, interpolatedVelocity2D.h:45-80). */
   const int32_t* fd_type;
   const int32_t* fd_normal;
+  /* {rho, u_x, u_y, u_z} per cell (all cells; read for the LBO_BOUNCE_BACK_VELOCITY ones) */
+  const double* bbv_value;
 } lbo_case;
 
 /* Run `steps` collide-and-stream steps in place.  stats (may be NULL) receives per step

@@ -247,6 +247,10 @@ static void FN(fd_u_of)(const lbo_desc* d, const lbo_case* c, const STORE_T* f, 
   if (m < 0) return;
   const int mat = c->material ? c->material[m] : LBO_FLUID;
   if (mat == LBO_SOLID || mat == LBO_BOUNCE_BACK) return;
+  if (mat == LBO_BOUNCE_BACK_VELOCITY) { /* FixedVelocityMomentum */
+    for (int a = 0; a < d->d; ++a) u[a] = (REAL)c->bbv_value[4 * m + 1 + a];
+    return;
+  }
   if (wrapped) {
     for (int i = 0; i < q; ++i) g[i] = LOAD(pre[i * n + m]);
     FN(bulk_u)(d, c, g, u);
@@ -272,6 +276,7 @@ static REAL FN(fd_rho_of)(const lbo_desc* d, const lbo_case* c, const STORE_T* f
   if (m < 0) return (REAL)1;
   const int mat = c->material ? c->material[m] : LBO_FLUID;
   if (mat == LBO_SOLID || mat == LBO_BOUNCE_BACK) return (REAL)1;
+  if (mat == LBO_BOUNCE_BACK_VELOCITY) return (REAL)c->bbv_value[4 * m]; /* FixedDensity */
   REAL g[27];
   for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + m]);
   const int64_t b = fdIndex[m];
@@ -462,6 +467,29 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
           f[i * n + x] = f[d->opp[i] * n + x];
           f[d->opp[i] * n + x] = a;
         }
+      } else if (m == LBO_BOUNCE_BACK_VELOCITY) {
+        /* collision::Revert, then NguyenLaddCorrection (collision.h:495-521):
+         * f_i += 2 rho u_a c_ia t_i invCs2, axis after axis; statistic {rho, |u|^2} */
+        REAL g[27];
+        for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
+        for (int i = 1; i <= q / 2; ++i) {
+          const REAL a = g[i];
+          g[i] = g[d->opp[i]];
+          g[d->opp[i]] = a;
+        }
+        const double* v = c->bbv_value + 4 * x;
+        const REAL rho = (REAL)v[0];
+        REAL u[3] = {0, 0, 0};
+        for (int a = 0; a < d->d; ++a) u[a] = (REAL)v[1 + a];
+        for (int i = 1; i < q; ++i) {
+          const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+          for (int a = 0; a < d->d; ++a) g[i] += (REAL)2 * rho * u[a] * (REAL)d->c[i][a] * t * (REAL)3;
+        }
+        for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);
+        REAL uSqr = 0;
+        for (int a = 0; a < d->d; ++a) uSqr += u[a] * u[a];
+        cellRho[x] = rho;
+        cellUsq[x] = uSqr;
       }
     }
     /* statistics, accumulated in cell order (latticeStatistics.hh:183-192, 60-90) */

@@ -30,13 +30,15 @@
  *    lbref geo --mat FILE --n NX NY [NZ] [--periodic PX PY [PZ]] [--dyn ...] [--omega W] ...
  *          [--bouzidi M,...] [--lid M --ulid U] [--bounceback M,...] [--outside M,...]
  *          [--ivel M,... (--poiseuille UMAX | --uconst UX UY [UZ])] [--ivel-lid M] [--ipres M --rho R]
+ *          [--bbvel M]
  *          [--classify M] [--classify-only] [--force-mat M --force-every K] [--moments]
  *          [--no-pops] [--steps S] [--out PREFIX]
  *  The geo case reads the int32 materials of the core cells from FILE (x slowest, z fastest)
  *  and sets the lattice up through the reference's own setters: bulk dynamics on material 1,
  *  NoDynamics elsewhere; setBouzidiBoundary (q = 1/2) from fluid 1 towards the --bouzidi and
  *  --lid materials, setBouzidiVelocity (x velocity U) on the lid; BounceBack dynamics on the
- *  --bounceback materials; boundary::set<InterpolatedVelocity> / <InterpolatedPressure> on the
+ *  --bounceback materials, BounceBackVelocity with velocity (--ulid, 0, 0) on the --bbvel
+ *  material; boundary::set<InterpolatedVelocity> / <InterpolatedPressure> on the
  *  --ivel / --ivel-lid / --ipres materials with fluid 1 and outside {0, --outside...}, which
  *  classifies every cell with computeBoundaryTypeAndNormal itself.  The imposed velocity of an
  *  --ivel material is RectanglePoiseuille3D over it (one --ivel material) with the zero-velocity
@@ -135,7 +137,7 @@ struct Options {
   int periodicFlags[3] = {0, 0, 0};
   std::vector<int> bouzidiMats, bouncebackMats, outsideMats;
   std::vector<int> ivelMats;
-  int lidMat = -1, ivelLidMat = -1, ipresMat = -1, classifyMat = -1, forceMat = -1;
+  int lidMat = -1, ivelLidMat = -1, ipresMat = -1, classifyMat = -1, forceMat = -1, bbvelMat = -1;
   long forceEvery = 0;
   double poiseuille = -1.0, uconst[3] = {0, 0, 0}, rhoOut = 1.0;
   bool classifyOnly = false, moments = false, noPops = false;
@@ -227,6 +229,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--lid") o.lidMat = std::atoi(next());
     else if (a == "--ivel") o.ivelMats = parseList(next());
     else if (a == "--ivel-lid") o.ivelLidMat = std::atoi(next());
+    else if (a == "--bbvel") o.bbvelMat = std::atoi(next());
     else if (a == "--ipres") o.ipresMat = std::atoi(next());
     else if (a == "--poiseuille") o.poiseuille = std::atof(next());
     else if (a == "--uconst") { for (int d = 0; d < D; ++d) o.uconst[d] = std::atof(next()); }
@@ -357,6 +360,7 @@ int runGeo(const Options& o) {
       lat, geo.getMaterialIndicator(std::vector<int>(o.bouzidiMats)), geo.getMaterialIndicator({1}), nowhere);
   }
   for (int m : o.bouncebackMats) lat.template defineDynamics<BounceBack>(geo, m);
+  if (o.bbvelMat >= 0) lat.template defineDynamics<BounceBackVelocity>(geo, o.bbvelMat);
   std::vector<int> ivelAll = o.ivelMats;
   if (o.ivelLidMat >= 0) ivelAll.push_back(o.ivelLidMat);
   for (int m : ivelAll)
@@ -445,6 +449,12 @@ int runGeo(const Options& o) {
       } else if (mat[c] == o.ipresMat) {
         cell.defineRho(T(o.rhoOut));
         vals[4 * c] = double(T(o.rhoOut));
+      } else if (mat[c] == o.bbvelMat) {  // moving bounce-back wall: (--ulid, 0, 0), rho 1
+        Vector<T,D> uv(T(0));
+        uv[0] = T(o.ulid);
+        cell.defineU(uv.data());
+        vals[4 * c] = 1.0;
+        vals[4 * c + 1] = double(uv[0]);
       }
       ++c;
     });

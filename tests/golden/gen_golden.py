@@ -146,6 +146,12 @@ GEO = {
     "geo_cavity_d2q9_ivel_rnd_f64": ("d2q9_f64_nocse", (13, 11), ["--dyn", "trt", "--omega", "1.5", "--magic", "0.25",
                                                                   "--ivel", "2", "--ivel-lid", "3", "--ulid", "0.08",
                                                                   *RND, "--steps", "80"]),
+    # bounce-back walls and a lid of BounceBackVelocity (Revert + Nguyen-Ladd correction)
+    "geo_cavity_d2q9_bbvel_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--bounceback", "2",
+                                                               "--bbvel", "3", "--ulid", "0.1", "--steps", "150"]),
+    "geo_cavity_d3q19_bbvel_f64": ("d3q19_f64_nocse", (9, 8, 10), ["--dyn", "trt", "--omega", "1.5", "--magic", "0.25",
+                                                                   "--bounceback", "2", "--bbvel", "3", "--ulid",
+                                                                   "0.05", *RND, "--steps", "60"]),
     # a 3D cavity with InterpolatedVelocity on every wall: flat faces, external edges and corners
     "geo_cavity_d3q19_ivel_bgk_f64": ("d3q19_f64_nocse", (9, 8, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
                                                                       "--ivel-lid", "3", "--ulid", "0.05", *RND,

@@ -146,6 +146,12 @@ def case_setup(fx: dict) -> dict:
             walls.append((meta["ulid"], 0.0, 0.0))
         if solid:
             setup["links"] = bouzidi_links(q, core, mat3, 1, solid, walls if a["lid"] is not None else None, per)
+        for m in a["bbvel"]:
+            cd[mat == m] = 4
+        if a["bbvel"]:
+            cells = np.nonzero(np.isin(mat, a["bbvel"]))[0].astype(np.int64)
+            setup["bbv"] = {"cells": cells, "rho": np.ascontiguousarray(fx["vals"][cells, 0]),
+                            "u": np.ascontiguousarray(fx["vals"][cells, 1:4])}
         bc = fx["bclass"]
         cd[bc[:, 0]] = 3
         setup["cell_dyn"] = cd
@@ -175,6 +181,7 @@ def geo_args(meta: dict) -> dict:
     lid = value("--lid")
     return {"bouzidi": ints("--bouzidi"), "bounceback": ints("--bounceback"), "ivel": ints("--ivel"),
             "ivel_lid": ints("--ivel-lid"), "ipres": ints("--ipres"), "lid": int(lid) if lid else None,
+            "bbvel": ints("--bbvel"),
             "force_mat": ints("--force-mat")}
 
 
@@ -195,7 +202,8 @@ class _Case(C.Structure):
                 ("n_links", C.c_int64), ("link_cell", C.c_void_p), ("link_dir", C.c_void_p),
                 ("link_wall", C.c_void_p), ("n_fd", C.c_int64), ("fd_cell", C.c_void_p),
                 ("fd_kind", C.c_void_p), ("fd_dir", C.c_void_p), ("fd_orient", C.c_void_p),
-                ("fd_value", C.c_void_p), ("fd_type", C.c_void_p), ("fd_normal", C.c_void_p)]
+                ("fd_value", C.c_void_p), ("fd_type", C.c_void_p), ("fd_normal", C.c_void_p),
+                ("bbv_value", C.c_void_p)]
 
 
 _oracle = None
@@ -238,7 +246,7 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
     c.force = (C.c_double * 3)(*(list(setup["force"]) + [0.0] * 3)[:3])
     if setup["cell_dyn"] is not None:
         cd = setup["cell_dyn"]
-        m = np.where(cd == 1, 1, np.where(cd == 2, 4, np.where(cd == 3, 5, 0))).astype(np.int32)
+        m = np.select([cd == 1, cd == 2, cd == 3, cd == 4], [1, 4, 5, 6], 0).astype(np.int32)
         keep.append(m)
         c.material = m.ctypes.data
     if setup.get("fd") is not None:
@@ -253,6 +261,14 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
             keep += arrs
             c.n_fd = len(arrs[0])
             c.fd_cell, c.fd_kind, c.fd_dir, c.fd_orient, c.fd_value = (a.ctypes.data for a in arrs)
+    if setup.get("bbv") is not None:
+        n_all = int(np.prod(setup["core"]))
+        bv = np.zeros((n_all, 4))
+        b = setup["bbv"]
+        bv[b["cells"], 0] = b["rho"]
+        bv[b["cells"], 1:4] = b["u"]
+        keep.append(bv)
+        c.bbv_value = bv.ctypes.data
     if setup["links"] is not None:
         cells, dirs, wall = (np.ascontiguousarray(a) for a in setup["links"])
         keep += [cells, dirs, wall]
@@ -314,3 +330,13 @@ def fluid_mask(fx: dict) -> np.ndarray:
         m[fx["bclass"][:, 0]] = True
         return m
     return fx["mat"] == 1
+
+
+def counted_cells(fx: dict) -> int:
+    """Cells the lattice statistics count: the compared cells, plus the bounce-back cells with a
+    wall velocity (their populations arriving from beyond the domain are not defined, so they are
+    not compared, but they report {rho, |u|^2})."""
+    n = int(fluid_mask(fx).sum())
+    if fx["meta"]["case"] == "geo":
+        n += int(np.isin(fx["mat"], geo_args(fx["meta"])["bbvel"]).sum())
+    return n
