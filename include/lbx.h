@@ -465,6 +465,30 @@ int lbx_autotune(lbx_lattice lattice, int32_t steps, lbx_tune_entry* out, int32_
 int lbx_ensemble_autotune(lbx_ensemble ens, int32_t steps, lbx_tune_entry* out, int32_t capacity,
                           int32_t* n_out, void* stream);
 
+/* ---- test hook -------------------------------------------------------------------------
+ * No reference counterpart.  Off by default; for tests of the error paths: it makes a bounded
+ * wait of the library's own kernels run out, or an allocation fail, without any GPU fault, so
+ * that the status the caller reads can be checked.
+ *   LBX_TEST_NONE              normal operation (param ignored)
+ *   LBX_TEST_ENSEMBLE_BARRIER  the persistent ensemble kernel's block 0 leaves before the first
+ *                              grid barrier; the other blocks give up after `param` polls (0: the
+ *                              normal bound), set the error flag and return, and
+ *                              lbx_ensemble_statuses reports LBX_ERR_CUDA.  Applies to the runs
+ *                              an ensemble prepares after the call (a new step count).
+ *   LBX_TEST_BULK_COPY         the bulk-copy step kernel (launch variant 3) of block 0 leaves one
+ *                              copy of its first tile unrequested; its wait gives up after `param`
+ *                              polls, and lbx_get_statistics reports LBX_ERR_CUDA.
+ *   LBX_TEST_ALLOCATION        the next `param` population-column or ensemble-slab allocations
+ *                              fail as cudaMalloc does when memory is short (LBX_ERR_OUT_OF_MEMORY).
+ * Process-wide; not for concurrent use. */
+typedef enum {
+  LBX_TEST_NONE = 0,
+  LBX_TEST_ENSEMBLE_BARRIER = 1,
+  LBX_TEST_BULK_COPY = 2,
+  LBX_TEST_ALLOCATION = 3
+} lbx_test_fault_kind;
+int lbx_test_fault(int32_t kind, int32_t param);
+
 /* Mass/momentum sums for callers that cannot allocate device memory.  No counterpart in the
  * reference.  lbx_reduce(LBX_REDUCE_MASS_MOMENTUM) needs a lattice handle, whose creation
  * calls cudaMalloc; a host program whose device memory is all owned by its own pool or arena,

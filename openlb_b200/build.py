@@ -3,8 +3,8 @@
     python -m openlb_b200.build            # compile what changed
     python -m openlb_b200.build --force    # rebuild everything
 
-Each .cu under csrc/ is compiled by nvcc for sm_100a only (no PTX for other targets) into
-openlb_b200/_build/, then linked into openlb_b200/lib/liblbx.so.  The FP64 instantiation
+Each .cu under csrc/ is compiled by nvcc for sm_100a only (no PTX for other targets), and each
+host-only .cpp by g++, into openlb_b200/_build/, then linked into openlb_b200/lib/liblbx.so.  The FP64 instantiation
 units are compiled with -fmad=false: FP64 rounds like the reference's CPU build and the float
 kernels fuse only where the source says so, identically in every kernel variant.
 """
@@ -43,15 +43,26 @@ def nvcc() -> str:
 
 
 def _sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    """CUDA units (.cu, nvcc) and host-only units (.cpp, g++: the request server)."""
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
-def _headers() -> list[Path]:
-    return sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+def _headers(src: Path) -> list[Path]:
+    if src.suffix == ".cpp":
+        return sorted(INCLUDE.glob("*.h"))
+    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [INCLUDE / "lbx.h"]
 
 
 def _compile(src: Path, verbose: bool) -> Path:
     obj = BUILD / (src.stem + ".o")
+    if src.suffix == ".cpp":
+        gxx = shutil.which("g++") or "/usr/bin/g++"
+        cmd = [gxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-fPIC", "-pthread", "-I", str(INCLUDE), "-c", str(src),
+               "-o", str(obj)]
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"g++ failed for {src.name}:\n{proc.stdout}\n{proc.stderr}")
+        return obj
     cmd = [nvcc(), *ARCH, *COMMON, *PER_UNIT.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
@@ -67,10 +78,10 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     """Compile changed units and (re)link liblbx.so; returns the library path."""
     BUILD.mkdir(exist_ok=True)
     LIB.parent.mkdir(exist_ok=True)
-    newest_header = max((p.stat().st_mtime for p in _headers()), default=0.0)
     todo = []
     for src in _sources():
         obj = BUILD / (src.stem + ".o")
+        newest_header = max((p.stat().st_mtime for p in _headers(src)), default=0.0)
         if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header):
             todo.append(src)
     jobs = jobs or min(len(todo) or 1, os.cpu_count() or 4)
@@ -78,7 +89,8 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         list(pool.map(lambda s: _compile(s, verbose), todo))
     objs = [BUILD / (s.stem + ".o") for s in _sources()]
     if force or todo or not LIB.exists():
-        cmd = [nvcc(), *ARCH, "-shared", "--cudart", "static", "-o", str(LIB), *map(str, objs)]
+        cmd = [nvcc(), *ARCH, "-shared", "--cudart", "static", "-Xcompiler", "-pthread", "-o", str(LIB),
+               *map(str, objs)]
         proc = subprocess.run(cmd, capture_output=True, text=True)
         if proc.returncode != 0:
             raise RuntimeError(f"link failed:\n{proc.stdout}\n{proc.stderr}")

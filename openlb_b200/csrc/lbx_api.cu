@@ -15,6 +15,7 @@
 
 #include "../../include/lbx.h"
 #include "lbx_kernels.cuh"
+#include "lbx_test.h"
 
 using namespace lbx;
 
@@ -79,6 +80,18 @@ double weight_of(int q, int i) {
 
 namespace lbx {
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+// lbx_test_fault's setting (process-wide; for tests only)
+TestFault& test_fault() {
+  static TestFault f;
+  return f;
+}
+bool test_allocation_fails() {
+  TestFault& f = test_fault();
+  if (f.kind != LBX_TEST_ALLOCATION || f.param <= 0) return false;
+  --f.param;
+  return true;
+}
 // lbx_normals.cu
 int discrete_normals(int q, const int32_t core[3], const int32_t periodic[3], const int32_t* material,
                      int32_t boundary, int32_t n_fluid, const int32_t* fluid, int32_t n_outside,
@@ -212,6 +225,9 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.bbvCell = L->bbvCell;
   a.bbvValue = L->bbvValue;
   a.err = L->devErr;
+  const TestFault& tf = test_fault();
+  a.waitLimit = (tf.kind == LBX_TEST_BULK_COPY && tf.param > 0) ? tf.param : (1 << 22);
+  a.faultBulk = tf.kind == LBX_TEST_BULK_COPY ? 1 : 0;
   return a;
 }
 
@@ -258,7 +274,7 @@ void rotate_all(lbx_lattice_s* L) {
 // Threads along the fastest core axis, filled up to 256 per block; the rest of the block
 // spans the next axis.
 void block_shape_for(int nf, int cellsPerThread, int& bx, int& by) {
-  const int groups = (nf + cellsPerThread - 1) / cellsPerThread;
+  const int groups = lbx::k_cells_threads(nf, cellsPerThread);
   bx = 32;
   while (bx < groups && bx < 256) bx *= 2;
   by = 256 / bx;
@@ -296,8 +312,7 @@ int64_t step_blocks(const lbx_lattice_s* L) {
     }
     return (a.flatEnd - a.flatBase + bt - 1) / bt;
   }
-  const int k = L->kernel == 2 ? L->cellsPerThread : 1;
-  const int64_t groups = (nf + k - 1) / k;
+  const int64_t groups = L->kernel == 2 ? lbx::k_cells_threads(nf, L->cellsPerThread) : nf;
   return ((groups + L->blockX - 1) / L->blockX) * int64_t((nm + L->blockY - 1) / L->blockY) * ns;
 }
 
@@ -445,6 +460,7 @@ bool try_doubled_columns(lbx_lattice_s* L, size_t es) {
 // Allocate the Q population columns: doubled mappings when the VMM API is available, one plain
 // allocation otherwise.  Contents start at zero.
 cudaError_t alloc_columns(lbx_lattice_s* L) {
+  if (test_allocation_fails()) return cudaErrorMemoryAllocation;  // lbx_test_fault
   const size_t es = storage_bytes(L->storage);
   if (!std::getenv("LBX_PLAIN_COLUMNS") && try_doubled_columns(L, es)) {
     // zero the first copy of every column (the second aliases it)
@@ -798,6 +814,14 @@ extern "C" {
 const char* lbx_last_error(void) { return g_error.c_str(); }
 
 int lbx_abi_version(void) { return LBX_ABI_VERSION; }
+
+int lbx_test_fault(int32_t kind, int32_t param) {
+  if (kind < LBX_TEST_NONE || kind > LBX_TEST_ALLOCATION) return fail(LBX_ERR_INVALID, "unknown test fault");
+  if (param < 0) return fail(LBX_ERR_INVALID, "the parameter must be >= 0");
+  test_fault().kind = kind;
+  test_fault().param = param;
+  return LBX_OK;
+}
 
 int lbx_device_count(void) {
   int count = 0;
@@ -1562,7 +1586,7 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
   const int maxK = storage_bytes(L->storage) == 2 ? 4 : 2;
   for (int k = 1; k <= maxK; k *= 2)
     for (int bx = 32; bx <= 256; bx *= 2) {
-      if (bx > 32 && bx >= 2 * ((nf + k - 1) / k)) break;  // wider blocks only idle more threads
+      if (bx > 32 && bx >= 2 * lbx::k_cells_threads(nf, k)) break;  // wider blocks only idle more threads
       for (int threads = 256; threads >= 128; threads /= 2)
         if (threads / bx >= 1) cands.push_back({2, bx, threads / bx, k});
     }

@@ -34,6 +34,7 @@
 
 #include "../../include/lbx.h"
 #include "lbx_kernels.cuh"
+#include "lbx_test.h"
 
 namespace lbx {
 int set_error(int code, const std::string& msg);
@@ -78,6 +79,8 @@ struct EnsArgs {
   int maxLattices;
   int steps;
   int check;
+  long long spinLimit;     // polls of a grid-barrier wait before it gives up
+  int faultBlock;          // test hook (lbx_test_fault): this block leaves without arriving (-1: none)
 };
 
 template <typename S> struct CgLoad;
@@ -112,7 +115,7 @@ struct FastDiv {
 
 // Grid-wide barrier for a co-resident grid (cooperative launch).  Returns false when another
 // block gave up or this block waited longer than the bound; the kernel then returns.
-__device__ bool grid_barrier(unsigned* barrier, int* err) {
+__device__ bool grid_barrier(unsigned* barrier, int* err, long long spinLimit) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -127,7 +130,7 @@ __device__ bool grid_barrier(unsigned* barrier, int* err) {
       long long spins = 0;
       while (*gen == my) {
         __nanosleep(64);
-        if (++spins > (1ll << 26) || *reinterpret_cast<volatile int*>(err)) {
+        if (++spins > spinLimit || *reinterpret_cast<volatile int*>(err)) {
           atomicExch(err, 1);
           break;
         }
@@ -429,12 +432,13 @@ __global__ void __launch_bounds__(256, EnsOccupancy<Q, S, K>::blocks) k_ensemble
     const long long g = *reinterpret_cast<volatile long long*>(a.globalStep);
     const int par = int(g & 1);
     ensemble_tiles<Q, S, false, K>(a, par, *a.nTiles, scratch[threadIdx.x >> 5]);
-    if (!grid_barrier(a.barrier, a.err)) return;
+    if (int(blockIdx.x) == a.faultBlock) return;  // test hook: never arrives at the barrier
+    if (!grid_barrier(a.barrier, a.err, a.spinLimit)) return;
     if (blockIdx.x == 0) {
       ensemble_book<Q>(a, par);
       if (threadIdx.x == 0) *a.globalStep = g + 1;
     }
-    if (!grid_barrier(a.barrier, a.err)) return;
+    if (!grid_barrier(a.barrier, a.err, a.spinLimit)) return;
   }
 }
 
@@ -731,7 +735,8 @@ int lbx_ensemble_create(int32_t q, int32_t storage, int64_t slab_bytes, int32_t 
   E->slotCells.assign(size_t(max_lattices), 0);
   E->slotLid.assign(size_t(max_lattices), 0.0);
   kernels_for(q, storage, E->kern);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&E->slab), size_t(E->slabBytes));
+  cudaError_t e = lbx::test_allocation_fails() ? cudaErrorMemoryAllocation  // lbx_test_fault
+                                               : cudaMalloc(reinterpret_cast<void**>(&E->slab), size_t(E->slabBytes));
   if (e == cudaSuccess) e = cudaMalloc(&E->dLat, size_t(max_lattices) * sizeof(EnsLattice));
   if (e == cudaSuccess) e = cudaMemset(E->dLat, 0, size_t(max_lattices) * sizeof(EnsLattice));
   if (e == cudaSuccess) e = cudaMalloc(&E->dRange, size_t(max_lattices) * sizeof(int2));
@@ -1141,6 +1146,10 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
     a.maxLattices = E->maxLattices;
     a.steps = steps;
     a.check = E->check;
+    const lbx::TestFault& tf = lbx::test_fault();
+    const bool fault = tf.kind == LBX_TEST_ENSEMBLE_BARRIER;
+    a.spinLimit = (fault && tf.param > 0) ? tf.param : (1ll << 26);
+    a.faultBlock = fault ? 0 : -1;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(unsigned(E->grid));
     cfg.blockDim = dim3(unsigned(E->threads));
@@ -1159,6 +1168,8 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaMemsetAsync(E->dErr, 0, sizeof(int), cap);
     if (e == cudaSuccess) e = cudaMemsetAsync(E->dTileCounter, 0, sizeof(int), cap);
+    // a run that gave up leaves the barrier count behind: every run starts from a clear barrier
+    if (e == cudaSuccess) e = cudaMemsetAsync(E->dBarrier, 0, 2 * sizeof(unsigned), cap);
     if (E->mode == 0) {
       if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, launch_kernel(E), a);
     } else {
@@ -1180,6 +1191,7 @@ int lbx_ensemble_run(lbx_ensemble E, int32_t steps, void* stream) {
       cfg.stream = s;
       ENS_TRY(cudaMemsetAsync(E->dErr, 0, sizeof(int), s));
       ENS_TRY(cudaMemsetAsync(E->dTileCounter, 0, sizeof(int), s));
+      ENS_TRY(cudaMemsetAsync(E->dBarrier, 0, 2 * sizeof(unsigned), s));
       if (E->mode == 0) {
         ENS_TRY(cudaLaunchKernelEx(&cfg, launch_kernel(E), a));
       } else {

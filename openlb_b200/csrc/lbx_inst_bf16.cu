@@ -1,12 +1,9 @@
-// Reduced-precision storage (binary16 / bfloat16 deviations, float collision) instantiations.
+// bfloat16 deviation storage (float collision) instantiations.
 #define LBX_KERNEL_TU
 #include "lbx_kernels.cuh"
 
 namespace lbx {
-LBX_INSTANTIATE(9, __half)
 LBX_INSTANTIATE(9, __nv_bfloat16)
-LBX_INSTANTIATE(19, __half)
 LBX_INSTANTIATE(19, __nv_bfloat16)
-LBX_INSTANTIATE(27, __half)
 LBX_INSTANTIATE(27, __nv_bfloat16)
 }  // namespace lbx

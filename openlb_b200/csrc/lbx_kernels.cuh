@@ -17,6 +17,8 @@
 // step is a single launch.
 #pragma once
 
+#include <type_traits>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -518,8 +520,8 @@ __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t by
 }
 
 // Bounded wait on an mbarrier phase; false (and the error flag set) if it did not complete.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (int it = 0; it < (1 << 22); ++it) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, int limit) {
+  for (int it = 0; it < limit; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if (it > 64) __nanosleep(64);
   }
@@ -531,7 +533,7 @@ template <int Q, typename S, int DYN>
 __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS) k_collide_stream_bulk(
     S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t base, int64_t nFlat, int64_t nTiles,
     CollisionParams<typename Storage<S>::R> p, const uint8_t* __restrict__ cellDyn, double* __restrict__ statPart,
-    int* __restrict__ err, FlatDiv dv) {
+    int* __restrict__ err, FlatDiv dv, int waitLimit, int faultSkip) {
   using R = typename Storage<S>::R;
   using C = BulkCfg<Q, S>;
   constexpr int ES = C::ES, BT = C::BT, NT = C::THREADS, VE = 16 / ES;
@@ -567,6 +569,9 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
     for (int i = 0; i < Q; ++i) {
       const int64_t first = (t0 + sh.s[i]) * ES;
       const int64_t a0 = first & ~int64_t(15), a1 = (first + cells * ES + 15) & ~int64_t(15);
+      // test hook (lbx_test_fault): block 0 leaves its first tile's column 0 unrequested, so that
+      // its bounded wait runs out
+      if (faultSkip && blockIdx.x == 0 && tile == int64_t(blockIdx.x) && i == 0) continue;
       bulk_g2s(stage + i * C::COL_BYTES, reinterpret_cast<const unsigned char*>(pop + i * g.stride) + a0,
                uint32_t(a1 - a0), &bar[st]);
     }
@@ -584,7 +589,7 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
       asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");  // its bulk stores have read it
       if (tile + stride < nTiles) issue(tile + stride, st ^ 1);
     }
-    if (!mbar_wait_bounded(&bar[st], uint32_t((k >> 1) & 1), err)) sAbort = 1;
+    if (!mbar_wait_bounded(&bar[st], uint32_t((k >> 1) & 1), err, waitLimit)) sAbort = 1;
     else if (tid == 0) ++waited[st];
     __syncthreads();
     if (sAbort) break;
@@ -653,17 +658,17 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
     // after an abort: let the loads still in flight land before the block exits (bounded)
     for (int st = 0; st < 2; ++st)
       while (waited[st] < issued[st]) {
-        mbar_wait_bounded(&bar[st], uint32_t(waited[st] & 1), err);
+        mbar_wait_bounded(&bar[st], uint32_t(waited[st] & 1), err, waitLimit);
         ++waited[st];
       }
   }
   if (statPart) block_partial(accRho, accUsq, accMax, accCount, statPart);
 }
 
-// ---- fused collide + PS stream, K consecutive cells per thread --------------------------
-// One thread owns K consecutive cells along the fastest core axis (z in 3D, y in 2D).  For
-// every population it forms ONE wrapped column index; the K values are then reached with
-// constant offsets (a separate per-element wrap is only needed in the rare group that
+// ---- fused collide + PS stream, K cells per thread ---------------------------------------
+// One thread owns K cells a warp (32 cells) apart along the fastest core axis (z in 3D, y in
+// 2D).  For every population it forms ONE wrapped column index; the K values are then reached
+// with constant offsets (a separate per-element wrap is only needed in the rare group that
 // straddles the cyclic end of the column).  All K*Q loads are issued before the first
 // collision.  Periodic faces are handled by k_periodic_halo after this kernel, so the hot
 // kernel carries no face logic.  Column indices are 32-bit: the column period is < 2^31.
@@ -701,7 +706,7 @@ template <> struct StepOccupancy<19, __nv_bfloat16, 4> { static constexpr int bl
 template <> struct StepOccupancy<9, __half, 4> { static constexpr int blocks = 2; };
 template <> struct StepOccupancy<9, __nv_bfloat16, 4> { static constexpr int blocks = 2; };
 
-template <int Q, typename S, int DYN, int K, bool DOUBLED>
+template <int Q, typename S, int DYN, int K, bool DOUBLED, bool MAPPED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
@@ -710,33 +715,50 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const uint32_t P = uint32_t(g.n);
-  int x, y, z0, nvalid;
+  // The K cells of a thread lie a warp apart along the fastest axis (z0, z0 + 32, ...): each
+  // warp-wide load or store then covers one contiguous run of 32 cells, which a 16-bit column
+  // moves in two full sectors, instead of every instruction touching twice the sectors it uses.
+  constexpr int W = 32;
+  int x, y, z0, nvalid;  // nvalid: cells k < nvalid of this thread lie in the core
   bool inside;
   {
     const int gi = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y * blockDim.y + threadIdx.y;
+    z0 = (gi / W) * (W * K) + gi % W;
+    const int nf = D::d == 3 ? g.nz : g.ny;
     if constexpr (D::d == 3) {
-      z0 = gi * K; y = m; x = blockIdx.z;
+      y = m; x = blockIdx.z;
       inside = z0 < g.nz && y < g.ny;
-      nvalid = g.nz - z0;
     } else {
-      z0 = gi * K; x = m; y = 0;
+      x = m; y = 0;
       inside = z0 < g.ny && x < g.nx;
-      nvalid = g.ny - z0;
     }
+    nvalid = (nf - z0 + W - 1) / W;
   }
   double accRho = 0.0, accUsq = 0.0, accMax = 0.0;
   unsigned accCount = 0;
   if (inside) {
-    // 3D: (x+1)*sx + (y+1)*sy + z0 + 1; 2D: the fast axis is y (sy = 1), z absent
+    // 3D: (x+1)*sx + (y+1)*sy + z0 + 1; 2D: the fast axis is y (sy = 1), z absent; cell k of
+    // the thread is n0 + W k
     const uint32_t n0 = (D::d == 3) ? uint32_t((x + 1) * g.sx + (y + 1) * g.sy + z0 + 1)
                                     : uint32_t((x + 1) * g.sx + z0 + 1);
     // the cell kinds first: a cell without dynamics is neither loaded nor stored, so the solid
     // part of a porous medium costs no population traffic (boundary cells of kinds 3 and 4 are
     // loaded and stored by their own kernels)
+    // (MAPPED: the lattice has a cell map; without one every core cell is bulk and the kernel
+    // compiles to plain loads)
     uint8_t kinds[K];
+    bool act[K];  // this kernel loads, collides and stores cell k
 #pragma unroll
-    for (int k = 0; k < K; ++k) kinds[k] = (k < nvalid) ? (cellDyn ? cellDyn[n0 + k] : uint8_t(1)) : uint8_t(0);
+    for (int k = 0; k < K; ++k) {
+      if constexpr (MAPPED) {
+        kinds[k] = (k < nvalid) ? cellDyn[n0 + W * k] : uint8_t(0);
+        act[k] = stepped_kind(kinds[k]);
+      } else {
+        kinds[k] = (k < nvalid) ? uint8_t(1) : uint8_t(0);
+        act[k] = k < nvalid;
+      }
+    }
     // raw loads next, all in straight-line code (the wrap is a select, not a branch), so every
     // load of the thread is in flight before the first value is used
     S raw[K][Q];
@@ -745,22 +767,22 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       if constexpr (DOUBLED) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (stepped_kind(kinds[k])) raw[k][I] = col[n0 + k];
+          if (act[k]) raw[k][I] = col[n0 + W * k];
       } else {
         uint32_t idx = n0 + cols.s[I];
         idx = idx >= P ? idx - P : idx;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          uint32_t ik = idx + k;
+          uint32_t ik = idx + W * k;
           if (k > 0) ik = ik >= P ? ik - P : ik;
-          if (stepped_kind(kinds[k])) raw[k][I] = col[ik];
+          if (act[k]) raw[k][I] = col[ik];
         }
       }
     });
     R f[K][Q];
 #pragma unroll
     for (int k = 0; k < K; ++k)
-      static_for<Q>([&](auto I) { f[k][I] = stepped_kind(kinds[k]) ? Storage<S>::load(&raw[k][I]) : R(0); });
+      static_for<Q>([&](auto I) { f[k][I] = act[k] ? Storage<S>::load(&raw[k][I]) : R(0); });
     // pairs of bulk BGK cells of a 16-bit form: one packed (f32x2) collision per pair, the same
     // bits as two scalar ones.  The 16-bit forms are limited by instruction issue, where the
     // packed form halves the collision's arithmetic; the FP32 form waits on HBM, and there the
@@ -823,9 +845,9 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         // no dynamics: nothing to carry across (see linkMask); boundary cells: their own kernels
-        if (!stepped_kind(kinds[k])) continue;
-        const int cz0 = D::d == 3 ? z0 + k : 0;
-        const int cy0 = D::d == 3 ? y : z0 + k;
+        if (!act[k]) continue;
+        const int cz0 = D::d == 3 ? z0 + W * k : 0;
+        const int cy0 = D::d == 3 ? y : z0 + W * k;
         static_for<Q>([&](auto I) {
           constexpr int cx = D::C[I][0], cy = D::C[I][1], cz = D::C[I][2];
           int tx = x + cx, ty = cy0 + cy, tz = cz0 + cz;
@@ -844,8 +866,8 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     } else if (g.pmask & (D::d == 3 ? 4 : 2)) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
-        const int fk = z0 + k;
-        if (!stepped_kind(kinds[k]) || (fk != 0 && fk != nf - 1)) continue;
+        const int fk = z0 + W * k;
+        if (!act[k] || (fk != 0 && fk != nf - 1)) continue;
         static_for<Q>([&](auto I) {
           constexpr int cf = D::d == 3 ? D::C[I][2] : D::C[I][1];
           if constexpr (cf != 0) {
@@ -853,7 +875,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
               constexpr int cx = D::C[I][0], cy = D::C[I][1];
               bool inside = x + cx >= 0 && x + cx < g.nx;
               if constexpr (D::d == 3) inside = inside && y + cy >= 0 && y + cy < g.ny;
-              if (inside) ghost_store(I, k, n0 + k - uint32_t(cf * nf));
+              if (inside) ghost_store(I, k, n0 + W * k - uint32_t(cf * nf));
             }
           }
         });
@@ -865,17 +887,17 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
     // opposite population, which the rotation of this step carries into f_opp(k)(x_b) -- the value
     // the link kernel would copy there after the stream.  The solid cell has no dynamics, so no
     // other thread writes that slot (cells without dynamics make no stores, ghost ones included).
-    if (linkMask) {
+    if (MAPPED && linkMask) {
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (kinds[k] != kCellBulkLinked) continue;
-        const uint32_t mk = linkMask[n0 + k];
+        const uint32_t mk = linkMask[n0 + W * k];
         static_for<Q>([&](auto I) {
           if ((mk >> int(I)) & 1u) {
             constexpr int O = D::OPP[I];
             const int32_t off = int32_t(D::C[I][0] * g.sx + D::C[I][1] * g.sy + D::C[I][2]);
             S* col = static_cast<S*>(cols.base[O]);
-            const uint32_t slot = n0 + k + uint32_t(off);
+            const uint32_t slot = n0 + W * k + uint32_t(off);
             if constexpr (DOUBLED) {
               Storage<S>::store(col + slot, f[k][I]);
             } else {
@@ -892,15 +914,15 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       if constexpr (DOUBLED) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (stepped_kind(kinds[k])) Storage<S>::store(col + n0 + k, f[k][I]);
+          if (act[k]) Storage<S>::store(col + n0 + W * k, f[k][I]);
       } else {
         uint32_t idx = n0 + cols.s[I];
         idx = idx >= P ? idx - P : idx;
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          uint32_t ik = idx + k;
+          uint32_t ik = idx + W * k;
           if (k > 0) ik = ik >= P ? ik - P : ik;
-          if (stepped_kind(kinds[k])) Storage<S>::store(col + ik, f[k][I]);
+          if (act[k]) Storage<S>::store(col + ik, f[k][I]);
         }
       }
     });
@@ -1662,7 +1684,13 @@ struct LaunchArgs {
   const uint32_t* bbvCell;   // their padded indices
   const double* bbvValue;    // {rho, u} per cell
   int* err;                  // device flag: a bounded wait of a step kernel gave up
+  int waitLimit;             // polls of a bounded wait before it gives up
+  int faultBulk;             // test hook: the bulk-copy kernel leaves one copy unrequested
 };
+
+// Threads along the fastest axis of the K-cells step kernel: whole warps of 32 threads, each
+// thread K cells a warp apart (k_collide_stream_groups).
+inline int k_cells_threads(int nf, int K) { return K == 1 ? nf : (nf + 32 * K - 1) / (32 * K) * 32; }
 
 // Blocks of 256 threads the boundary-cell collision adds to a step's statistics partials.
 inline int64_t fd_blocks(int64_t nFd) { return (nFd + 255) / 256; }
@@ -1775,7 +1803,8 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     FlatDiv::make(uint32_t(g.sx), dv.mx, dv.lx);
     FlatDiv::make(uint32_t(g.sy), dv.my, dv.ly);
     k_collide_stream_bulk<Q, S, DYN><<<unsigned(grid), BC::THREADS, BC::SMEM, stream>>>(
-        pop, g, sh, a.flatBase, a.flatEnd, tiles, p, a.cellDyn, a.stats ? a.statPart : nullptr, a.err, dv);
+        pop, g, sh, a.flatBase, a.flatEnd, tiles, p, a.cellDyn, a.stats ? a.statPart : nullptr, a.err, dv,
+        a.waitLimit, a.faultBulk);
     nblocks = grid;
   } else if (a.kernel == 1) {
     dim3 block(a.blockX, a.blockY, 1);
@@ -1793,27 +1822,35 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     }
     const int K = a.cellsPerThread;
     const int nf = Desc<Q>::d == 3 ? g.nz : g.ny;
-    const int groups = (nf + K - 1) / K;
+    const int groups = k_cells_threads(nf, K);
     dim3 block(a.blockX, a.blockY, 1);
     dim3 grid;
     if (Desc<Q>::d == 3) grid = dim3((groups + a.blockX - 1) / a.blockX, (g.ny + a.blockY - 1) / a.blockY, g.nx);
     else grid = dim3((groups + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
-    const int sel = K * 2 + (a.doubled ? 1 : 0);
     nblocks = int64_t(grid.x) * grid.y * grid.z;
     if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
     double* part = a.stats ? a.statPart : nullptr;
-    switch (sel) {
-    case 2: k_collide_stream_groups<Q, S, DYN, 1, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
-    case 3: k_collide_stream_groups<Q, S, DYN, 1, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
-    case 4: k_collide_stream_groups<Q, S, DYN, 2, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
-    case 5: k_collide_stream_groups<Q, S, DYN, 2, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part); break;
-    case 8:
-    case 9:
+    auto go = [&](auto kk, auto doubled, auto mapped) {
+      k_collide_stream_groups<Q, S, DYN, decltype(kk)::value, decltype(doubled)::value, decltype(mapped)::value>
+          <<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part);
+    };
+    auto go_k = [&](auto kk) {
+      if (a.doubled) {
+        if (a.cellDyn) go(kk, std::true_type{}, std::true_type{});
+        else go(kk, std::true_type{}, std::false_type{});
+      } else {
+        if (a.cellDyn) go(kk, std::false_type{}, std::true_type{});
+        else go(kk, std::false_type{}, std::false_type{});
+      }
+    };
+    switch (K) {
+    case 1: go_k(std::integral_constant<int, 1>{}); break;
+    case 2: go_k(std::integral_constant<int, 2>{}); break;
+    case 4:
       // four cells per thread: the 16-bit forms only (their per-cell arithmetic, not HBM, is
       // what limits them; four cells share one thread's index and address work)
       if constexpr (sizeof(S) == 2) {
-        if (sel == 8) k_collide_stream_groups<Q, S, DYN, 4, false><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part);
-        else k_collide_stream_groups<Q, S, DYN, 4, true><<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part);
+        go_k(std::integral_constant<int, 4>{});
         break;
       }
       return cudaErrorInvalidValue;

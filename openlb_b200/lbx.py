@@ -69,6 +69,39 @@ def _tune(fn, handle, steps: int, stream, where: str) -> list[dict]:
 
 
 SLOT_FREE, SLOT_RUNNING, SLOT_CONVERGED, SLOT_MAX_STEPS, SLOT_DIVERGED = 0, 1, 2, 3, 4
+SERVER_REJECTED, SERVER_CANCELLED = 5, 6
+
+
+class ServerRequest(C.Structure):
+    _fields_ = [("id", C.c_int64), ("arrival", C.c_double), ("request", EnsembleRequest)]
+
+
+class ServerRecord(C.Structure):
+    _fields_ = [("id", C.c_int64), ("cells", C.c_int64), ("arrival", C.c_double), ("admitted", C.c_double),
+                ("finished", C.c_double), ("steps", C.c_int64), ("state", C.c_int32), ("slot", C.c_int32),
+                ("residual", C.c_double)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("min_chunk", C.c_int32), ("max_chunk", C.c_int32), ("realtime", C.c_int32), ("pad", C.c_int32)]
+
+
+ENGINE_ADMIT = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(EnsembleRequest), C.POINTER(C.c_int32))
+ENGINE_RUN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int32)
+ENGINE_STATUSES = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(EnsembleStatus), C.c_int32)
+ENGINE_RETIRE = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int32)
+FINISH_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(ServerRecord))
+
+
+class ServerEngine(C.Structure):
+    _fields_ = [("admit", ENGINE_ADMIT), ("run", ENGINE_RUN), ("statuses", ENGINE_STATUSES),
+                ("retire", ENGINE_RETIRE), ("slots", C.c_int32), ("pad", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "pending", "waiting", "running", "finished", "runs", "steps",
+                                         "short_runs", "long_runs")] + [("busy_seconds", C.c_double),
+                                                                         ("clock", C.c_double)]
 
 
 def _load() -> C.CDLL:
@@ -128,6 +161,17 @@ def _load() -> C.CDLL:
         "lbx_ensemble_retire": ([VP, I32], C.c_int),
         "lbx_ensemble_set_config": ([VP, I32, I32, I32], C.c_int),
         "lbx_get_kernel_timing": ([VP, P(D)], C.c_int),
+        "lbx_server_create": ([VP, I32, P(ServerConfig), VP, P(VP)], C.c_int),
+        "lbx_server_create_with_engine": ([P(ServerEngine), VP, P(ServerConfig), P(VP)], C.c_int),
+        "lbx_server_set_finish_callback": ([VP, FINISH_FN, VP], C.c_int),
+        "lbx_server_submit": ([VP, P(ServerRequest), I32], C.c_int),
+        "lbx_server_start": ([VP], C.c_int),
+        "lbx_server_close": ([VP], C.c_int),
+        "lbx_server_cancel": ([VP, I64], C.c_int),
+        "lbx_server_wait": ([VP, D, P(I32)], C.c_int),
+        "lbx_server_records": ([VP, P(ServerRecord), I32, P(I32)], C.c_int),
+        "lbx_server_get_stats": ([VP, P(ServerStats)], C.c_int),
+        "lbx_server_destroy": ([VP], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -516,9 +560,13 @@ class Ensemble:
         self.close()
 
     def footprint(self, req: EnsembleRequest) -> int:
+        return Ensemble.footprint_of(self.q, self.storage, req)
+
+    @staticmethod
+    def footprint_of(q: int, storage: str, req: EnsembleRequest) -> int:
+        """Slab bytes a request needs (no ensemble or device needed)."""
         b = C.c_int64()
-        check(lib.lbx_ensemble_footprint(self.q, STORAGE[self.storage], C.byref(req), C.byref(b)),
-              "lbx_ensemble_footprint")
+        check(lib.lbx_ensemble_footprint(q, STORAGE[storage], C.byref(req), C.byref(b)), "lbx_ensemble_footprint")
         return b.value
 
     def admit(self, req: EnsembleRequest) -> int | None:
@@ -583,3 +631,84 @@ class Ensemble:
 
     def set_config(self, threads: int = 256, blocks_per_sm: int = 0, check_interval: int = 100) -> None:
         check(lib.lbx_ensemble_set_config(self._h, threads, blocks_per_sm, check_interval), "lbx_ensemble_set_config")
+
+
+class Server:
+    """The native continuous-batching request loop (lbx_server_*): admission by slab footprint,
+    one ensemble run of an adaptive chunk of steps per round, retirement on convergence, all on a
+    host thread of the library's own.  `engine` is an Ensemble, or a ServerEngine with its
+    context for a caller-supplied engine."""
+
+    def __init__(self, engine, min_chunk: int = 100, max_chunk: int = 500, realtime: bool = True,
+                 stream=None, on_finish=None, ctx=None):
+        cfg = ServerConfig(min_chunk, max_chunk, 1 if realtime else 0, 0)
+        h = C.c_void_p()
+        if isinstance(engine, Ensemble):
+            check(lib.lbx_server_create(engine._h, engine.max_lattices, C.byref(cfg), _stream_ptr(stream),
+                                        C.byref(h)), "lbx_server_create")
+        else:
+            check(lib.lbx_server_create_with_engine(C.byref(engine), ctx, C.byref(cfg), C.byref(h)),
+                  "lbx_server_create_with_engine")
+        self._h = h
+        self._engine = engine  # kept alive with the callbacks it holds
+        self._cb = None
+        if on_finish is not None:
+            self._cb = FINISH_FN(lambda _user, rec: on_finish(rec.contents))
+            check(lib.lbx_server_set_finish_callback(self._h, self._cb, None), "lbx_server_set_finish_callback")
+
+    def submit(self, requests) -> None:
+        """requests: iterable of (id, arrival seconds or -1 for now, EnsembleRequest)."""
+        items = list(requests)
+        arr = (ServerRequest * max(len(items), 1))()
+        for i, (rid, arrival, req) in enumerate(items):
+            arr[i].id = rid
+            arr[i].arrival = arrival
+            arr[i].request = req
+        check(lib.lbx_server_submit(self._h, arr, len(items)), "lbx_server_submit")
+
+    def start(self) -> None:
+        check(lib.lbx_server_start(self._h), "lbx_server_start")
+
+    def close(self) -> None:
+        check(lib.lbx_server_close(self._h), "lbx_server_close")
+
+    def cancel(self, rid: int) -> None:
+        check(lib.lbx_server_cancel(self._h, rid), "lbx_server_cancel")
+
+    def wait(self, timeout: float = -1.0) -> bool:
+        """True once the loop has ended (raises the error that stopped it, if any)."""
+        fin = C.c_int32(0)
+        check(lib.lbx_server_wait(self._h, timeout, C.byref(fin)), "lbx_server_wait")
+        return bool(fin.value)
+
+    def records(self, capacity: int = 4096) -> list[dict]:
+        out = []
+        arr = (ServerRecord * capacity)()
+        while True:
+            n = C.c_int32()
+            check(lib.lbx_server_records(self._h, arr, capacity, C.byref(n)), "lbx_server_records")
+            out += [{k: getattr(arr[i], k) for k, _ in ServerRecord._fields_} for i in range(n.value)]
+            if n.value < capacity:
+                return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib.lbx_server_get_stats(self._h, C.byref(st)), "lbx_server_get_stats")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.lbx_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()

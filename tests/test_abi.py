@@ -11,17 +11,18 @@ import pytest
 import lbcases as L
 from openlb_b200 import lbx
 
-HEADER = Path(__file__).resolve().parent.parent / "include" / "lbx.h"
+HEADERS = sorted((Path(__file__).resolve().parent.parent / "include").glob("*.h"))
 
 
 def declared_functions() -> list[str]:
-    text = HEADER.read_text()
+    text = "\n".join(h.read_text() for h in HEADERS)
     return sorted(set(re.findall(r"^(?:int|const char\*)\s+(lbx_\w+)\s*\(", text, flags=re.M)))
 
 
 def test_every_declared_symbol_is_exported():
     names = declared_functions()
     assert len(names) >= 18
+    assert "lbx_server_create" in names and "lbx_mass_momentum_noalloc" in names
     lib = ctypes.CDLL(str(lbx.LIB_PATH))
     for n in names:
         assert hasattr(lib, n), n

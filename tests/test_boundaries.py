@@ -136,6 +136,9 @@ def build_from_materials(fx, storage):
             wall = np.zeros((len(solid), 3))
             wall[-1, 0] = meta["ulid"]
         lat.set_bouzidi_boundary(mat, 1, solid, wall)
+    if a["bbvel"]:
+        cells = np.nonzero(np.isin(mat, a["bbvel"]))[0]
+        lat.set_bounce_back_velocity(cells, fx["vals"][cells, 0], fx["vals"][cells, 1:4])
     for m in a["ivel"] + a["ivel_lid"]:
         lat.set_interpolated_boundary(lbx.FD_VELOCITY, mat, m, fx["vals"])
     for m in a["ipres"]:
