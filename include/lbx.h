@@ -347,8 +347,12 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
  * counterpart; the reference's CUDA platform launches fixed 32-thread blocks,
  * gpu/cuda/operator.hh:425-441).  variant 0: pipelined shared-memory tiles of 256 cells;
  * variant 1: one cell per thread in (block_x, block_y) blocks; variant 2 (default):
- * cells_per_thread (1 or 2) consecutive cells per thread in (block_x, block_y) blocks,
- * block_x along the fastest axis. */
+ * cells_per_thread (1 or 2; 4 for 16-bit storage) cells a warp apart per thread in
+ * (block_x, block_y) blocks, block_x along the fastest axis; variant 3: tiles moved by TMA bulk
+ * copies, two stages per block; variant 4: tiles moved by TMA bulk copies through a ring of
+ * four stages, one producer warp and eight consumer warps per block (block_x, block_y and
+ * cells_per_thread are ignored by 0, 3 and 4).  Variants 3 and 4 need the doubled column
+ * layout.  Every variant computes identical populations. */
 int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread);
 

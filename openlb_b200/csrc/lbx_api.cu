@@ -299,11 +299,12 @@ int64_t step_blocks(const lbx_lattice_s* L) {
     const LaunchArgs a = args_of(L);
     return (a.flatEnd - a.flatBase + TILE - 1) / TILE;
   }
-  if (L->kernel == 3) {  // at most one persistent block per tile (the grid is capped by residency)
+  if (L->kernel == 3 || L->kernel == 4) {  // at most one persistent block per tile (the grid is capped by residency)
     const LaunchArgs a = args_of(L);
     int64_t bt = 0;
     switch (L->q * 4 + L->storage) {
-#define LBX_BT(QQ, SS, ST) case QQ * 4 + ST: bt = BulkCfg<QQ, SS>::BT; break;
+#define LBX_BT(QQ, SS, ST) \
+  case QQ * 4 + ST: bt = L->kernel == 3 ? BulkCfg<QQ, SS>::BT : WsCfg<QQ, SS>::BT; break;
       LBX_BT(9, double, LBX_F64) LBX_BT(9, float, LBX_F32) LBX_BT(9, __half, LBX_F16DEV) LBX_BT(9, __nv_bfloat16, LBX_BF16DEV)
       LBX_BT(19, double, LBX_F64) LBX_BT(19, float, LBX_F32) LBX_BT(19, __half, LBX_F16DEV) LBX_BT(19, __nv_bfloat16, LBX_BF16DEV)
       LBX_BT(27, double, LBX_F64) LBX_BT(27, float, LBX_F32) LBX_BT(27, __half, LBX_F16DEV) LBX_BT(27, __nv_bfloat16, LBX_BF16DEV)
@@ -1553,9 +1554,9 @@ int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
 int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
-  if (variant < 0 || variant > 3) return fail(LBX_ERR_INVALID, "variant must be 0, 1, 2 or 3");
-  if (variant == 3 && (!L->doubled || L->period >= (int64_t(1) << 31)))
-    return fail(LBX_ERR_UNSUPPORTED, "variant 3 (bulk copies) needs the doubled column mapping and fewer than 2^31 cells");
+  if (variant < 0 || variant > 4) return fail(LBX_ERR_INVALID, "variant must be 0, 1, 2, 3 or 4");
+  if ((variant == 3 || variant == 4) && (!L->doubled || L->period >= (int64_t(1) << 31)))
+    return fail(LBX_ERR_UNSUPPORTED, "variants 3 and 4 (bulk copies) need the doubled column mapping and fewer than 2^31 cells");
   if (variant == 2 && L->period >= (int64_t(1) << 31))
     return fail(LBX_ERR_UNSUPPORTED, "variant 2 needs a column period below 2^31 cells");
   if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2 &&
@@ -1595,7 +1596,10 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
     block_shape_for(nf, 1, bx, by);
     cands.push_back({1, bx, by, 1});
     cands.push_back({0, 256, 1, 1});
-    if (L->doubled && L->period < (int64_t(1) << 31)) cands.push_back({3, 256, 1, 1});
+    if (L->doubled && L->period < (int64_t(1) << 31)) {
+      cands.push_back({3, 256, 1, 1});
+      cands.push_back({4, 256, 1, 1});
+    }
   }
   if (n_out) *n_out = int32_t(cands.size());
   const Cand keep{L->kernel, L->blockX, L->blockY, L->cellsPerThread};

@@ -665,6 +665,231 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
   if (statPart) block_partial(accRho, accUsq, accMax, accCount, statPart);
 }
 
+// ---- fused collide + PS stream, warp-specialised bulk-copy pipeline -----------------------
+// Variant 4.  The tile scheme of variant 3 (BT consecutive flat cells; per population one
+// contiguous run, brought in by one 1D bulk copy), rebuilt so that no block-wide barrier sits on
+// the path of a tile:
+//   - warp 0 is the producer: its lane 0 issues the bulk loads of a tile into a ring of NS
+//     stages (completion: the stage's `full` mbarrier, by bytes), and, once the consumers have
+//     released a stage (its `empty` mbarrier, one arrival per consumer warp), the bulk stores of
+//     the 16-byte-aligned interior of every column's run; the stage is loaded again when those
+//     stores have read it (the store group one behind the newest), so NS - 1 tiles are in flight
+//     ahead of the one being computed;
+//   - warps 1..8 are consumers: each waits for its tile's `full` phase, collides its cells in
+//     shared memory (16-bit BGK pairs with the packed two-cell collision), writes the unaligned
+//     head and tail elements of each run straight to their slots, makes its shared-memory
+//     writes visible to the bulk-copy proxy and arrives on the stage's `empty` barrier.
+// A fast consumer warp runs ahead into the next loaded stage instead of waiting for the block.
+// Ghost and spare cells of a tile go back unchanged; the periodic overlap copy runs afterwards
+// (k_periodic_halo), as for variant 3.  Every wait is bounded: a wait that gives up sets the
+// error flag and the abort word, and every warp leaves its loop; the producer then waits
+// (bounded) for its loads still in flight and its stores before the block exits.
+template <int Q, typename S> struct WsCfg {
+  static constexpr int ES = int(sizeof(S));
+  static constexpr int BT = (20480 / (Q * ES)) / 64 * 64;  // cells per tile: ~20 KB of populations
+  static constexpr int COL_BYTES = BT * ES + 32;           // one column's run + alignment slack
+  static constexpr int STAGE_BYTES = Q * COL_BYTES;
+  static constexpr int NS = 4;                              // stages in the ring
+  static constexpr int CONSUMER_WARPS = 8;
+  static constexpr int THREADS = 32 * (1 + CONSUMER_WARPS);
+  static constexpr int SMEM = NS * STAGE_BYTES + 2 * NS * 8;  // stages, then the full and empty mbarriers
+  static constexpr int BLOCKS = 2;                          // resident blocks per SM
+  static_assert(BT >= 64 && COL_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "tile layout");
+  static_assert(BT <= 4095, "packed run bounds hold 12 bits");
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+
+template <int Q, typename S, int DYN>
+__global__ void __launch_bounds__(WsCfg<Q, S>::THREADS, WsCfg<Q, S>::BLOCKS) k_collide_stream_ws(
+    S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t base, int64_t nFlat, int64_t nTiles,
+    CollisionParams<typename Storage<S>::R> p, const uint8_t* __restrict__ cellDyn, double* __restrict__ statPart,
+    int* __restrict__ err, FlatDiv dv, int waitLimit) {
+  using R = typename Storage<S>::R;
+  using C = WsCfg<Q, S>;
+  constexpr int ES = C::ES, BT = C::BT, NS = C::NS;
+  constexpr int COL = C::COL_BYTES / ES;      // elements per column buffer
+  constexpr int NCT = 32 * C::CONSUMER_WARPS;  // consumer threads
+  constexpr bool PACKED = sizeof(R) == 4 && sizeof(S) == 2 && DYN == DYN_BGK;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * C::STAGE_BYTES);
+  uint64_t* empty = full + NS;
+  // per stage and column: bits 0-3 the elements from the aligned run start to the tile's first
+  // cell, bits 4-15 the cells of the unaligned head, bits 16-27 the first cell of the tail
+  __shared__ uint32_t sRun[NS][Q];
+  __shared__ volatile int sAbort;
+  const int warp = int(threadIdx.x) >> 5, lane = int(threadIdx.x) & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NS; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], C::CONSUMER_WARPS);
+    }
+    sAbort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const int64_t grid = gridDim.x;
+  const int64_t nloc = int64_t(blockIdx.x) < nTiles ? (nTiles - int64_t(blockIdx.x) + grid - 1) / grid : 0;
+  auto tile_first = [&](int64_t k) { return base + (int64_t(blockIdx.x) + k * grid) * BT; };
+  auto tile_cells = [&](int64_t t0) { return int((t0 + BT <= nFlat) ? BT : nFlat - t0); };
+  double accRho = 0.0, accUsq = 0.0, accMax = 0.0, accCount = 0.0;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int64_t issued = 0;
+      auto issue = [&](int64_t k) {
+        const int s = int(k % NS);
+        const int64_t t0 = tile_first(k);
+        const int cells = tile_cells(t0);
+        uint32_t total = 0;
+        for (int i = 0; i < Q; ++i) {
+          const int64_t first = (t0 + sh.s[i]) * ES, last = first + int64_t(cells) * ES;
+          const int64_t a0 = first & ~int64_t(15), a1 = (last + 15) & ~int64_t(15);
+          const int64_t b0 = (first + 15) & ~int64_t(15), b1 = last & ~int64_t(15);
+          const uint32_t head = b1 > b0 ? uint32_t((b0 - first) / ES) : uint32_t(cells);
+          const uint32_t tail = b1 > b0 ? uint32_t((b1 - first) / ES) : uint32_t(cells);
+          sRun[s][i] = uint32_t((first - a0) / ES) | (head << 4) | (tail << 16);
+          total += uint32_t(a1 - a0);
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(&full[s], total);
+        unsigned char* stage = smem_raw + s * C::STAGE_BYTES;
+        for (int i = 0; i < Q; ++i) {
+          const int64_t first = (t0 + sh.s[i]) * ES;
+          const int64_t a0 = first & ~int64_t(15), a1 = (first + int64_t(cells) * ES + 15) & ~int64_t(15);
+          bulk_g2s(stage + i * C::COL_BYTES, reinterpret_cast<const unsigned char*>(pop + i * g.stride) + a0,
+                   uint32_t(a1 - a0), &full[s]);
+        }
+        ++issued;
+      };
+      while (issued < nloc && issued < NS) issue(issued);
+      for (int64_t k = 0; k < nloc; ++k) {
+        const int s = int(k % NS);
+        if (!mbar_wait_bounded(&empty[s], uint32_t((k / NS) & 1), err, waitLimit)) {
+          sAbort = 1;
+          break;
+        }
+        const int64_t t0 = tile_first(k);
+        const int cells = tile_cells(t0);
+        unsigned char* stage = smem_raw + s * C::STAGE_BYTES;
+        for (int i = 0; i < Q; ++i) {
+          const int64_t first = (t0 + sh.s[i]) * ES;
+          const int64_t b0 = (first + 15) & ~int64_t(15), b1 = (first + int64_t(cells) * ES) & ~int64_t(15);
+          if (b1 > b0)
+            bulk_s2g(reinterpret_cast<unsigned char*>(pop + i * g.stride) + b0,
+                     stage + i * C::COL_BYTES + (b0 - (first & ~int64_t(15))), uint32_t(b1 - b0));
+        }
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+        // the previous tile's stage is free once its stores have read it: every store group but
+        // the newest (this tile's) has
+        if (k >= 1 && issued < nloc) {
+          asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+          if (sAbort) break;
+          issue(issued);
+        }
+      }
+      asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+      // loads still in flight (after an abort) land before the block exits: the phase of the
+      // last load issued into each stage (no later phase follows it)
+      for (int s = 0; s < NS; ++s)
+        if (issued > s) {
+          const int64_t kl = s + ((issued - 1 - s) / NS) * NS;
+          mbar_wait_bounded(&full[s], uint32_t((kl / NS) & 1), err, waitLimit);
+        }
+    }
+  } else {
+    const int ct = int(threadIdx.x) - 32;
+    for (int64_t k = 0; k < nloc; ++k) {
+      if (sAbort) break;
+      const int s = int(k % NS);
+      if (!mbar_wait_bounded(&full[s], uint32_t((k / NS) & 1), err, waitLimit)) {
+        sAbort = 1;
+        break;
+      }
+      const int64_t t0 = tile_first(k);
+      const int cells = tile_cells(t0);
+      S* stage = reinterpret_cast<S*>(smem_raw + s * C::STAGE_BYTES);
+      for (int j0 = ct; j0 < cells; j0 += 2 * NCT) {
+        int jj[2] = {j0, j0 + NCT};
+        bool act[2];
+        bool bulk[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int j = jj[c];
+          act[c] = false;
+          bulk[c] = false;
+          if (j >= cells) continue;
+          // core test of flat cell t0 + j by multiply-high division (the divisors sx, sy are fixed)
+          const uint32_t un = uint32_t(t0 + j);
+          const uint32_t px = (__umulhi(un, dv.mx) + un) >> dv.lx;
+          const uint32_t rem = un - px * uint32_t(g.sx);
+          const uint32_t py = (__umulhi(rem, dv.my) + rem) >> dv.ly;
+          const int x = int(px) - 1, y = int(py) - 1, z = int(rem - py * uint32_t(g.sy)) - g.pz;
+          if (!(x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz)) continue;
+          const uint8_t kind = cellDyn ? cellDyn[t0 + j] : uint8_t(1);
+          bulk[c] = bulk_kind(kind);
+          act[c] = bulk[c] || kind == 2;
+        }
+        R f[2][Q];
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+          static_for<Q>([&](auto I) {
+            f[c][I] = act[c] ? Storage<S>::load(stage + I * COL + (sRun[s][I] & 15u) + jj[c]) : R(0);
+          });
+        bool packedDone = false;
+        if constexpr (PACKED) {
+          if (bulk[0] && bulk[1]) {
+            float rr[2], uu[2];
+            collide_bgk_x2<Q>(f, p.omega, rr, uu);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              accRho += double(rr[c]);
+              accUsq += double(uu[c]);
+              accMax = fmax(accMax, double(uu[c]));
+              accCount += 1.0;
+            }
+            packedDone = true;
+          }
+        }
+        if (!packedDone) {
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            if (bulk[c]) {
+              R rho, usq;
+              collide<Q, R, DYN>(f[c], p, rho, usq);
+              accRho += double(rho);
+              accUsq += double(usq);
+              accMax = fmax(accMax, double(usq));
+              accCount += 1.0;
+            } else if (act[c]) {
+              revert<Q, R>(f[c]);
+            }
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          if (!act[c]) continue;
+          const int j = jj[c];
+          static_for<Q>([&](auto I) {
+            const uint32_t run = sRun[s][I];
+            Storage<S>::store(stage + I * COL + (run & 15u) + j, f[c][I]);
+            if (uint32_t(j) < ((run >> 4) & 0xfffu) || uint32_t(j) >= (run >> 16))
+              Storage<S>::store(pop + I * g.stride + t0 + sh.s[I] + j, f[c][I]);
+          });
+        }
+      }
+      // this warp's shared-memory writes become visible to the bulk stores the producer issues
+      // after the stage's empty barrier completes
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  if (statPart) block_partial(accRho, accUsq, accMax, accCount, statPart);
+}
+
 // ---- fused collide + PS stream, K cells per thread ---------------------------------------
 // One thread owns K cells a warp (32 cells) apart along the fastest core axis (z in 3D, y in
 // 2D).  For every population it forms ONE wrapped column index; the K values are then reached
@@ -1805,6 +2030,35 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     k_collide_stream_bulk<Q, S, DYN><<<unsigned(grid), BC::THREADS, BC::SMEM, stream>>>(
         pop, g, sh, a.flatBase, a.flatEnd, tiles, p, a.cellDyn, a.stats ? a.statPart : nullptr, a.err, dv,
         a.waitLimit, a.faultBulk);
+    nblocks = grid;
+  } else if (a.kernel == 4) {
+    using WC = WsCfg<Q, S>;
+    static unsigned long long configured = 0;  // one bit per device ordinal
+    static int residentBlocks[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!(configured >> (dev & 63) & 1ull)) {
+      cudaError_t e = cudaFuncSetAttribute(k_collide_stream_ws<Q, S, DYN>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, WC::SMEM);
+      if (e != cudaSuccess) return e;
+      int perSM = 0, sms = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k_collide_stream_ws<Q, S, DYN>, WC::THREADS, WC::SMEM);
+      if (e != cudaSuccess) return e;
+      e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      residentBlocks[dev & 63] = (perSM > 0 ? perSM : 1) * sms;
+      configured |= 1ull << (dev & 63);
+    }
+    if (!a.doubled) return cudaErrorInvalidValue;  // bulk runs need the doubled columns (no wrap)
+    const int64_t tiles = (a.flatEnd - a.flatBase + WC::BT - 1) / WC::BT;
+    const int64_t grid = tiles < residentBlocks[dev & 63] ? tiles : residentBlocks[dev & 63];
+    if (a.stats && grid > a.statCapacity) return cudaErrorInvalidValue;
+    FlatDiv dv;
+    FlatDiv::make(uint32_t(g.sx), dv.mx, dv.lx);
+    FlatDiv::make(uint32_t(g.sy), dv.my, dv.ly);
+    k_collide_stream_ws<Q, S, DYN><<<unsigned(grid), WC::THREADS, WC::SMEM, stream>>>(
+        pop, g, sh, a.flatBase, a.flatEnd, tiles, p, a.cellDyn, a.stats ? a.statPart : nullptr, a.err, dv,
+        a.waitLimit);
     nblocks = grid;
   } else if (a.kernel == 1) {
     dim3 block(a.blockX, a.blockY, 1);

@@ -235,6 +235,43 @@ def time_ensemble(edges, steps: int, storage: str = "f32", mode: int = 1, cells:
             "blocks_per_sm": blocks_per_sm, "ms_per_step": ms, "mlups": n / ms / 1e3}
 
 
+def sweep(n: int, seed: int = 2024, max_steps: int = 50000, slab_gb: float = 24.0, sequential: bool = True,
+          device: int = 0) -> dict:
+    """The cavity parameter sweep as configured (edge ~ U{32..192}, Re log-uniform [10, 1000], lid
+    0.05, Poisson arrivals at 200/s, residual < 1e-6 or `max_steps`), `n` requests of it: served by
+    the ensemble server in real time, then (optionally) solved one after another."""
+    import torch
+
+    reqs = sample_requests(n, seed=seed, max_steps=max_steps)
+    out: dict = {"requests": n, "seed": seed, "max_steps": max_steps, "slab_gb": slab_gb}
+    with lbx.Ensemble(19, "f32", slab_bytes=int(slab_gb * (1 << 30)), max_lattices=512, device=device) as ens:
+        ens.set_config(threads=256, blocks_per_sm=0, check_interval=100)
+        probe = [ens.admit(CavityRequest(i, e, 100.0).engine_request()) for i, e in enumerate((32, 64, 128, 192))]
+        ens.autotune(steps=10)
+        for slot in probe:
+            ens.retire(slot)
+        server = EnsembleServer(ens, chunk=500, min_chunk=100)
+        server.serve(sample_requests(4, seed=1, edges=(16,), max_steps=1000), realtime=False)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        recs = server.serve(reqs)
+        torch.cuda.synchronize(device)
+        out["server"] = summarise(recs, time.perf_counter() - t0)
+        out["server"]["loop"] = server.last_stats
+        steps = np.array([r.steps for r in recs])
+        out["server"]["steps_p50_p99_max"] = [int(np.percentile(steps, 50)), int(np.percentile(steps, 99)),
+                                              int(steps.max())]
+    if sequential:
+        t0 = time.perf_counter()
+        seq = solve_sequential(reqs, check_interval=100, device=device)
+        torch.cuda.synchronize(device)
+        out["sequential"] = summarise(seq, time.perf_counter() - t0)
+        out["speedup_vs_sequential"] = round(out["sequential"]["wall_s"] / out["server"]["wall_s"], 3)
+        same = [(a.state, a.steps) == (b.state, b.steps) for a, b in zip(recs, seq)]
+        out["same_state_and_steps_as_sequential"] = f"{sum(same)}/{len(same)}"
+    return out
+
+
 def main(argv=None) -> int:
     import argparse
     import json
@@ -247,7 +284,14 @@ def main(argv=None) -> int:
     ap.add_argument("--cells", type=int, default=2, help="cells per thread (1 or 2)")
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--blocks-per-sm", type=int, default=2)
+    ap.add_argument("--sweep", type=int, default=0,
+                    help="serve this many requests of the cavity sweep as configured instead (50,000-step cap)")
+    ap.add_argument("--max-steps", type=int, default=50000)
+    ap.add_argument("--no-sequential", action="store_true")
     a = ap.parse_args(argv)
+    if a.sweep:
+        print(json.dumps(sweep(a.sweep, max_steps=a.max_steps, sequential=not a.no_sequential)))
+        return 0
     edges = [int(v) for v in a.edges.split(",")]
     print(json.dumps(time_ensemble(edges, a.steps, a.storage, a.mode, a.cells, a.threads, a.blocks_per_sm)))
     return 0

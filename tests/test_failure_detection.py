@@ -9,7 +9,6 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-import lbcases as L
 from openlb_b200 import lbx
 
 pytestmark = pytest.mark.gpu
@@ -45,29 +44,36 @@ def test_ensemble_grid_barrier_timeout_is_reported_and_the_context_stays_usable(
         assert all(s[0] == lbx.SLOT_RUNNING for s in st[:2])
 
 
-def test_bulk_copy_wait_timeout_is_reported_and_the_lattice_stays_usable():
-    rng = np.random.default_rng(3)
+def _bulk_lattice(f0):
     lat = lbx.BlockLattice(19, (32, 32, 32), (1, 1, 1), "f16dev")
     lat.define_dynamics("bgk", omega=1.5)
-    f0 = (rng.random((19, 32 ** 3)) - 0.5) * 1e-3
     lat.set_populations(f0)
     lat.set_launch_config(3, 256, 1, 1)
+    return lat
+
+
+def test_bulk_copy_wait_timeout_is_reported_and_the_lattice_stays_usable():
+    rng = np.random.default_rng(3)
+    f0 = (rng.random((19, 32 ** 3)) - 0.5) * 1e-3
+    lat = _bulk_lattice(f0)
     _fault(BULK, 20000)
     lat.collide_and_stream(1, statistics=True)
     with pytest.raises(lbx.LbxError, match="gave up waiting"):
         lat.get_statistics()
     _fault(NONE, 0)
-    # the error flag was cleared by the report; steps run again from a fresh state
+    # the error flag was cleared by the report; steps run again from a fresh state and give the
+    # bits of a lattice that never saw the timeout
     lat.set_populations(f0)
     lat.collide_and_stream(3, statistics=True)
     st = lat.get_statistics()
     assert np.isfinite(st["average_rho"])
-    fx_setup = {"q": 19, "core": (32, 32, 32), "periodic": (1, 1, 1), "dyn": "bgk", "omega": 1.5, "magic": 0.25,
-                "cs": 0.12, "force": [0, 0, 0], "links": None, "cell_dyn": None}
-    want, _ = L.run_oracle(fx_setup, f0, 3, storage="f16dev")
     got = lat.get_populations(np.float32)
-    assert L.errors(19, got, want)["u_l2"] <= 1e-6
     lat.close()
+    ref = _bulk_lattice(f0)
+    ref.collide_and_stream(3, statistics=True)
+    assert np.array_equal(got, ref.get_populations(np.float32))
+    assert ref.get_statistics() == st
+    ref.close()
 
 
 def test_lattice_allocation_failure_is_reported_and_the_next_one_succeeds():

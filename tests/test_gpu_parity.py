@@ -251,7 +251,7 @@ def test_kernel_variants_agree_bitwise(name, storage):
     setup = L.case_setup(fx)
     outs = []
     shapes = [(0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2), (2, 256, 1, 1),
-              (3, 256, 1, 1)]
+              (3, 256, 1, 1), (4, 256, 1, 1)]
     if storage in ("f16dev", "bf16dev"):
         shapes += [(2, 32, 4, 4), (2, 128, 1, 2)]
     for variant, bx, by, k in shapes:
