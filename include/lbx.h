@@ -469,6 +469,33 @@ int lbx_autotune(lbx_lattice lattice, int32_t steps, lbx_tune_entry* out, int32_
 int lbx_ensemble_autotune(lbx_ensemble ens, int32_t steps, lbx_tune_entry* out, int32_t capacity,
                           int32_t* n_out, void* stream);
 
+/* ---- slab decomposition -------------------------------------------------------------------
+ * One lattice cut along x into n_slabs slabs (as equal as the extent allows, each at least two
+ * planes thick), each an lbx_lattice of its own on devices[k] (NULL: all on device 0), stepped in
+ * lock-step with one face exchange per step between the collision and the post-stream links and
+ * boundary cells: the single-process form of the reference's block decomposition and overlap
+ * communication (core/superLattice.hh:150-155, gpu/cuda/communicator.hh:355-510).  Every
+ * population that leaves a slab across an x face is copied into the plane of the neighbour slab
+ * it streams into (periodic x joins the last slab to the first); slabs on different devices send
+ * their face buffers by cudaMemcpyPeerAsync.  A decomposed lattice computes the populations of
+ * the undivided one bit for bit.
+ * Set-up goes through each slab's handle (lbx_slabs_get: the handle, its first x and its
+ * extent; cell k of a slab is global cell (x0 + x, y, z)): dynamics, cell maps, links and boundary
+ * cells as for any lattice, with two rules: a link whose solid neighbour lies in the next slab is
+ * given to the slab of its fluid cell (its neighbour then lies in that slab's ghost plane), and a
+ * velocity / pressure boundary cell must have two planes of its own slab on each side that meets
+ * another slab (its finite differences and neighbour momenta stay inside its slab).  ConstRhoBGK is refused (LBX_ERR_UNSUPPORTED).
+ * lbx_slabs_collide_and_stream returns once the work is queued (one stream per slab, ordered
+ * with the default stream); lbx_slabs_get_statistics waits and combines the slabs' statistics. */
+typedef struct lbx_slabs_s* lbx_slabs;
+int lbx_slabs_create(int32_t q, const int32_t core[3], const int32_t periodic[3], int32_t storage, int32_t n_slabs,
+                     const int32_t* devices, lbx_slabs* out);
+int lbx_slabs_destroy(lbx_slabs slabs);
+int lbx_slabs_get(lbx_slabs slabs, int32_t k, lbx_lattice* lattice, int32_t* x0, int32_t* nx);
+int lbx_slabs_collide_and_stream(lbx_slabs slabs, int64_t steps, uint32_t flags);
+int lbx_slabs_synchronize(lbx_slabs slabs);
+int lbx_slabs_get_statistics(lbx_slabs slabs, double out[4]);
+
 /* ---- test hook -------------------------------------------------------------------------
  * No reference counterpart.  Off by default; for tests of the error paths: it makes a bounded
  * wait of the library's own kernels run out, or an allocation fail, without any GPU fault, so

@@ -65,20 +65,24 @@ def poiseuille_inlet(material: np.ndarray, inlet: int, peak: float) -> np.ndarra
 
 
 def channel_sphere(storage: str = "f16dev", extent=(512, 128, 128), u_peak: float = 0.04, d: float = 24,
-                   re: float = 50.0, center=None, rho_out: float = 1.0):
+                   re: float = 50.0, center=None, rho_out: float = 1.0, slabs: int = 0):
     """The channel lattice at rest, post-processed once as SuperLattice::initialize does.
     D3Q27 TRT with magic 1/4, nu = u_peak d / Re; no-slip side walls of BounceBack dynamics
     (collision::Revert), halfway bounce-back on the sphere (link group 0);
     boundary::set<InterpolatedVelocity> on the inlet with the RectanglePoiseuille3D
     profile of peak u_peak along x, <InterpolatedPressure> with rho_out on the outlet.  Returns
-    (lattice, material map)."""
+    (lattice, material map); with slabs > 0 the lattice is a SlabLattice cut into that many
+    slabs along x."""
     nx, ny, nz = extent
     if center is None:
         center = (nx // 4, ny // 2, nz // 2)
     nu = u_peak * d / re
     omega = 1.0 / (3 * nu + 0.5)
     mat = channel_materials(extent, center, d)
-    lat = lbx.BlockLattice(27, extent, (0, 0, 0), storage)
+    if slabs:
+        lat = lbx.SlabLattice(27, extent, (0, 0, 0), storage, slabs)
+    else:
+        lat = lbx.BlockLattice(27, extent, (0, 0, 0), storage)
     lat.define_dynamics("trt", omega=omega, magic=0.25)
     cell = np.zeros(mat.shape, np.uint8)
     cell[mat == 1] = lbx.CELL_BULK
@@ -166,10 +170,15 @@ def porous_spheres(n: int, seed: int = 7, porosity: float = 0.6, d_min: float = 
 
 
 def porous_medium(solid: np.ndarray, storage: str = "f16dev", nu: float = 0.05, force: float = 1e-6,
-                  cs: float = 0.12) -> lbx.BlockLattice:
+                  cs: float = 0.12, slabs: int = 0):
+    """The porous box: Smagorinsky-forced BGK in the pores, no dynamics in the solid, halfway
+    bounce-back links on every pore-solid face; a SlabLattice of `slabs` slabs when slabs > 0."""
     n = solid.shape[0]
     mat = np.where(solid, 2, 1).astype(np.int32)
-    lat = lbx.BlockLattice(27, (n, n, n), (1, 1, 1), storage)
+    if slabs:
+        lat = lbx.SlabLattice(27, (n, n, n), (1, 1, 1), storage, slabs)
+    else:
+        lat = lbx.BlockLattice(27, (n, n, n), (1, 1, 1), storage)
     lat.define_dynamics("smagorinsky_forced_bgk", omega=1.0 / (3 * nu + 0.5), smagorinsky=cs, force=(force, 0, 0))
     lat.set_cell_dynamics(np.where(solid, 0, 1).astype(np.uint8).reshape(-1))
     lat.set_bouzidi_boundary(mat, 1, (2,))

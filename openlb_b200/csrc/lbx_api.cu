@@ -127,6 +127,7 @@ struct lbx_lattice_s {
   // host copies: the cell map as set (public ids incl. the boundary list's marks; empty = bulk
   // everywhere) and the links (padded cell, direction, wall term) in their device order
   std::vector<uint8_t> hostMap;
+  uint64_t mapVersion = 0;  // counts refresh_cell_map calls (slab face lists depend on the map)
   std::vector<uint32_t> linkHostCell;
   std::vector<uint8_t> linkHostDir;
   std::vector<double> linkHostDelta;
@@ -543,6 +544,7 @@ bool device_ok(int device, std::string& why) {
 // into the K-cells step kernel (bit k of linkMask[x_b], x_b marked kCellBulkLinked); every other
 // link stays with the link kernel, which with the other kernel variants applies all links.
 int refresh_cell_map(lbx_lattice_s* L) {
+  ++L->mapVersion;
   const bool need = !L->hostMap.empty() || L->nLinks > 0;
   cudaFree(L->linkMask);
   cudaFree(L->restCell);
@@ -806,6 +808,48 @@ int set_links_impl(lbx_lattice_s* L, int64_t n, const int64_t* cells, const int3
   L->linkHostDir = hd;
   L->linkHostDelta = delta;
   return refresh_cell_map(L);
+}
+
+// One step in two phases, so that a decomposed lattice can exchange its slab faces between
+// them (lbx_slabs_collide_and_stream): the collision with the fused stores, the periodic overlap
+// copy and the shift rotation; then the post-stream links and boundary cells.
+// ConstRhoBGK reads the previous step's average density, so its statistics are kept on every
+// step, as the reference keeps them whenever statistics are enabled (its default).
+int step_collide(lbx_lattice_s* L, bool statistics, cudaStream_t s, cudaEvent_t (&ev)[4]) {
+  LaunchArgs a = args_of(L);
+  if (statistics || L->dynamics == LBX_CONST_RHO_BGK) {
+    if (int rc = ensure_stat_capacity(L)) return rc;
+    a.stats = L->stats;
+    a.statPart = L->statPart;
+    a.statCapacity = L->statCapacity;
+  }
+  if (L->timing) {
+    if (L->pending.size() >= 4 * 2048) drain_timing(L);
+    for (auto& e : ev) e = take_event(L);
+    if (ev[0]) cudaEventRecord(ev[0], s);
+  }
+  LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_step<Q, S>(a, s))));
+  if (ev[1]) cudaEventRecord(ev[1], s);
+  LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_halo<Q, S>(a, s))));
+  if (ev[2]) cudaEventRecord(ev[2], s);
+  rotate_all(L);
+  return LBX_OK;
+}
+
+int step_post_stream(lbx_lattice_s* L, cudaStream_t s) {
+  if (L->nLinks > 0 || L->nFd > 0) {
+    const LaunchArgs b = args_of(L);
+    // the K-cells kernel applied the resting links itself (linkMask); the link kernel does
+    // the rest, or all of them after the other kernel variants
+    if (b.linkMask) {
+      if (L->nRest > 0)
+        LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->restCell, L->restDir, L->restDelta, L->nRest, s))));
+    } else if (L->nLinks > 0) {
+      LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
+    }
+    if (L->nFd > 0) LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_fd_boundary<Q, S>(b, s))));
+  }
+  return LBX_OK;
 }
 
 }  // namespace
@@ -1329,40 +1373,10 @@ int lbx_collide_and_stream(lbx_lattice L, int64_t steps, uint32_t flags, void* s
   if (steps < 0) return fail(LBX_ERR_INVALID, "steps must be >= 0");
   DeviceGuard guard(L->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // ConstRhoBGK reads the previous step's average density, so its statistics are kept on
-  // every step, as the reference keeps them whenever statistics are enabled (its default)
-  const bool everyStep = L->dynamics == LBX_CONST_RHO_BGK;
   for (int64_t k = 0; k < steps; ++k) {
-    LaunchArgs a = args_of(L);
-    if (((flags & LBX_STEP_STATISTICS) && k == steps - 1) || everyStep) {
-      if (int rc = ensure_stat_capacity(L)) return rc;
-      a.stats = L->stats;
-      a.statPart = L->statPart;
-      a.statCapacity = L->statCapacity;
-    }
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    if (L->timing) {
-      if (L->pending.size() >= 4 * 2048) drain_timing(L);
-      for (auto& e : ev) e = take_event(L);
-      if (ev[0]) cudaEventRecord(ev[0], s);
-    }
-    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_step<Q, S>(a, s))));
-    if (ev[1]) cudaEventRecord(ev[1], s);
-    LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_halo<Q, S>(a, s))));
-    if (ev[2]) cudaEventRecord(ev[2], s);
-    rotate_all(L);
-    if (L->nLinks > 0 || L->nFd > 0) {
-      const LaunchArgs b = args_of(L);
-      // the K-cells kernel applied the resting links itself (linkMask); the link kernel does
-      // the rest, or all of them after the other kernel variants
-      if (b.linkMask) {
-        if (L->nRest > 0)
-          LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->restCell, L->restDir, L->restDelta, L->nRest, s))));
-      } else if (L->nLinks > 0) {
-        LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_bouzidi<Q, S>(b, L->linkCell, L->linkDir, L->linkDelta, L->nLinks, s))));
-      }
-      if (L->nFd > 0) LBX_CUDA_TRY(LBX_DISPATCH(L, (launch_fd_boundary<Q, S>(b, s))));
-    }
+    if (int rc = step_collide(L, ((flags & LBX_STEP_STATISTICS) && k == steps - 1), s, ev)) return rc;
+    if (int rc = step_post_stream(L, s)) return rc;
     if (ev[3]) {
       cudaEventRecord(ev[3], s);
       if (ev[0] && ev[1] && ev[2]) {
@@ -1675,6 +1689,348 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
   L->cellsPerThread = pick.k;
   if (rc != LBX_OK) return fail(rc, "autotune: " + err);
   if (e != cudaSuccess) return fail(LBX_ERR_CUDA, std::string("autotune: ") + cudaGetErrorString(e));
+  return LBX_OK;
+}
+
+}  // extern "C"
+
+// ---- slab decomposition (lbx_slabs_*) -----------------------------------------------------
+// One lattice cut along x into slabs, each an lbx_lattice of its own (on one device, or on
+// several devices of this process), stepped in lock-step with one face exchange per step between
+// the collision and the post-stream phase -- the single-process form of the reference's block
+// decomposition and overlap communication (core/superLattice.hh:150-155,
+// gpu/cuda/communicator.hh:355-510).
+//
+// After a slab's collision and shift rotation, every population that left the slab across an x
+// face sits in the slab's own ghost plane (x = -1 or nx): the plain store of the step kernel put
+// it at the slot that the rotation then associates with the ghost cell.  The exchange copies it
+// into the neighbour slab's first (or last) plane, at the target cell the population reaches in
+// the whole lattice (across periodic y and z faces too).  Copies come only from cells that are
+// stepped: the population of a cell without dynamics is supplied by the link that faces it, as
+// in the whole lattice.  Each directed face is a list of (source slot, target slot) pairs made on
+// the host from the slabs' cell maps (remade when a map changes); per step the sending slab
+// gathers the listed slots into a face buffer (its own memory), the buffer crosses to the
+// receiving device by cudaMemcpyPeerAsync when the slabs sit on different devices, and the
+// receiving slab scatters it into its slots.  Each slab runs on a stream of its own; events order
+// a gather after the sender's collision, the scatter after the receiver's collision, and the
+// next gather into the buffer after the last scatter from it.
+namespace {
+
+struct SlabFace {
+  int src = 0, dst = 0;             // slab indices
+  int64_t n = 0;                    // listed slots
+  uint32_t* srcCell = nullptr;      // on the sender's device
+  uint8_t* srcDir = nullptr;
+  uint32_t* dstCell = nullptr;      // on the receiver's device
+  uint8_t* dstDir = nullptr;
+  void* sendBuf = nullptr;          // sender's device
+  void* recvBuf = nullptr;          // receiver's device (nullptr: same device, scatter reads sendBuf)
+  cudaEvent_t sent = nullptr;       // recorded on the sender's stream after the gather
+  cudaEvent_t consumed = nullptr;   // recorded on the receiver's stream after the scatter
+};
+
+void free_face(SlabFace& f, const std::vector<lbx_lattice_s*>& slabs) {
+  {
+    DeviceGuard g(slabs[size_t(f.src)]->device);
+    cudaFree(f.srcCell);
+    cudaFree(f.srcDir);
+    cudaFree(f.sendBuf);
+    if (f.sent) cudaEventDestroy(f.sent);
+  }
+  {
+    DeviceGuard g(slabs[size_t(f.dst)]->device);
+    cudaFree(f.dstCell);
+    cudaFree(f.dstDir);
+    cudaFree(f.recvBuf);
+    if (f.consumed) cudaEventDestroy(f.consumed);
+  }
+  f = SlabFace{};
+}
+
+}  // namespace
+
+struct lbx_slabs_s {
+  int q = 19, d = 3, storage = LBX_F32;
+  int core[3] = {0, 0, 0}, periodic[3] = {0, 0, 0};
+  std::vector<lbx_lattice_s*> slab;
+  std::vector<int> x0;
+  std::vector<cudaStream_t> stream;
+  std::vector<SlabFace> face;
+  std::vector<uint64_t> versions;  // the slabs' map versions the face lists were made from
+  bool facesBuilt = false;
+};
+
+namespace {
+
+// Whether padded cell n of a slab is stepped by its own kernels (any kind but "no dynamics").
+bool slab_stepped(const lbx_lattice_s* L, int64_t n) {
+  return L->hostMap.empty() ? true : L->hostMap[size_t(n)] != LBX_CELL_NONE;
+}
+
+// The (source slot, target slot) pairs of the face from slab `a` to its neighbour `b`; side +1:
+// b lies at higher x (populations with c_x = +1 enter b's plane x = 0), -1: at lower x.
+void face_pairs(const lbx_lattice_s* A, const lbx_lattice_s* B, int side, std::vector<uint32_t>& sc,
+                std::vector<uint8_t>& sd, std::vector<uint32_t>& dc, std::vector<uint8_t>& dd) {
+  const Geometry ga = geometry_of(A), gb = geometry_of(B);
+  const int ny = ga.ny, nz = ga.nz;
+  const int xs = side > 0 ? ga.nx - 1 : 0, xt = side > 0 ? 0 : gb.nx - 1;
+  auto pad = [](const Geometry& g, int x, int y, int z) {
+    return int64_t(x + 1) * g.sx + int64_t(y + 1) * g.sy + (z + g.pz);
+  };
+  for (int i = 1; i < A->q; ++i) {
+    const int* c = velocity(A->q, i);
+    if (c[0] != side) continue;
+    const int cy = c[1], cz = A->d == 3 ? c[2] : 0;
+    for (int yt = 0; yt < ny; ++yt)
+      for (int zt = 0; zt < nz; ++zt) {
+        int ys = yt - cy, zs = zt - cz;
+        if (ys < 0 || ys >= ny) {
+          if (!A->periodic[1]) continue;
+          ys = (ys + ny) % ny;
+        }
+        if (zs < 0 || zs >= nz) {
+          if (A->d != 3 || !A->periodic[2]) continue;
+          zs = (zs + nz) % nz;
+        }
+        if (!slab_stepped(A, pad(ga, xs, ys, zs))) continue;
+        sc.push_back(uint32_t(pad(ga, xs + side, ys + cy, zs + cz)));
+        sd.push_back(uint8_t(i));
+        dc.push_back(uint32_t(pad(gb, xt, yt, zt)));
+        dd.push_back(uint8_t(i));
+      }
+  }
+}
+
+template <typename T>
+cudaError_t upload_vec(T** dst, const std::vector<T>& v) {
+  *dst = nullptr;
+  if (v.empty()) return cudaSuccess;
+  cudaError_t e = cudaMalloc(dst, v.size() * sizeof(T));
+  if (e == cudaSuccess) e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+int build_faces(lbx_slabs_s* S) {
+  for (auto& f : S->face) free_face(f, S->slab);
+  S->face.clear();
+  const int ns = int(S->slab.size());
+  for (int k = 0; k < ns; ++k) {
+    const int up = k + 1 < ns ? k + 1 : (S->periodic[0] ? 0 : -1);
+    if (up < 0 || up == k) continue;
+    for (int side : {+1, -1}) {
+      SlabFace f;
+      f.src = side > 0 ? k : up;
+      f.dst = side > 0 ? up : k;
+      std::vector<uint32_t> sc, dc;
+      std::vector<uint8_t> sd, dd;
+      face_pairs(S->slab[size_t(f.src)], S->slab[size_t(f.dst)], side, sc, sd, dc, dd);
+      f.n = int64_t(sc.size());
+      const lbx_lattice_s* A = S->slab[size_t(f.src)];
+      const lbx_lattice_s* B = S->slab[size_t(f.dst)];
+      const size_t bytes = size_t(std::max<int64_t>(f.n, 1)) * size_t(storage_bytes(A->storage));
+      cudaError_t e;
+      {
+        DeviceGuard g(A->device);
+        e = upload_vec(&f.srcCell, sc);
+        if (e == cudaSuccess) e = upload_vec(&f.srcDir, sd);
+        if (e == cudaSuccess) e = cudaMalloc(&f.sendBuf, bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.sent, cudaEventDisableTiming);
+      }
+      if (e == cudaSuccess) {
+        DeviceGuard g(B->device);
+        e = upload_vec(&f.dstCell, dc);
+        if (e == cudaSuccess) e = upload_vec(&f.dstDir, dd);
+        if (e == cudaSuccess && B->device != A->device) e = cudaMalloc(&f.recvBuf, bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.consumed, cudaEventDisableTiming);
+      }
+      S->face.push_back(f);
+      if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? LBX_ERR_OUT_OF_MEMORY : LBX_ERR_CUDA,
+                    std::string("slab face set-up: ") + cudaGetErrorString(e));
+    }
+  }
+  S->versions.clear();
+  for (auto* L : S->slab) S->versions.push_back(L->mapVersion);
+  S->facesBuilt = true;
+  return LBX_OK;
+}
+
+bool faces_stale(const lbx_slabs_s* S) {
+  if (!S->facesBuilt) return true;
+  for (size_t k = 0; k < S->slab.size(); ++k)
+    if (S->versions[k] != S->slab[k]->mapVersion) return true;
+  return false;
+}
+
+void destroy_slabs(lbx_slabs_s* S) {
+  for (auto& f : S->face) free_face(f, S->slab);
+  for (size_t k = 0; k < S->slab.size(); ++k) {
+    if (k < S->stream.size() && S->stream[k]) {
+      DeviceGuard g(S->slab[k]->device);
+      cudaStreamDestroy(S->stream[k]);
+    }
+    lbx_lattice_destroy(S->slab[k]);
+  }
+  delete S;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbx_slabs_create(int32_t q, const int32_t core[3], const int32_t periodic[3], int32_t storage, int32_t n_slabs,
+                     const int32_t* devices, lbx_slabs* out) {
+  if (!out || !core) return fail(LBX_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (n_slabs < 1) return fail(LBX_ERR_INVALID, "n_slabs must be >= 1");
+  if (core[0] < 2 * n_slabs) return fail(LBX_ERR_INVALID, "every slab needs at least two x planes");
+  auto* S = new lbx_slabs_s();
+  S->q = q;
+  S->d = q == 9 ? 2 : 3;
+  S->storage = storage;
+  for (int a = 0; a < 3; ++a) {
+    S->core[a] = core[a];
+    S->periodic[a] = periodic ? (periodic[a] != 0) : 0;
+  }
+  int x = 0;
+  for (int k = 0; k < n_slabs; ++k) {
+    const int nx = core[0] / n_slabs + (k < core[0] % n_slabs ? 1 : 0);
+    const int32_t sc[3] = {nx, core[1], core[2]};
+    // x is periodic inside a slab only when it is the whole lattice
+    const int32_t sp[3] = {n_slabs == 1 ? S->periodic[0] : 0, S->periodic[1], S->periodic[2]};
+    lbx_lattice L = nullptr;
+    if (int rc = lbx_lattice_create(q, sc, sp, storage, devices ? devices[k] : 0, &L)) {
+      const std::string msg = g_error;
+      destroy_slabs(S);
+      return fail(rc, "slab " + std::to_string(k) + ": " + msg);
+    }
+    S->slab.push_back(L);
+    S->x0.push_back(x);
+    x += nx;
+    cudaStream_t st = nullptr;
+    DeviceGuard g(L->device);
+    cudaError_t e = cudaStreamCreate(&st);
+    S->stream.push_back(st);
+    if (e != cudaSuccess) {
+      destroy_slabs(S);
+      return fail(LBX_ERR_CUDA, std::string("slab stream: ") + cudaGetErrorString(e));
+    }
+  }
+  // slabs on different devices read nothing of each other (the face buffers cross by copies),
+  // but direct peer copies need peer access where the devices offer it
+  for (size_t a = 0; a < S->slab.size(); ++a)
+    for (size_t b = 0; b < S->slab.size(); ++b) {
+      const int da = S->slab[a]->device, db = S->slab[b]->device;
+      if (da == db) continue;
+      int can = 0;
+      if (cudaDeviceCanAccessPeer(&can, da, db) == cudaSuccess && can) {
+        DeviceGuard g(da);
+        if (cudaDeviceEnablePeerAccess(db, 0) != cudaSuccess) cudaGetLastError();  // already enabled
+      }
+    }
+  *out = S;
+  return LBX_OK;
+}
+
+int lbx_slabs_destroy(lbx_slabs S) {
+  if (!S) return LBX_OK;
+  for (size_t k = 0; k < S->slab.size(); ++k) {
+    DeviceGuard g(S->slab[k]->device);
+    cudaStreamSynchronize(S->stream[k]);
+  }
+  destroy_slabs(S);
+  return LBX_OK;
+}
+
+int lbx_slabs_get(lbx_slabs S, int32_t k, lbx_lattice* lattice, int32_t* x0, int32_t* nx) {
+  if (!S || k < 0 || k >= int32_t(S->slab.size())) return fail(LBX_ERR_INVALID, "no such slab");
+  if (lattice) *lattice = S->slab[size_t(k)];
+  if (x0) *x0 = S->x0[size_t(k)];
+  if (nx) *nx = S->slab[size_t(k)]->core[0];
+  return LBX_OK;
+}
+
+int lbx_slabs_collide_and_stream(lbx_slabs SL, int64_t steps, uint32_t flags) {
+  if (!SL) return fail(LBX_ERR_INVALID, "null slabs");
+  if (steps < 0) return fail(LBX_ERR_INVALID, "steps must be >= 0");
+  for (auto* L : SL->slab)
+    if (L->dynamics == LBX_CONST_RHO_BGK)
+      return fail(LBX_ERR_UNSUPPORTED, "ConstRhoBGK couples every cell to the whole lattice's density; not on slabs");
+  if (faces_stale(SL))
+    if (int rc = build_faces(SL)) return rc;
+  const size_t ns = SL->slab.size();
+  for (int64_t k = 0; k < steps; ++k) {
+    const bool stats = (flags & LBX_STEP_STATISTICS) && k == steps - 1;
+    for (size_t j = 0; j < ns; ++j) {
+      lbx_lattice_s* L = SL->slab[j];
+      DeviceGuard g(L->device);
+      cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+      const bool timing = L->timing;
+      L->timing = false;  // per-kernel timing is a single-lattice tool
+      const int rc = step_collide(L, stats, SL->stream[j], ev);
+      L->timing = timing;
+      if (rc) return rc;
+    }
+    for (auto& f : SL->face) {
+      lbx_lattice_s* A = SL->slab[size_t(f.src)];
+      lbx_lattice_s* B = SL->slab[size_t(f.dst)];
+      cudaStream_t sa = SL->stream[size_t(f.src)], sb = SL->stream[size_t(f.dst)];
+      const size_t bytes = size_t(f.n) * size_t(storage_bytes(A->storage));
+      {
+        DeviceGuard g(A->device);
+        // the buffer is free once the previous step's scatter has read it
+        if (f.consumed && k > 0) LBX_CUDA_TRY(cudaStreamWaitEvent(sa, f.consumed, 0));
+        const LaunchArgs a = args_of(A);
+        LBX_CUDA_TRY(LBX_DISPATCH(A, (launch_face_copy<Q, S>(a, f.sendBuf, f.srcCell, f.srcDir, f.n, true, sa))));
+        LBX_CUDA_TRY(cudaEventRecord(f.sent, sa));
+      }
+      {
+        DeviceGuard g(B->device);
+        LBX_CUDA_TRY(cudaStreamWaitEvent(sb, f.sent, 0));
+        void* in = f.sendBuf;
+        if (f.recvBuf) {
+          if (bytes) LBX_CUDA_TRY(cudaMemcpyPeerAsync(f.recvBuf, B->device, f.sendBuf, A->device, bytes, sb));
+          in = f.recvBuf;
+        }
+        const LaunchArgs b = args_of(B);
+        LBX_CUDA_TRY(LBX_DISPATCH(B, (launch_face_copy<Q, S>(b, in, f.dstCell, f.dstDir, f.n, false, sb))));
+        LBX_CUDA_TRY(cudaEventRecord(f.consumed, sb));
+      }
+    }
+    for (size_t j = 0; j < ns; ++j) {
+      lbx_lattice_s* L = SL->slab[j];
+      DeviceGuard g(L->device);
+      if (int rc = step_post_stream(L, SL->stream[j])) return rc;
+    }
+  }
+  return LBX_OK;
+}
+
+int lbx_slabs_synchronize(lbx_slabs S) {
+  if (!S) return fail(LBX_ERR_INVALID, "null slabs");
+  for (size_t k = 0; k < S->slab.size(); ++k) {
+    DeviceGuard g(S->slab[k]->device);
+    LBX_CUDA_TRY(cudaStreamSynchronize(S->stream[k]));
+  }
+  return LBX_OK;
+}
+
+int lbx_slabs_get_statistics(lbx_slabs S, double out[4]) {
+  if (!S || !out) return fail(LBX_ERR_INVALID, "null argument");
+  if (int rc = lbx_slabs_synchronize(S)) return rc;
+  double sumRho = 0.0, sumE = 0.0, maxU = 0.0, cells = 0.0;
+  for (auto* L : S->slab) {
+    double st[4];
+    if (int rc = lbx_get_statistics(L, st, nullptr)) return rc;
+    sumRho += st[0] * st[3];
+    sumE += st[1] * st[3];
+    maxU = std::max(maxU, st[2]);
+    cells += st[3];
+  }
+  out[0] = cells > 0 ? sumRho / cells : 1.0;
+  out[1] = cells > 0 ? sumE / cells : 1.0;
+  out[2] = maxU;
+  out[3] = cells;
   return LBX_OK;
 }
 

@@ -698,6 +698,15 @@ template <int Q, typename S> struct WsCfg {
   static_assert(BT <= 4095, "packed run bounds hold 12 bits");
 };
 
+// Bounded wait without sleeping: try_wait itself suspends the thread for a while before it
+// reports an incomplete phase, so the pipeline's waits need no back-off of their own.
+__device__ __forceinline__ bool mbar_wait_spin(uint64_t* bar, uint32_t parity, int* err, int limit) {
+  for (int it = 0; it < limit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicExch(err, 1);
+  return false;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
 }
@@ -767,7 +776,7 @@ __global__ void __launch_bounds__(WsCfg<Q, S>::THREADS, WsCfg<Q, S>::BLOCKS) k_c
       while (issued < nloc && issued < NS) issue(issued);
       for (int64_t k = 0; k < nloc; ++k) {
         const int s = int(k % NS);
-        if (!mbar_wait_bounded(&empty[s], uint32_t((k / NS) & 1), err, waitLimit)) {
+        if (!mbar_wait_spin(&empty[s], uint32_t((k / NS) & 1), err, waitLimit)) {
           sAbort = 1;
           break;
         }
@@ -782,10 +791,10 @@ __global__ void __launch_bounds__(WsCfg<Q, S>::THREADS, WsCfg<Q, S>::BLOCKS) k_c
                      stage + i * C::COL_BYTES + (b0 - (first & ~int64_t(15))), uint32_t(b1 - b0));
         }
         asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-        // the previous tile's stage is free once its stores have read it: every store group but
-        // the newest (this tile's) has
-        if (k >= 1 && issued < nloc) {
-          asm volatile("cp.async.bulk.wait_group.read 1;\n" ::: "memory");
+        // the stage is free again once these stores have read it; the next tile for it is then
+        // NS - 1 tiles ahead of the consumers
+        if (issued < nloc) {
+          asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
           if (sAbort) break;
           issue(issued);
         }
@@ -796,7 +805,7 @@ __global__ void __launch_bounds__(WsCfg<Q, S>::THREADS, WsCfg<Q, S>::BLOCKS) k_c
       for (int s = 0; s < NS; ++s)
         if (issued > s) {
           const int64_t kl = s + ((issued - 1 - s) / NS) * NS;
-          mbar_wait_bounded(&full[s], uint32_t((kl / NS) & 1), err, waitLimit);
+          mbar_wait_spin(&full[s], uint32_t((kl / NS) & 1), err, waitLimit);
         }
     }
   } else {
@@ -804,7 +813,7 @@ __global__ void __launch_bounds__(WsCfg<Q, S>::THREADS, WsCfg<Q, S>::BLOCKS) k_c
     for (int64_t k = 0; k < nloc; ++k) {
       if (sAbort) break;
       const int s = int(k % NS);
-      if (!mbar_wait_bounded(&full[s], uint32_t((k / NS) & 1), err, waitLimit)) {
+      if (!mbar_wait_spin(&full[s], uint32_t((k / NS) & 1), err, waitLimit)) {
         sAbort = 1;
         break;
       }
@@ -1946,6 +1955,12 @@ cudaError_t launch_link_force(const LaunchArgs& a, const uint32_t* cell, const u
                               int want, int64_t nLinks, double* part, double* out, cudaStream_t stream);
 template <int Q, typename S>
 cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, double* out, cudaStream_t stream);
+// Slab faces (lbx_slabs_*): gather = true copies the listed slots of this lattice into buf,
+// false copies buf into the listed slots; slot e is population dir[e] of padded cell cell[e] at
+// the lattice's current shift.
+template <int Q, typename S>
+cudaError_t launch_face_copy(const LaunchArgs& a, void* buf, const uint32_t* cell, const uint8_t* dir, int64_t n,
+                             bool gather, cudaStream_t stream);
 
 template <int Q>
 inline Shifts<Q> shifts_of(const LaunchArgs& a) {
@@ -2264,6 +2279,33 @@ cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, doub
   k_finalize4<4><<<1, kFinalizeThreads, 0, stream>>>(part, blocks, out);
   return cudaGetLastError();
 }
+// One thread per listed slot of a slab face: gather (populations -> buffer) on the lattice that
+// sends, scatter (buffer -> populations) on the lattice that receives.  The shift of each
+// population is taken from the kernel's parameters, so the lists hold cells, not addresses.
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_face_copy(S* __restrict__ pop, int64_t stride, int64_t period, Shifts<Q> sh,
+                                                   S* __restrict__ buf, const uint32_t* __restrict__ cell,
+                                                   const uint8_t* __restrict__ dir, int64_t n, int gather) {
+  const int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int i = dir[e];
+  int64_t shift = 0;
+  static_for<Q>([&](auto I) {
+    if (int(I) == i) shift = sh.s[I];
+  });
+  S* slot = pop + int64_t(i) * stride + wrap_add(int64_t(cell[e]), shift, period);
+  if (gather) buf[e] = *slot;
+  else *slot = buf[e];
+}
+template <int Q, typename S>
+cudaError_t launch_face_copy(const LaunchArgs& a, void* buf, const uint32_t* cell, const uint8_t* dir, int64_t n,
+                             bool gather, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  k_face_copy<Q, S><<<unsigned((n + 255) / 256), 256, 0, stream>>>(static_cast<S*>(a.pop), a.g.stride, a.g.n,
+                                                                    shifts_of<Q>(a), static_cast<S*>(buf), cell, dir,
+                                                                    n, gather ? 1 : 0);
+  return cudaGetLastError();
+}
 // Explicit instantiation of every launcher for one (descriptor, storage) pair.
 #define LBX_INSTANTIATE(Q, S)                                                                          \
   template cudaError_t launch_step<Q, S>(const LaunchArgs&, cudaStream_t);                            \
@@ -2278,7 +2320,9 @@ cudaError_t launch_residual(const LaunchArgs& a, float* snap, double* part, doub
   template cudaError_t launch_link_force<Q, S>(const LaunchArgs&, const uint32_t*, const uint8_t*,    \
                                                const uint8_t*, int, int64_t, double*, double*,         \
                                                cudaStream_t);                                          \
-  template cudaError_t launch_residual<Q, S>(const LaunchArgs&, float*, double*, double*, cudaStream_t);
+  template cudaError_t launch_residual<Q, S>(const LaunchArgs&, float*, double*, double*, cudaStream_t); \
+  template cudaError_t launch_face_copy<Q, S>(const LaunchArgs&, void*, const uint32_t*, const uint8_t*, int64_t, \
+                                              bool, cudaStream_t);
 #endif  // LBX_KERNEL_TU
 
 }  // namespace lbx

@@ -161,6 +161,12 @@ def _load() -> C.CDLL:
         "lbx_ensemble_retire": ([VP, I32], C.c_int),
         "lbx_ensemble_set_config": ([VP, I32, I32, I32], C.c_int),
         "lbx_get_kernel_timing": ([VP, P(D)], C.c_int),
+        "lbx_slabs_create": ([I32, P(I32), P(I32), I32, I32, VP, P(VP)], C.c_int),
+        "lbx_slabs_destroy": ([VP], C.c_int),
+        "lbx_slabs_get": ([VP, I32, P(VP), P(I32), P(I32)], C.c_int),
+        "lbx_slabs_collide_and_stream": ([VP, I64, U32], C.c_int),
+        "lbx_slabs_synchronize": ([VP], C.c_int),
+        "lbx_slabs_get_statistics": ([VP, P(D)], C.c_int),
         "lbx_server_create": ([VP, I32, P(ServerConfig), VP, P(VP)], C.c_int),
         "lbx_server_create_with_engine": ([P(ServerEngine), VP, P(ServerConfig), P(VP)], C.c_int),
         "lbx_server_set_finish_callback": ([VP, FINISH_FN, VP], C.c_int),
@@ -295,10 +301,27 @@ class BlockLattice:
         self._dyn = "bgk"
         self._params = Params(1.0, 0.25, 0.12, (C.c_double * 3)(0, 0, 0))
 
+    @classmethod
+    def _borrow(cls, handle: C.c_void_p, q: int, core, storage: str, device: int) -> "BlockLattice":
+        """A view of a lattice owned elsewhere (a slab of a SlabLattice): close() leaves it."""
+        lat = cls.__new__(cls)
+        lat._h = handle
+        lat._owned = False
+        lat.q = q
+        lat.d = 2 if q == 9 else 3
+        lat.core = tuple(core)
+        lat.storage = storage
+        lat.device = device
+        lat.n_core = int(np.prod(core))
+        lat._dyn = "bgk"
+        lat._params = Params(1.0, 0.25, 0.12, (C.c_double * 3)(0, 0, 0))
+        return lat
+
     # -- lifetime --------------------------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
-            lib.lbx_lattice_destroy(self._h)
+            if getattr(self, "_owned", True):
+                lib.lbx_lattice_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -712,3 +735,164 @@ class Server:
 
     def __exit__(self, *exc):
         self.destroy()
+
+
+class SlabLattice:
+    """One lattice cut along x into slabs stepped together with a face exchange per step
+    (lbx_slabs_*), with the set-up of BlockLattice: global arrays in, global arrays out.  Each
+    slab is a BlockLattice view (`slabs[k]`, first x plane `x0[k]`, extent `nx[k]`)."""
+
+    def __init__(self, q: int, core, periodic=(False, False, False), storage: str = "f32", n_slabs: int = 2,
+                 devices=None):
+        core = list(core) + [1] * (3 - len(core))
+        h = C.c_void_p()
+        dev = None if devices is None else (C.c_int32 * n_slabs)(*[int(d) for d in devices])
+        check(lib.lbx_slabs_create(q, _i32x3(core), _i32x3(periodic), STORAGE[storage], n_slabs, dev, C.byref(h)),
+              "lbx_slabs_create")
+        self._h = h
+        self.q, self.d, self.core, self.storage = q, (2 if q == 9 else 3), tuple(core), storage
+        self.periodic = tuple(bool(p) for p in (list(periodic) + [False] * 3)[:3])
+        self.n_core = int(np.prod(core))
+        self.plane = int(core[1]) * int(core[2])
+        self.slabs: list[BlockLattice] = []
+        self.x0: list[int] = []
+        self.nx: list[int] = []
+        for k in range(n_slabs):
+            lh, x0, nx = C.c_void_p(), C.c_int32(), C.c_int32()
+            check(lib.lbx_slabs_get(h, k, C.byref(lh), C.byref(x0), C.byref(nx)), "lbx_slabs_get")
+            d = 0 if devices is None else int(devices[k])
+            self.slabs.append(BlockLattice._borrow(lh, q, (nx.value, core[1], core[2]), storage, d))
+            self.x0.append(x0.value)
+            self.nx.append(nx.value)
+        self._fd: list[list] = [[] for _ in range(n_slabs)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            for s in self.slabs:
+                s._h = None
+            lib.lbx_slabs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- splitting of global arrays over core cells (x slowest) ----------------------------
+    def _range(self, k: int) -> slice:
+        return slice(self.x0[k] * self.plane, (self.x0[k] + self.nx[k]) * self.plane)
+
+    def _slab_of(self, cells: np.ndarray) -> np.ndarray:
+        x = np.asarray(cells, np.int64) // self.plane
+        return np.searchsorted(np.asarray(self.x0), x, side="right") - 1
+
+    # -- set-up --------------------------------------------------------------------------------
+    def define_dynamics(self, dynamics: str, **kw) -> None:
+        for s in self.slabs:
+            s.define_dynamics(dynamics, **kw)
+
+    def set_cell_dynamics(self, ids) -> None:
+        if ids is None:
+            for s in self.slabs:
+                s.set_cell_dynamics(None)
+            return
+        a = np.ascontiguousarray(ids, dtype=np.uint8).reshape(-1)
+        for k, s in enumerate(self.slabs):
+            s.set_cell_dynamics(a[self._range(k)])
+
+    def set_bouzidi_links(self, cells, dirs, wall=None) -> None:
+        """Links in global core-cell numbering; each goes to the slab of its fluid cell."""
+        c = np.asarray(cells, np.int64)
+        d = np.asarray(dirs, np.int32)
+        w = None if wall is None else np.asarray(wall, np.float64)
+        owner = self._slab_of(c)
+        for k, s in enumerate(self.slabs):
+            sel = owner == k
+            s.set_bouzidi_links(c[sel] - self.x0[k] * self.plane, d[sel], None if w is None else w[sel])
+
+    def set_bouzidi_boundary(self, material: np.ndarray, fluid: int = 1, solid=(2,), wall_velocity=None) -> None:
+        """setBouzidiBoundary over the whole lattice's material map (q = 1/2)."""
+        cells, dirs, wall = build_bouzidi_links(self.q, self.core, material, fluid, solid, wall_velocity,
+                                                self.periodic)
+        self.set_bouzidi_links(cells, dirs, wall)
+
+    def set_boundary_cells(self, cells, kinds, types, normals, values) -> None:
+        """Velocity / pressure boundary cells in global numbering (lbx_set_boundary_cells per
+        slab); each must have two planes of its slab towards every face shared with a slab."""
+        c = np.asarray(cells, np.int64)
+        arrs = [np.asarray(kinds, np.int32), np.asarray(types, np.int32),
+                np.asarray(normals, np.int32).reshape(-1, 3), np.asarray(values, np.float64).reshape(-1, 4)]
+        owner = self._slab_of(c)
+        ns = len(self.slabs)
+        for k in range(ns):
+            sel = owner == k
+            xl = c[sel] // self.plane - self.x0[k]
+            lo_shared = k > 0 or (self.periodic[0] and ns > 1)
+            hi_shared = k < ns - 1 or (self.periodic[0] and ns > 1)
+            if (lo_shared and (xl < 2).any()) or (hi_shared and (xl > self.nx[k] - 3).any()):
+                raise LbxError(-4, f"slab {k}: a boundary cell lies within two planes of a face between slabs")
+            self._fd[k] = [c[sel] - self.x0[k] * self.plane] + [a[sel] for a in arrs]
+            self.slabs[k].set_boundary_cells(*self._fd[k])
+
+    def set_interpolated_boundary(self, kind: int, material: np.ndarray, boundary: int, values: np.ndarray,
+                                  fluid=(1,), outside=(0,)) -> None:
+        """boundary::set<InterpolatedVelocity | InterpolatedPressure> over the whole lattice:
+        the cells are classified on the whole material map, then handed to their slabs (added to
+        the cells set before)."""
+        mat = np.asarray(material, np.int32)
+        cells, types, normals = discrete_normals(mat.reshape(self.core[: self.d]), boundary, fluid, outside,
+                                                 self.periodic)
+        zero = ~np.abs(normals).any(axis=1)
+        if zero.any() or (types < 0).any():
+            raise LbxError(-4, "could not set boundary: a cell has no discrete normal")
+        if kind == FD_PRESSURE:
+            keep = types == NORMAL_FLAT
+            cells, types, normals = cells[keep], types[keep], normals[keep]
+        vals = np.asarray(values, np.float64).reshape(-1, 4)[cells]
+        new = [cells, np.full(len(cells), kind, np.int32), types, normals, vals]
+        prev = [[f[0] + self.x0[k] * self.plane] + list(f[1:]) for k, f in enumerate(self._fd) if f]
+        if prev:
+            old = [np.concatenate([p[j] for p in prev]) for j in range(5)]
+            stay = ~np.isin(old[0], cells)
+            new = [np.concatenate([o[stay], n]) for o, n in zip(old, new)]
+        order = np.argsort(new[0], kind="stable")
+        self.set_boundary_cells(*[a[order] for a in new])
+
+    def post_process(self) -> None:
+        for s in self.slabs:
+            s.post_process()
+
+    # -- data movement -------------------------------------------------------------------------
+    def set_populations(self, f: np.ndarray) -> None:
+        a = np.asarray(f)
+        for k, s in enumerate(self.slabs):
+            s.set_populations(np.ascontiguousarray(a[:, self._range(k)]))
+
+    def get_populations(self, dtype=np.float64) -> np.ndarray:
+        self.synchronize()
+        return np.concatenate([s.get_populations(dtype) for s in self.slabs], axis=1)
+
+    def compute_moments(self):
+        self.synchronize()
+        parts = [s.compute_moments() for s in self.slabs]
+        return np.concatenate([p[0] for p in parts]), np.concatenate([p[1] for p in parts], axis=1)
+
+    # -- steps -------------------------------------------------------------------------------------
+    def collide_and_stream(self, steps: int = 1, statistics: bool = False) -> None:
+        check(lib.lbx_slabs_collide_and_stream(self._h, steps, STEP_STATISTICS if statistics else 0),
+              "lbx_slabs_collide_and_stream")
+
+    def synchronize(self) -> None:
+        check(lib.lbx_slabs_synchronize(self._h), "lbx_slabs_synchronize")
+
+    def get_statistics(self) -> dict:
+        out = (C.c_double * 4)()
+        check(lib.lbx_slabs_get_statistics(self._h, out), "lbx_slabs_get_statistics")
+        return {"average_rho": out[0], "average_energy": out[1], "max_u": out[2], "cells": int(out[3])}
