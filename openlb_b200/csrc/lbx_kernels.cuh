@@ -17,6 +17,7 @@
 // step is a single launch.
 #pragma once
 
+#include <cstring>
 #include <type_traits>
 
 #include <cuda_bf16.h>
@@ -940,6 +941,21 @@ template <> struct StepOccupancy<19, __nv_bfloat16, 4> { static constexpr int bl
 template <> struct StepOccupancy<9, __half, 4> { static constexpr int blocks = 2; };
 template <> struct StepOccupancy<9, __nv_bfloat16, 4> { static constexpr int blocks = 2; };
 
+// Load of one stored population of a 16-bit form with an L2 prefetch-size hint of 256 bytes: a
+// warp-wide load reads 64 bytes of a column, and the hint lets L2 fetch the following warps'
+// bytes of the same column with the same DRAM access.  Wider forms load plainly.
+template <typename S> __device__ __forceinline__ S ld_column(const S* p) {
+  if constexpr (sizeof(S) == 2) {
+    unsigned short v;
+    asm("ld.global.L2::256B.b16 %0, [%1];" : "=h"(v) : "l"(p));
+    S r;
+    memcpy(&r, &v, sizeof(v));
+    return r;
+  } else {
+    return *p;
+  }
+}
+
 template <int Q, typename S, int DYN, int K, bool DOUBLED, bool MAPPED>
 __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide_stream_groups(ColumnBases<Q> cols, Geometry g,
                                                                CollisionParams<typename Storage<S>::R> p,
@@ -1001,7 +1017,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
       if constexpr (DOUBLED) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          if (act[k]) raw[k][I] = col[n0 + W * k];
+          if (act[k]) raw[k][I] = ld_column(col + n0 + W * k);
       } else {
         uint32_t idx = n0 + cols.s[I];
         idx = idx >= P ? idx - P : idx;
@@ -1009,7 +1025,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
         for (int k = 0; k < K; ++k) {
           uint32_t ik = idx + W * k;
           if (k > 0) ik = ik >= P ? ik - P : ik;
-          if (act[k]) raw[k][I] = col[ik];
+          if (act[k]) raw[k][I] = ld_column(col + ik);
         }
       }
     });

@@ -55,7 +55,13 @@ def test_mass_and_energy_decay_at_full_size():
     assert abs(st["average_energy"] / e1 / expected - 1) < 0.01, (st["average_energy"] / e1, expected)
 
 
-@pytest.mark.parametrize("storage,tol", [("f32", 5e-5), ("f16dev", 1e-3), ("bf16dev", 1e-2)])
+# The precision bound for a 16-bit form is a velocity L2 error of 1e-3 against FP64.  FP16
+# meets it.  BF16 does not: its 8-bit mantissa rounds each stored deviation to about 4e-3 of
+# itself, and the TGV ends near 2e-3 to 3e-3; the test states that as an expected failure.
+@pytest.mark.parametrize("storage,tol", [
+    ("f32", 5e-5), ("f16dev", 1e-3),
+    pytest.param("bf16dev", 1e-3, marks=pytest.mark.xfail(strict=True, reason="BF16 misses the 1e-3 bound")),
+])
 def test_storage_forms_against_fp64_at_full_size(storage, tol):
     ref = lattice("f64")
     ref.collide_and_stream(300)
