@@ -72,10 +72,20 @@ typedef enum {
   LBX_CELL_BOUNCE_BACK_VELOCITY = 4 /* BounceBackVelocity (set by lbx_set_bounce_back_velocity) */
 } lbx_cell_dynamics;
 
-/* Kinds of flat-face boundary cells (lbx_set_fd_boundaries). */
+/* Kinds of velocity / pressure boundary cells (lbx_set_fd_boundaries, lbx_set_boundary_cells,
+ * lbx_set_interpolated_boundary). */
 typedef enum {
-  LBX_FD_VELOCITY = 1,      /* boundary::InterpolatedVelocity, boundary/interpolatedVelocity3D.h:45-52 */
-  LBX_FD_PRESSURE = 2       /* boundary::InterpolatedPressure, boundary/interpolatedPressure3D.h:48-90 */
+  LBX_FD_VELOCITY = 1,       /* boundary::InterpolatedVelocity, boundary/interpolatedVelocity3D.h:45-52 */
+  LBX_FD_PRESSURE = 2,       /* boundary::InterpolatedPressure, boundary/interpolatedPressure3D.h:48-90 */
+  /* boundary::LocalVelocity / LocalPressure with BGKdynamics as the mixed-in dynamics
+   * (boundary/localVelocity3D.h:47-115, localVelocity2D.h, localPressure3D.h): a flat cell is
+   * CombinedRLBdynamics (dynamics/dynamics.h:470-523) -- its populations are rebuilt in the
+   * collision as f^eq(rho, u) + fromPiToFneq(Pi) with Pi from RegularizedBoundaryStress
+   * (boundary/helper.h:31-81), then collided by BGK with the same boundary momenta -- and has no
+   * post-processor; velocity edges and corners are those of InterpolatedVelocity; pressure cells
+   * exist on flat faces only (the reference throws elsewhere). */
+  LBX_FD_LOCAL_VELOCITY = 3,
+  LBX_FD_LOCAL_PRESSURE = 4
 } lbx_fd_kind;
 
 /* Parameters of the bulk dynamics (the ParametersD fields OMEGA, TRT::MAGIC,
@@ -203,7 +213,9 @@ int lbx_set_boundary_cells(lbx_lattice lattice, int64_t n, const int64_t* cells,
                            const int32_t* types, const int32_t* normals, const double* values);
 
 /* boundary::set<InterpolatedVelocity> (kind LBX_FD_VELOCITY) or <InterpolatedPressure>
- * (LBX_FD_PRESSURE) over the core cells of material `boundary`, with the given fluid and outside
+ * (LBX_FD_PRESSURE), or <LocalVelocity> / <LocalPressure> (LBX_FD_LOCAL_VELOCITY /
+ * LBX_FD_LOCAL_PRESSURE; a local pressure cell that is not flat returns LBX_ERR_UNSUPPORTED, as
+ * the reference's "No valid discrete normal found"), over the core cells of material `boundary`, with the given fluid and outside
  * material lists, or (n_fluid = 0, n_outside = 0) those of the reference's default overload
  * (boundary/setBoundary.h:112-121: fluid 1, outside 0), followed by the values the application
  * would give them with

@@ -147,7 +147,7 @@ struct lbx_lattice_s {
   // flat-face velocity / pressure boundary cells (lbx_set_fd_boundaries)
   int64_t nFd = 0;
   uint32_t* fdCell = nullptr;
-  uint8_t* fdMeta = nullptr;
+  uint16_t* fdMeta = nullptr;
   double* fdValue = nullptr;
   double* fdMom = nullptr;
   std::vector<uint32_t> fdHostCells;  // padded indices, to re-mark after lbx_set_cell_dynamics
@@ -648,13 +648,14 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
   const int64_t n = int64_t(list.size());
   for (const FdHostCell& c : list) {
     if (c.core < 0 || c.core >= L->ncore) return fail(LBX_ERR_INVALID, "boundary cell out of range");
-    if (c.kind != LBX_FD_VELOCITY && c.kind != LBX_FD_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+    if (c.kind < LBX_FD_VELOCITY || c.kind > LBX_FD_LOCAL_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
     if (c.type == LBX_NORMAL_INTERNAL_CORNER || c.type == LBX_NORMAL_INTERNAL_EDGE)
       return fail(LBX_ERR_UNSUPPORTED, "internal corners and edges (concave boundaries) are not provided");
     if (c.type != LBX_NORMAL_FLAT && c.type != LBX_NORMAL_EXTERNAL_CORNER && c.type != LBX_NORMAL_EXTERNAL_EDGE)
       return fail(LBX_ERR_INVALID, "unknown normal type");
     if (c.type == LBX_NORMAL_EXTERNAL_EDGE && L->d != 3) return fail(LBX_ERR_INVALID, "edges exist in 3D only");
-    if (c.kind == LBX_FD_PRESSURE && c.type != LBX_NORMAL_FLAT)
+    const bool pressure = c.kind == LBX_FD_PRESSURE || c.kind == LBX_FD_LOCAL_PRESSURE;
+    if (pressure && c.type != LBX_NORMAL_FLAT)
       return fail(LBX_ERR_UNSUPPORTED, "pressure boundaries are provided on flat faces only");
     int nonzero = 0;
     for (int a = 0; a < 3; ++a) {
@@ -674,20 +675,27 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
     }
     for (int k = 0; k < 4; ++k)
       if (!std::isfinite(c.v[k])) return fail(LBX_ERR_INVALID, "boundary values must be finite");
-    if (c.kind == LBX_FD_PRESSURE && !(c.v[0] > 0)) return fail(LBX_ERR_INVALID, "boundary density must be > 0");
+    if (pressure && !(c.v[0] > 0)) return fail(LBX_ERR_INVALID, "boundary density must be > 0");
   }
   std::sort(list.begin(), list.end(), [](const FdHostCell& x, const FdHostCell& y) { return x.core < y.core; });
   for (int64_t i = 1; i < n; ++i)
     if (list[size_t(i)].core == list[size_t(i - 1)].core) return fail(LBX_ERR_INVALID, "duplicate boundary cell");
   std::vector<uint32_t> hc(static_cast<size_t>(n));
-  std::vector<uint8_t> hm(static_cast<size_t>(n));
+  std::vector<uint16_t> hm(static_cast<size_t>(n));
   std::vector<double> hv(static_cast<size_t>(4 * n));
   int64_t corners = 0;
   for (int64_t k = 0; k < n; ++k) {
     const FdHostCell& c = list[size_t(k)];
     hc[size_t(k)] = uint32_t(core_index_to_padded(L, c.core));
     int t = FD_FLAT_VELOCITY;
-    if (c.type == LBX_NORMAL_FLAT) t = c.kind == LBX_FD_PRESSURE ? FD_FLAT_PRESSURE : FD_FLAT_VELOCITY;
+    if (c.type == LBX_NORMAL_FLAT) {
+      switch (c.kind) {
+        case LBX_FD_PRESSURE: t = FD_FLAT_PRESSURE; break;
+        case LBX_FD_LOCAL_VELOCITY: t = FD_FLAT_VELOCITY_LOCAL; break;
+        case LBX_FD_LOCAL_PRESSURE: t = FD_FLAT_PRESSURE_LOCAL; break;
+        default: t = FD_FLAT_VELOCITY;
+      }
+    }
     else if (c.type == LBX_NORMAL_EXTERNAL_EDGE) t = FD_EDGE_VELOCITY;
     else t = FD_CORNER_VELOCITY;
     corners += t == FD_CORNER_VELOCITY;
@@ -717,11 +725,11 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
   if (int rc = refresh_cell_map(L)) return rc;
   if (n == 0) return LBX_OK;
   LBX_CUDA_TRY(cudaMalloc(&L->fdCell, size_t(n) * sizeof(uint32_t)));
-  LBX_CUDA_TRY(cudaMalloc(&L->fdMeta, size_t(n)));
+  LBX_CUDA_TRY(cudaMalloc(&L->fdMeta, size_t(n) * sizeof(uint16_t)));
   LBX_CUDA_TRY(cudaMalloc(&L->fdValue, size_t(4 * n) * sizeof(double)));
   LBX_CUDA_TRY(cudaMalloc(&L->fdMom, size_t(7 * n) * sizeof(double)));
   LBX_CUDA_TRY(cudaMemcpy(L->fdCell, hc.data(), size_t(n) * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  LBX_CUDA_TRY(cudaMemcpy(L->fdMeta, hm.data(), size_t(n), cudaMemcpyHostToDevice));
+  LBX_CUDA_TRY(cudaMemcpy(L->fdMeta, hm.data(), size_t(n) * sizeof(uint16_t), cudaMemcpyHostToDevice));
   LBX_CUDA_TRY(cudaMemcpy(L->fdValue, hv.data(), size_t(4 * n) * sizeof(double), cudaMemcpyHostToDevice));
   L->nFd = n;
   L->nFdCorners = corners;
@@ -1062,7 +1070,8 @@ int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* ma
                                   int32_t n_fluid, const int32_t* fluid, int32_t n_outside, const int32_t* outside,
                                   const double* values) {
   if (!L || !material || !values) return fail(LBX_ERR_INVALID, "null argument");
-  if (kind != LBX_FD_VELOCITY && kind != LBX_FD_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+  if (kind < LBX_FD_VELOCITY || kind > LBX_FD_LOCAL_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+  const bool pressureKind = kind == LBX_FD_PRESSURE || kind == LBX_FD_LOCAL_PRESSURE;
   const int32_t defFluid = 1, defOutside = 0;
   if (n_fluid == 0) {
     fluid = &defFluid;
@@ -1083,8 +1092,10 @@ int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* ma
     const int* nn = &normals[3 * k];
     if (t < 0) return fail(LBX_ERR_INVALID, "the boundary material is also a fluid or outside material");
     const bool zero = nn[0] == 0 && nn[1] == 0 && nn[2] == 0;
-    if (kind == LBX_FD_PRESSURE && (t != LBX_NORMAL_FLAT || zero)) {
+    if (pressureKind && (t != LBX_NORMAL_FLAT || zero)) {
       if (zero) return fail(LBX_ERR_UNSUPPORTED, "could not set boundary: a pressure cell has no discrete normal");
+      if (kind == LBX_FD_LOCAL_PRESSURE)
+        return fail(LBX_ERR_UNSUPPORTED, "LocalPressure: no valid discrete normal (flat faces only)");
       continue;  // InterpolatedPressure installs nothing on edges and corners
     }
     if (zero) return fail(LBX_ERR_UNSUPPORTED, "could not set boundary: a velocity cell has no discrete normal");

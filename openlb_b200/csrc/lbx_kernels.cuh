@@ -1279,27 +1279,39 @@ __global__ void __launch_bounds__(256) k_bouzidi(S* __restrict__ pop, Geometry g
                     v - (delta ? delta[l] : R(0)));
 }
 
-// ---- velocity / pressure boundaries (InterpolatedVelocity / InterpolatedPressure) ---------
-// A boundary cell carries a meta byte: bits 0-1 the cell type (0 flat velocity, 1 flat
+// ---- velocity / pressure boundaries (Interpolated and Local Velocity / Pressure) ----------
+// A boundary cell carries a meta word (FdMeta: the cell type -- 0 flat velocity, 1 flat
 // pressure, 2 external edge (3D) with imposed velocity, 3 external corner with imposed
-// velocity), bits 2-7 the outward discrete normal, two bits per axis (0: 0, 1: +1, 2: -1), and
-// four values: the imposed velocity, or {rho, tangential velocity}.  Reference: the boundary
+// velocity, 4 / 5 flat velocity / pressure of a local boundary -- and the outward discrete
+// normal) and four values: the imposed velocity, or {rho, tangential velocity}.  Reference: the boundary
 // momenta mixed into BGKdynamics for the collision (momenta::BasicDirichletVelocityBoundaryTuple
 // / BasicDirichletPressureBoundaryTuple on flat faces, FixedVelocityBoundaryTuple on edges and
 // corners, dynamics/momenta/aliases.h:173-220), and the post-stream processors
 // PlaneFdBoundaryProcessor3D / StraightFdBoundaryProcessor2D (boundary/boundaryPostProcessors3D.hh:
 // 39-93, boundaryPostProcessors2D.hh:39-76), OuterVelocityEdgeProcessor3D (3D.hh:164-238) and
 // OuterVelocityCornerProcessor3D / 2D (3D.hh:240-294, 2D.hh:276-323).
-enum FdType { FD_FLAT_VELOCITY = 0, FD_FLAT_PRESSURE = 1, FD_EDGE_VELOCITY = 2, FD_CORNER_VELOCITY = 3 };
+// Types 4 and 5 are the flat cells of the local boundaries (LocalVelocity / LocalPressure with
+// BGK mixed in): regularised in their collision (CombinedRLBdynamics, dynamics/dynamics.h:
+// 470-523), no post-processor.
+enum FdType {
+  FD_FLAT_VELOCITY = 0, FD_FLAT_PRESSURE = 1, FD_EDGE_VELOCITY = 2, FD_CORNER_VELOCITY = 3,
+  FD_FLAT_VELOCITY_LOCAL = 4, FD_FLAT_PRESSURE_LOCAL = 5
+};
 
+// Meta word of a boundary cell: bits 0-2 the type, bits 3-8 the outward discrete normal, two bits
+// per axis (0: 0, 1: +1, 2: -1).
 struct FdMeta {
   int type;
   int n[3];         // outward normal
   int dir, orient;  // flat cells: the normal axis and its sign
-  int pressure;
-  __host__ __device__ __forceinline__ explicit FdMeta(uint8_t m) : type(m & 3), dir(0), orient(0), pressure((m & 3) == 1) {
+  int pressure;     // flat pressure cell (interpolated or local)
+  int local;        // flat cell of a local boundary
+  int flat;
+  __host__ __device__ __forceinline__ explicit FdMeta(uint16_t m)
+      : type(m & 7), dir(0), orient(0), pressure((m & 7) == 1 || (m & 7) == 5), local((m & 7) >= 4),
+        flat((m & 7) != FD_EDGE_VELOCITY && (m & 7) != FD_CORNER_VELOCITY) {
     for (int a = 0; a < 3; ++a) {
-      const int code = (m >> (2 + 2 * a)) & 3;
+      const int code = (m >> (3 + 2 * a)) & 3;
       n[a] = code == 1 ? 1 : (code == 2 ? -1 : 0);
     }
     for (int a = 2; a >= 0; --a)
@@ -1308,10 +1320,10 @@ struct FdMeta {
         orient = n[a];
       }
   }
-  static __host__ __device__ __forceinline__ uint8_t encode(int type, const int* normal) {
-    unsigned m = unsigned(type & 3);
-    for (int a = 0; a < 3; ++a) m |= unsigned(normal[a] == 1 ? 1 : (normal[a] == -1 ? 2 : 0)) << (2 + 2 * a);
-    return uint8_t(m);
+  static __host__ __device__ __forceinline__ uint16_t encode(int type, const int* normal) {
+    unsigned m = unsigned(type & 7);
+    for (int a = 0; a < 3; ++a) m |= unsigned(normal[a] == 1 ? 1 : (normal[a] == -1 ? 2 : 0)) << (3 + 2 * a);
+    return uint16_t(m);
   }
 };
 
@@ -1333,7 +1345,7 @@ __device__ __forceinline__ void fd_momenta(const R (&f)[Q], FdMeta m, const doub
                                            R (&u)[3]) {
   using D = Desc<Q>;
   u[0] = u[1] = u[2] = R(0);
-  if (m.type >= FD_EDGE_VELOCITY) {
+  if (!m.flat) {
     static_for<D::d>([&](auto A) { u[A] = R(v[A]); });
     rho = bulk_rho<Q, R>(f);
     return;
@@ -1396,6 +1408,67 @@ __device__ __forceinline__ void fd_decode(const Geometry& g, int64_t n, int& x, 
   z = int(r - int64_t(y + 1) * g.sy) - int(g.pz);
 }
 
+// The regularisation of a flat cell of a local boundary (CombinedRLBdynamics::collide,
+// dynamics/dynamics.h:505-516) before its BGK collision: Pi from RegularizedBoundaryStress
+// (BoundaryHelpers::computeStress, boundary/helper.h:31-81: f^neq of the populations with
+// c_d = 0, none for i = 0, and of those with c_d = orientation, the latter counted twice, summed
+// in index order), then f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270).
+template <int Q, typename R>
+__device__ __forceinline__ void local_regularize(R (&f)[Q], FdMeta m, R rho, const R (&u)[3]) {
+  using D = Desc<Q>;
+  constexpr int NPI = D::d == 3 ? 6 : 3;
+  R uSqr = R(0);
+  static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+  R fneq[Q];
+  static_for<Q>([&](auto I) {
+    constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+    const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+    fneq[I] = (int(I) != 0 && (c == 0 || c == m.orient)) ? f[I] - equilibrium_plain<Q, I>(rho, u, uSqr) : R(0);
+  });
+  R pi[NPI];
+  {
+    int iPi = 0;
+    static_for<D::d>([&](auto A) {
+      static_for<D::d>([&](auto B) {
+        if constexpr (int(B) >= int(A)) {
+          R p = R(0);
+          static_for<Q>([&](auto I) {
+            constexpr int cc = D::C[I][A] * D::C[I][B];
+            constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+            const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+            if (c == 0) p += R(cc) * fneq[I];
+          });
+          static_for<Q>([&](auto I) {
+            constexpr int cc = 2 * D::C[I][A] * D::C[I][B];
+            constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+            const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+            if (c == m.orient) p += R(cc) * fneq[I];
+          });
+          pi[iPi++] = p;
+        }
+      });
+    });
+  }
+  static_for<Q>([&](auto I) {
+    constexpr R t = weight<Q, R>(I);
+    R fn = R(0);
+    int iPi = 0;
+    static_for<D::d>([&](auto A) {
+      static_for<D::d>([&](auto B) {
+        if constexpr (int(B) >= int(A)) {
+          R toAdd = R(D::C[I][A] * D::C[I][B]);
+          if constexpr (int(A) == int(B)) toAdd -= R(1) / R(3);
+          else toAdd *= R(2);
+          toAdd *= pi[iPi++];
+          fn += toAdd;
+        }
+      });
+    });
+    fn *= t * R(3) * R(3) / R(2);
+    f[I] = equilibrium_plain<Q, I>(rho, u, uSqr) + fn;
+  });
+}
+
 // Collision of the boundary cells: BGKdynamics with the boundary momenta
 // (collision::BGK::apply with lbm::bgkCollision, dynamics/collision.h:68-78, lbm.h:395-403),
 // in place at the current shifts, after the bulk step kernel left these cells untouched.  A cell
@@ -1404,7 +1477,7 @@ __device__ __forceinline__ void fd_decode(const Geometry& g, int64_t n, int& x, 
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometry g, Shifts<Q> sh, double omega,
                                                     int64_t nFd, const uint32_t* __restrict__ fdCell,
-                                                    const uint8_t* __restrict__ fdMeta,
+                                                    const uint16_t* __restrict__ fdMeta,
                                                     const double* __restrict__ fdValue, double* __restrict__ statPart) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
@@ -1417,6 +1490,10 @@ __global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometr
     static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
     R rho, u[3];
     fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
+    if (m.local) {  // regularised first, then collided with the momenta of the rebuilt cell
+      local_regularize<Q, R>(f, m, rho, u);
+      fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
+    }
     R uSqr = R(0);
     static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
     const R w = R(omega);
@@ -1515,7 +1592,7 @@ __global__ void __launch_bounds__(256) k_bbv_collide(S* __restrict__ pop, Geomet
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_fd_momenta(const S* __restrict__ pop, Geometry g, Shifts<Q> sh, int64_t nFd,
                                                     const uint32_t* __restrict__ fdCell,
-                                                    const uint8_t* __restrict__ fdMeta,
+                                                    const uint16_t* __restrict__ fdMeta,
                                                     const double* __restrict__ fdValue, double hfx, double hfy,
                                                     double hfz, double* __restrict__ fdMom) {
   using R = typename Storage<S>::R;
@@ -1571,7 +1648,7 @@ __device__ __forceinline__ int64_t fd_find(const uint32_t* __restrict__ fdCell, 
 template <int Q, typename S>
 __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geometry g, Shifts<Q> sh, double omega,
                                                        int64_t nFd, const uint32_t* __restrict__ fdCell,
-                                                       const uint8_t* __restrict__ fdMeta,
+                                                       const uint16_t* __restrict__ fdMeta,
                                                        const double* __restrict__ fdValue,
                                                        const uint8_t* __restrict__ cellDyn, double hfx, double hfy,
                                                        double hfz, const double* __restrict__ fdMom, int corners,
@@ -1582,6 +1659,7 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (b >= nFd) return;
   const FdMeta m(fdMeta[b]);
+  if (m.local) return;  // local boundaries have no post-processor
   if ((m.type == FD_CORNER_VELOCITY) != (corners != 0)) return;
   const int64_t n = fdCell[b];
   int pos[3];
@@ -1925,7 +2003,7 @@ struct LaunchArgs {
   int64_t flatEnd;
   int64_t nFd;               // velocity/pressure boundary cells
   const uint32_t* fdCell;    // their padded indices, ascending
-  const uint8_t* fdMeta;     // type and outward normal (FdMeta)
+  const uint16_t* fdMeta;    // type and outward normal (FdMeta)
   const double* fdValue;     // 4 imposed values per cell
   double* fdMom;             // 7 doubles per cell of scratch (k_fd_momenta)
   int64_t nFdCorners;        // how many of them are corners (regularised in a second pass)

@@ -241,7 +241,7 @@ def build_bouzidi_links(q: int, core, material: np.ndarray, fluid: int = 1, soli
     return cells, dirs, wall
 
 
-FD_VELOCITY, FD_PRESSURE = 1, 2
+FD_VELOCITY, FD_PRESSURE, FD_LOCAL_VELOCITY, FD_LOCAL_PRESSURE = 1, 2, 3, 4
 
 
 NORMAL_FLAT, NORMAL_EXTERNAL_CORNER, NORMAL_INTERNAL_CORNER, NORMAL_EXTERNAL_EDGE, NORMAL_INTERNAL_EDGE = 0, 1, 2, 3, 4
@@ -852,8 +852,10 @@ class SlabLattice:
         zero = ~np.abs(normals).any(axis=1)
         if zero.any() or (types < 0).any():
             raise LbxError(-4, "could not set boundary: a cell has no discrete normal")
-        if kind == FD_PRESSURE:
+        if kind in (FD_PRESSURE, FD_LOCAL_PRESSURE):
             keep = types == NORMAL_FLAT
+            if kind == FD_LOCAL_PRESSURE and not keep.all():
+                raise LbxError(-4, "LocalPressure: no valid discrete normal (flat faces only)")
             cells, types, normals = cells[keep], types[keep], normals[keep]
         vals = np.asarray(values, np.float64).reshape(-1, 4)[cells]
         new = [cells, np.full(len(cells), kind, np.int32), types, normals, vals]

@@ -54,7 +54,11 @@ typedef struct {
    * src/boundary/interpolatedVelocity3D.h:45-52,78-80, interpolatedPressure3D.h:48-90. */
   int64_t n_fd;
   const int64_t* fd_cell;    /* core cell, ascending */
-  const int32_t* fd_kind;    /* 1 velocity, 2 pressure */
+  const int32_t* fd_kind;    /* 1 velocity, 2 pressure (interpolated); 3 velocity, 4 pressure
+                                (local: boundary::LocalVelocity / LocalPressure with BGK mixed
+                                in; flat cells regularised in the collision, no post-processor;
+                                src/boundary/localVelocity3D.h:47-115, localPressure3D.h,
+                                dynamics/dynamics.h:470-523) */
   const int32_t* fd_dir;     /* normal axis */
   const int32_t* fd_orient;  /* outward normal sign, -1 or +1 */
   const double* fd_value;    /* 4 per cell: the velocity, or {rho, tangential velocity} */

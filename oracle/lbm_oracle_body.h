@@ -166,13 +166,71 @@ static void FN(fd_momenta)(const lbo_desc* d, const REAL* g, int kind, int type,
     if (d->c[i][dir] == 0) onWall += g[i];
   for (int i = 0; i < q; ++i)
     if (d->c[i][dir] == orient) normal += g[i];
-  if (kind == 1) {
+  if (kind == 1 || kind == 3) {
     for (int a = 0; a < dim; ++a) u[a] = (REAL)value[a];
     *rho = ((REAL)2 * normal + onWall + (REAL)1) / ((REAL)1 + (REAL)orient * u[dir]);
   } else {
     for (int a = 0; a < dim; ++a) u[a] = (REAL)value[1 + a];
     *rho = (REAL)value[0];
     u[dir] = (REAL)orient * (((REAL)2 * normal + onWall + (REAL)1) / *rho - (REAL)1);
+  }
+}
+
+/* f_i^eq - t_i: equilibrium::secondOrder (src/dynamics/lbm.h) with c.u summed axis by axis. */
+static REAL FN(second_order)(const lbo_desc* d, int i, REAL rho, const REAL* u, REAL uSqr)
+{
+  const REAL invCs2 = (REAL)3;
+  const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+  REAL cu = 0;
+  for (int a = 0; a < d->d; ++a) cu += (REAL)d->c[i][a] * u[a];
+  return rho * t * ((REAL)1 + invCs2 * cu + invCs2 * invCs2 * (REAL)0.5 * cu * cu - invCs2 * (REAL)0.5 * uSqr) - t;
+}
+
+/* The regularisation of a local boundary cell (CombinedRLBdynamics::collide, src/dynamics/
+ * dynamics.h:505-516, before the mixed-in BGK collision): rho and u from the boundary momenta,
+ * Pi from RegularizedBoundaryStress (BoundaryHelpers::computeStress, src/boundary/helper.h:31-81:
+ * f^neq of the populations with c_d = 0 (none for i = 0) and of those with c_d = o, the latter
+ * counted twice), then f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (src/dynamics/lbm.h:247-270). */
+static void FN(local_regularize)(const lbo_desc* d, REAL rho, const REAL* u, const int* nrm, REAL* g)
+{
+  const int q = d->q, dim = d->d;
+  const REAL invCs2 = (REAL)3;
+  int dir = 0, orient = 0;
+  for (int a = dim - 1; a >= 0; --a)
+    if (nrm[a] != 0) { dir = a; orient = nrm[a]; }
+  REAL uSqr = 0;
+  for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+  REAL fneq[27];
+  for (int i = 0; i < q; ++i) fneq[i] = 0;
+  for (int i = 1; i < q; ++i)
+    if (d->c[i][dir] == 0) fneq[i] = g[i] - FN(second_order)(d, i, rho, u, uSqr);
+  for (int i = 0; i < q; ++i)
+    if (d->c[i][dir] == orient) fneq[i] = g[i] - FN(second_order)(d, i, rho, u, uSqr);
+  REAL pi[6];
+  int iPi = 0;
+  for (int a = 0; a < dim; ++a)
+    for (int b = a; b < dim; ++b) {
+      pi[iPi] = 0;
+      for (int i = 0; i < q; ++i)
+        if (d->c[i][dir] == 0) pi[iPi] += (REAL)(d->c[i][a] * d->c[i][b]) * fneq[i];
+      for (int i = 0; i < q; ++i)
+        if (d->c[i][dir] == orient) pi[iPi] += (REAL)(2 * d->c[i][a] * d->c[i][b]) * fneq[i];
+      ++iPi;
+    }
+  for (int i = 0; i < q; ++i) {
+    const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+    REAL fn = 0;
+    iPi = 0;
+    for (int a = 0; a < dim; ++a)
+      for (int b = a; b < dim; ++b) {
+        REAL toAdd = (REAL)(d->c[i][a] * d->c[i][b]);
+        if (a == b) toAdd -= (REAL)1 / invCs2;
+        else toAdd *= (REAL)2;
+        toAdd *= pi[iPi++];
+        fn += toAdd;
+      }
+    fn *= t * invCs2 * invCs2 / (REAL)2;
+    g[i] = FN(second_order)(d, i, rho, u, uSqr) + fn;
   }
 }
 
@@ -317,6 +375,7 @@ static void FN(fd_postprocess)(const lbo_desc* d, const lbo_case* c, STORE_T* f,
       int type, nrm[3];
       FN(fd_meta)(c, b, &type, nrm);
       if ((type == 1) != (pass == 1)) continue;
+      if (c->fd_kind[b] >= 3 && type == 0) continue;  /* local flat cells: no post-processor */
       const int64_t cell = c->fd_cell[b];
       const int64_t pos[3] = {cell / (ny * nz), (cell / nz) % ny, cell % nz};
       REAL g[27], rho, u[3] = {0, 0, 0};
@@ -458,6 +517,11 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
         FN(fd_meta)(c, b, &type, nrm);
         for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
         FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
+        if (c->fd_kind[b] >= 3 && type == 0) {
+          /* local boundary: regularised first, then the BGK collision with the same momenta */
+          FN(local_regularize)(d, rho, u, nrm, g);
+          FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
+        }
         cellUsq[x] = FN(bgk_with)(d, (REAL)c->omega, rho, u, g);
         cellRho[x] = rho;
         for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);

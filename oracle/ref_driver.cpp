@@ -30,7 +30,7 @@
  *    lbref geo --mat FILE --n NX NY [NZ] [--periodic PX PY [PZ]] [--dyn ...] [--omega W] ...
  *          [--bouzidi M,...] [--lid M --ulid U] [--bounceback M,...] [--outside M,...]
  *          [--ivel M,... (--poiseuille UMAX | --uconst UX UY [UZ])] [--ivel-lid M] [--ipres M --rho R]
- *          [--bbvel M]
+ *          [--bbvel M] [--local]
  *          [--classify M] [--classify-only] [--force-mat M --force-every K] [--moments]
  *          [--no-pops] [--steps S] [--out PREFIX]
  *  The geo case reads the int32 materials of the core cells from FILE (x slowest, z fastest)
@@ -44,6 +44,10 @@
  *  --ivel material is RectanglePoiseuille3D over it (one --ivel material) with the zero-velocity
  *  planes half a cell outside it (peak UMAX along +x), or a constant; the --ivel-lid material
  *  moves with (--ulid, 0, 0).  Populations start at rest (all zero) or random (--init random).
+ *  --local sets boundary::LocalVelocity / LocalPressure with BGK as the mixed-in dynamics on the
+ *  --ivel / --ivel-lid / --ipres materials instead (src/boundary/localVelocity3D.h:47-115,
+ *  localPressure3D.h, localVelocity2D.h: CombinedRLBdynamics on flat faces, the interpolated
+ *  boundary's edges and corners).
  *  --classify M writes PREFIX.normals.bin (int32 {core cell, type, n0, n1, n2} per cell of
  *  material M, fluid 1, outside {0, --outside...}); --classify-only stops there.
  *  --force-mat M writes PREFIX.force.txt: "step Fx Fy Fz" every K steps, the sum of
@@ -141,6 +145,7 @@ struct Options {
   long forceEvery = 0;
   double poiseuille = -1.0, uconst[3] = {0, 0, 0}, rhoOut = 1.0;
   bool classifyOnly = false, moments = false, noPops = false;
+  bool local = false;  // --local: LocalVelocity / LocalPressure (BGK mixin) instead of the interpolated ones
 };
 
 std::vector<int> parseList(const char* s) {
@@ -230,6 +235,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--ivel") o.ivelMats = parseList(next());
     else if (a == "--ivel-lid") o.ivelLidMat = std::atoi(next());
     else if (a == "--bbvel") o.bbvelMat = std::atoi(next());
+    else if (a == "--local") o.local = true;
     else if (a == "--ipres") o.ipresMat = std::atoi(next());
     else if (a == "--poiseuille") o.poiseuille = std::atof(next());
     else if (a == "--uconst") { for (int d = 0; d < D; ++d) o.uconst[d] = std::atof(next()); }
@@ -363,13 +369,23 @@ int runGeo(const Options& o) {
   if (o.bbvelMat >= 0) lat.template defineDynamics<BounceBackVelocity>(geo, o.bbvelMat);
   std::vector<int> ivelAll = o.ivelMats;
   if (o.ivelLidMat >= 0) ivelAll.push_back(o.ivelLidMat);
-  for (int m : ivelAll)
-    boundary::set<T, DESCRIPTOR, boundary::InterpolatedVelocity<T,DESCRIPTOR>>(
-      lat, geo.getMaterialIndicator({m}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+  for (int m : ivelAll) {
+    if (o.local)
+      boundary::set<T, DESCRIPTOR, boundary::LocalVelocity<T,DESCRIPTOR,BGKdynamics<T,DESCRIPTOR>>>(
+        lat, geo.getMaterialIndicator({m}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+    else
+      boundary::set<T, DESCRIPTOR, boundary::InterpolatedVelocity<T,DESCRIPTOR>>(
+        lat, geo.getMaterialIndicator({m}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+  }
   auto isIvel = [&](int m) { return std::find(ivelAll.begin(), ivelAll.end(), m) != ivelAll.end(); };
-  if (o.ipresMat >= 0)
-    boundary::set<T, DESCRIPTOR, boundary::InterpolatedPressure<T,DESCRIPTOR>>(
-      lat, geo.getMaterialIndicator({o.ipresMat}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+  if (o.ipresMat >= 0) {
+    if (o.local)
+      boundary::set<T, DESCRIPTOR, boundary::LocalPressure<T,DESCRIPTOR,BGKdynamics<T,DESCRIPTOR>>>(
+        lat, geo.getMaterialIndicator({o.ipresMat}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+    else
+      boundary::set<T, DESCRIPTOR, boundary::InterpolatedPressure<T,DESCRIPTOR>>(
+        lat, geo.getMaterialIndicator({o.ipresMat}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+  }
 
   // the classification boundary::set gave every cell it set up: rows {cell, kind (1 velocity,
   // 2 pressure), type, n0, n1, n2}; pressure cells only where the reference installs a condition

@@ -183,9 +183,26 @@ GEO = {
                                                                         "--rho", "0.99", "--bounceback", "2", "--bouzidi", "5",
                                                                         "--force-mat", "5", "--force-every", "5",
                                                                         *RND, "--steps", "60"]),
+    # boundary::LocalVelocity / LocalPressure with BGK mixed in (cavity3dBenchmark's walls): flat
+    # cells regularised in their collision (CombinedRLBdynamics), edges and corners as for the
+    # interpolated boundary
+    "geo_cavity_d3q19_lvel_bgk_f64": ("d3q19_f64_nocse", (9, 8, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                      "--ivel-lid", "3", "--ulid", "0.05", "--local",
+                                                                      *RND, "--steps", "60"]),
+    "geo_cavity_d2q9_lvel_bgk_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
+                                                                  "--ivel-lid", "3", "--ulid", "0.1", "--local",
+                                                                  "--steps", "150"]),
+    "geo_cavity_d3q27_lvel_trt_f64": ("d3q27_f64_nocse", (8, 9, 7), ["--dyn", "trt", "--omega", "1.6", "--magic",
+                                                                     "0.25", "--ivel", "2", "--ivel-lid", "3",
+                                                                     "--ulid", "0.05", "--local", "--steps", "80"]),
+    "geo_channel_d3q19_lvel_lpres_f64": ("d3q19_f64_nocse", (20, 12, 11), ["--dyn", "bgk", "--omega", "1.3", "--ivel",
+                                                                           "3", "--poiseuille", "0.05", "--ipres", "4",
+                                                                           "--rho", "0.99", "--bounceback", "2",
+                                                                           "--bouzidi", "5", "--local", *RND,
+                                                                           "--steps", "60"]),
 }
 GEO_SPHERE = {"geo_channel_d3q27_trt_f64": (8, 7, 7, 3), "geo_channel_d3q27_trt_f32": (8, 7, 7, 3),
-              "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5)}
+              "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5), "geo_channel_d3q19_lvel_lpres_f64": (6, 5, 6, 2.5)}
 
 
 def geo_material(name: str) -> np.ndarray:

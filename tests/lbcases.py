@@ -155,7 +155,10 @@ def case_setup(fx: dict) -> dict:
         bc = fx["bclass"]
         cd[bc[:, 0]] = 3
         setup["cell_dyn"] = cd
-        setup["fd"] = {"cells": bc[:, 0].astype(np.int64), "kinds": bc[:, 1].astype(np.int32),
+        kinds = bc[:, 1].astype(np.int32)
+        if a["local"]:
+            kinds = kinds + 2  # LocalVelocity / LocalPressure: kinds 3 and 4
+        setup["fd"] = {"cells": bc[:, 0].astype(np.int64), "kinds": kinds,
                        "types": bc[:, 2].astype(np.int32), "normals": np.ascontiguousarray(bc[:, 3:6], np.int32),
                        "values": np.ascontiguousarray(fx["vals"][bc[:, 0]])}
     elif meta["case"] == "channel":
@@ -181,7 +184,7 @@ def geo_args(meta: dict) -> dict:
     lid = value("--lid")
     return {"bouzidi": ints("--bouzidi"), "bounceback": ints("--bounceback"), "ivel": ints("--ivel"),
             "ivel_lid": ints("--ivel-lid"), "ipres": ints("--ipres"), "lid": int(lid) if lid else None,
-            "bbvel": ints("--bbvel"),
+            "bbvel": ints("--bbvel"), "local": "--local" in args,
             "force_mat": ints("--force-mat")}
 
 
@@ -328,8 +331,36 @@ def fluid_mask(fx: dict) -> np.ndarray:
     if fx["meta"]["case"] == "geo":
         m = fx["mat"] == 1
         m[fx["bclass"][:, 0]] = True
+        m[local_flat_cells(fx)] = False
         return m
     return fx["mat"] == 1
+
+
+def local_flat_cells(fx: dict) -> np.ndarray:
+    """Flat cells of a LocalVelocity / LocalPressure boundary.  Their populations entering from
+    beyond the domain are, after a stream, whatever the padding held (in the reference: its
+    storage's leftovers); the next collision rebuilds them from the others, so only the others are
+    compared (known_populations)."""
+    if fx["meta"]["case"] != "geo" or not geo_args(fx["meta"])["local"]:
+        return np.zeros(0, np.int64)
+    bc = fx["bclass"]
+    return bc[bc[:, 2] == 0, 0].astype(np.int64)
+
+
+def known_populations(fx: dict) -> tuple[np.ndarray, np.ndarray]:
+    """(population, cell) index pairs of the local flat cells' populations that do not enter
+    from beyond the domain: c_i . n >= 0 for the outward normal n."""
+    bc = fx["bclass"]
+    q = fx["meta"]["q"]
+    vel = VEL[q]
+    pops, cells = [], []
+    for row in bc[bc[:, 2] == 0]:
+        n = row[3:6]
+        for i in range(q):
+            if int(np.dot(vel[i, :3], n)) >= 0:
+                pops.append(i)
+                cells.append(int(row[0]))
+    return np.asarray(pops, np.int64), np.asarray(cells, np.int64)
 
 
 def counted_cells(fx: dict) -> int:
@@ -339,4 +370,5 @@ def counted_cells(fx: dict) -> int:
     n = int(fluid_mask(fx).sum())
     if fx["meta"]["case"] == "geo":
         n += int(np.isin(fx["mat"], geo_args(fx["meta"])["bbvel"]).sum())
+        n += len(local_flat_cells(fx))
     return n

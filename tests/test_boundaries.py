@@ -32,6 +32,12 @@ def _shape(meta):
     return (int(e[0]), int(e[1])) if meta["q"] == 9 else (int(e[0]), int(e[1]), int(e[2]))
 
 
+def test_local_boundary_fixtures_are_present():
+    local = [n for n in GEO if "_lvel" in n]
+    assert any("d2q9" in n for n in local) and any("d3q19" in n for n in local)
+    assert any("lpres" in n for n in local)
+
+
 def test_geo_fixtures_cover_edges_and_corners():
     kinds = set()
     for name in GEO:
@@ -139,10 +145,11 @@ def build_from_materials(fx, storage):
     if a["bbvel"]:
         cells = np.nonzero(np.isin(mat, a["bbvel"]))[0]
         lat.set_bounce_back_velocity(cells, fx["vals"][cells, 0], fx["vals"][cells, 1:4])
+    vel, pres = (lbx.FD_LOCAL_VELOCITY, lbx.FD_LOCAL_PRESSURE) if a["local"] else (lbx.FD_VELOCITY, lbx.FD_PRESSURE)
     for m in a["ivel"] + a["ivel_lid"]:
-        lat.set_interpolated_boundary(lbx.FD_VELOCITY, mat, m, fx["vals"])
+        lat.set_interpolated_boundary(vel, mat, m, fx["vals"])
     for m in a["ipres"]:
-        lat.set_interpolated_boundary(lbx.FD_PRESSURE, mat, m, fx["vals"])
+        lat.set_interpolated_boundary(pres, mat, m, fx["vals"])
     return lat
 
 
@@ -160,6 +167,10 @@ def test_material_setters_match_the_reference(name):
     assert e["pop"] <= 2e-12, e
     orc, _ = L.run_oracle(setup, fx["f0"], fx["meta"]["steps"])
     assert L.errors(fx["meta"]["q"], out, orc, L.fluid_mask(fx))["pop"] <= 1e-13
+    if len(L.local_flat_cells(fx)):
+        pops, cells = L.known_populations(fx)
+        scale = np.abs(fx["fS"]).max()
+        assert np.abs(out[pops, cells] - np.asarray(fx["fS"])[pops, cells]).max() <= 2e-12 * scale
 
 
 @pytest.mark.gpu

@@ -43,6 +43,11 @@ def test_oracle_matches_reference(name):
     rel = np.abs(stats - ref) / np.maximum(np.abs(ref), 1e-30)
     assert rel[:, 0].max() <= ts  # average rho
     assert rel[:, 2].max() <= max(ts, 1e-9)  # max |u|
+    pops, cells = L.known_populations(fx) if len(L.local_flat_cells(fx)) else (None, None)
+    if pops is not None:
+        # the local flat cells: every population not entering from beyond the domain
+        got, want = out[pops, cells], np.asarray(fx["fS"])[pops, cells]
+        assert np.abs(got - want).max() <= tp * np.abs(fx["fS"]).max()
 
 
 def test_fixture_set_covers_the_hot_path():
