@@ -69,7 +69,10 @@ typedef enum {
   LBX_CELL_BULK = 1,        /* the lattice's bulk dynamics */
   LBX_CELL_BOUNCE_BACK = 2, /* BounceBack = collision::Revert (collision.h:465-484) */
   LBX_CELL_FD_BOUNDARY = 3, /* a cell of the lbx_set_fd_boundaries list (set by that call) */
-  LBX_CELL_BOUNCE_BACK_VELOCITY = 4 /* BounceBackVelocity (set by lbx_set_bounce_back_velocity) */
+  LBX_CELL_BOUNCE_BACK_VELOCITY = 4, /* BounceBackVelocity (set by lbx_set_bounce_back_velocity) */
+  LBX_CELL_BULK_CLASS_1 = 8,  /* the bulk dynamics with the parameters of class 1, 2, 3 */
+  LBX_CELL_BULK_CLASS_2 = 9,  /* (lbx_set_dynamics_class) */
+  LBX_CELL_BULK_CLASS_3 = 10
 } lbx_cell_dynamics;
 
 /* Kinds of velocity / pressure boundary cells (lbx_set_fd_boundaries, lbx_set_boundary_cells,
@@ -134,6 +137,21 @@ int lbx_get_info(lbx_lattice lattice, lbx_info* info);
 /* Select the bulk dynamics and its parameters (BlockDynamicsMap::set + setParameter,
  * core/blockLattice.h:559-576; ConcreteParametersD H2D, gpu/cuda/context.hh:412-467). */
 int lbx_set_dynamics(lbx_lattice lattice, int32_t dynamics, const lbx_params* params);
+
+/* A second (third, fourth) fluid dynamics in one lattice: parameter classes 1..3 of the bulk
+ * dynamics.  A reference block may carry different dynamics per material (dynamics::set,
+ * core/blockDynamicsMap.h:264-310 keeps one collision operator per dynamics type); here the
+ * cells marked LBX_CELL_BULK_CLASS_c in the cell map collide with the lattice's dynamics but
+ * with these parameters (omega, TRT magic, Smagorinsky constant, force).  That covers a block
+ * whose dynamics differ in their parameters, e.g. BGKdynamics beside ForcedBGKdynamics (the
+ * forced dynamics with force 0 in one class) or regions of different viscosity.  A lattice with
+ * classes steps with launch variant 1 (one cell per thread; lbx_set_launch_config refuses the
+ * others and the autotuner tries only its block shapes), and its halfway bounce-back links all
+ * run in the link kernel.  The moments, the residual and the velocity of a class cell seen by a
+ * neighbouring velocity / pressure boundary cell use the lattice's own force.  params = NULL
+ * removes class `cls` (its cells then use the lattice's parameters).  ConstRhoBGK takes no
+ * classes (LBX_ERR_UNSUPPORTED). */
+int lbx_set_dynamics_class(lbx_lattice lattice, int32_t cls, const lbx_params* params);
 
 /* Per-cell dynamics ids for the core cells ([core cells], lbx_cell_dynamics); NULL resets
  * to "bulk everywhere" (defineDynamics over a material, core/blockLattice.hh:274-286). */

@@ -164,6 +164,10 @@ struct lbx_lattice_s {
   void* stage = nullptr;             // ncore doubles
   int dynamics = LBX_BGK;
   lbx_params params{1.0, 0.25, 0.12, {0, 0, 0}};
+  // parameter classes 1..3 of the bulk dynamics (lbx_set_dynamics_class): bit c - 1 set when
+  // class c is defined
+  int classMask = 0;
+  lbx_params classParams[3] = {};
   int blockX = 256, blockY = 1;
   int kernel = 2;
   int cellsPerThread = 1;
@@ -229,6 +233,14 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   const TestFault& tf = test_fault();
   a.waitLimit = (tf.kind == LBX_TEST_BULK_COPY && tf.param > 0) ? tf.param : (1 << 22);
   a.faultBulk = tf.kind == LBX_TEST_BULK_COPY ? 1 : 0;
+  a.classes = L->classMask != 0 ? 1 : 0;
+  for (int c = 0; c < 3; ++c) {  // a class never defined collides with the lattice's own parameters
+    const lbx_params& pc = (L->classMask >> c & 1) ? L->classParams[c] : L->params;
+    a.classParam[c][0] = pc.omega;
+    a.classParam[c][1] = pc.magic;
+    a.classParam[c][2] = pc.smagorinsky;
+    for (int k = 0; k < 3; ++k) a.classParam[c][3 + k] = pc.force[k];
+  }
   return a;
 }
 
@@ -1007,8 +1019,28 @@ int lbx_set_dynamics(lbx_lattice L, int32_t dynamics, const lbx_params* params) 
     return fail(LBX_ERR_INVALID, "Smagorinsky constant must be >= 0");
   for (int k = 0; k < 3; ++k)
     if (!std::isfinite(params->force[k])) return fail(LBX_ERR_INVALID, "force must be finite");
+  if (dynamics == LBX_CONST_RHO_BGK && L->classMask)
+    return fail(LBX_ERR_UNSUPPORTED, "ConstRhoBGK couples every cell to one average density; no classes");
   L->dynamics = dynamics;
   L->params = *params;
+  return LBX_OK;
+}
+
+int lbx_set_dynamics_class(lbx_lattice L, int32_t cls, const lbx_params* params) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (cls < 1 || cls > 3) return fail(LBX_ERR_INVALID, "parameter class must be 1, 2 or 3");
+  if (!params) {
+    L->classMask &= ~(1 << (cls - 1));
+    return LBX_OK;
+  }
+  if (!(params->omega > 0.0 && params->omega < 2.0)) return fail(LBX_ERR_INVALID, "omega must lie in (0, 2)");
+  if (L->dynamics == LBX_CONST_RHO_BGK)
+    return fail(LBX_ERR_UNSUPPORTED, "ConstRhoBGK couples every cell to one average density; no classes");
+  L->classParams[cls - 1] = *params;
+  L->classMask |= 1 << (cls - 1);
+  // the classes run on the one-cell-per-thread step kernel
+  L->kernel = 1;
+  L->cellsPerThread = 1;
   return LBX_OK;
 }
 
@@ -1018,7 +1050,7 @@ int lbx_set_cell_dynamics(lbx_lattice L, const uint8_t* ids) {
   std::vector<uint8_t> padded(static_cast<size_t>(L->n), 0);
   for (int64_t c = 0; c < L->ncore; ++c) {
     const uint8_t id = ids ? ids[c] : uint8_t(LBX_CELL_BULK);
-    if (id > LBX_CELL_FD_BOUNDARY)
+    if (id > LBX_CELL_FD_BOUNDARY && (id < LBX_CELL_BULK_CLASS_1 || id > LBX_CELL_BULK_CLASS_3))
       return fail(LBX_ERR_INVALID, "cell dynamics id out of range (boundary cells are set by their own calls)");
     padded[size_t(core_index_to_padded(L, c))] = id;
   }
@@ -1580,6 +1612,8 @@ int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32
                           int32_t cells_per_thread) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
   if (variant < 0 || variant > 4) return fail(LBX_ERR_INVALID, "variant must be 0, 1, 2, 3 or 4");
+  if (L->classMask && variant != 1)
+    return fail(LBX_ERR_UNSUPPORTED, "a lattice with parameter classes steps with launch variant 1");
   if ((variant == 3 || variant == 4) && (!L->doubled || L->period >= (int64_t(1) << 31)))
     return fail(LBX_ERR_UNSUPPORTED, "variants 3 and 4 (bulk copies) need the doubled column mapping and fewer than 2^31 cells");
   if (variant == 2 && L->period >= (int64_t(1) << 31))
@@ -1610,7 +1644,7 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
   std::vector<Cand> cands;
   const int nf = (L->d == 3) ? L->core[2] : L->core[1];
   const int maxK = storage_bytes(L->storage) == 2 ? 4 : 2;
-  for (int k = 1; k <= maxK; k *= 2)
+  for (int k = 1; k <= maxK && !L->classMask; k *= 2)
     for (int bx = 32; bx <= 256; bx *= 2) {
       if (bx > 32 && bx >= 2 * lbx::k_cells_threads(nf, k)) break;  // wider blocks only idle more threads
       for (int threads = 256; threads >= 128; threads /= 2)
@@ -1620,8 +1654,12 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
     int bx, by;
     block_shape_for(nf, 1, bx, by);
     cands.push_back({1, bx, by, 1});
-    cands.push_back({0, 256, 1, 1});
-    if (L->doubled && L->period < (int64_t(1) << 31)) {
+    if (L->classMask) {  // the classes run on variant 1 only: its block shapes
+      for (int bx1 = 32; bx1 <= 256; bx1 *= 2)
+        if (bx1 != bx) cands.push_back({1, bx1, 256 / bx1, 1});
+    }
+    if (!L->classMask) cands.push_back({0, 256, 1, 1});
+    if (!L->classMask && L->doubled && L->period < (int64_t(1) << 31)) {
       cands.push_back({3, 256, 1, 1});
       cands.push_back({4, 256, 1, 1});
     }

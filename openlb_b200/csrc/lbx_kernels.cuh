@@ -78,7 +78,12 @@ __device__ __forceinline__ int64_t wrap_add(int64_t a, int64_t s, int64_t n) {
 // own kernels after the bulk kernel, which neither loads nor stores them.
 constexpr uint8_t kCellBulkLinked = 7;
 constexpr uint8_t kCellBounceBackVelocity = 4;
-__device__ __forceinline__ bool bulk_kind(uint8_t k) { return k == 1 || k == kCellBulkLinked; }
+// 8, 9, 10: bulk cells colliding with the parameters of class 1, 2, 3 (lbx_set_dynamics_class;
+// stepped by the one-cell-per-thread kernel only, which a lattice with classes always uses)
+constexpr uint8_t kCellClassFirst = 8, kCellClassLast = 10;
+__device__ __forceinline__ bool bulk_kind(uint8_t k) {
+  return k == 1 || k == kCellBulkLinked || (k >= kCellClassFirst && k <= kCellClassLast);
+}
 // the kinds the K-cells step kernel loads, collides and stores itself
 __device__ __forceinline__ bool stepped_kind(uint8_t k) { return bulk_kind(k) || k == 2; }
 
@@ -225,11 +230,25 @@ static __global__ void __launch_bounds__(kFinalizeThreads) k_finalize4(const dou
 // ---- fused collide + PS stream --------------------------------------------------------
 // One thread per core cell; threadIdx.x runs along the fastest core axis (z in 3D, y in 2D)
 // so that every population load and store of a warp is one contiguous run.
+// The parameters of the three classes of a lattice (lbx_set_dynamics_class); `used` is 0 when the
+// lattice has none.
+template <typename R> struct ClassParams {
+  CollisionParams<R> p[3];
+  int used;
+};
+// Class c's parameters by value selects (no indexing into the parameter space).
+template <typename R>
+__device__ __forceinline__ CollisionParams<R> class_params(const ClassParams<R>& cls, int c) {
+  CollisionParams<R> r = c == 0 ? cls.p[0] : (c == 1 ? cls.p[1] : cls.p[2]);
+  return r;
+}
+
 template <int Q, typename S, int DYN>
 __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geometry g, Shifts<Q> sh,
                                                         CollisionParams<typename Storage<S>::R> p,
                                                         const uint8_t* __restrict__ cellDyn,
-                                                        double* __restrict__ statPart) {
+                                                        double* __restrict__ statPart,
+                                                        ClassParams<typename Storage<S>::R> cls) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   int x, y, z;
@@ -256,7 +275,12 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
       static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(n, sh.s[I], g.n)); });
     }
     if (bulk_kind(kind)) {
-      collide<Q, R, DYN>(f, p, rho, usq);
+      if (cls.used && kind >= kCellClassFirst) {
+        const CollisionParams<R> pc = class_params(cls, int(kind) - kCellClassFirst);
+        collide<Q, R, DYN>(f, pc, rho, usq);
+      } else {
+        collide<Q, R, DYN>(f, p, rho, usq);
+      }
       valid = true;
     } else if (kind == 2) {
       revert<Q, R>(f);
@@ -1993,6 +2017,8 @@ struct LaunchArgs {
   const uint8_t* cellDyn;
   StatAcc* stats;       // statistics of this step requested: totals land here
   const StatAcc* avgSrc;  // ConstRhoBGK: statistics of the previous step (average density)
+  int classes;              // parameter classes in use (then the step runs kernel 1)
+  double classParam[3][6];  // per class: omega, magic, smagorinsky, force[3]
   double* statPart;     // block partials of the statistics (4 doubles per block)
   int64_t statCapacity; // blocks statPart can hold
   int blockX, blockY;
@@ -2176,7 +2202,17 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     else grid = dim3((g.ny + a.blockX - 1) / a.blockX, (g.nx + a.blockY - 1) / a.blockY, 1);
     nblocks = int64_t(grid.x) * grid.y * grid.z;
     if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
-    k_collide_stream<Q, S, DYN><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats ? a.statPart : nullptr);
+    ClassParams<R> cls;
+    cls.used = a.classes;
+    for (int c = 0; c < 3; ++c) {
+      cls.p[c] = p;
+      cls.p[c].omega = R(a.classParam[c][0]);
+      cls.p[c].magic = R(a.classParam[c][1]);
+      cls.p[c].smagorinsky = R(a.classParam[c][2]);
+      for (int k = 0; k < 3; ++k) cls.p[c].force[k] = R(a.classParam[c][3 + k]);
+    }
+    k_collide_stream<Q, S, DYN><<<grid, block, 0, stream>>>(pop, g, sh, p, a.cellDyn, a.stats ? a.statPart : nullptr,
+                                                            cls);
   } else {
     ColumnBases<Q> cols;
     for (int i = 0; i < Q; ++i) {

@@ -29,6 +29,7 @@ STORAGE_BYTES = {"f64": 8, "f32": 4, "f16dev": 2, "bf16dev": 2}
 DYNAMICS = {"bgk": 1, "trt": 2, "smagorinsky_bgk": 3, "forced_bgk": 4, "smagorinsky_forced_bgk": 5,
             "const_rho_bgk": 6}
 CELL_NONE, CELL_BULK, CELL_BOUNCE_BACK, CELL_FD_BOUNDARY, CELL_BOUNCE_BACK_VELOCITY = 0, 1, 2, 3, 4
+CELL_BULK_CLASS_1, CELL_BULK_CLASS_2, CELL_BULK_CLASS_3 = 8, 9, 10
 STEP_STATISTICS = 1
 REDUCE_MASS_MOMENTUM, REDUCE_DRAG, REDUCE_RESIDUAL = 1, 2, 3
 
@@ -118,6 +119,7 @@ def _load() -> C.CDLL:
         "lbx_get_info": ([VP, P(Info)], C.c_int),
         "lbx_set_dynamics": ([VP, I32, P(Params)], C.c_int),
         "lbx_set_cell_dynamics": ([VP, VP], C.c_int),
+        "lbx_set_dynamics_class": ([VP, I32, P(Params)], C.c_int),
         "lbx_set_bouzidi_links": ([VP, I64, VP, VP, VP], C.c_int),
         "lbx_set_bouzidi_from_materials": ([VP, VP, I32, I32, VP, VP], C.c_int),
         "lbx_build_bouzidi_links": ([I32, P(I32), P(I32), VP, I32, I32, VP, VP, I64, VP, VP, VP, P(I64)], C.c_int),
@@ -364,6 +366,25 @@ class BlockLattice:
         """setParameter<OMEGA | TRT::MAGIC | LES::SMAGORINSKY | FORCE>."""
         key = {"omega": "omega", "magic": "magic", "smagorinsky": "smagorinsky", "force": "force"}[name.lower()]
         self.define_dynamics(self._dyn, **{key: value})
+
+    def set_dynamics_class(self, cls: int, omega: float | None = None, magic: float | None = None,
+                           smagorinsky: float | None = None, force=None, remove: bool = False) -> None:
+        """Parameters of class `cls` (1..3) of the bulk dynamics (lbx_set_dynamics_class): cells
+        marked CELL_BULK_CLASS_<cls> collide with them; unspecified values are the lattice's."""
+        if remove:
+            check(lib.lbx_set_dynamics_class(self._h, cls, None), "lbx_set_dynamics_class")
+            return
+        p = Params(self._params.omega, self._params.magic, self._params.smagorinsky,
+                   (C.c_double * 3)(*self._params.force))
+        if omega is not None:
+            p.omega = omega
+        if magic is not None:
+            p.magic = magic
+        if smagorinsky is not None:
+            p.smagorinsky = smagorinsky
+        if force is not None:
+            p.force = (C.c_double * 3)(*(list(force) + [0.0] * 3)[:3])
+        check(lib.lbx_set_dynamics_class(self._h, cls, C.byref(p)), "lbx_set_dynamics_class")
 
     def set_cell_dynamics(self, ids: np.ndarray | None) -> None:
         if ids is None:

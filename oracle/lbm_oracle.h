@@ -34,7 +34,13 @@ enum lbo_material {
   LBO_FLUID = 1,      /* the case's bulk dynamics */
   LBO_BOUNCE_BACK = 4,/* BounceBack = collision::Revert (collision.h:465-484) */
   LBO_FD_BOUNDARY = 5, /* velocity / pressure boundary cell: BGK with boundary momenta (fd_* below) */
-  LBO_BOUNCE_BACK_VELOCITY = 6 /* BounceBackVelocity (dynamics.h:629-637): bbv_value below */
+  LBO_BOUNCE_BACK_VELOCITY = 6, /* BounceBackVelocity (dynamics.h:629-637): bbv_value below */
+  /* the case's bulk dynamics with the parameters of class 1, 2 or 3 (class_params below): a
+   * second fluid dynamics of the same kind in one block, e.g. BGK beside ForcedBGK (class force
+   * 0) as dynamics::set gives them per material */
+  LBO_FLUID_CLASS_1 = 8,
+  LBO_FLUID_CLASS_2 = 9,
+  LBO_FLUID_CLASS_3 = 10
 };
 
 typedef struct {
@@ -70,6 +76,9 @@ typedef struct {
   const int32_t* fd_normal;
   /* {rho, u_x, u_y, u_z} per cell (all cells; read for the LBO_BOUNCE_BACK_VELOCITY ones) */
   const double* bbv_value;
+  /* {omega, magic, smagorinsky, force_x, force_y, force_z} of classes 1..3 (read for the
+   * LBO_FLUID_CLASS_* cells) */
+  const double* class_params;
 } lbo_case;
 
 /* Run `steps` collide-and-stream steps in place.  stats (may be NULL) receives per step

@@ -503,10 +503,18 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
       const int m = c->material ? c->material[x] : LBO_FLUID;
       cellRho[x] = (REAL)-1;
       cellUsq[x] = (REAL)-1;
-      if (m == LBO_FLUID) {
+      if (m == LBO_FLUID || (m >= LBO_FLUID_CLASS_1 && m <= LBO_FLUID_CLASS_3 && c->class_params)) {
+        lbo_case cc = *c;
+        if (m != LBO_FLUID) {
+          const double* cp = c->class_params + 6 * (m - LBO_FLUID_CLASS_1);
+          cc.omega = cp[0];
+          cc.magic = cp[1];
+          cc.smagorinsky = cp[2];
+          for (int a = 0; a < 3; ++a) cc.force[a] = cp[3 + a];
+        }
         REAL g[27];
         for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
-        FN(collide)(d, c, g, avgRho, &cellRho[x], &cellUsq[x]);
+        FN(collide)(d, &cc, g, avgRho, &cellRho[x], &cellUsq[x]);
         for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);
       } else if (m == LBO_FD_BOUNDARY && fdIndex[x] >= 0) {
         /* BGKdynamics with the boundary momenta exchanged in (collision::BGK::apply,

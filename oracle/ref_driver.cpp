@@ -30,7 +30,7 @@
  *    lbref geo --mat FILE --n NX NY [NZ] [--periodic PX PY [PZ]] [--dyn ...] [--omega W] ...
  *          [--bouzidi M,...] [--lid M --ulid U] [--bounceback M,...] [--outside M,...]
  *          [--ivel M,... (--poiseuille UMAX | --uconst UX UY [UZ])] [--ivel-lid M] [--ipres M --rho R]
- *          [--bbvel M] [--local]
+ *          [--bbvel M] [--local] [--bgk-mat M]
  *          [--classify M] [--classify-only] [--force-mat M --force-every K] [--moments]
  *          [--no-pops] [--steps S] [--out PREFIX]
  *  The geo case reads the int32 materials of the core cells from FILE (x slowest, z fastest)
@@ -48,6 +48,7 @@
  *  --ivel / --ivel-lid / --ipres materials instead (src/boundary/localVelocity3D.h:47-115,
  *  localPressure3D.h, localVelocity2D.h: CombinedRLBdynamics on flat faces, the interpolated
  *  boundary's edges and corners).
+ *  --bgk-mat M puts BGKdynamics on material M beside the --dyn dynamics of material 1.
  *  --classify M writes PREFIX.normals.bin (int32 {core cell, type, n0, n1, n2} per cell of
  *  material M, fluid 1, outside {0, --outside...}); --classify-only stops there.
  *  --force-mat M writes PREFIX.force.txt: "step Fx Fy Fz" every K steps, the sum of
@@ -146,6 +147,7 @@ struct Options {
   double poiseuille = -1.0, uconst[3] = {0, 0, 0}, rhoOut = 1.0;
   bool classifyOnly = false, moments = false, noPops = false;
   bool local = false;  // --local: LocalVelocity / LocalPressure (BGK mixin) instead of the interpolated ones
+  int bgkMat = -1;     // --bgk-mat M: BGKdynamics on material M beside the --dyn dynamics on material 1
 };
 
 std::vector<int> parseList(const char* s) {
@@ -236,6 +238,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--ivel-lid") o.ivelLidMat = std::atoi(next());
     else if (a == "--bbvel") o.bbvelMat = std::atoi(next());
     else if (a == "--local") o.local = true;
+    else if (a == "--bgk-mat") o.bgkMat = std::atoi(next());
     else if (a == "--ipres") o.ipresMat = std::atoi(next());
     else if (a == "--poiseuille") o.poiseuille = std::atof(next());
     else if (a == "--uconst") { for (int d = 0; d < D; ++d) o.uconst[d] = std::atof(next()); }
@@ -350,6 +353,9 @@ int runGeo(const Options& o) {
   else if (o.dyn == "fsmag") defineFluid<SmagorinskyForcedBGKdynamics<T,DESCRIPTOR>>(lat, geo);
 #endif
   else { std::fprintf(stderr, "unsupported --dyn %s\n", o.dyn.c_str()); return 2; }
+  // a second fluid dynamics on one material (a block with two dynamics, as an application sets
+  // them per material with dynamics::set)
+  if (o.bgkMat >= 0) lat.template defineDynamics<BGKdynamics<T,DESCRIPTOR>>(geo, o.bgkMat);
 
   Nowhere<D> nowhere;
   if (o.lidMat >= 0) {
@@ -437,7 +443,7 @@ int runGeo(const Options& o) {
         cell.template setField<FORCE>(fv);
       }
 #endif
-      if (o.init == "random" && (mat[c] == 1 || isIvel(mat[c]) || mat[c] == o.ipresMat)) {
+      if (o.init == "random" && (mat[c] == 1 || isIvel(mat[c]) || mat[c] == o.ipresMat || mat[c] == o.bgkMat)) {
         T rho = T(1.0 + o.amp * (unit(o.seed, c, 60) - 0.5));
         T u[D] = {};
         for (int d = 0; d < D; ++d) u[d] = T(o.u0 * (unit(o.seed, c, 61 + d) - 0.5));

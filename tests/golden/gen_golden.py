@@ -124,6 +124,15 @@ def geo_box(shape, lid=True):
     return mat
 
 
+def geo_two_dynamics(shape):
+    """A periodic box of fluid (material 1) with a block in its middle of material 6, which
+    carries a second fluid dynamics (--bgk-mat 6)."""
+    mat = np.ones(shape, np.int32)
+    inner = tuple(slice(s // 3, s - s // 3) for s in shape)
+    mat[inner] = 6
+    return mat
+
+
 def geo_channel(shape, sphere):
     """The channel past a sphere of the full-size configuration (openlb_b200.configs.
     channel_materials) at a reduced size: sphere = (centre x, y, z, radius)."""
@@ -200,6 +209,13 @@ GEO = {
                                                                            "--rho", "0.99", "--bounceback", "2",
                                                                            "--bouzidi", "5", "--local", *RND,
                                                                            "--steps", "60"]),
+    # two fluid dynamics in one block: ForcedBGK on material 1 and BGK on material 6 (periodic)
+    "geo_two_dyn_d3q19_fbgk_bgk_f64": ("d3q19_f64_nocse", (12, 10, 9), ["--dyn", "fbgk", "--omega", "1.3", "--force",
+                                                                        "1e-4", "2e-5", "0", "--periodic", "1", "1",
+                                                                        "1", "--bgk-mat", "6", *RND, "--steps", "40"]),
+    "geo_two_dyn_d2q9_fbgk_bgk_f64": ("d2q9_f64_nocse", (16, 14), ["--dyn", "fbgk", "--omega", "1.6", "--force",
+                                                                   "1e-4", "-3e-5", "--periodic", "1", "1",
+                                                                   "--bgk-mat", "6", *RND, "--steps", "60"]),
 }
 GEO_SPHERE = {"geo_channel_d3q27_trt_f64": (8, 7, 7, 3), "geo_channel_d3q27_trt_f32": (8, 7, 7, 3),
               "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5), "geo_channel_d3q19_lvel_lpres_f64": (6, 5, 6, 2.5)}
@@ -209,6 +225,8 @@ def geo_material(name: str) -> np.ndarray:
     shape = GEO[name][1]
     if name in GEO_SPHERE:
         return geo_channel(shape, GEO_SPHERE[name])
+    if "_two_dyn_" in name:
+        return geo_two_dynamics(shape)
     return geo_box(shape)
 
 

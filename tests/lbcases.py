@@ -148,11 +148,17 @@ def case_setup(fx: dict) -> dict:
             setup["links"] = bouzidi_links(q, core, mat3, 1, solid, walls if a["lid"] is not None else None, per)
         for m in a["bbvel"]:
             cd[mat == m] = 4
+        if a["bgk_mat"] is not None:
+            # the second fluid dynamics: BGK beside ForcedBGK is the forced dynamics with a zero
+            # force, parameter class 1 (cell id 8)
+            cd[mat == a["bgk_mat"]] = 8
+            setup["classes"] = {1: {"omega": meta["omega"], "magic": meta["magic"], "cs": meta["cs"],
+                                    "force": [0.0, 0.0, 0.0]}}
         if a["bbvel"]:
             cells = np.nonzero(np.isin(mat, a["bbvel"]))[0].astype(np.int64)
             setup["bbv"] = {"cells": cells, "rho": np.ascontiguousarray(fx["vals"][cells, 0]),
                             "u": np.ascontiguousarray(fx["vals"][cells, 1:4])}
-        bc = fx["bclass"]
+        bc = fx["bclass"] if "bclass" in fx else np.zeros((0, 6), np.int32)
         cd[bc[:, 0]] = 3
         setup["cell_dyn"] = cd
         kinds = bc[:, 1].astype(np.int32)
@@ -185,6 +191,7 @@ def geo_args(meta: dict) -> dict:
     return {"bouzidi": ints("--bouzidi"), "bounceback": ints("--bounceback"), "ivel": ints("--ivel"),
             "ivel_lid": ints("--ivel-lid"), "ipres": ints("--ipres"), "lid": int(lid) if lid else None,
             "bbvel": ints("--bbvel"), "local": "--local" in args,
+            "bgk_mat": int(value("--bgk-mat")) if value("--bgk-mat") else None,
             "force_mat": ints("--force-mat")}
 
 
@@ -206,7 +213,7 @@ class _Case(C.Structure):
                 ("link_wall", C.c_void_p), ("n_fd", C.c_int64), ("fd_cell", C.c_void_p),
                 ("fd_kind", C.c_void_p), ("fd_dir", C.c_void_p), ("fd_orient", C.c_void_p),
                 ("fd_value", C.c_void_p), ("fd_type", C.c_void_p), ("fd_normal", C.c_void_p),
-                ("bbv_value", C.c_void_p)]
+                ("bbv_value", C.c_void_p), ("class_params", C.c_void_p)]
 
 
 _oracle = None
@@ -249,7 +256,8 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
     c.force = (C.c_double * 3)(*(list(setup["force"]) + [0.0] * 3)[:3])
     if setup["cell_dyn"] is not None:
         cd = setup["cell_dyn"]
-        m = np.select([cd == 1, cd == 2, cd == 3, cd == 4], [1, 4, 5, 6], 0).astype(np.int32)
+        m = np.select([cd == 1, cd == 2, cd == 3, cd == 4, cd == 8, cd == 9, cd == 10], [1, 4, 5, 6, 8, 9, 10],
+                      0).astype(np.int32)
         keep.append(m)
         c.material = m.ctypes.data
     if setup.get("fd") is not None:
@@ -272,6 +280,12 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
         bv[b["cells"], 1:4] = b["u"]
         keep.append(bv)
         c.bbv_value = bv.ctypes.data
+    if setup.get("classes"):
+        cp = np.zeros((3, 6))
+        for k, prm in setup["classes"].items():
+            cp[k - 1] = [prm["omega"], prm["magic"], prm["cs"], *list(prm["force"])[:3]]
+        keep.append(cp)
+        c.class_params = cp.ctypes.data
     if setup["links"] is not None:
         cells, dirs, wall = (np.ascontiguousarray(a) for a in setup["links"])
         keep += [cells, dirs, wall]
@@ -330,7 +344,11 @@ def fluid_mask(fx: dict) -> np.ndarray:
         return np.isin(fx["mat"], (1, 3, 4))
     if fx["meta"]["case"] == "geo":
         m = fx["mat"] == 1
-        m[fx["bclass"][:, 0]] = True
+        bgk = geo_args(fx["meta"])["bgk_mat"]
+        if bgk is not None:
+            m |= fx["mat"] == bgk
+        if "bclass" in fx:
+            m[fx["bclass"][:, 0]] = True
         m[local_flat_cells(fx)] = False
         return m
     return fx["mat"] == 1

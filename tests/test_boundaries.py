@@ -134,6 +134,9 @@ def build_from_materials(fx, storage):
     cd = np.where(mat == 1, 1, 0).astype(np.uint8)
     for m in a["bounceback"]:
         cd[mat == m] = 2
+    if a["bgk_mat"] is not None:  # BGK beside ForcedBGK: the forced dynamics with force 0
+        lat.set_dynamics_class(1, force=(0.0, 0.0, 0.0))
+        cd[mat == a["bgk_mat"]] = lbx.CELL_BULK_CLASS_1
     lat.set_cell_dynamics(cd)
     solid = list(a["bouzidi"]) + ([a["lid"]] if a["lid"] is not None else [])
     if solid:

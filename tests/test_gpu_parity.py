@@ -27,10 +27,12 @@ def make_lattice(setup: dict, storage: str) -> lbx.BlockLattice:
     lat = lbx.BlockLattice(setup["q"], setup["core"], setup["periodic"], storage)
     lat.define_dynamics(L.GPU_DYN[setup["dyn"]], omega=setup["omega"], magic=setup["magic"],
                         smagorinsky=setup["cs"], force=setup["force"])
+    for k, prm in (setup.get("classes") or {}).items():
+        lat.set_dynamics_class(k, omega=prm["omega"], magic=prm["magic"], smagorinsky=prm["cs"], force=prm["force"])
     if setup["cell_dyn"] is not None:
         # boundary cells (ids 3 and 4) are marked by their own setters below
         cd = setup["cell_dyn"]
-        lat.set_cell_dynamics(np.where(cd >= 3, 0, cd).astype(np.uint8))
+        lat.set_cell_dynamics(np.where((cd == 3) | (cd == 4), 0, cd).astype(np.uint8))
     if setup["links"] is not None:
         lat.set_bouzidi_links(*setup["links"])
     if setup.get("bbv") is not None:
