@@ -139,6 +139,9 @@ struct lbx_lattice_s {
   uint32_t* bbvCell = nullptr;
   double* bbvValue = nullptr;
   std::vector<uint32_t> bbvHostCells;
+  // per padded cell: its index in the boundary list (>= 0), -2 - its index in the bounce-back
+  // velocity list, or -1 (the boundary kernels' neighbour lookups); null without such cells
+  int32_t* bIdx = nullptr;
   uint32_t* linkMask = nullptr;
   uint32_t* restCell = nullptr;
   uint8_t* restDir = nullptr;
@@ -229,6 +232,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.nBbv = L->nBbv;
   a.bbvCell = L->bbvCell;
   a.bbvValue = L->bbvValue;
+  a.bIdx = L->bIdx;
   a.err = L->devErr;
   const TestFault& tf = test_fault();
   a.waitLimit = (tf.kind == LBX_TEST_BULK_COPY && tf.param > 0) ? tf.param : (1 << 22);
@@ -555,8 +559,22 @@ bool device_ok(int device, std::string& why) {
 // from a bulk cell (x_b, k) towards a cell without dynamics, at rest (no wall term), is fused
 // into the K-cells step kernel (bit k of linkMask[x_b], x_b marked kCellBulkLinked); every other
 // link stays with the link kernel, which with the other kernel variants applies all links.
+// The per-cell boundary index (lbx_lattice_s::bIdx) from the two boundary lists.
+int refresh_boundary_index(lbx_lattice_s* L) {
+  cudaFree(L->bIdx);
+  L->bIdx = nullptr;
+  if (L->fdHostCells.empty() && L->bbvHostCells.empty()) return LBX_OK;
+  std::vector<int32_t> idx(static_cast<size_t>(L->n), -1);
+  for (size_t j = 0; j < L->fdHostCells.size(); ++j) idx[L->fdHostCells[j]] = int32_t(j);
+  for (size_t j = 0; j < L->bbvHostCells.size(); ++j) idx[L->bbvHostCells[j]] = -2 - int32_t(j);
+  LBX_CUDA_TRY(cudaMalloc(&L->bIdx, idx.size() * sizeof(int32_t)));
+  LBX_CUDA_TRY(cudaMemcpy(L->bIdx, idx.data(), idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  return LBX_OK;
+}
+
 int refresh_cell_map(lbx_lattice_s* L) {
   ++L->mapVersion;
+  if (int rc = refresh_boundary_index(L)) return rc;
   const bool need = !L->hostMap.empty() || L->nLinks > 0;
   cudaFree(L->linkMask);
   cudaFree(L->restCell);
@@ -972,6 +990,7 @@ int lbx_lattice_destroy(lbx_lattice L) {
   cudaFree(L->restCell);
   cudaFree(L->restDir);
   cudaFree(L->restDelta);
+  cudaFree(L->bIdx);
   cudaFree(L->bbvCell);
   cudaFree(L->bbvValue);
   cudaFree(L->fdCell);

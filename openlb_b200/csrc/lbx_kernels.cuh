@@ -1637,19 +1637,6 @@ __global__ void __launch_bounds__(256) k_fd_momenta(const S* __restrict__ pop, G
   out[6] = double(rho);
 }
 
-// Index of padded cell n in the ascending boundary list, or -1.
-__device__ __forceinline__ int64_t fd_find(const uint32_t* __restrict__ fdCell, int64_t nFd, uint32_t n) {
-  int64_t lo = 0, hi = nFd - 1;
-  while (lo <= hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    const uint32_t v = fdCell[mid];
-    if (v == n) return mid;
-    if (v < n) lo = mid + 1;
-    else hi = mid - 1;
-  }
-  return -1;
-}
-
 // Post-stream passes 2 and 3: the regularised populations f_i = f_i^eq(rho, u) +
 // fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270) with Pi = -rho / (c_s^-2 omega) (grad u + grad u^T)
 // of every boundary cell.  Velocity gradients by fd::DirectedGradients (utilities/
@@ -1677,7 +1664,8 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
                                                        const uint8_t* __restrict__ cellDyn, double hfx, double hfy,
                                                        double hfz, const double* __restrict__ fdMom, int corners,
                                                        int64_t nBbv, const uint32_t* __restrict__ bbvCell,
-                                                       const double* __restrict__ bbvValue) {
+                                                       const double* __restrict__ bbvValue,
+                                                       const int32_t* __restrict__ bIdx) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -1700,7 +1688,8 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
   };
   auto velocity_at = [&](const int (&p)[3], bool wrapped, R (&v)[3]) {
     const int64_t nn = padded_of(p);
-    const int64_t j = fd_find(fdCell, nFd, uint32_t(nn));
+    const int32_t bi = bIdx[nn];  // the cell's boundary-list entry (see lbx_lattice_s::bIdx)
+    const int64_t j = bi >= 0 ? bi : -1;
     if (j >= 0) {
       const double* mm = fdMom + 7 * j + (wrapped ? 3 : 0);
       v[0] = R(mm[0]);
@@ -1714,7 +1703,7 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
       load_cell(nn, f);
       bulk_velocity<Q, R>(f, halfF, v);
     } else if (kind == kCellBounceBackVelocity) {  // FixedVelocityMomentum: the wall velocity
-      const int64_t jb = fd_find(bbvCell, nBbv, uint32_t(nn));
+      const int64_t jb = bi <= -2 ? int64_t(-2 - bi) : -1;
       v[0] = v[1] = v[2] = R(0);
       if (jb >= 0)
         for (int a = 0; a < D::d; ++a) v[a] = R(bbvValue[4 * jb + 1 + a]);
@@ -1724,7 +1713,8 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
   };
   auto rho_at = [&](const int (&p)[3]) -> R {
     const int64_t nn = padded_of(p);
-    const int64_t j = fd_find(fdCell, nFd, uint32_t(nn));
+    const int32_t bi = bIdx[nn];
+    const int64_t j = bi >= 0 ? bi : -1;
     if (j >= 0) {
       if (!corners) return R(fdMom[7 * j + 6]);
       R f[Q], r, v[3];
@@ -1734,7 +1724,7 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
     }
     const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
     if (kind == kCellBounceBackVelocity) {  // FixedDensity
-      const int64_t jb = fd_find(bbvCell, nBbv, uint32_t(nn));
+      const int64_t jb = bi <= -2 ? int64_t(-2 - bi) : -1;
       return jb >= 0 ? R(bbvValue[4 * jb]) : R(1);
     }
     if (!bulk_kind(kind)) return R(1);
@@ -2017,6 +2007,7 @@ struct LaunchArgs {
   const uint8_t* cellDyn;
   StatAcc* stats;       // statistics of this step requested: totals land here
   const StatAcc* avgSrc;  // ConstRhoBGK: statistics of the previous step (average density)
+  const int32_t* bIdx;      // per padded cell: boundary-list entry (lbx_lattice_s::bIdx)
   int classes;              // parameter classes in use (then the step runs kernel 1)
   double classParam[3][6];  // per class: omega, magic, smagorinsky, force[3]
   double* statPart;     // block partials of the statistics (4 doubles per block)
@@ -2298,7 +2289,7 @@ cudaError_t launch_fd_boundary(const LaunchArgs& a, cudaStream_t stream) {
   for (int corners = 0; corners < (a.nFdCorners > 0 ? 2 : 1); ++corners) {
     k_fd_regularize<Q, S><<<blocks, 256, 0, stream>>>(pop, a.g, sh, a.omega, a.nFd, a.fdCell, a.fdMeta, a.fdValue,
                                                       a.cellDyn, hf[0], hf[1], hf[2], a.fdMom, corners, a.nBbv,
-                                                      a.bbvCell, a.bbvValue);
+                                                      a.bbvCell, a.bbvValue, a.bIdx);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
