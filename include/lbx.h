@@ -5,7 +5,7 @@
  * (paths relative to the reference project).  Conventions:
  *   - every function returns LBX_OK (0) or a negative lbx_status; lbx_last_error() gives a
  *     thread-local message.  Nothing throws across the ABI.  The reference's CUDA platform
- *     turns a failed call into std::runtime_error (gpu/cuda/device.hh:48-53); the C++ host
+ *     turns a failed call into std::runtime_error (core/platform/gpu/cuda/device.hh:48-53); the C++ host
  *     layer above this ABI does the same.
  *   - device memory is owned by the lattice handle; host buffers are caller-owned and only
  *     used during the call.
@@ -125,7 +125,7 @@ int lbx_abi_version(void);
 int lbx_device_count(void);
 
 /* Create a block lattice of `core` cells (ConcreteBlockLattice ctor, core/blockLattice.h:462;
- * population storage ImplementationOf<AbstractCyclicColumn>, gpu/cuda/column.h:100-171).
+ * population storage ImplementationOf<AbstractCyclicColumn>, core/platform/gpu/cuda/column.h:100-171).
  * periodic[3] flags make the block periodic along that axis (CuboidDecomposition::
  * setPeriodicity, geometry/cuboidDecomposition.hh:182 plus the PostCollide overlap copy,
  * core/superLattice.hh:150-155).  Populations start at 0 (= rest equilibrium at rho = 1). */
@@ -135,7 +135,7 @@ int lbx_lattice_destroy(lbx_lattice lattice);
 int lbx_get_info(lbx_lattice lattice, lbx_info* info);
 
 /* Select the bulk dynamics and its parameters (BlockDynamicsMap::set + setParameter,
- * core/blockLattice.h:559-576; ConcreteParametersD H2D, gpu/cuda/context.hh:412-467). */
+ * core/blockLattice.h:559-576; ConcreteParametersD H2D, core/platform/gpu/cuda/context.hh:412-467). */
 int lbx_set_dynamics(lbx_lattice lattice, int32_t dynamics, const lbx_params* params);
 
 /* A second (third, fourth) fluid dynamics in one lattice: parameter classes 1..3 of the bulk
@@ -285,13 +285,13 @@ int lbx_build_bouzidi_links(int32_t q, const int32_t core[3], const int32_t peri
 
 /* Populations of the core cells, host layout [q][core cells] of doubles (host_type 0) or
  * floats (host_type 1), f_i - w_i.  The Simulation/Evaluation context switches of the
- * population columns (gpu/cuda/column.hh:285-296), restricted to the core cells. */
+ * population columns (core/platform/gpu/cuda/column.hh:285-296), restricted to the core cells. */
 int lbx_upload_populations(lbx_lattice lattice, const void* host, int32_t host_type, void* stream);
 int lbx_download_populations(lbx_lattice lattice, void* host, int32_t host_type, void* stream);
 
 /* Checkpoint and resume (SuperLattice::save / load into a buffer, core/serializer.h:77-79 and
  * 187-189; a CUDA column serialises its data with its periodic-shift offset,
- * gpu/cuda/column.hh:305-321).  A checkpoint is a host buffer of lbx_checkpoint_bytes bytes: a
+ * core/platform/gpu/cuda/column.hh:305-321).  A checkpoint is a host buffer of lbx_checkpoint_bytes bytes: a
  * 128-byte header (format tag, descriptor, storage form, core extent, periodic axes, the
  * statistics of the last statistics step) followed by the core cells' populations in the
  * layout of lbx_download_populations, FP64 for the FP64 form and FP32 for the others, which is
@@ -314,7 +314,7 @@ int lbx_ini_equilibrium(lbx_lattice lattice, const double* rho, const double* u,
  * periodic overlap copy, the periodic-shift rotation of every population column
  * (ConcreteBlockLattice::stream, core/blockLattice.hh:316-338) and the PostStream
  * bounce-back links.  With LBX_STEP_STATISTICS the last step also accumulates the lattice
- * statistics (StatisticsPostProcessor, gpu/cuda/statistics.hh:80-117) in FP64. */
+ * statistics (StatisticsPostProcessor, core/platform/gpu/cuda/statistics.hh:80-117) in FP64. */
 #define LBX_STEP_STATISTICS 1u
 int lbx_collide_and_stream(lbx_lattice lattice, int64_t steps, uint32_t flags, void* stream);
 
@@ -359,12 +359,12 @@ int lbx_boundary_force(lbx_lattice lattice, int32_t group, double out[3], void* 
 
 /* Periodic-shift bookkeeping for a platform that keeps the reference's split collide /
  * stream calls: the device base of population column i at the current shift
- * (CyclicColumn::operator[] / deviceData, gpu/cuda/column.h:100-171) and a column rotation
- * by `offset` cells (CyclicColumn::rotate, gpu/cuda/column.h:144-154). */
+ * (CyclicColumn::operator[] / deviceData, core/platform/gpu/cuda/column.h:100-171) and a column rotation
+ * by `offset` cells (CyclicColumn::rotate, core/platform/gpu/cuda/column.h:144-154). */
 int lbx_population_shift(lbx_lattice lattice, int32_t pop, int64_t* shift);
 /* Device address of population column `pop` for code outside this library that works on the
  * populations in place (ConcreteBlockLattice::getPopulationPointers, core/blockLattice.h:134,
- * 676-681; CyclicColumn::deviceData, gpu/cuda/column.h:100-171).  Population i of padded cell n
+ * 676-681; CyclicColumn::deviceData, core/platform/gpu/cuda/column.h:100-171).  Population i of padded cell n
  * (n = (x + 1) * padded[1] * padded[2] + (y + 1) * padded[2] + z + 1 in 3D, see lbx_info) is at
  * ((S*)*ptr)[(n + *shift) % column_period], S the storage type.  With the columns mapped twice
  * (the default layout) *shift is 0 and the index needs no wrap; a plain layout returns the
@@ -375,7 +375,7 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
 
 /* Launch configuration of the step kernel, the knob the autotuner turns (no reference
  * counterpart; the reference's CUDA platform launches fixed 32-thread blocks,
- * gpu/cuda/operator.hh:425-441).  variant 0: pipelined shared-memory tiles of 256 cells;
+ * core/platform/gpu/cuda/operator.hh:425-441).  variant 0: pipelined shared-memory tiles of 256 cells;
  * variant 1: one cell per thread in (block_x, block_y) blocks; variant 2 (default):
  * cells_per_thread (1 or 2; 4 for 16-bit storage) cells a warp apart per thread in
  * (block_x, block_y) blocks, block_x along the fastest axis; variant 3: tiles moved by TMA bulk
@@ -475,7 +475,7 @@ int lbx_ensemble_set_cells_per_thread(lbx_ensemble ens, int32_t cells);
 
 /* ---- autotuner ----------------------------------------------------------------------------
  * No reference counterpart (the reference's CUDA platform launches fixed 32-thread blocks,
- * gpu/cuda/operator.hh:425-441).  Both calls time every candidate launch shape on the caller's
+ * core/platform/gpu/cuda/operator.hh:425-441).  Both calls time every candidate launch shape on the caller's
  * own data with CUDA events on `stream`, each candidate starting from the same saved state, then
  * keep the fastest and put the state back as it was: populations, column shifts (and for an
  * ensemble every lattice's step count, residual and state) are unchanged on return, and since
@@ -504,7 +504,7 @@ int lbx_ensemble_autotune(lbx_ensemble ens, int32_t steps, lbx_tune_entry* out, 
  * planes thick), each an lbx_lattice of its own on devices[k] (NULL: all on device 0), stepped in
  * lock-step with one face exchange per step between the collision and the post-stream links and
  * boundary cells: the single-process form of the reference's block decomposition and overlap
- * communication (core/superLattice.hh:150-155, gpu/cuda/communicator.hh:355-510).  Every
+ * communication (core/superLattice.hh:150-155, core/platform/gpu/cuda/communicator.hh:355-510).  Every
  * population that leaves a slab across an x face is copied into the plane of the neighbour slab
  * it streams into (periodic x joins the last slab to the first); slabs on different devices send
  * their face buffers by cudaMemcpyPeerAsync.  A decomposed lattice computes the populations of

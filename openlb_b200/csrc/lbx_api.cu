@@ -356,7 +356,7 @@ int ensure_stage(lbx_lattice_s* L) {
 // into one reserved virtual range: element j and element j + P alias.  A population index
 // n + shift (< 2P) then never needs the modulo of the periodic-shift pattern, which removes
 // the wrap arithmetic from every access of the step kernel.  This is the technique of the
-// reference's CUDA CyclicColumn (gpu/cuda/column.hh:217-256), built here on the CUDA VMM
+// reference's CUDA CyclicColumn (core/platform/gpu/cuda/column.hh:217-256), built here on the CUDA VMM
 // API.  Without it (entry points missing, or any step failing) the columns fall back to one
 // plain allocation and the kernels wrap explicitly.
 namespace vmm {
@@ -1767,7 +1767,7 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
 // several devices of this process), stepped in lock-step with one face exchange per step between
 // the collision and the post-stream phase -- the single-process form of the reference's block
 // decomposition and overlap communication (core/superLattice.hh:150-155,
-// gpu/cuda/communicator.hh:355-510).
+// core/platform/gpu/cuda/communicator.hh:355-510).
 //
 // After a slab's collision and shift rotation, every population that left the slab across an x
 // face sits in the slab's own ghost plane (x = -1 or nx): the plain store of the step kernel put

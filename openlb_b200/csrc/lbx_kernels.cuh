@@ -5,14 +5,14 @@
 // n = (x+1)*sx + (y+1)*sy + (z+pz) (z fastest; 2D: sy = 1, pz = 0), as the reference's
 // BlockStructure orders cells (src/core/blockStructure.h:71).  Population i of cell n lives
 // at column_i[(n + shift_i) mod N]: the periodic-shift (PS) pattern of the reference's
-// CyclicColumn (src/core/platform/cpu/sisd/column.h:128-221, gpu/cuda/column.h:100-171).
+// CyclicColumn (src/core/platform/cpu/sisd/column.h:128-221, core/platform/gpu/cuda/column.h:100-171).
 // Streaming is the rotation shift_i -= c_i . (sx, sy, 1) done on the host between launches
 // (ConcreteBlockLattice::stream, core/blockLattice.hh:316-338): no population moves.
 //
 // The fused step kernel therefore reads and writes every population of a core cell exactly
 // once, in place (2 Q elements per lattice update).  On periodic axes the ghost layer has to
 // carry the post-collision populations of the opposite face before the rotation (the
-// reference's PostCollide overlap copy, core/superLattice.hh:150-155, gpu/cuda/
+// reference's PostCollide overlap copy, core/superLattice.hh:150-155, core/platform/gpu/cuda/
 // communicator.hh:111-124); the step kernel writes those few values itself, so a periodic
 // step is a single launch.
 #pragma once
@@ -329,7 +329,7 @@ struct TileCfg {
 
 // Post-collision values that leave the core across a periodic face are written into the ghost
 // cell from which the next rotation carries them into the opposite face (the reference's
-// PostCollide overlap copy, core/superLattice.hh:150-155, gpu/cuda/communicator.hh:111-124).
+// PostCollide overlap copy, core/superLattice.hh:150-155, core/platform/gpu/cuda/communicator.hh:111-124).
 template <int Q, typename S>
 __device__ __forceinline__ void periodic_ghost_writes(S* __restrict__ pop, const Geometry& g, const Shifts<Q>& sh,
                                                       int x, int y, int z, const typename Storage<S>::R (&f)[Q]) {
@@ -771,68 +771,80 @@ __global__ void __launch_bounds__(WsCfg<Q, S>::THREADS, WsCfg<Q, S>::BLOCKS) k_c
   double accRho = 0.0, accUsq = 0.0, accMax = 0.0, accCount = 0.0;
 
   if (warp == 0) {
-    if (lane == 0) {
-      int64_t issued = 0;
-      auto issue = [&](int64_t k) {
-        const int s = int(k % NS);
-        const int64_t t0 = tile_first(k);
-        const int cells = tile_cells(t0);
-        uint32_t total = 0;
-        for (int i = 0; i < Q; ++i) {
-          const int64_t first = (t0 + sh.s[i]) * ES, last = first + int64_t(cells) * ES;
-          const int64_t a0 = first & ~int64_t(15), a1 = (last + 15) & ~int64_t(15);
-          const int64_t b0 = (first + 15) & ~int64_t(15), b1 = last & ~int64_t(15);
-          const uint32_t head = b1 > b0 ? uint32_t((b0 - first) / ES) : uint32_t(cells);
-          const uint32_t tail = b1 > b0 ? uint32_t((b1 - first) / ES) : uint32_t(cells);
-          sRun[s][i] = uint32_t((first - a0) / ES) | (head << 4) | (tail << 16);
-          total += uint32_t(a1 - a0);
-        }
+    // the whole producer warp: lane i < Q looks after column i (its run bounds, its bulk load and
+    // its bulk store), lane 0 alone arms the stage's barrier with the total byte count
+    const bool col = lane < Q;
+    int64_t shift = 0;  // this lane's column shift (a select: no indexing into the parameters)
+    static_for<Q>([&](auto I) {
+      if (int(I) == lane) shift = sh.s[I];
+    });
+    const S* srcCol = pop + int64_t(col ? lane : 0) * g.stride;
+    int64_t issued = 0;
+    auto issue = [&](int64_t k) {
+      const int s = int(k % NS);
+      const int64_t t0 = tile_first(k);
+      const int cells = tile_cells(t0);
+      uint32_t bytes = 0;
+      int64_t a0 = 0;
+      if (col) {
+        const int64_t first = (t0 + shift) * ES, last = first + int64_t(cells) * ES;
+        a0 = first & ~int64_t(15);
+        const int64_t a1 = (last + 15) & ~int64_t(15);
+        const int64_t b0 = (first + 15) & ~int64_t(15), b1 = last & ~int64_t(15);
+        const uint32_t head = b1 > b0 ? uint32_t((b0 - first) / ES) : uint32_t(cells);
+        const uint32_t tail = b1 > b0 ? uint32_t((b1 - first) / ES) : uint32_t(cells);
+        sRun[s][lane] = uint32_t((first - a0) / ES) | (head << 4) | (tail << 16);
+        bytes = uint32_t(a1 - a0);
+      }
+      uint32_t total = bytes;
+      for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+      __syncwarp();  // the lanes' run bounds precede lane 0's arrival, which releases them
+      if (lane == 0) {
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_expect_tx(&full[s], total);
-        unsigned char* stage = smem_raw + s * C::STAGE_BYTES;
-        for (int i = 0; i < Q; ++i) {
-          const int64_t first = (t0 + sh.s[i]) * ES;
-          const int64_t a0 = first & ~int64_t(15), a1 = (first + int64_t(cells) * ES + 15) & ~int64_t(15);
-          bulk_g2s(stage + i * C::COL_BYTES, reinterpret_cast<const unsigned char*>(pop + i * g.stride) + a0,
-                   uint32_t(a1 - a0), &full[s]);
-        }
-        ++issued;
-      };
-      while (issued < nloc && issued < NS) issue(issued);
-      for (int64_t k = 0; k < nloc; ++k) {
-        const int s = int(k % NS);
-        if (!mbar_wait_spin(&empty[s], uint32_t((k / NS) & 1), err, waitLimit)) {
-          sAbort = 1;
-          break;
-        }
-        const int64_t t0 = tile_first(k);
-        const int cells = tile_cells(t0);
-        unsigned char* stage = smem_raw + s * C::STAGE_BYTES;
-        for (int i = 0; i < Q; ++i) {
-          const int64_t first = (t0 + sh.s[i]) * ES;
-          const int64_t b0 = (first + 15) & ~int64_t(15), b1 = (first + int64_t(cells) * ES) & ~int64_t(15);
-          if (b1 > b0)
-            bulk_s2g(reinterpret_cast<unsigned char*>(pop + i * g.stride) + b0,
-                     stage + i * C::COL_BYTES + (b0 - (first & ~int64_t(15))), uint32_t(b1 - b0));
-        }
-        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-        // the stage is free again once these stores have read it; the next tile for it is then
-        // NS - 1 tiles ahead of the consumers
-        if (issued < nloc) {
-          asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
-          if (sAbort) break;
-          issue(issued);
-        }
       }
-      asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
-      // loads still in flight (after an abort) land before the block exits: the phase of the
-      // last load issued into each stage (no later phase follows it)
+      __syncwarp();
+      if (col)
+        bulk_g2s(smem_raw + s * C::STAGE_BYTES + lane * C::COL_BYTES,
+                 reinterpret_cast<const unsigned char*>(srcCol) + a0, bytes, &full[s]);
+      ++issued;
+    };
+    while (issued < nloc && issued < NS) issue(issued);
+    for (int64_t k = 0; k < nloc; ++k) {
+      const int s = int(k % NS);
+      const bool ok = mbar_wait_spin(&empty[s], uint32_t((k / NS) & 1), err, waitLimit);
+      if (!__all_sync(0xffffffffu, ok)) {
+        sAbort = 1;
+        break;
+      }
+      const int64_t t0 = tile_first(k);
+      const int cells = tile_cells(t0);
+      if (col) {
+        const int64_t first = (t0 + shift) * ES;
+        const int64_t b0 = (first + 15) & ~int64_t(15), b1 = (first + int64_t(cells) * ES) & ~int64_t(15);
+        if (b1 > b0)
+          bulk_s2g(reinterpret_cast<unsigned char*>(const_cast<S*>(srcCol)) + b0,
+                   smem_raw + s * C::STAGE_BYTES + lane * C::COL_BYTES + (b0 - (first & ~int64_t(15))),
+                   uint32_t(b1 - b0));
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+      }
+      // the stage is free again once every lane's stores have read it; the next tile for it is
+      // then NS - 1 tiles ahead of the consumers
+      if (issued < nloc) {
+        if (col) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+        if (__any_sync(0xffffffffu, sAbort != 0)) break;  // the same decision in every lane
+        issue(issued);
+      }
+    }
+    if (col) asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+    // loads still in flight (after an abort) land before the block exits: the phase of the
+    // last load issued into each stage (no later phase follows it)
+    if (lane == 0)
       for (int s = 0; s < NS; ++s)
         if (issued > s) {
           const int64_t kl = s + ((issued - 1 - s) / NS) * NS;
           mbar_wait_spin(&full[s], uint32_t((kl / NS) & 1), err, waitLimit);
         }
-    }
   } else {
     const int ct = int(threadIdx.x) - 32;
     for (int64_t k = 0; k < nloc; ++k) {
@@ -967,7 +979,9 @@ template <> struct StepOccupancy<9, __nv_bfloat16, 4> { static constexpr int blo
 
 // Load of one stored population of a 16-bit form with an L2 prefetch-size hint of 256 bytes: a
 // warp-wide load reads 64 bytes of a column, and the hint lets L2 fetch the following warps'
-// bytes of the same column with the same DRAM access.  Wider forms load plainly.
+// bytes of the same column with the same DRAM access.  (The line stays in L1: the second cell of
+// a thread, 32 cells on, reads the other half of it; loads that skip L1 ran 23 % slower.)  Wider
+// forms load plainly.
 template <typename S> __device__ __forceinline__ S ld_column(const S* p) {
   if constexpr (sizeof(S) == 2) {
     unsigned short v;
@@ -1208,7 +1222,7 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
 // After the collision, every population that leaves the core across a periodic face is
 // copied into the ghost cell from which the next rotation carries it into the opposite face
 // -- the single-block form of the reference's periodic overlap communication
-// (core/superLattice.hh:150-155, gpu/cuda/communicator.hh:111-124).  One thread per (face
+// (core/superLattice.hh:150-155, core/platform/gpu/cuda/communicator.hh:111-124).  One thread per (face
 // cell, leaving population); the threads are ordered (axis, side, population, cell) so that a
 // warp copies one population of consecutive face cells.  A population leaving across two faces
 // at once (an edge) is copied by both faces' threads to the same ghost slot with the same value.

@@ -4,7 +4,7 @@
 // written once:
 //   - RAII ownership of a lattice handle;
 //   - errors turned into exceptions, as the reference's CUDA platform does with device::check
-//     (gpu/cuda/device.hh:48-53): std::runtime_error, and std::domain_error for a combination
+//     (core/platform/gpu/cuda/device.hh:48-53): std::runtime_error, and std::domain_error for a combination
 //     the library does not provide (the reference throws that for unsupported dynamics);
 //   - compile-time mapping of dynamics and parameter tags to the ABI's ids.
 // The names follow the reference's SuperLattice / BlockLattice API, so setup code reads like

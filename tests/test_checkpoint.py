@@ -1,5 +1,5 @@
 """Checkpoint and resume (SuperLattice::save / load, core/serializer.h:77-79; the CUDA columns
-serialise their data with the periodic-shift offset, gpu/cuda/column.hh:305-321).
+serialise their data with the periodic-shift offset, core/platform/gpu/cuda/column.hh:305-321).
 
 A run that is checkpointed, continued, and then resumed from the checkpoint in a fresh lattice
 with the same set-up must reproduce the continued run bit for bit: populations and statistics.
