@@ -322,3 +322,84 @@ def test_population_ptr_reaches_the_populations_in_place(storage, typestr):
         got = col[(padded + shift) % info.column_period]
         assert np.array_equal(got.astype(np.float64), want[i])
     lat.close()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16dev"])
+def test_parameter_classes_match_single_dynamics_lattices(storage):
+    """Cells of a parameter class collide exactly as a lattice whose own parameters are the
+    class's: a box split into two halves of different omega and force equals, cell for cell, the
+    two lattices that carry one parameter set each where the halves do not interact yet (the
+    first step), and a lattice whose every cell is class 2 equals one with those parameters."""
+    rng = np.random.default_rng(5)
+    core = (12, 10, 8)
+    n = int(np.prod(core))
+    f0 = (rng.random((19, n)) - 0.5) * 2e-3
+    main = dict(omega=1.3, force=(1e-4, 0.0, 0.0))
+    other = dict(omega=0.9, force=(0.0, -2e-5, 0.0))
+
+    def run(setup_fn, steps):
+        lat = lbx.BlockLattice(19, core, (1, 1, 1), storage)
+        lat.define_dynamics("forced_bgk", **main)
+        setup_fn(lat)
+        lat.set_populations(f0)
+        lat.collide_and_stream(steps, statistics=True)
+        out = lat.get_populations()
+        st = lat.get_statistics()
+        lat.close()
+        return out, st
+
+    def all_class(lat):
+        lat.set_dynamics_class(2, **other)
+        lat.set_cell_dynamics(np.full(n, lbx.CELL_BULK_CLASS_2, np.uint8))
+
+    def plain_other(lat):
+        lat.define_dynamics("forced_bgk", **other)
+        lat.set_launch_config(1, 128, 2, 1)
+
+    got, st = run(all_class, 7)
+    want, st_want = run(plain_other, 7)
+    assert np.array_equal(got, want)
+    for k in ("average_rho", "average_energy", "max_u"):
+        assert abs(st[k] - st_want[k]) <= 1e-12 * abs(st_want[k])
+    # half and half: after one step each cell of the class half equals the single-dynamics run
+    half = np.zeros(core, np.uint8)
+    half[: core[0] // 2] = 1
+    half[core[0] // 2:] = lbx.CELL_BULK_CLASS_1
+
+    def halves(lat):
+        lat.set_dynamics_class(1, **other)
+        lat.set_cell_dynamics(half.reshape(-1))
+
+    mixed, _ = run(halves, 1)
+    a, _ = run(lambda lat: lat.set_launch_config(1, 128, 2, 1), 1)
+    inner_main = np.zeros(core, bool)
+    inner_main[1: core[0] // 2 - 1] = True
+    inner_other = np.zeros(core, bool)
+    inner_other[core[0] // 2 + 1: -1] = True
+    assert np.array_equal(mixed[:, inner_main.reshape(-1)], a[:, inner_main.reshape(-1)])
+    assert np.array_equal(mixed[:, inner_other.reshape(-1)], want_1step(core, f0, storage, other)[:, inner_other.reshape(-1)])
+
+
+def want_1step(core, f0, storage, params):
+    lat = lbx.BlockLattice(19, core, (1, 1, 1), storage)
+    lat.define_dynamics("forced_bgk", **params)
+    lat.set_launch_config(1, 128, 2, 1)
+    lat.set_populations(f0)
+    lat.collide_and_stream(1)
+    out = lat.get_populations()
+    lat.close()
+    return out
+
+
+def test_parameter_class_arguments_are_checked():
+    lat = lbx.BlockLattice(19, (8, 8, 8), (1, 1, 1), "f32")
+    lat.define_dynamics("bgk", omega=1.2)
+    with pytest.raises(lbx.LbxError):
+        lat.set_dynamics_class(4, omega=1.0)
+    with pytest.raises(lbx.LbxError):
+        lat.set_dynamics_class(1, omega=2.5)
+    lat.set_dynamics_class(1, omega=1.0)
+    with pytest.raises(lbx.LbxError, match="variant 1"):
+        lat.set_launch_config(2, 128, 1, 1)
+    lat.set_dynamics_class(1, remove=True)
+    lat.close()
