@@ -156,7 +156,7 @@ def tgv_fields(n: int):
 
 
 STEP_KERNEL = {0: "k_collide_stream_tiled", 1: "k_collide_stream", 2: "k_collide_stream_groups",
-               3: "k_collide_stream_bulk", 4: "k_collide_stream_ws"}
+               3: "k_collide_stream_bulk", 4: "k_collide_stream_ws", 5: "k_collide_stream_groups"}
 
 
 def current_config(tuning: list[dict]) -> dict:

@@ -380,9 +380,11 @@ int lbx_rotate(lbx_lattice lattice, int32_t pop, int64_t offset);
  * cells_per_thread (1 or 2; 4 for 16-bit storage) cells a warp apart per thread in
  * (block_x, block_y) blocks, block_x along the fastest axis; variant 3: tiles moved by TMA bulk
  * copies, two stages per block; variant 4: tiles moved by TMA bulk copies through a ring of
- * four stages, one producer warp and eight consumer warps per block (block_x, block_y and
- * cells_per_thread are ignored by 0, 3 and 4).  Variants 3 and 4 need the doubled column
- * layout.  Every variant computes identical populations. */
+ * four stages, one producer warp and sixteen consumer warps per block (block_x, block_y and
+ * cells_per_thread are ignored by 0, 3 and 4); variant 5: variant 2 plus an L2 bulk prefetch,
+ * at the start of each block, of the populations of the block one wave of resident blocks later
+ * in launch order.  Variants 3, 4 and 5 need the doubled column layout (variant 5 without it
+ * runs as variant 2).  Every variant computes identical populations. */
 int lbx_set_launch_config(lbx_lattice lattice, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread);
 

@@ -92,6 +92,8 @@ bool test_allocation_fails() {
   --f.param;
   return true;
 }
+// launch variants that run the K-cells step kernel (variant 5 adds its L2 prefetch)
+inline bool groups_kernel(int variant) { return variant == 2 || variant == 5; }
 // lbx_normals.cu
 int discrete_normals(int q, const int32_t core[3], const int32_t periodic[3], const int32_t* material,
                      int32_t boundary, int32_t n_fluid, const int32_t* fluid, int32_t n_outside,
@@ -228,7 +230,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
   a.fdValue = L->fdValue;
   a.fdMom = L->fdMom;
   a.nFdCorners = L->nFdCorners;
-  a.linkMask = L->kernel == 2 ? L->linkMask : nullptr;
+  a.linkMask = groups_kernel(L->kernel) ? L->linkMask : nullptr;
   a.nBbv = L->nBbv;
   a.bbvCell = L->bbvCell;
   a.bbvValue = L->bbvValue;
@@ -330,7 +332,7 @@ int64_t step_blocks(const lbx_lattice_s* L) {
     }
     return (a.flatEnd - a.flatBase + bt - 1) / bt;
   }
-  const int64_t groups = L->kernel == 2 ? lbx::k_cells_threads(nf, L->cellsPerThread) : nf;
+  const int64_t groups = groups_kernel(L->kernel) ? lbx::k_cells_threads(nf, L->cellsPerThread) : nf;
   return ((groups + L->blockX - 1) / L->blockX) * int64_t((nm + L->blockY - 1) / L->blockY) * ns;
 }
 
@@ -516,7 +518,7 @@ void drain_timing(lbx_lattice_s* L) {
     float ms = 0.f;
     if (cudaEventSynchronize(e[3]) == cudaSuccess) {
       if (cudaEventElapsedTime(&ms, e[0], e[1]) == cudaSuccess) { L->timedMs[0] += ms; ++L->timedLaunches[0]; }
-      if ((L->periodic[0] || L->periodic[1] || L->periodic[2]) && L->kernel != 2) {  // variant 2: no copy launch
+      if ((L->periodic[0] || L->periodic[1] || L->periodic[2]) && !groups_kernel(L->kernel)) {  // variants 2, 5: no copy launch
         if (cudaEventElapsedTime(&ms, e[1], e[2]) == cudaSuccess) { L->timedMs[1] += ms; ++L->timedLaunches[1]; }
       }
       if (L->nLinks > 0) {
@@ -1630,14 +1632,14 @@ int lbx_rotate(lbx_lattice L, int32_t pop, int64_t offset) {
 int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32_t block_y,
                           int32_t cells_per_thread) {
   if (!L) return fail(LBX_ERR_INVALID, "null lattice");
-  if (variant < 0 || variant > 4) return fail(LBX_ERR_INVALID, "variant must be 0, 1, 2, 3 or 4");
+  if (variant < 0 || variant > 5) return fail(LBX_ERR_INVALID, "variant must be 0, 1, 2, 3, 4 or 5");
   if (L->classMask && variant != 1)
     return fail(LBX_ERR_UNSUPPORTED, "a lattice with parameter classes steps with launch variant 1");
   if ((variant == 3 || variant == 4) && (!L->doubled || L->period >= (int64_t(1) << 31)))
     return fail(LBX_ERR_UNSUPPORTED, "variants 3 and 4 (bulk copies) need the doubled column mapping and fewer than 2^31 cells");
-  if (variant == 2 && L->period >= (int64_t(1) << 31))
-    return fail(LBX_ERR_UNSUPPORTED, "variant 2 needs a column period below 2^31 cells");
-  if (variant == 2 && cells_per_thread != 1 && cells_per_thread != 2 &&
+  if (groups_kernel(variant) && L->period >= (int64_t(1) << 31))
+    return fail(LBX_ERR_UNSUPPORTED, "variants 2 and 5 need a column period below 2^31 cells");
+  if (groups_kernel(variant) && cells_per_thread != 1 && cells_per_thread != 2 &&
       !(cells_per_thread == 4 && storage_bytes(L->storage) == 2))
     return fail(LBX_ERR_INVALID, "cells_per_thread must be 1 or 2 (or 4 for 16-bit storage)");
   if (variant != 0) {
@@ -1646,7 +1648,7 @@ int lbx_set_launch_config(lbx_lattice L, int32_t variant, int32_t block_x, int32
     L->blockX = block_x;
     L->blockY = block_y;
   }
-  L->cellsPerThread = variant == 2 ? cells_per_thread : 1;
+  L->cellsPerThread = groups_kernel(variant) ? cells_per_thread : 1;
   L->kernel = variant;
   return LBX_OK;
 }
@@ -1668,6 +1670,8 @@ int lbx_autotune(lbx_lattice L, int32_t steps, lbx_tune_entry* out, int32_t capa
       if (bx > 32 && bx >= 2 * lbx::k_cells_threads(nf, k)) break;  // wider blocks only idle more threads
       for (int threads = 256; threads >= 128; threads /= 2)
         if (threads / bx >= 1) cands.push_back({2, bx, threads / bx, k});
+      // variant 5 (the L2 prefetch) with one row a block: the shapes where it can pay
+      if (L->doubled && bx >= 128) cands.push_back({5, bx, 1, k});
     }
   {
     int bx, by;

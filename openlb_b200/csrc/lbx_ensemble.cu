@@ -250,6 +250,24 @@ __device__ __forceinline__ void ensemble_tiles(const EnsArgs& a, int par, int nT
     const int slots = (last + 31) / 32;
     double tileDu2 = 0.0, tileU2 = 0.0;  // the tile's sums, slot by slot
     for (int g = 0; g < slots; g += K) {
+      // The warp walks the tile round by round, each round a batch of loads that waits on the
+      // previous one: lane i < Q first prefetches column i's run of the next round's cells into
+      // L2 (one bulk prefetch), so that batch finds its populations there.  Straight tiles only
+      // (the run is contiguous); widened to 16-byte bounds, which stay inside the lattice's
+      // region of the slab (regions are multiples of 256 bytes).  On the eight-cavity mix this
+      // raised the kernel from 28.0k to 28.6k MLUPS (graph mode) and 27.2k to 27.8k (persistent).
+      if (straight && lane < Q && g + K < slots) {
+        const int f0 = t.y + (g + K) * 32, f1 = t.y + min((g + 2 * K) * 32, last) - 1;
+        auto padded = [&](int c) {
+          const uint32_t xy = FastDiv::div(uint32_t(c), mz, lz);
+          const uint32_t px = FastDiv::div(xy, my, ly);
+          return (px + 1) * uint32_t(sx) + (xy - px * uint32_t(ny) + 1) * uint32_t(sy) + (uint32_t(c) - xy * uint32_t(nz)) + 1;
+        };
+        const S* col = w.col[lane];
+        const uintptr_t p0 = reinterpret_cast<uintptr_t>(col + padded(f0)) & ~uintptr_t(15);
+        const uintptr_t p1 = (reinterpret_cast<uintptr_t>(col + padded(f1) + 1) + 15) & ~uintptr_t(15);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p0), "r"(uint32_t(p1 - p0)) : "memory");
+      }
       uint32_t n[K];
       int fm[K];  // face mask of the lane's cell in slot g + k; -1: no cell
       double du2[K], u2[K];

@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
 //     the 16-byte-aligned interior of every column's run; the stage is loaded again when those
 //     stores have read it (the store group one behind the newest), so NS - 1 tiles are in flight
 //     ahead of the one being computed;
-//   - warps 1..8 are consumers: each waits for its tile's `full` phase, collides its cells in
+//   - warps 1..16 are consumers: each waits for its tile's `full` phase, collides its cells in
 //     shared memory (16-bit BGK pairs with the packed two-cell collision), writes the unaligned
 //     head and tail elements of each run straight to their slots, makes its shared-memory
 //     writes visible to the bulk-copy proxy and arrives on the stage's `empty` barrier.
@@ -711,14 +711,16 @@ __global__ void __launch_bounds__(BulkCfg<Q, S>::THREADS, BulkCfg<Q, S>::BLOCKS)
 // (bounded) for its loads still in flight and its stores before the block exits.
 template <int Q, typename S> struct WsCfg {
   static constexpr int ES = int(sizeof(S));
-  static constexpr int BT = (20480 / (Q * ES)) / 64 * 64;  // cells per tile: ~20 KB of populations
+  // cells per tile: ~40 KB of populations, so that each bulk copy moves 1-4 KB (the per-copy
+  // cost of the copy engine, not the bytes, bounded the first form with 20 KB tiles)
+  static constexpr int BT = (40960 / (Q * ES)) / 64 * 64;
   static constexpr int COL_BYTES = BT * ES + 32;           // one column's run + alignment slack
   static constexpr int STAGE_BYTES = Q * COL_BYTES;
   static constexpr int NS = 4;                              // stages in the ring
-  static constexpr int CONSUMER_WARPS = 8;
+  static constexpr int CONSUMER_WARPS = 16;
   static constexpr int THREADS = 32 * (1 + CONSUMER_WARPS);
   static constexpr int SMEM = NS * STAGE_BYTES + 2 * NS * 8;  // stages, then the full and empty mbarriers
-  static constexpr int BLOCKS = 2;                          // resident blocks per SM
+  static constexpr int BLOCKS = 1;                          // resident blocks per SM
   static_assert(BT >= 64 && COL_BYTES % 16 == 0 && STAGE_BYTES % 16 == 0, "tile layout");
   static_assert(BT <= 4095, "packed run bounds hold 12 bits");
 };
@@ -999,10 +1001,46 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
                                                                CollisionParams<typename Storage<S>::R> p,
                                                                const uint8_t* __restrict__ cellDyn,
                                                                const uint32_t* __restrict__ linkMask,
-                                                               double* __restrict__ statPart) {
+                                                               double* __restrict__ statPart, int ahead) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
   const uint32_t P = uint32_t(g.n);
+  // L2 prefetch of the block `ahead` blocks later in launch order (about one wave of resident
+  // blocks on): its Q column runs, one cp.async.bulk.prefetch per column and row, issued by the
+  // first Q x rows threads.  That block then finds its populations in L2 instead of waiting on
+  // DRAM latency.  Doubled columns only (every run is contiguous); a prefetch changes no value.
+  // The runs are widened to 16-byte bounds, which stay inside the column's two mappings.
+  // Launch variant 5 passes ahead > 0, variant 2 passes 0: on periodic D3Q19 boxes with one-row
+  // blocks it gained 3-4 %, on lattices with a cell map and on D3Q27 it lost 12-26 % (solid
+  // cells are prefetched but never loaded), so the autotuner decides.
+  if constexpr (DOUBLED) {
+    const unsigned tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (ahead > 0 && (blockDim.x & 31u) == 0 && tid < unsigned(Q) * blockDim.y) {
+      const uint64_t t = blockIdx.x + uint64_t(gridDim.x) * (blockIdx.y + uint64_t(gridDim.y) * blockIdx.z) +
+                         uint64_t(ahead);
+      if (t < uint64_t(gridDim.x) * gridDim.y * gridDim.z) {
+        const uint32_t bx = uint32_t(t % gridDim.x);
+        const uint64_t r = t / gridDim.x;
+        const uint32_t by = uint32_t(r % gridDim.y), bz = uint32_t(r / gridDim.y);
+        const int col = int(tid % unsigned(Q));
+        const int row = int(by * blockDim.y + tid / unsigned(Q));  // y (3D) or x (2D)
+        const int nf = D::d == 3 ? g.nz : g.ny, nrows = D::d == 3 ? g.ny : g.nx;
+        const int zlo = int(bx * blockDim.x) * K;  // the block's cells along the fastest axis
+        const int zhi = min(nf, zlo + int(blockDim.x) * K);
+        if (row < nrows && zlo < zhi) {
+          const uint32_t nlo = (D::d == 3) ? uint32_t((int(bz) + 1) * g.sx + (row + 1) * g.sy + zlo + 1)
+                                           : uint32_t((row + 1) * g.sx + zlo + 1);
+          const S* base = nullptr;
+          static_for<Q>([&](auto I) {
+            if (int(I) == col) base = static_cast<const S*>(cols.base[I]);
+          });
+          const uintptr_t a0 = reinterpret_cast<uintptr_t>(base + nlo) & ~uintptr_t(15);
+          const uintptr_t a1 = (reinterpret_cast<uintptr_t>(base + nlo + (zhi - zlo)) + 15) & ~uintptr_t(15);
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a0), "r"(uint32_t(a1 - a0)) : "memory");
+        }
+      }
+    }
+  }
   // The K cells of a thread lie a warp apart along the fastest axis (z0, z0 + 32, ...): each
   // warp-wide load or store then covers one contiguous run of 32 cells, which a 16-bit column
   // moves in two full sectors, instead of every instruction touching twice the sectors it uses.
@@ -1682,6 +1720,14 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
                                                        const int32_t* __restrict__ bIdx) {
   using R = typename Storage<S>::R;
   using D = Desc<Q>;
+  // One thread per boundary cell, its neighbour lookups in stages so that the loads of every
+  // stage are in flight together: the boundary-list entries of all neighbours, then the cell
+  // kinds of those not on the list, then the momenta of the listed ones and the fixed values,
+  // then the populations of the bulk neighbours two cells at a time.  Slots 0 .. 2d-1 are the
+  // velocities of the gradient (slot 2a the first neighbour along axis a, 2a + 1 the second),
+  // slots 6 .. 11 the densities of an edge or corner extrapolation.  (Against one lookup after
+  // the other this took the pass from 22 to 19 us a launch on a 128 x 64 x 64 channel; a warp per
+  // cell, every lane repeating the cell's arithmetic, was slower at 26 us.)
   const int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (b >= nFd) return;
   const FdMeta m(fdMeta[b]);
@@ -1693,108 +1739,151 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
   const int ext[3] = {g.nx, g.ny, g.nz};
   const R halfF[3] = {R(hfx), R(hfy), R(hfz)};
   const double* own = fdMom + 7 * b;
-  R u[3] = {R(own[0]), R(own[1]), R(own[2])};
-  auto padded_of = [&](const int (&p)[3]) -> int64_t {
-    return int64_t(p[0] + 1) * g.sx + int64_t(p[1] + 1) * g.sy + (p[2] + g.pz);
-  };
-  auto load_cell = [&](int64_t nn, R (&f)[Q]) {
-    static_for<Q>([&](auto I) { f[I] = Storage<S>::load(pop + I * g.stride + wrap_add(nn, sh.s[I], g.n)); });
-  };
-  auto velocity_at = [&](const int (&p)[3], bool wrapped, R (&v)[3]) {
-    const int64_t nn = padded_of(p);
-    const int32_t bi = bIdx[nn];  // the cell's boundary-list entry (see lbx_lattice_s::bIdx)
-    const int64_t j = bi >= 0 ? bi : -1;
-    if (j >= 0) {
-      const double* mm = fdMom + 7 * j + (wrapped ? 3 : 0);
-      v[0] = R(mm[0]);
-      v[1] = R(mm[1]);
-      v[2] = R(mm[2]);
-      return;
-    }
-    const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
-    if (bulk_kind(kind)) {
-      R f[Q];
-      load_cell(nn, f);
-      bulk_velocity<Q, R>(f, halfF, v);
-    } else if (kind == kCellBounceBackVelocity) {  // FixedVelocityMomentum: the wall velocity
-      const int64_t jb = bi <= -2 ? int64_t(-2 - bi) : -1;
-      v[0] = v[1] = v[2] = R(0);
-      if (jb >= 0)
-        for (int a = 0; a < D::d; ++a) v[a] = R(bbvValue[4 * jb + 1 + a]);
-    } else {
-      v[0] = v[1] = v[2] = R(0);
-    }
-  };
-  auto rho_at = [&](const int (&p)[3]) -> R {
-    const int64_t nn = padded_of(p);
-    const int32_t bi = bIdx[nn];
-    const int64_t j = bi >= 0 ? bi : -1;
-    if (j >= 0) {
-      if (!corners) return R(fdMom[7 * j + 6]);
-      R f[Q], r, v[3];
-      load_cell(nn, f);
-      fd_momenta<Q, R>(f, FdMeta(fdMeta[j]), fdValue + 4 * j, r, v);
-      return r;
-    }
-    const uint8_t kind = cellDyn ? cellDyn[nn] : uint8_t(1);
-    if (kind == kCellBounceBackVelocity) {  // FixedDensity
-      const int64_t jb = bi <= -2 ? int64_t(-2 - bi) : -1;
-      return jb >= 0 ? R(bbvValue[4 * jb]) : R(1);
-    }
-    if (!bulk_kind(kind)) return R(1);
-    R f[Q];
-    load_cell(nn, f);
-    return bulk_rho<Q, R>(f);
-  };
-  // density at the cell `step` cells inward along axis a
-  auto rho_in = [&](int a, int step) -> R {
+  const bool flatRho = m.type == FD_FLAT_VELOCITY || m.type == FD_FLAT_PRESSURE;
+  const bool edgeRule = !flatRho && (m.type == FD_EDGE_VELOCITY || D::d == 2);
+  // the two normal axes A < B (in the cyclic order after the edge axis) of an edge; x, y in 2D
+  int A = 0, B = 1;
+  if (D::d == 3 && edgeRule) {
+    int plane = 0;
+    for (int a = 0; a < 3; ++a)
+      if (m.n[a] == 0) plane = a;
+    A = (plane + 1) % 3;
+    B = (plane + 2) % 3;
+  }
+  constexpr int NS = 12;
+  int64_t nn[NS];
+  bool use[NS], wrapped[6];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
     int p[3] = {pos[0], pos[1], pos[2]};
-    p[a] -= step * m.n[a];
-    return rho_at(p);
-  };
-  R rho;
-  if (m.type == FD_FLAT_VELOCITY || m.type == FD_FLAT_PRESSURE) {
-    rho = R(own[6]);
-  } else if (m.type == FD_EDGE_VELOCITY || D::d == 2) {
-    int A = 0, B = 1;
-    if (D::d == 3) {
-      int plane = 0;
-      for (int a = 0; a < 3; ++a)
-        if (m.n[a] == 0) plane = a;
-      A = (plane + 1) % 3;
-      B = (plane + 2) % 3;
+    use[s] = false;
+    if (s < 6) {
+      wrapped[s] = false;
+      const int a = s >> 1, second = s & 1;
+      if (a < D::d) {
+        use[s] = true;
+        if (m.n[a] != 0) {
+          p[a] -= (second ? 2 : 1) * m.n[a];
+        } else {
+          // across a periodic face the partner cell is read (its overlap copy carries bulk
+          // dynamics); across a non-periodic one the padding cell, which has none
+          const bool per = (g.pmask >> a) & 1;
+          if (!second) {
+            p[a] += 1;
+            wrapped[s] = per && p[a] >= ext[a];
+            if (wrapped[s]) p[a] -= ext[a];
+          } else {
+            p[a] -= 1;
+            wrapped[s] = per && p[a] < 0;
+            if (wrapped[s]) p[a] += ext[a];
+          }
+        }
+      }
+    } else if (!flatRho) {
+      // density at the cell `step` cells inward along axis `ax`: edges (A, 1), (B, 1), (A, 2),
+      // (B, 2); 3D corners (x, 1), (y, 1), (z, 1), (x, 2), (y, 2), (z, 2)
+      const int r = s - 6;
+      int ax = -1, step = 1;
+      if (edgeRule) {
+        if (r < 4) {
+          ax = (r & 1) ? B : A;
+          step = 1 + (r >> 1);
+        }
+      } else {
+        ax = r % 3;
+        step = 1 + r / 3;
+      }
+      if (ax >= 0) {
+        use[s] = true;
+        p[ax] -= step * m.n[ax];
+      }
     }
-    const R r10 = rho_in(A, 1), r01 = rho_in(B, 1), r20 = rho_in(A, 2), r02 = rho_in(B, 2);
+    nn[s] = int64_t(p[0] + 1) * g.sx + int64_t(p[1] + 1) * g.sy + (p[2] + g.pz);
+  }
+  int32_t bi[NS];  // boundary-list entries (see lbx_lattice_s::bIdx)
+#pragma unroll
+  for (int s = 0; s < NS; ++s) bi[s] = use[s] ? bIdx[nn[s]] : -1;
+  uint8_t kind[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) kind[s] = (use[s] && bi[s] < 0 && cellDyn) ? cellDyn[nn[s]] : uint8_t(1);
+  R nv[6][3], nr[6];
+  bool pend[NS];  // the value comes from the cell's populations
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    pend[s] = false;
+    const int64_t jb = bi[s] <= -2 ? int64_t(-2 - bi[s]) : -1;  // bounce-back-with-velocity entry
+    if (s < 6) {
+      nv[s][0] = nv[s][1] = nv[s][2] = R(0);
+      if (!use[s]) continue;
+      if (bi[s] >= 0) {
+        const double* mm = fdMom + 7 * int64_t(bi[s]) + (wrapped[s] ? 3 : 0);
+        nv[s][0] = R(mm[0]);
+        nv[s][1] = R(mm[1]);
+        nv[s][2] = R(mm[2]);
+      } else if (bulk_kind(kind[s])) {
+        pend[s] = true;
+      } else if (kind[s] == kCellBounceBackVelocity && jb >= 0) {  // FixedVelocityMomentum
+        for (int a = 0; a < D::d; ++a) nv[s][a] = R(bbvValue[4 * jb + 1 + a]);
+      }
+    } else {
+      nr[s - 6] = R(0);
+      if (!use[s]) continue;
+      if (bi[s] >= 0) {
+        if (!corners) nr[s - 6] = R(fdMom[7 * int64_t(bi[s]) + 6]);
+        else pend[s] = true;  // the populations the flat and edge pass left
+      } else if (kind[s] == kCellBounceBackVelocity) {  // FixedDensity
+        nr[s - 6] = jb >= 0 ? R(bbvValue[4 * jb]) : R(1);
+      } else if (!bulk_kind(kind[s])) {
+        nr[s - 6] = R(1);
+      } else {
+        pend[s] = true;
+      }
+    }
+  }
+  auto finish = [&](int s, const R (&f)[Q]) {
+    if (s < 6) {
+      bulk_velocity<Q, R>(f, halfF, nv[s]);
+    } else if (bi[s] >= 0) {
+      R r, v[3];
+      fd_momenta<Q, R>(f, FdMeta(fdMeta[bi[s]]), fdValue + 4 * int64_t(bi[s]), r, v);
+      nr[s - 6] = r;
+    } else {
+      nr[s - 6] = bulk_rho<Q, R>(f);
+    }
+  };
+#pragma unroll
+  for (int s0 = 0; s0 < NS; s0 += 2) {
+    if (!(pend[s0] || pend[s0 + 1])) continue;
+    R f0[Q], f1[Q];
+    static_for<Q>([&](auto I) {
+      f0[I] = pend[s0] ? Storage<S>::load(pop + I * g.stride + wrap_add(nn[s0], sh.s[I], g.n)) : R(0);
+      f1[I] = pend[s0 + 1] ? Storage<S>::load(pop + I * g.stride + wrap_add(nn[s0 + 1], sh.s[I], g.n)) : R(0);
+    });
+    if (pend[s0]) finish(s0, f0);
+    if (pend[s0 + 1]) finish(s0 + 1, f1);
+  }
+  R u[3] = {R(own[0]), R(own[1]), R(own[2])};
+  R rho;
+  if (flatRho) {
+    rho = R(own[6]);
+  } else if (edgeRule) {
+    const R r10 = nr[0], r01 = nr[1], r20 = nr[2], r02 = nr[3];
     rho = R(2) / R(3) * (r01 + r10) - R(1) / R(6) * (r02 + r20);
   } else {
-    const R r100 = rho_in(0, 1), r010 = rho_in(1, 1), r001 = rho_in(2, 1);
-    const R r200 = rho_in(0, 2), r020 = rho_in(1, 2), r002 = rho_in(2, 2);
+    const R r100 = nr[0], r010 = nr[1], r001 = nr[2];
+    const R r200 = nr[3], r020 = nr[4], r002 = nr[5];
     rho = R(4) / R(9) * (r001 + r010 + r100) - R(1) / R(9) * (r002 + r020 + r200);
   }
   R grad[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
+#pragma unroll
   for (int a = 0; a < D::d; ++a) {
-    R ua[3] = {R(0), R(0), R(0)}, ub[3] = {R(0), R(0), R(0)};
+    const R* ua = nv[2 * a];
+    const R* ub = nv[2 * a + 1];
     if (m.n[a] != 0) {
       const int o = m.n[a];
-      int p1[3] = {pos[0], pos[1], pos[2]}, p2[3] = {pos[0], pos[1], pos[2]};
-      p1[a] -= o;
-      p2[a] -= 2 * o;
-      velocity_at(p1, false, ua);
-      velocity_at(p2, false, ub);
       for (int iD = 0; iD < D::d; ++iD)
         grad[a][iD] = R(-o) * (((R(-3) * u[iD] + R(4) * ua[iD]) - R(1) * ub[iD]) / R(2));
     } else {
-      int pp[3] = {pos[0], pos[1], pos[2]}, pm[3] = {pos[0], pos[1], pos[2]};
-      pp[a] += 1;
-      pm[a] -= 1;
-      // across a periodic face the partner cell is read (its overlap copy carries bulk
-      // dynamics); across a non-periodic one the padding cell, which has none
-      const bool per = (g.pmask >> a) & 1;
-      const bool wp = per && pp[a] >= ext[a], wm = per && pm[a] < 0;
-      if (wp) pp[a] -= ext[a];
-      if (wm) pm[a] += ext[a];
-      velocity_at(pp, wp, ua);
-      velocity_at(pm, wm, ub);
       for (int iD = 0; iD < D::d; ++iD) grad[a][iD] = (ua[iD] - ub[iD]) / R(2);
     }
   }
@@ -1813,7 +1902,7 @@ __global__ void __launch_bounds__(256) k_fd_regularize(S* __restrict__ pop, Geom
     pi[1] = (grad[0][1] + grad[1][0]) * sToPi;
   }
   R uSqr = R(0);
-  static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+  static_for<D::d>([&](auto AX) { uSqr += u[AX] * u[AX]; });
   static_for<Q>([&](auto I) {
     constexpr R t = weight<Q, R>(I);
     R fneq = R(0);
@@ -2054,6 +2143,27 @@ inline int k_cells_threads(int nf, int K) { return K == 1 ? nf : (nf + 32 * K - 
 // Blocks of 256 threads the boundary-cell collision adds to a step's statistics partials.
 inline int64_t fd_blocks(int64_t nFd) { return (nFd + 255) / 256; }
 
+// How far ahead in launch order the step kernel prefetches into L2: one wave of resident blocks
+// (the block that takes over a finishing block's SM).  `cache` belongs to one kernel: per device,
+// the block size it was computed for and the resident blocks.
+template <typename F>
+int l2_ahead_blocks(F kern, int threads, int (&cache)[64][2]) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  int* c = cache[dev & 63];
+  if (c[0] != threads) {
+    int perSM = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    c[1] = perSM * sms;
+    c[0] = threads;
+  }
+  return c[1];
+}
+
 template <int Q, typename S>
 cudaError_t launch_step(const LaunchArgs& a, cudaStream_t stream);
 template <int Q, typename S>
@@ -2235,8 +2345,13 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
     double* part = a.stats ? a.statPart : nullptr;
     auto go = [&](auto kk, auto doubled, auto mapped) {
-      k_collide_stream_groups<Q, S, DYN, decltype(kk)::value, decltype(doubled)::value, decltype(mapped)::value>
-          <<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part);
+      auto kern =
+          k_collide_stream_groups<Q, S, DYN, decltype(kk)::value, decltype(doubled)::value, decltype(mapped)::value>;
+      static int aheadCache[64][2] = {};  // one per instantiation of this lambda, i.e. per kernel
+      int ahead = 0;
+      if constexpr (decltype(doubled)::value)
+        if (a.kernel == 5) ahead = l2_ahead_blocks(kern, int(block.x * block.y), aheadCache);
+      kern<<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part, ahead);
     };
     auto go_k = [&](auto kk) {
       if (a.doubled) {
@@ -2318,7 +2433,7 @@ cudaError_t launch_halo(const LaunchArgs& a, cudaStream_t stream) {
   S* pop = static_cast<S*>(a.pop);
   constexpr int NF = FaceCount<Q>::n;
   // the K-cells step kernel (variant 2) does the whole overlap copy itself
-  if (a.kernel == 2) return cudaSuccess;
+  if (a.kernel == 2 || a.kernel == 5) return cudaSuccess;
   const int mask = g.pmask;
   const int64_t cntX = (mask & 1) ? 2 * NF * int64_t(g.ny) * g.nz : 0;
   const int64_t cntY = (mask & 2) ? 2 * NF * int64_t(g.nx) * g.nz : 0;

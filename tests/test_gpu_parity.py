@@ -253,7 +253,7 @@ def test_kernel_variants_agree_bitwise(name, storage):
     setup = L.case_setup(fx)
     outs = []
     shapes = [(0, 256, 1, 1), (1, 64, 4, 1), (1, 32, 8, 1), (2, 32, 8, 1), (2, 64, 4, 2), (2, 256, 1, 1),
-              (3, 256, 1, 1), (4, 256, 1, 1)]
+              (3, 256, 1, 1), (4, 256, 1, 1), (5, 128, 1, 1)]
     if storage in ("f16dev", "bf16dev"):
         shapes += [(2, 32, 4, 4), (2, 128, 1, 2)]
     for variant, bx, by, k in shapes:
@@ -268,6 +268,27 @@ def test_kernel_variants_agree_bitwise(name, storage):
     mask = L.fluid_mask(fx)
     for o in outs[1:]:
         assert np.array_equal(outs[0][:, mask], o[:, mask])
+
+
+@pytest.mark.parametrize("q,core,storage,k", [(19, (48, 64, 64), "f32", 1), (19, (48, 64, 256), "f16dev", 2),
+                                              (27, (40, 48, 40), "f64", 1), (9, (700, 384, 1), "bf16dev", 2)])
+def test_l2_prefetch_variant_matches_variant_2(q, core, storage, k):
+    """Launch variant 5 (variant 2 plus the L2 bulk prefetch of the block one wave ahead) on
+    lattices with several waves of blocks, so that the prefetch is issued: the same bits as
+    variant 2 after 9 steps."""
+    n = int(np.prod(core))
+    rng = np.random.default_rng(q + k)
+    f0 = (rng.random((q, n)) - 0.5) * 1e-3
+    outs = []
+    for variant in (2, 5):
+        lat = lbx.BlockLattice(q, core, (1, 1, 1) if q != 9 else (1, 1, 0), storage)
+        lat.define_dynamics("bgk", omega=1.4)
+        lat.set_launch_config(variant, 128, 1, k)
+        lat.set_populations(f0)
+        lat.collide_and_stream(9)
+        outs.append(lat.get_populations())
+        lat.close()
+    assert np.array_equal(outs[0], outs[1])
 
 
 @pytest.mark.parametrize("name", ["periodic_d3q19_bgk_f64", "porous_d3q27_fsmag_f64", "cavity_d2q9_bgk_f64"])
