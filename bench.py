@@ -229,7 +229,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
     lat.define_dynamics("bgk", omega=OMEGA)
     lat.ini_equilibrium(rho, u, stream=stream)
     lat.collide_and_stream(args.warmup, stream=stream)
-    tuning = lat.autotune(steps=10, stream=stream) if not (args.no_autotune or args.launch_config) else []
+    tuning = lat.autotune(steps=30, stream=stream) if not (args.no_autotune or args.launch_config) else []
     if args.launch_config:
         lat.set_launch_config(*args.launch_config)
         tuning = [{"variant": args.launch_config[0], "block_x": args.launch_config[1],
@@ -290,7 +290,7 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
             fl.define_dynamics("bgk", omega=OMEGA)
             fl.ini_equilibrium(rho, u, stream=stream)
             fl.collide_and_stream(args.warmup, stream=stream)
-            f_tuning = fl.autotune(steps=10, stream=stream) if not args.no_autotune else []
+            f_tuning = fl.autotune(steps=30, stream=stream) if not args.no_autotune else []
             fms = timed_steps(fl, k)
             fl.set_kernel_timing(True)
             timed_steps(fl, k)
@@ -316,6 +316,9 @@ def run_b200(args, rank: int, world: int, device: int, dist) -> dict | None:
                 "rho_linf": float(np.abs(r - rho64).max()),
                 "after_steps": int(args.warmup + 2 * max(10, args.steps // 4))}
         del fields
+        # against the FP32 form's own run of the same length (vs_f32_mlups: against the headline)
+        for form in forms:
+            forms[form]["vs_f32_form_mlups"] = round(forms[form]["mlups"] / forms["f32"]["mlups"], 3)
 
     ensemble = None if args.ensemble_requests <= 0 else run_ensemble(args, device, stream)
 
