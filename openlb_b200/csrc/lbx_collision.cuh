@@ -319,31 +319,16 @@ __device__ __forceinline__ void collide(R (&f)[Q], const CollisionParams<R>& p, 
 // Each packed operation rounds every lane exactly as the scalar operation does, so a pair of
 // cells computed here gets the same bits as two calls of the scalar float path below: the
 // operation sequence of collide<Q, float, DYN_BGK> is kept step for step.
-struct F2 {
-  float x, y;
-};
-__device__ __forceinline__ F2 f2(float v) { return F2{v, v}; }
-#define LBX_F32X2_BINOP(NAME, OP)                                                                          \
-  __device__ __forceinline__ F2 NAME(F2 a, F2 b) {                                                        \
-    F2 d;                                                                                                 \
-    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2,%3};\n mov.b64 rb, {%4,%5};\n " OP " rd, ra, rb;\n" \
-        " mov.b64 {%0,%1}, rd;\n}\n"                                                                     \
-        : "=f"(d.x), "=f"(d.y)                                                                            \
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                                        \
-    return d;                                                                                             \
-  }
-LBX_F32X2_BINOP(add2, "add.rn.f32x2")
-LBX_F32X2_BINOP(sub2, "sub.rn.f32x2")
-LBX_F32X2_BINOP(mul2, "mul.rn.f32x2")
-#undef LBX_F32X2_BINOP
-__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
-  F2 d;
-  asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2,%3};\n mov.b64 rb, {%4,%5};\n mov.b64 rc, {%6,%7};\n"
-      " fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0,%1}, rd;\n}\n"
-      : "=f"(d.x), "=f"(d.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-  return d;
-}
+// The pairs are CUDA's float2 and the operations its sm_100 packed intrinsics, whose rounding per
+// component is that of __fadd_rn, __fmul_rn and __fmaf_rn; the compiler keeps a pair in a
+// register pair instead of packing two floats around every operation.
+using F2 = float2;
+__device__ __forceinline__ F2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ F2 add2(F2 a, F2 b) { return __fadd2_rn(a, b); }
+// a - b with one rounding, as __fsub_rn: b * (-1) is exact, so the fused form rounds a + (-b) once
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return __ffma2_rn(a, b, c); }
 
 // BGK collision of two cells (f[k][i], k = 0, 1) in place: collide_bgk_f32 on pairs, the same
 // operation sequence (no product ever meets a separate add, so no contraction can differ).

@@ -1010,10 +1010,10 @@ __global__ void __launch_bounds__(256, StepOccupancy<Q, S, K>::blocks) k_collide
   // first Q x rows threads.  That block then finds its populations in L2 instead of waiting on
   // DRAM latency.  Doubled columns only (every run is contiguous); a prefetch changes no value.
   // The runs are widened to 16-byte bounds, which stay inside the column's two mappings.
-  // Launch variant 5 passes ahead > 0 (one wave, two for the 16-bit forms), variant 2 passes 0:
-  // on periodic D3Q19 boxes with one-row blocks it gained 3-5 %, on lattices with a cell map and
-  // on D3Q27 it lost 12-26 % (solid cells are prefetched but never loaded), so the autotuner
-  // decides.
+  // Launch variant 5 passes ahead > 0 (one wave), variant 2 passes 0.  On periodic D3Q19 boxes
+  // with one-row blocks it was within -4 % .. +4 % of variant 2 from box to box, on lattices with
+  // a cell map and on D3Q27 it lost 12-26 % (solid cells are prefetched but never loaded), so the
+  // autotuner decides.
   if constexpr (DOUBLED) {
     const unsigned tid = threadIdx.y * blockDim.x + threadIdx.x;
     if (ahead > 0 && (blockDim.x & 31u) == 0 && tid < unsigned(Q) * blockDim.y) {
@@ -2351,8 +2351,7 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
       static int aheadCache[64][2] = {};  // one per instantiation of this lambda, i.e. per kernel
       int ahead = 0;
       if constexpr (decltype(doubled)::value)
-        if (a.kernel == 5)  // one wave ahead; two for the 16-bit forms, whose blocks finish sooner
-          ahead = l2_ahead_blocks(kern, int(block.x * block.y), aheadCache) * (sizeof(S) == 2 ? 2 : 1);
+        if (a.kernel == 5) ahead = l2_ahead_blocks(kern, int(block.x * block.y), aheadCache);
       kern<<<grid, block, 0, stream>>>(cols, g, p, a.cellDyn, a.linkMask, part, ahead);
     };
     auto go_k = [&](auto kk) {
