@@ -204,8 +204,8 @@ int lbx_discrete_normals(int32_t q, const int32_t core[3], const int32_t periodi
                          const int32_t* outside, int64_t cap, int64_t* cells, int32_t* types, int32_t* normals,
                          int64_t* n_out);
 
-/* Velocity / pressure boundary cells with their discrete normals: flat faces, external edges
- * and external corners, what boundary::set<InterpolatedVelocity> / <InterpolatedPressure>
+/* Velocity / pressure boundary cells with their discrete normals: flat faces, external and
+ * internal edges and corners, what boundary::set<InterpolatedVelocity> / <InterpolatedPressure>
  * install for each normal type (boundary/interpolatedVelocity3D.h:45-90,
  * interpolatedVelocity2D.h:45-80, interpolatedPressure3D.h:48-90):
  *   flat, velocity or pressure: as lbx_set_fd_boundaries (PlaneFdBoundaryProcessor3D /
@@ -216,13 +216,18 @@ int lbx_discrete_normals(int32_t q, const int32_t core[3], const int32_t periodi
  *   external corner, velocity: the same momenta and OuterVelocityCornerProcessor3D
  *     (boundaryPostProcessors3D.hh:240-294) / OuterVelocityCornerProcessor2D
  *     (boundaryPostProcessors2D.hh:278-323), run after the flat and edge processors as their
- *     priority 1 orders them.
+ *     priority 1 orders them;
+ *   internal edge (3D) and internal corner, velocity (interpolated or local alike):
+ *     CombinedRLBdynamics with momenta::InnerEdgeVelocityTuple3D / InnerCornerVelocityTuple2D /
+ *     InnerCornerVelocityTuple3D (dynamics/momenta/aliases.h:224-243): u imposed, rho the mean of
+ *     velocityBMRho along the normal axes, Pi from the cell with its unknown populations bounced
+ *     back in non-equilibrium; regularised in the collision, no post-processor.
  * kinds: lbx_fd_kind; types: lbx_normal_type; normals[3 * i + a]: outward normal components in
  * {-1, 0, 1} (a flat cell has one non-zero component, an edge two, a corner d); values[4 * i]:
  * the imposed velocity, or {rho, tangential velocity} of a pressure cell.  Every cell needs the
  * two cells inward along each non-zero normal component inside the core, and no normal
- * component may lie along a periodic axis.  Internal corners and edges, and pressure cells that
- * are not flat, return LBX_ERR_UNSUPPORTED.  A neighbour that carries no dynamics or plain
+ * component may lie along a periodic axis.  Pressure cells that are not flat return
+ * LBX_ERR_UNSUPPORTED.  A neighbour that carries no dynamics or plain
  * bounce-back (and a padding cell beyond a non-periodic face, the reference's NoDynamics
  * overlap) reads as u = 0, rho = 1 in the finite differences, as their momenta
  * (momenta::ZeroMomentum, OneDensity / FixedDensity) give it.  Replaces the boundary list of

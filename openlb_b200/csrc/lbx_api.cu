@@ -681,11 +681,9 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
   for (const FdHostCell& c : list) {
     if (c.core < 0 || c.core >= L->ncore) return fail(LBX_ERR_INVALID, "boundary cell out of range");
     if (c.kind < LBX_FD_VELOCITY || c.kind > LBX_FD_LOCAL_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
-    if (c.type == LBX_NORMAL_INTERNAL_CORNER || c.type == LBX_NORMAL_INTERNAL_EDGE)
-      return fail(LBX_ERR_UNSUPPORTED, "internal corners and edges (concave boundaries) are not provided");
-    if (c.type != LBX_NORMAL_FLAT && c.type != LBX_NORMAL_EXTERNAL_CORNER && c.type != LBX_NORMAL_EXTERNAL_EDGE)
-      return fail(LBX_ERR_INVALID, "unknown normal type");
-    if (c.type == LBX_NORMAL_EXTERNAL_EDGE && L->d != 3) return fail(LBX_ERR_INVALID, "edges exist in 3D only");
+    if (c.type < LBX_NORMAL_FLAT || c.type > LBX_NORMAL_INTERNAL_EDGE) return fail(LBX_ERR_INVALID, "unknown normal type");
+    const bool edge = c.type == LBX_NORMAL_EXTERNAL_EDGE || c.type == LBX_NORMAL_INTERNAL_EDGE;
+    if (edge && L->d != 3) return fail(LBX_ERR_INVALID, "edges exist in 3D only");
     const bool pressure = c.kind == LBX_FD_PRESSURE || c.kind == LBX_FD_LOCAL_PRESSURE;
     if (pressure && c.type != LBX_NORMAL_FLAT)
       return fail(LBX_ERR_UNSUPPORTED, "pressure boundaries are provided on flat faces only");
@@ -694,7 +692,7 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
       if (c.n[a] < -1 || c.n[a] > 1 || (a >= L->d && c.n[a] != 0)) return fail(LBX_ERR_INVALID, "normal components must be -1, 0 or 1");
       nonzero += c.n[a] != 0;
     }
-    const int want = c.type == LBX_NORMAL_FLAT ? 1 : (c.type == LBX_NORMAL_EXTERNAL_EDGE ? 2 : L->d);
+    const int want = c.type == LBX_NORMAL_FLAT ? 1 : (edge ? 2 : L->d);
     if (nonzero != want) return fail(LBX_ERR_INVALID, "the normal does not match the normal type");
     const int64_t ny = L->core[1], nz = (L->d == 3) ? L->core[2] : 1;
     const int p[3] = {int(c.core / (ny * nz)), int((c.core / nz) % ny), int(c.core % nz)};
@@ -729,6 +727,8 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
       }
     }
     else if (c.type == LBX_NORMAL_EXTERNAL_EDGE) t = FD_EDGE_VELOCITY;
+    else if (c.type == LBX_NORMAL_INTERNAL_EDGE) t = FD_INNER_EDGE_VELOCITY;
+    else if (c.type == LBX_NORMAL_INTERNAL_CORNER) t = FD_INNER_CORNER_VELOCITY;
     else t = FD_CORNER_VELOCITY;
     corners += t == FD_CORNER_VELOCITY;
     hm[size_t(k)] = FdMeta::encode(t, c.n);
@@ -1152,8 +1152,6 @@ int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* ma
       continue;  // InterpolatedPressure installs nothing on edges and corners
     }
     if (zero) return fail(LBX_ERR_UNSUPPORTED, "could not set boundary: a velocity cell has no discrete normal");
-    if (t == LBX_NORMAL_INTERNAL_CORNER || t == LBX_NORMAL_INTERNAL_EDGE)
-      return fail(LBX_ERR_UNSUPPORTED, "internal corners and edges (concave boundaries) are not provided");
     FdHostCell c;
     c.core = cells[k];
     c.kind = kind;

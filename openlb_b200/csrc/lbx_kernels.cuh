@@ -1369,10 +1369,13 @@ __global__ void __launch_bounds__(256) k_bouzidi(S* __restrict__ pop, Geometry g
 // OuterVelocityCornerProcessor3D / 2D (3D.hh:240-294, 2D.hh:276-323).
 // Types 4 and 5 are the flat cells of the local boundaries (LocalVelocity / LocalPressure with
 // BGK mixed in): regularised in their collision (CombinedRLBdynamics, dynamics/dynamics.h:
-// 470-523), no post-processor.
+// 470-523), no post-processor.  Types 6 and 7 are the internal (concave) edges and corners of a
+// velocity boundary, interpolated or local alike: CombinedRLBdynamics with InnerEdgeVelocityTuple3D
+// / InnerCornerVelocityTuple2D / 3D (boundary/interpolatedVelocity3D.h:56-67,
+// interpolatedVelocity2D.h:59-62, dynamics/momenta/aliases.h:224-243), no post-processor.
 enum FdType {
   FD_FLAT_VELOCITY = 0, FD_FLAT_PRESSURE = 1, FD_EDGE_VELOCITY = 2, FD_CORNER_VELOCITY = 3,
-  FD_FLAT_VELOCITY_LOCAL = 4, FD_FLAT_PRESSURE_LOCAL = 5
+  FD_FLAT_VELOCITY_LOCAL = 4, FD_FLAT_PRESSURE_LOCAL = 5, FD_INNER_EDGE_VELOCITY = 6, FD_INNER_CORNER_VELOCITY = 7
 };
 
 // Meta word of a boundary cell: bits 0-2 the type, bits 3-8 the outward discrete normal, two bits
@@ -1382,11 +1385,12 @@ struct FdMeta {
   int n[3];         // outward normal
   int dir, orient;  // flat cells: the normal axis and its sign
   int pressure;     // flat pressure cell (interpolated or local)
-  int local;        // flat cell of a local boundary
+  int local;        // regularised in its collision, no post-processor (types 4 to 7)
   int flat;
+  int inner;        // internal edge or corner
   __host__ __device__ __forceinline__ explicit FdMeta(uint16_t m)
       : type(m & 7), dir(0), orient(0), pressure((m & 7) == 1 || (m & 7) == 5), local((m & 7) >= 4),
-        flat((m & 7) != FD_EDGE_VELOCITY && (m & 7) != FD_CORNER_VELOCITY) {
+        flat((m & 7) <= 1 || (m & 7) == 4 || (m & 7) == 5), inner((m & 7) >= 6) {
     for (int a = 0; a < 3; ++a) {
       const int code = (m >> (3 + 2 * a)) & 3;
       n[a] = code == 1 ? 1 : (code == 2 ? -1 : 0);
@@ -1412,16 +1416,52 @@ __device__ __forceinline__ R bulk_rho(const R (&f)[Q]) {
   return rho + R(1);
 }
 
+// velocityBMRho (dynamics/momenta/elements.h:54-71) along axis `dir` with outward sign `orient`
+template <int Q, typename R>
+__device__ __forceinline__ R bm_rho(const R (&f)[Q], int dir, int orient, const R (&u)[3]) {
+  using D = Desc<Q>;
+  R onWall = R(0), normal = R(0);
+  static_for<Q>([&](auto I) {
+    constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+    const int c = dir == 0 ? c0 : (dir == 1 ? c1 : c2);
+    if (c == 0) onWall += f[I];
+  });
+  static_for<Q>([&](auto I) {
+    constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+    const int c = dir == 0 ? c0 : (dir == 1 ? c1 : c2);
+    if (c == orient) normal += f[I];
+  });
+  return (R(2) * normal + onWall + R(1)) / (R(1) + R(orient) * u[dir]);
+}
+
 // rho and u of a boundary cell from its momenta.  Flat velocity: u imposed, rho = velocityBMRho
 // (dynamics/momenta/elements.h:54-71) with rho_onWall summing the populations with c_d = 0 and
 // rho_normal those with c_d = orientation, each in index order.  Flat pressure: rho imposed,
 // the tangential velocity imposed and u_d from the populations (FixedPressureMomentum::computeU,
-// elements.h:653-690).  Edge and corner: u imposed, rho = sum f + 1 (BulkDensity).
+// elements.h:653-690).  Edge and corner: u imposed, rho = sum f + 1 (BulkDensity).  Internal
+// edge and corner: u imposed, rho the mean of velocityBMRho along the normal axes
+// (InnerEdgeDensity3D: the two axes after the edge axis; InnerCornerDensity2D / 3D: x, y (, z);
+// elements.h:406-483).
 template <int Q, typename R>
 __device__ __forceinline__ void fd_momenta(const R (&f)[Q], FdMeta m, const double* __restrict__ v, R& rho,
                                            R (&u)[3]) {
   using D = Desc<Q>;
   u[0] = u[1] = u[2] = R(0);
+  if (m.inner) {
+    static_for<D::d>([&](auto A) { u[A] = R(v[A]); });
+    if (m.type == FD_INNER_EDGE_VELOCITY) {
+      int plane = 0;
+      for (int a = 0; a < 3; ++a)
+        if (m.n[a] == 0) plane = a;
+      const int a1 = (plane + 1) % 3, a2 = (plane + 2) % 3;
+      rho = (bm_rho<Q, R>(f, a1, m.n[a1], u) + bm_rho<Q, R>(f, a2, m.n[a2], u)) / R(2);
+    } else if constexpr (D::d == 3) {
+      rho = (bm_rho<Q, R>(f, 0, m.n[0], u) + bm_rho<Q, R>(f, 1, m.n[1], u) + bm_rho<Q, R>(f, 2, m.n[2], u)) / R(3);
+    } else {
+      rho = (bm_rho<Q, R>(f, 0, m.n[0], u) + bm_rho<Q, R>(f, 1, m.n[1], u)) / R(2);
+    }
+    return;
+  }
   if (!m.flat) {
     static_for<D::d>([&](auto A) { u[A] = R(v[A]); });
     rho = bulk_rho<Q, R>(f);
@@ -1546,6 +1586,70 @@ __device__ __forceinline__ void local_regularize(R (&f)[Q], FdMeta m, R rho, con
   });
 }
 
+// The regularisation of an internal edge or corner (CombinedRLBdynamics::collide with
+// InnerEdgeStress3D / InnerCornerStress2D / 3D, dynamics/momenta/elements.h:1814-1897): Pi from a
+// copy of the cell whose unknown populations -- c equal to -n along every normal axis of the edge
+// (the two axes after the edge axis) or corner -- are replaced by f_opp - f^eq_opp + f^eq_i
+// (lbm::computeStress, dynamics/lbm.h:333-351: sum c_a c_b f - rho u_a u_b, less (rho - 1) / 3
+// on the diagonal), then f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) as for the flat cells.
+template <int Q, typename R>
+__device__ __forceinline__ void inner_regularize(R (&f)[Q], FdMeta m, R rho, const R (&u)[3]) {
+  using D = Desc<Q>;
+  constexpr int NPI = D::d == 3 ? 6 : 3;
+  R uSqr = R(0);
+  static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+  int plane = -1;  // the edge axis, none for a corner
+  if (m.type == FD_INNER_EDGE_VELOCITY)
+    for (int a = 0; a < 3; ++a)
+      if (m.n[a] == 0) plane = a;
+  R h[Q];
+  static_for<Q>([&](auto I) {
+    bool unknown = true;
+    static_for<D::d>([&](auto A) {
+      constexpr int c = D::C[I][A];
+      if (int(A) != plane && c != -m.n[A]) unknown = false;
+    });
+    constexpr int O = D::OPP[I];
+    h[I] = unknown ? f[O] - equilibrium_plain<Q, O>(rho, u, uSqr) + equilibrium_plain<Q, I>(rho, u, uSqr) : f[I];
+  });
+  R pi[NPI];
+  {
+    int iPi = 0;
+    static_for<D::d>([&](auto A) {
+      static_for<D::d>([&](auto B) {
+        if constexpr (int(B) >= int(A)) {
+          R p = R(0);
+          static_for<Q>([&](auto I) {
+            constexpr int cc = D::C[I][A] * D::C[I][B];
+            if constexpr (cc != 0) p += R(cc) * h[I];
+          });
+          p -= rho * u[A] * u[B];
+          if constexpr (int(A) == int(B)) p -= R(1) / R(3) * (rho - R(1));
+          pi[iPi++] = p;
+        }
+      });
+    });
+  }
+  static_for<Q>([&](auto I) {
+    constexpr R t = weight<Q, R>(I);
+    R fn = R(0);
+    int iPi = 0;
+    static_for<D::d>([&](auto A) {
+      static_for<D::d>([&](auto B) {
+        if constexpr (int(B) >= int(A)) {
+          R toAdd = R(D::C[I][A] * D::C[I][B]);
+          if constexpr (int(A) == int(B)) toAdd -= R(1) / R(3);
+          else toAdd *= R(2);
+          toAdd *= pi[iPi++];
+          fn += toAdd;
+        }
+      });
+    });
+    fn *= t * R(3) * R(3) / R(2);
+    f[I] = equilibrium_plain<Q, I>(rho, u, uSqr) + fn;
+  });
+}
+
 // Collision of the boundary cells: BGKdynamics with the boundary momenta
 // (collision::BGK::apply with lbm::bgkCollision, dynamics/collision.h:68-78, lbm.h:395-403),
 // in place at the current shifts, after the bulk step kernel left these cells untouched.  A cell
@@ -1568,7 +1672,8 @@ __global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometr
     R rho, u[3];
     fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
     if (m.local) {  // regularised first, then collided with the momenta of the rebuilt cell
-      local_regularize<Q, R>(f, m, rho, u);
+      if (m.inner) inner_regularize<Q, R>(f, m, rho, u);
+      else local_regularize<Q, R>(f, m, rho, u);
       fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
     }
     R uSqr = R(0);

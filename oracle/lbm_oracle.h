@@ -69,9 +69,11 @@ typedef struct {
   const int32_t* fd_orient;  /* outward normal sign, -1 or +1 */
   const double* fd_value;    /* 4 per cell: the velocity, or {rho, tangential velocity} */
   /* Optional (NULL: every cell flat with the normal of fd_dir / fd_orient): the discrete normal
-   * type (0 flat, 1 external corner, 3 external edge; geometry/discreteNormals.h:33-39) and the
-   * outward normal, 3 per cell.  Edges and corners carry an imposed velocity
-   * (boundary/interpolatedVelocity3D.h:45-90, interpolatedVelocity2D.h:45-80). */
+   * type (0 flat, 1 external corner, 2 internal corner, 3 external edge, 4 internal edge;
+   * geometry/discreteNormals.h:33-39) and the outward normal, 3 per cell.  Edges and corners
+   * carry an imposed velocity (boundary/interpolatedVelocity3D.h:45-90,
+   * interpolatedVelocity2D.h:45-80); internal ones are regularised in their collision
+   * (CombinedRLBdynamics with the inner edge / corner momenta, no post-processor). */
   const int32_t* fd_type;
   const int32_t* fd_normal;
   /* {rho, u_x, u_y, u_z} per cell (all cells; read for the LBO_BOUNCE_BACK_VELOCITY ones) */

@@ -145,12 +145,42 @@ static void FN(fd_meta)(const lbo_case* c, int64_t b, int* type, int n[3])
  *            elements.h:270-280), u = imposed tangential velocity with
  *            u_d = o ((2 rho_normal + rho_onWall + 1) / rho - 1) (FixedPressureMomentum::computeU,
  *            elements.h:653-690);
- *  external edge / corner (FixedVelocityBoundaryTuple): u = imposed, rho = sum f + 1 (BulkDensity).
+ *  external edge / corner (FixedVelocityBoundaryTuple): u = imposed, rho = sum f + 1 (BulkDensity);
+ *  internal edge / corner (InnerEdgeVelocityTuple3D, InnerCornerVelocityTuple2D / 3D,
+ *            aliases.h:224-243): u = imposed, rho = the mean of velocityBMRho along the normal
+ *            axes (InnerEdgeDensity3D: axes (plane+1)%3 and (plane+2)%3, plane the edge axis;
+ *            InnerCornerDensity2D / 3D: x, y (, z); elements.h:406-483).
  * rho_onWall sums the populations with c_d = 0, rho_normal those with c_d = o, in index order. */
+static REAL FN(bm_rho)(const lbo_desc* d, const REAL* g, int dir, int orient, const REAL* u)
+{
+  REAL onWall = 0, normal = 0;
+  for (int i = 0; i < d->q; ++i)
+    if (d->c[i][dir] == 0) onWall += g[i];
+  for (int i = 0; i < d->q; ++i)
+    if (d->c[i][dir] == orient) normal += g[i];
+  return ((REAL)2 * normal + onWall + (REAL)1) / ((REAL)1 + (REAL)orient * u[dir]);
+}
+
 static void FN(fd_momenta)(const lbo_desc* d, const REAL* g, int kind, int type, const int* nrm,
                            const double* value, REAL* rho, REAL* u)
 {
   const int q = d->q, dim = d->d;
+  if (type == 2 || type == 4) {
+    for (int a = 0; a < dim; ++a) u[a] = (REAL)value[a];
+    if (type == 4) {
+      int plane = 0;
+      for (int a = 0; a < 3; ++a)
+        if (nrm[a] == 0) plane = a;
+      const int a1 = (plane + 1) % 3, a2 = (plane + 2) % 3;
+      *rho = (FN(bm_rho)(d, g, a1, nrm[a1], u) + FN(bm_rho)(d, g, a2, nrm[a2], u)) / (REAL)2;
+    } else if (dim == 3) {
+      *rho = (FN(bm_rho)(d, g, 0, nrm[0], u) + FN(bm_rho)(d, g, 1, nrm[1], u) + FN(bm_rho)(d, g, 2, nrm[2], u)) /
+             (REAL)3;
+    } else {
+      *rho = (FN(bm_rho)(d, g, 0, nrm[0], u) + FN(bm_rho)(d, g, 1, nrm[1], u)) / (REAL)2;
+    }
+    return;
+  }
   if (type != 0) {
     REAL r = 0;
     for (int i = 0; i < q; ++i) r += g[i];
@@ -215,6 +245,67 @@ static void FN(local_regularize)(const lbo_desc* d, REAL rho, const REAL* u, con
         if (d->c[i][dir] == 0) pi[iPi] += (REAL)(d->c[i][a] * d->c[i][b]) * fneq[i];
       for (int i = 0; i < q; ++i)
         if (d->c[i][dir] == orient) pi[iPi] += (REAL)(2 * d->c[i][a] * d->c[i][b]) * fneq[i];
+      ++iPi;
+    }
+  for (int i = 0; i < q; ++i) {
+    const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+    REAL fn = 0;
+    iPi = 0;
+    for (int a = 0; a < dim; ++a)
+      for (int b = a; b < dim; ++b) {
+        REAL toAdd = (REAL)(d->c[i][a] * d->c[i][b]);
+        if (a == b) toAdd -= (REAL)1 / invCs2;
+        else toAdd *= (REAL)2;
+        toAdd *= pi[iPi++];
+        fn += toAdd;
+      }
+    fn *= t * invCs2 * invCs2 / (REAL)2;
+    g[i] = FN(second_order)(d, i, rho, u, uSqr) + fn;
+  }
+}
+
+/* The regularisation of an internal edge or corner (CombinedRLBdynamics::collide with
+ * InnerEdgeStress3D / InnerCornerStress2D / 3D, src/dynamics/momenta/elements.h:1814-1897): a
+ * copy of the cell whose unknown populations -- c along every normal axis of the edge (the two
+ * axes after the edge axis) or corner equal to -n -- are replaced by f_opp - f^eq_opp + f^eq_i;
+ * Pi from its second moment (lbm::computeStress, src/dynamics/lbm.h:333-351:
+ * sum_i c_ia c_ib f_i - rho u_a u_b - (rho - 1) / c_s^-2 on the diagonal), then
+ * f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi). */
+static void FN(inner_regularize)(const lbo_desc* d, REAL rho, const REAL* u, int type, const int* nrm, REAL* g)
+{
+  const int q = d->q, dim = d->d;
+  const REAL invCs2 = (REAL)3;
+  REAL uSqr = 0;
+  for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+  int axes[3], na = 0;
+  if (type == 4) {
+    int plane = 0;
+    for (int a = 0; a < 3; ++a)
+      if (nrm[a] == 0) plane = a;
+    axes[na++] = (plane + 1) % 3;
+    axes[na++] = (plane + 2) % 3;
+  } else {
+    for (int a = 0; a < dim; ++a) axes[na++] = a;
+  }
+  REAL h[27];
+  for (int i = 0; i < q; ++i) h[i] = g[i];
+  for (int i = 0; i < q; ++i) {
+    int unknown = 1;
+    for (int k = 0; k < na; ++k)
+      if (d->c[i][axes[k]] != -nrm[axes[k]]) unknown = 0;
+    if (unknown) {
+      const int o = d->opp[i];
+      h[i] = g[o] - FN(second_order)(d, o, rho, u, uSqr) + FN(second_order)(d, i, rho, u, uSqr);
+    }
+  }
+  REAL pi[6];
+  int iPi = 0;
+  for (int a = 0; a < dim; ++a)
+    for (int b = a; b < dim; ++b) {
+      pi[iPi] = 0;
+      for (int i = 0; i < q; ++i) pi[iPi] += (REAL)(d->c[i][a] * d->c[i][b]) * h[i];
+      pi[iPi] -= rho * u[a] * u[b];
+      if (a == b) pi[iPi] -= (REAL)1 / invCs2 * (rho - (REAL)1);
       ++iPi;
     }
   for (int i = 0; i < q; ++i) {
@@ -376,6 +467,7 @@ static void FN(fd_postprocess)(const lbo_desc* d, const lbo_case* c, STORE_T* f,
       FN(fd_meta)(c, b, &type, nrm);
       if ((type == 1) != (pass == 1)) continue;
       if (c->fd_kind[b] >= 3 && type == 0) continue;  /* local flat cells: no post-processor */
+      if (type == 2 || type == 4) continue;              /* internal edges and corners: none either */
       const int64_t cell = c->fd_cell[b];
       const int64_t pos[3] = {cell / (ny * nz), (cell / nz) % ny, cell % nz};
       REAL g[27], rho, u[3] = {0, 0, 0};
@@ -528,6 +620,10 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
         if (c->fd_kind[b] >= 3 && type == 0) {
           /* local boundary: regularised first, then the BGK collision with the same momenta */
           FN(local_regularize)(d, rho, u, nrm, g);
+          FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
+        } else if (type == 2 || type == 4) {
+          /* internal edge / corner: CombinedRLBdynamics, regularised the same way */
+          FN(inner_regularize)(d, rho, u, type, nrm, g);
           FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
         }
         cellUsq[x] = FN(bgk_with)(d, (REAL)c->omega, rho, u, g);

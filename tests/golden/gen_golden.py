@@ -124,6 +124,30 @@ def geo_box(shape, lid=True):
     return mat
 
 
+def geo_step(shape, block):
+    """A closed box with a block cut out of one corner of its inside (slices `block`), so that
+    the fluid has internal (concave) edges and corners: the fluid (1) is the inside less the
+    block, the cells next to it (diagonals included) the walls (2; 3 on the top layer along y,
+    the lid), every other cell outside (0)."""
+    import itertools
+    fluid = np.zeros(shape, bool)
+    fluid[tuple(slice(1, s - 1) for s in shape)] = True
+    fluid[block] = False
+    pad = np.pad(fluid, 1)
+    near = np.zeros(shape, bool)
+    for off in itertools.product((-1, 0, 1), repeat=len(shape)):
+        if any(off):
+            near |= pad[tuple(slice(1 + o, 1 + o + s) for o, s in zip(off, shape))]
+    mat = np.zeros(shape, np.int32)
+    mat[fluid] = 1
+    wall = ~fluid & near
+    mat[wall] = 2
+    top = np.zeros(shape, bool)
+    top[:, -1, ...] = True
+    mat[wall & top] = 3
+    return mat
+
+
 def geo_two_dynamics(shape):
     """A periodic box of fluid (material 1) with a block in its middle of material 6, which
     carries a second fluid dynamics (--bgk-mat 6)."""
@@ -209,6 +233,22 @@ GEO = {
                                                                            "--rho", "0.99", "--bounceback", "2",
                                                                            "--bouzidi", "5", "--local", *RND,
                                                                            "--steps", "60"]),
+    # a cavity with a block cut out of a corner: internal (concave) edges and corners of the
+    # velocity boundary (CombinedRLBdynamics with the inner edge / corner momenta), beside flat
+    # faces and external edges and corners
+    "geo_step_d2q9_ivel_bgk_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
+                                                                "--ivel-lid", "3", "--ulid", "0.1", "--steps", "150"]),
+    "geo_step_d3q19_ivel_bgk_f64": ("d3q19_f64_nocse", (12, 11, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                      "--ivel-lid", "3", "--ulid", "0.05", *RND,
+                                                                      "--steps", "60"]),
+    "geo_step_d3q27_ivel_trt_f64": ("d3q27_f64_nocse", (11, 10, 9), ["--dyn", "trt", "--omega", "1.6", "--magic",
+                                                                     "0.25", "--ivel", "2", "--ivel-lid", "3",
+                                                                     "--ulid", "0.05", "--steps", "80"]),
+    "geo_step_d3q19_lvel_bgk_f64": ("d3q19_f64_nocse", (12, 11, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                      "--ivel-lid", "3", "--ulid", "0.05", "--local",
+                                                                      *RND, "--steps", "60"]),
+    "geo_step_d3q19_ivel_bgk_f32": ("d3q19_f32", (12, 11, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                "--ivel-lid", "3", "--ulid", "0.05", "--steps", "60"]),
     # two fluid dynamics in one block: ForcedBGK on material 1 and BGK on material 6 (periodic)
     "geo_two_dyn_d3q19_fbgk_bgk_f64": ("d3q19_f64_nocse", (12, 10, 9), ["--dyn", "fbgk", "--omega", "1.3", "--force",
                                                                         "1e-4", "2e-5", "0", "--periodic", "1", "1",
@@ -217,6 +257,11 @@ GEO = {
                                                                    "1e-4", "-3e-5", "--periodic", "1", "1",
                                                                    "--bgk-mat", "6", *RND, "--steps", "60"]),
 }
+GEO_STEP = {"geo_step_d2q9_ivel_bgk_f64": (slice(8, None), slice(None, 5)),
+            "geo_step_d3q19_ivel_bgk_f64": (slice(7, None), slice(None, 5), slice(6, None)),
+            "geo_step_d3q27_ivel_trt_f64": (slice(6, None), slice(None, 5), slice(5, None)),
+            "geo_step_d3q19_lvel_bgk_f64": (slice(7, None), slice(None, 5), slice(6, None)),
+            "geo_step_d3q19_ivel_bgk_f32": (slice(7, None), slice(None, 5), slice(6, None))}
 GEO_SPHERE = {"geo_channel_d3q27_trt_f64": (8, 7, 7, 3), "geo_channel_d3q27_trt_f32": (8, 7, 7, 3),
               "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5), "geo_channel_d3q19_lvel_lpres_f64": (6, 5, 6, 2.5)}
 
@@ -227,6 +272,8 @@ def geo_material(name: str) -> np.ndarray:
         return geo_channel(shape, GEO_SPHERE[name])
     if "_two_dyn_" in name:
         return geo_two_dynamics(shape)
+    if name in GEO_STEP:
+        return geo_step(shape, GEO_STEP[name])
     return geo_box(shape)
 
 

@@ -355,27 +355,44 @@ def fluid_mask(fx: dict) -> np.ndarray:
 
 
 def local_flat_cells(fx: dict) -> np.ndarray:
-    """Flat cells of a LocalVelocity / LocalPressure boundary.  Their populations entering from
-    beyond the domain are, after a stream, whatever the padding held (in the reference: its
-    storage's leftovers); the next collision rebuilds them from the others, so only the others are
-    compared (known_populations)."""
-    if fx["meta"]["case"] != "geo" or not geo_args(fx["meta"])["local"]:
+    """Cells regularised in their collision whose populations entering from beyond the domain
+    are, after a stream, whatever the cells there held (in the reference: its storage's
+    leftovers): the flat cells of a LocalVelocity / LocalPressure boundary and the internal
+    edges and corners of any velocity boundary.  The next collision rebuilds those populations
+    from the others, so only the others are compared (known_populations)."""
+    if fx["meta"]["case"] != "geo" or "bclass" not in fx:
         return np.zeros(0, np.int64)
     bc = fx["bclass"]
-    return bc[bc[:, 2] == 0, 0].astype(np.int64)
+    pick = np.isin(bc[:, 2], (2, 4))
+    if geo_args(fx["meta"])["local"]:
+        pick |= bc[:, 2] == 0
+    return bc[pick, 0].astype(np.int64)
+
+
+def _unknown(vel: np.ndarray, i: int, ntype: int, n: np.ndarray) -> bool:
+    """Population i enters from beyond the domain: c_i . n < 0 on a flat cell; c_i = -n along
+    every normal axis of an internal corner, and along the two normal axes of an internal edge."""
+    c = vel[i, :3]
+    if ntype == 0:
+        return int(np.dot(c, n)) < 0
+    axes = [a for a in range(3) if n[a] != 0]
+    return all(c[a] == -n[a] for a in axes)
 
 
 def known_populations(fx: dict) -> tuple[np.ndarray, np.ndarray]:
-    """(population, cell) index pairs of the local flat cells' populations that do not enter
-    from beyond the domain: c_i . n >= 0 for the outward normal n."""
+    """(population, cell) index pairs of the cells of local_flat_cells whose populations do not
+    enter from beyond the domain."""
     bc = fx["bclass"]
     q = fx["meta"]["q"]
     vel = VEL[q]
+    cells_of = set(local_flat_cells(fx).tolist())
     pops, cells = [], []
-    for row in bc[bc[:, 2] == 0]:
+    for row in bc:
+        if int(row[0]) not in cells_of:
+            continue
         n = row[3:6]
         for i in range(q):
-            if int(np.dot(vel[i, :3], n)) >= 0:
+            if not _unknown(vel, i, int(row[2]), n):
                 pops.append(i)
                 cells.append(int(row[0]))
     return np.asarray(pops, np.int64), np.asarray(cells, np.int64)

@@ -45,6 +45,7 @@ def test_geo_fixtures_cover_edges_and_corners():
         kinds |= {(fx["meta"]["d"], int(t)) for t in fx["bclass"][:, 2]}
     assert (2, 0) in kinds and (2, 1) in kinds  # 2D flat faces and external corners
     assert (3, 0) in kinds and (3, 1) in kinds and (3, 3) in kinds  # 3D flat, corners, edges
+    assert (2, 2) in kinds and (3, 2) in kinds and (3, 4) in kinds  # internal corners and edges
     assert any(n.startswith("geo_channel_d3q27_trt") for n in GEO)
 
 
@@ -230,8 +231,10 @@ def test_boundary_cell_arguments_are_checked():
     from openlb_b200 import lbx
     lat = lbx.BlockLattice(19, (8, 6, 5), (0, 0, 0), "f64")
     v = np.zeros((1, 4))
-    with pytest.raises(lbx.LbxError, match="internal"):
+    with pytest.raises(lbx.LbxError, match="two cells inward"):
         lat.set_boundary_cells([0], [1], [lbx.NORMAL_INTERNAL_CORNER], [[1, 1, 1]], v)
+    with pytest.raises(lbx.LbxError, match="flat faces only"):
+        lat.set_boundary_cells([0], [2], [lbx.NORMAL_INTERNAL_EDGE], [[-1, -1, 0]], np.array([[1.0, 0, 0, 0]]))
     with pytest.raises(lbx.LbxError, match="flat faces only"):
         v2 = np.array([[1.0, 0, 0, 0]])
         lat.set_boundary_cells([0], [2], [lbx.NORMAL_EXTERNAL_EDGE], [[-1, -1, 0]], v2)
