@@ -88,7 +88,12 @@ typedef enum {
    * post-processor; velocity edges and corners are those of InterpolatedVelocity; pressure cells
    * exist on flat faces only (the reference throws elsewhere). */
   LBX_FD_LOCAL_VELOCITY = 3,
-  LBX_FD_LOCAL_PRESSURE = 4
+  LBX_FD_LOCAL_PRESSURE = 4,
+  /* the same with their default mixed-in dynamics, RLBdynamics (boundary/localVelocity.h:44-49,
+   * localPressure.h:31-36; collision::RLB, dynamics/collision.h:82-112): every cell of the
+   * boundary, external edges and corners included, is collided by RLB with its momenta */
+  LBX_FD_LOCAL_VELOCITY_RLB = 5,
+  LBX_FD_LOCAL_PRESSURE_RLB = 6
 } lbx_fd_kind;
 
 /* Parameters of the bulk dynamics (the ParametersD fields OMEGA, TRT::MAGIC,

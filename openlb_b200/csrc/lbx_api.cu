@@ -680,11 +680,12 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
   const int64_t n = int64_t(list.size());
   for (const FdHostCell& c : list) {
     if (c.core < 0 || c.core >= L->ncore) return fail(LBX_ERR_INVALID, "boundary cell out of range");
-    if (c.kind < LBX_FD_VELOCITY || c.kind > LBX_FD_LOCAL_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+    if (c.kind < LBX_FD_VELOCITY || c.kind > LBX_FD_LOCAL_PRESSURE_RLB) return fail(LBX_ERR_INVALID, "unknown boundary kind");
     if (c.type < LBX_NORMAL_FLAT || c.type > LBX_NORMAL_INTERNAL_EDGE) return fail(LBX_ERR_INVALID, "unknown normal type");
     const bool edge = c.type == LBX_NORMAL_EXTERNAL_EDGE || c.type == LBX_NORMAL_INTERNAL_EDGE;
     if (edge && L->d != 3) return fail(LBX_ERR_INVALID, "edges exist in 3D only");
-    const bool pressure = c.kind == LBX_FD_PRESSURE || c.kind == LBX_FD_LOCAL_PRESSURE;
+    const bool pressure =
+        c.kind == LBX_FD_PRESSURE || c.kind == LBX_FD_LOCAL_PRESSURE || c.kind == LBX_FD_LOCAL_PRESSURE_RLB;
     if (pressure && c.type != LBX_NORMAL_FLAT)
       return fail(LBX_ERR_UNSUPPORTED, "pressure boundaries are provided on flat faces only");
     int nonzero = 0;
@@ -721,8 +722,10 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
     if (c.type == LBX_NORMAL_FLAT) {
       switch (c.kind) {
         case LBX_FD_PRESSURE: t = FD_FLAT_PRESSURE; break;
-        case LBX_FD_LOCAL_VELOCITY: t = FD_FLAT_VELOCITY_LOCAL; break;
-        case LBX_FD_LOCAL_PRESSURE: t = FD_FLAT_PRESSURE_LOCAL; break;
+        case LBX_FD_LOCAL_VELOCITY:
+        case LBX_FD_LOCAL_VELOCITY_RLB: t = FD_FLAT_VELOCITY_LOCAL; break;
+        case LBX_FD_LOCAL_PRESSURE:
+        case LBX_FD_LOCAL_PRESSURE_RLB: t = FD_FLAT_PRESSURE_LOCAL; break;
         default: t = FD_FLAT_VELOCITY;
       }
     }
@@ -731,7 +734,8 @@ int install_boundary_list(lbx_lattice_s* L, std::vector<FdHostCell> list) {
     else if (c.type == LBX_NORMAL_INTERNAL_CORNER) t = FD_INNER_CORNER_VELOCITY;
     else t = FD_CORNER_VELOCITY;
     corners += t == FD_CORNER_VELOCITY;
-    hm[size_t(k)] = FdMeta::encode(t, c.n);
+    const bool rlb = c.kind == LBX_FD_LOCAL_VELOCITY_RLB || c.kind == LBX_FD_LOCAL_PRESSURE_RLB;
+    hm[size_t(k)] = FdMeta::encode(t, c.n, rlb ? 1 : 0);
     for (int v = 0; v < 4; ++v) hv[size_t(4 * k + v)] = c.v[v];
   }
   cudaDeviceSynchronize();
@@ -1123,8 +1127,8 @@ int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* ma
                                   int32_t n_fluid, const int32_t* fluid, int32_t n_outside, const int32_t* outside,
                                   const double* values) {
   if (!L || !material || !values) return fail(LBX_ERR_INVALID, "null argument");
-  if (kind < LBX_FD_VELOCITY || kind > LBX_FD_LOCAL_PRESSURE) return fail(LBX_ERR_INVALID, "unknown boundary kind");
-  const bool pressureKind = kind == LBX_FD_PRESSURE || kind == LBX_FD_LOCAL_PRESSURE;
+  if (kind < LBX_FD_VELOCITY || kind > LBX_FD_LOCAL_PRESSURE_RLB) return fail(LBX_ERR_INVALID, "unknown boundary kind");
+  const bool pressureKind = kind == LBX_FD_PRESSURE || kind == LBX_FD_LOCAL_PRESSURE || kind == LBX_FD_LOCAL_PRESSURE_RLB;
   const int32_t defFluid = 1, defOutside = 0;
   if (n_fluid == 0) {
     fluid = &defFluid;
@@ -1147,7 +1151,7 @@ int lbx_set_interpolated_boundary(lbx_lattice L, int32_t kind, const int32_t* ma
     const bool zero = nn[0] == 0 && nn[1] == 0 && nn[2] == 0;
     if (pressureKind && (t != LBX_NORMAL_FLAT || zero)) {
       if (zero) return fail(LBX_ERR_UNSUPPORTED, "could not set boundary: a pressure cell has no discrete normal");
-      if (kind == LBX_FD_LOCAL_PRESSURE)
+      if (kind == LBX_FD_LOCAL_PRESSURE || kind == LBX_FD_LOCAL_PRESSURE_RLB)
         return fail(LBX_ERR_UNSUPPORTED, "LocalPressure: no valid discrete normal (flat faces only)");
       continue;  // InterpolatedPressure installs nothing on edges and corners
     }

@@ -1379,7 +1379,7 @@ enum FdType {
 };
 
 // Meta word of a boundary cell: bits 0-2 the type, bits 3-8 the outward discrete normal, two bits
-// per axis (0: 0, 1: +1, 2: -1).
+// per axis (0: 0, 1: +1, 2: -1), bit 9 the RLB mixin.
 struct FdMeta {
   int type;
   int n[3];         // outward normal
@@ -1388,9 +1388,10 @@ struct FdMeta {
   int local;        // regularised in its collision, no post-processor (types 4 to 7)
   int flat;
   int inner;        // internal edge or corner
+  int rlb;          // collided by RLB (the default mixin of LocalVelocity / LocalPressure), not BGK
   __host__ __device__ __forceinline__ explicit FdMeta(uint16_t m)
       : type(m & 7), dir(0), orient(0), pressure((m & 7) == 1 || (m & 7) == 5), local((m & 7) >= 4),
-        flat((m & 7) <= 1 || (m & 7) == 4 || (m & 7) == 5), inner((m & 7) >= 6) {
+        flat((m & 7) <= 1 || (m & 7) == 4 || (m & 7) == 5), inner((m & 7) >= 6), rlb((m >> 9) & 1) {
     for (int a = 0; a < 3; ++a) {
       const int code = (m >> (3 + 2 * a)) & 3;
       n[a] = code == 1 ? 1 : (code == 2 ? -1 : 0);
@@ -1401,8 +1402,8 @@ struct FdMeta {
         orient = n[a];
       }
   }
-  static __host__ __device__ __forceinline__ uint16_t encode(int type, const int* normal) {
-    unsigned m = unsigned(type & 7);
+  static __host__ __device__ __forceinline__ uint16_t encode(int type, const int* normal, int rlb = 0) {
+    unsigned m = unsigned(type & 7) | (rlb ? 1u << 9 : 0u);
     for (int a = 0; a < 3; ++a) m |= unsigned(normal[a] == 1 ? 1 : (normal[a] == -1 ? 2 : 0)) << (3 + 2 * a);
     return uint16_t(m);
   }
@@ -1525,15 +1526,12 @@ __device__ __forceinline__ void fd_decode(const Geometry& g, int64_t n, int& x, 
   z = int(r - int64_t(y + 1) * g.sy) - int(g.pz);
 }
 
-// The regularisation of a flat cell of a local boundary (CombinedRLBdynamics::collide,
-// dynamics/dynamics.h:505-516) before its BGK collision: Pi from RegularizedBoundaryStress
-// (BoundaryHelpers::computeStress, boundary/helper.h:31-81: f^neq of the populations with
-// c_d = 0, none for i = 0, and of those with c_d = orientation, the latter counted twice, summed
-// in index order), then f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270).
+// Pi of a flat local boundary cell: RegularizedBoundaryStress (BoundaryHelpers::computeStress,
+// boundary/helper.h:31-81): f^neq of the populations with c_d = 0, none for i = 0, and of those
+// with c_d = orientation, the latter counted twice, summed in index order.
 template <int Q, typename R>
-__device__ __forceinline__ void local_regularize(R (&f)[Q], FdMeta m, R rho, const R (&u)[3]) {
+__device__ __forceinline__ void flat_stress(const R (&f)[Q], FdMeta m, R rho, const R (&u)[3], R (&pi)[6]) {
   using D = Desc<Q>;
-  constexpr int NPI = D::d == 3 ? 6 : 3;
   R uSqr = R(0);
   static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
   R fneq[Q];
@@ -1542,60 +1540,59 @@ __device__ __forceinline__ void local_regularize(R (&f)[Q], FdMeta m, R rho, con
     const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
     fneq[I] = (int(I) != 0 && (c == 0 || c == m.orient)) ? f[I] - equilibrium_plain<Q, I>(rho, u, uSqr) : R(0);
   });
-  R pi[NPI];
-  {
-    int iPi = 0;
-    static_for<D::d>([&](auto A) {
-      static_for<D::d>([&](auto B) {
-        if constexpr (int(B) >= int(A)) {
-          R p = R(0);
-          static_for<Q>([&](auto I) {
-            constexpr int cc = D::C[I][A] * D::C[I][B];
-            constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
-            const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
-            if (c == 0) p += R(cc) * fneq[I];
-          });
-          static_for<Q>([&](auto I) {
-            constexpr int cc = 2 * D::C[I][A] * D::C[I][B];
-            constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
-            const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
-            if (c == m.orient) p += R(cc) * fneq[I];
-          });
-          pi[iPi++] = p;
-        }
-      });
+  int iPi = 0;
+  static_for<D::d>([&](auto A) {
+    static_for<D::d>([&](auto B) {
+      if constexpr (int(B) >= int(A)) {
+        R p = R(0);
+        static_for<Q>([&](auto I) {
+          constexpr int cc = D::C[I][A] * D::C[I][B];
+          constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+          const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+          if (c == 0) p += R(cc) * fneq[I];
+        });
+        static_for<Q>([&](auto I) {
+          constexpr int cc = 2 * D::C[I][A] * D::C[I][B];
+          constexpr int c0 = D::C[I][0], c1 = D::C[I][1], c2 = D::C[I][2];
+          const int c = m.dir == 0 ? c0 : (m.dir == 1 ? c1 : c2);
+          if (c == m.orient) p += R(cc) * fneq[I];
+        });
+        pi[iPi++] = p;
+      }
     });
-  }
-  static_for<Q>([&](auto I) {
-    constexpr R t = weight<Q, R>(I);
-    R fn = R(0);
-    int iPi = 0;
-    static_for<D::d>([&](auto A) {
-      static_for<D::d>([&](auto B) {
-        if constexpr (int(B) >= int(A)) {
-          R toAdd = R(D::C[I][A] * D::C[I][B]);
-          if constexpr (int(A) == int(B)) toAdd -= R(1) / R(3);
-          else toAdd *= R(2);
-          toAdd *= pi[iPi++];
-          fn += toAdd;
-        }
-      });
-    });
-    fn *= t * R(3) * R(3) / R(2);
-    f[I] = equilibrium_plain<Q, I>(rho, u, uSqr) + fn;
   });
 }
 
-// The regularisation of an internal edge or corner (CombinedRLBdynamics::collide with
-// InnerEdgeStress3D / InnerCornerStress2D / 3D, dynamics/momenta/elements.h:1814-1897): Pi from a
-// copy of the cell whose unknown populations -- c equal to -n along every normal axis of the edge
-// (the two axes after the edge axis) or corner -- are replaced by f_opp - f^eq_opp + f^eq_i
-// (lbm::computeStress, dynamics/lbm.h:333-351: sum c_a c_b f - rho u_a u_b, less (rho - 1) / 3
-// on the diagonal), then f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) as for the flat cells.
+// Pi from the second moment of populations h (lbm::computeStress, dynamics/lbm.h:333-351:
+// sum c_a c_b h - rho u_a u_b, less (rho - 1) / 3 on the diagonal): BulkStress (the external
+// edges and corners of a local boundary), and the internal edges' and corners' completed cell.
 template <int Q, typename R>
-__device__ __forceinline__ void inner_regularize(R (&f)[Q], FdMeta m, R rho, const R (&u)[3]) {
+__device__ __forceinline__ void moment_stress(const R (&h)[Q], R rho, const R (&u)[3], R (&pi)[6]) {
   using D = Desc<Q>;
-  constexpr int NPI = D::d == 3 ? 6 : 3;
+  int iPi = 0;
+  static_for<D::d>([&](auto A) {
+    static_for<D::d>([&](auto B) {
+      if constexpr (int(B) >= int(A)) {
+        R p = R(0);
+        static_for<Q>([&](auto I) {
+          constexpr int cc = D::C[I][A] * D::C[I][B];
+          if constexpr (cc != 0) p += R(cc) * h[I];
+        });
+        p -= rho * u[A] * u[B];
+        if constexpr (int(A) == int(B)) p -= R(1) / R(3) * (rho - R(1));
+        pi[iPi++] = p;
+      }
+    });
+  });
+}
+
+// Pi of an internal edge or corner (InnerEdgeStress3D / InnerCornerStress2D / 3D,
+// dynamics/momenta/elements.h:1814-1897): the second moment of a copy of the cell whose unknown
+// populations -- c equal to -n along every normal axis of the edge (the two axes after the edge
+// axis) or corner -- are replaced by f_opp - f^eq_opp + f^eq_i.
+template <int Q, typename R>
+__device__ __forceinline__ void inner_stress(const R (&f)[Q], FdMeta m, R rho, const R (&u)[3], R (&pi)[6]) {
+  using D = Desc<Q>;
   R uSqr = R(0);
   static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
   int plane = -1;  // the edge axis, none for a corner
@@ -1612,42 +1609,69 @@ __device__ __forceinline__ void inner_regularize(R (&f)[Q], FdMeta m, R rho, con
     constexpr int O = D::OPP[I];
     h[I] = unknown ? f[O] - equilibrium_plain<Q, O>(rho, u, uSqr) + equilibrium_plain<Q, I>(rho, u, uSqr) : f[I];
   });
-  R pi[NPI];
-  {
-    int iPi = 0;
-    static_for<D::d>([&](auto A) {
-      static_for<D::d>([&](auto B) {
-        if constexpr (int(B) >= int(A)) {
-          R p = R(0);
-          static_for<Q>([&](auto I) {
-            constexpr int cc = D::C[I][A] * D::C[I][B];
-            if constexpr (cc != 0) p += R(cc) * h[I];
-          });
-          p -= rho * u[A] * u[B];
-          if constexpr (int(A) == int(B)) p -= R(1) / R(3) * (rho - R(1));
-          pi[iPi++] = p;
-        }
-      });
+  moment_stress<Q, R>(h, rho, u, pi);
+}
+
+// Pi of a boundary cell through its momenta: flat local cells RegularizedBoundaryStress, internal
+// edges and corners their inner stress, external edges and corners BulkStress
+// (momenta::FixedVelocityBoundaryTuple, aliases.h:215-220).
+template <int Q, typename R>
+__device__ __forceinline__ void boundary_stress(const R (&f)[Q], FdMeta m, R rho, const R (&u)[3], R (&pi)[6]) {
+  if (m.flat) flat_stress<Q, R>(f, m, rho, u, pi);
+  else if (m.inner) inner_stress<Q, R>(f, m, rho, u, pi);
+  else moment_stress<Q, R>(f, rho, u, pi);
+}
+
+// fromPiToFneq(i, Pi) (dynamics/lbm.h:247-270)
+template <int Q, int I, typename R>
+__device__ __forceinline__ R fneq_of_pi(const R (&pi)[6]) {
+  using D = Desc<Q>;
+  constexpr R t = weight<Q, R>(I);
+  R fn = R(0);
+  int iPi = 0;
+  static_for<D::d>([&](auto A) {
+    static_for<D::d>([&](auto B) {
+      if constexpr (int(B) >= int(A)) {
+        R toAdd = R(D::C[I][A] * D::C[I][B]);
+        if constexpr (int(A) == int(B)) toAdd -= R(1) / R(3);
+        else toAdd *= R(2);
+        toAdd *= pi[iPi++];
+        fn += toAdd;
+      }
     });
-  }
-  static_for<Q>([&](auto I) {
-    constexpr R t = weight<Q, R>(I);
-    R fn = R(0);
-    int iPi = 0;
-    static_for<D::d>([&](auto A) {
-      static_for<D::d>([&](auto B) {
-        if constexpr (int(B) >= int(A)) {
-          R toAdd = R(D::C[I][A] * D::C[I][B]);
-          if constexpr (int(A) == int(B)) toAdd -= R(1) / R(3);
-          else toAdd *= R(2);
-          toAdd *= pi[iPi++];
-          fn += toAdd;
-        }
-      });
-    });
-    fn *= t * R(3) * R(3) / R(2);
-    f[I] = equilibrium_plain<Q, I>(rho, u, uSqr) + fn;
   });
+  fn *= t * R(3) * R(3) / R(2);
+  return fn;
+}
+
+// The regularisation of a local boundary cell -- flat, or an internal edge or corner of any
+// velocity boundary -- before its mixed-in collision (CombinedRLBdynamics::collide,
+// dynamics/dynamics.h:505-516): Pi from the boundary momenta, then
+// f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi).
+template <int Q, typename R>
+__device__ __forceinline__ void local_regularize(R (&f)[Q], FdMeta m, R rho, const R (&u)[3]) {
+  using D = Desc<Q>;
+  R uSqr = R(0);
+  static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+  R pi[6];
+  boundary_stress<Q, R>(f, m, rho, u, pi);
+  static_for<Q>([&](auto I) { f[I] = equilibrium_plain<Q, I>(rho, u, uSqr) + fneq_of_pi<Q, I, R>(pi); });
+}
+
+// The RLB collision with the boundary momenta (collision::RLB, dynamics/collision.h:82-112), the
+// default mixed-in dynamics of LocalVelocity / LocalPressure: f_i = f_i^eq(rho, u) +
+// (1 - omega) fromPiToFneq(i, Pi), Pi from the momenta's stress.  Returns |u|^2.
+template <int Q, typename R>
+__device__ __forceinline__ R rlb_relax(R (&f)[Q], FdMeta m, R rho, const R (&u)[3], R omega) {
+  using D = Desc<Q>;
+  R uSqr = R(0);
+  static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+  R pi[6];
+  boundary_stress<Q, R>(f, m, rho, u, pi);
+  static_for<Q>([&](auto I) {
+    f[I] = equilibrium_plain<Q, I>(rho, u, uSqr) + (R(1) - omega) * fneq_of_pi<Q, I, R>(pi);
+  });
+  return uSqr;
 }
 
 // Collision of the boundary cells: BGKdynamics with the boundary momenta
@@ -1672,17 +1696,20 @@ __global__ void __launch_bounds__(256) k_fd_collide(S* __restrict__ pop, Geometr
     R rho, u[3];
     fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
     if (m.local) {  // regularised first, then collided with the momenta of the rebuilt cell
-      if (m.inner) inner_regularize<Q, R>(f, m, rho, u);
-      else local_regularize<Q, R>(f, m, rho, u);
+      local_regularize<Q, R>(f, m, rho, u);
       fd_momenta<Q, R>(f, m, fdValue + 4 * b, rho, u);
     }
     R uSqr = R(0);
-    static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
     const R w = R(omega);
-    static_for<Q>([&](auto I) {
-      f[I] *= R(1) - w;
-      f[I] += w * equilibrium_plain<Q, I>(rho, u, uSqr);
-    });
+    if (m.rlb) {  // the RLB mixin of a local boundary
+      uSqr = rlb_relax<Q, R>(f, m, rho, u, w);
+    } else {
+      static_for<D::d>([&](auto A) { uSqr += u[A] * u[A]; });
+      static_for<Q>([&](auto I) {
+        f[I] *= R(1) - w;
+        f[I] += w * equilibrium_plain<Q, I>(rho, u, uSqr);
+      });
+    }
     static_for<Q>([&](auto I) { Storage<S>::store(pop + I * g.stride + wrap_add(n, sh.s[I], g.n), f[I]); });
     if (g.pmask) {
       int x, y, z;

@@ -244,6 +244,8 @@ def build_bouzidi_links(q: int, core, material: np.ndarray, fluid: int = 1, soli
 
 
 FD_VELOCITY, FD_PRESSURE, FD_LOCAL_VELOCITY, FD_LOCAL_PRESSURE = 1, 2, 3, 4
+# LocalVelocity / LocalPressure with their default RLB mixin
+FD_LOCAL_VELOCITY_RLB, FD_LOCAL_PRESSURE_RLB = 5, 6
 
 
 NORMAL_FLAT, NORMAL_EXTERNAL_CORNER, NORMAL_INTERNAL_CORNER, NORMAL_EXTERNAL_EDGE, NORMAL_INTERNAL_EDGE = 0, 1, 2, 3, 4
@@ -873,9 +875,9 @@ class SlabLattice:
         zero = ~np.abs(normals).any(axis=1)
         if zero.any() or (types < 0).any():
             raise LbxError(-4, "could not set boundary: a cell has no discrete normal")
-        if kind in (FD_PRESSURE, FD_LOCAL_PRESSURE):
+        if kind in (FD_PRESSURE, FD_LOCAL_PRESSURE, FD_LOCAL_PRESSURE_RLB):
             keep = types == NORMAL_FLAT
-            if kind == FD_LOCAL_PRESSURE and not keep.all():
+            if kind in (FD_LOCAL_PRESSURE, FD_LOCAL_PRESSURE_RLB) and not keep.all():
                 raise LbxError(-4, "LocalPressure: no valid discrete normal (flat faces only)")
             cells, types, normals = cells[keep], types[keep], normals[keep]
         vals = np.asarray(values, np.float64).reshape(-1, 4)[cells]

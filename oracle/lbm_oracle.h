@@ -64,7 +64,8 @@ typedef struct {
                                 (local: boundary::LocalVelocity / LocalPressure with BGK mixed
                                 in; flat cells regularised in the collision, no post-processor;
                                 src/boundary/localVelocity3D.h:47-115, localPressure3D.h,
-                                dynamics/dynamics.h:470-523) */
+                                dynamics/dynamics.h:470-523); 5 velocity, 6 pressure (local with
+                                their default RLB mixin, src/dynamics/collision.h:82-112) */
   const int32_t* fd_dir;     /* normal axis */
   const int32_t* fd_orient;  /* outward normal sign, -1 or +1 */
   const double* fd_value;    /* 4 per cell: the velocity, or {rho, tangential velocity} */

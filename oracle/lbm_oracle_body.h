@@ -196,7 +196,7 @@ static void FN(fd_momenta)(const lbo_desc* d, const REAL* g, int kind, int type,
     if (d->c[i][dir] == 0) onWall += g[i];
   for (int i = 0; i < q; ++i)
     if (d->c[i][dir] == orient) normal += g[i];
-  if (kind == 1 || kind == 3) {
+  if (kind == 1 || kind == 3 || kind == 5) {
     for (int a = 0; a < dim; ++a) u[a] = (REAL)value[a];
     *rho = ((REAL)2 * normal + onWall + (REAL)1) / ((REAL)1 + (REAL)orient * u[dir]);
   } else {
@@ -216,15 +216,12 @@ static REAL FN(second_order)(const lbo_desc* d, int i, REAL rho, const REAL* u, 
   return rho * t * ((REAL)1 + invCs2 * cu + invCs2 * invCs2 * (REAL)0.5 * cu * cu - invCs2 * (REAL)0.5 * uSqr) - t;
 }
 
-/* The regularisation of a local boundary cell (CombinedRLBdynamics::collide, src/dynamics/
- * dynamics.h:505-516, before the mixed-in BGK collision): rho and u from the boundary momenta,
- * Pi from RegularizedBoundaryStress (BoundaryHelpers::computeStress, src/boundary/helper.h:31-81:
- * f^neq of the populations with c_d = 0 (none for i = 0) and of those with c_d = o, the latter
- * counted twice), then f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi) (src/dynamics/lbm.h:247-270). */
-static void FN(local_regularize)(const lbo_desc* d, REAL rho, const REAL* u, const int* nrm, REAL* g)
+/* Pi of a flat local boundary cell: RegularizedBoundaryStress (BoundaryHelpers::computeStress,
+ * src/boundary/helper.h:31-81): f^neq of the populations with c_d = 0 (none for i = 0) and of
+ * those with c_d = o, the latter counted twice. */
+static void FN(flat_stress)(const lbo_desc* d, const REAL* g, REAL rho, const REAL* u, const int* nrm, REAL* pi)
 {
   const int q = d->q, dim = d->d;
-  const REAL invCs2 = (REAL)3;
   int dir = 0, orient = 0;
   for (int a = dim - 1; a >= 0; --a)
     if (nrm[a] != 0) { dir = a; orient = nrm[a]; }
@@ -236,7 +233,6 @@ static void FN(local_regularize)(const lbo_desc* d, REAL rho, const REAL* u, con
     if (d->c[i][dir] == 0) fneq[i] = g[i] - FN(second_order)(d, i, rho, u, uSqr);
   for (int i = 0; i < q; ++i)
     if (d->c[i][dir] == orient) fneq[i] = g[i] - FN(second_order)(d, i, rho, u, uSqr);
-  REAL pi[6];
   int iPi = 0;
   for (int a = 0; a < dim; ++a)
     for (int b = a; b < dim; ++b) {
@@ -247,34 +243,34 @@ static void FN(local_regularize)(const lbo_desc* d, REAL rho, const REAL* u, con
         if (d->c[i][dir] == orient) pi[iPi] += (REAL)(2 * d->c[i][a] * d->c[i][b]) * fneq[i];
       ++iPi;
     }
-  for (int i = 0; i < q; ++i) {
-    const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
-    REAL fn = 0;
-    iPi = 0;
-    for (int a = 0; a < dim; ++a)
-      for (int b = a; b < dim; ++b) {
-        REAL toAdd = (REAL)(d->c[i][a] * d->c[i][b]);
-        if (a == b) toAdd -= (REAL)1 / invCs2;
-        else toAdd *= (REAL)2;
-        toAdd *= pi[iPi++];
-        fn += toAdd;
-      }
-    fn *= t * invCs2 * invCs2 / (REAL)2;
-    g[i] = FN(second_order)(d, i, rho, u, uSqr) + fn;
-  }
 }
 
-/* The regularisation of an internal edge or corner (CombinedRLBdynamics::collide with
- * InnerEdgeStress3D / InnerCornerStress2D / 3D, src/dynamics/momenta/elements.h:1814-1897): a
- * copy of the cell whose unknown populations -- c along every normal axis of the edge (the two
- * axes after the edge axis) or corner equal to -n -- are replaced by f_opp - f^eq_opp + f^eq_i;
- * Pi from its second moment (lbm::computeStress, src/dynamics/lbm.h:333-351:
- * sum_i c_ia c_ib f_i - rho u_a u_b - (rho - 1) / c_s^-2 on the diagonal), then
- * f_i = f_i^eq(rho, u) + fromPiToFneq(i, Pi). */
-static void FN(inner_regularize)(const lbo_desc* d, REAL rho, const REAL* u, int type, const int* nrm, REAL* g)
+/* Pi from the second moment of populations h (lbm::computeStress, src/dynamics/lbm.h:333-351:
+ * sum_i c_ia c_ib h_i - rho u_a u_b - (rho - 1) / c_s^-2 on the diagonal): BulkStress, and the
+ * inner edge / corner stress on their completed cell. */
+static void FN(moment_stress)(const lbo_desc* d, const REAL* h, REAL rho, const REAL* u, REAL* pi)
 {
   const int q = d->q, dim = d->d;
   const REAL invCs2 = (REAL)3;
+  int iPi = 0;
+  for (int a = 0; a < dim; ++a)
+    for (int b = a; b < dim; ++b) {
+      pi[iPi] = 0;
+      for (int i = 0; i < q; ++i) pi[iPi] += (REAL)(d->c[i][a] * d->c[i][b]) * h[i];
+      pi[iPi] -= rho * u[a] * u[b];
+      if (a == b) pi[iPi] -= (REAL)1 / invCs2 * (rho - (REAL)1);
+      ++iPi;
+    }
+}
+
+/* Pi of an internal edge or corner (InnerEdgeStress3D / InnerCornerStress2D / 3D, src/dynamics/
+ * momenta/elements.h:1814-1897): a copy of the cell whose unknown populations -- c equal to -n
+ * along every normal axis of the edge (the two axes after the edge axis) or corner -- are
+ * replaced by f_opp - f^eq_opp + f^eq_i, then its second moment. */
+static void FN(inner_stress)(const lbo_desc* d, const REAL* g, REAL rho, const REAL* u, int type, const int* nrm,
+                             REAL* pi)
+{
+  const int q = d->q, dim = d->d;
   REAL uSqr = 0;
   for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
   int axes[3], na = 0;
@@ -298,31 +294,66 @@ static void FN(inner_regularize)(const lbo_desc* d, REAL rho, const REAL* u, int
       h[i] = g[o] - FN(second_order)(d, o, rho, u, uSqr) + FN(second_order)(d, i, rho, u, uSqr);
     }
   }
-  REAL pi[6];
+  FN(moment_stress)(d, h, rho, u, pi);
+}
+
+/* fromPiToFneq(i, Pi) (src/dynamics/lbm.h:247-270). */
+static REAL FN(fneq_of_pi)(const lbo_desc* d, int i, const REAL* pi)
+{
+  const int dim = d->d;
+  const REAL invCs2 = (REAL)3;
+  const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
+  REAL fn = 0;
   int iPi = 0;
   for (int a = 0; a < dim; ++a)
     for (int b = a; b < dim; ++b) {
-      pi[iPi] = 0;
-      for (int i = 0; i < q; ++i) pi[iPi] += (REAL)(d->c[i][a] * d->c[i][b]) * h[i];
-      pi[iPi] -= rho * u[a] * u[b];
-      if (a == b) pi[iPi] -= (REAL)1 / invCs2 * (rho - (REAL)1);
-      ++iPi;
+      REAL toAdd = (REAL)(d->c[i][a] * d->c[i][b]);
+      if (a == b) toAdd -= (REAL)1 / invCs2;
+      else toAdd *= (REAL)2;
+      toAdd *= pi[iPi++];
+      fn += toAdd;
     }
-  for (int i = 0; i < q; ++i) {
-    const REAL t = (REAL)d->tn[i] / (REAL)d->td[i];
-    REAL fn = 0;
-    iPi = 0;
-    for (int a = 0; a < dim; ++a)
-      for (int b = a; b < dim; ++b) {
-        REAL toAdd = (REAL)(d->c[i][a] * d->c[i][b]);
-        if (a == b) toAdd -= (REAL)1 / invCs2;
-        else toAdd *= (REAL)2;
-        toAdd *= pi[iPi++];
-        fn += toAdd;
-      }
-    fn *= t * invCs2 * invCs2 / (REAL)2;
-    g[i] = FN(second_order)(d, i, rho, u, uSqr) + fn;
-  }
+  fn *= t * invCs2 * invCs2 / (REAL)2;
+  return fn;
+}
+
+/* Pi of boundary cell with normal type `type` and kind `kind` through its momenta: flat local
+ * cells RegularizedBoundaryStress, internal edges and corners their inner stress, external edges
+ * and corners BulkStress (momenta::FixedVelocityBoundaryTuple). */
+static void FN(boundary_stress)(const lbo_desc* d, const REAL* g, REAL rho, const REAL* u, int type,
+                                const int* nrm, REAL* pi)
+{
+  if (type == 0) FN(flat_stress)(d, g, rho, u, nrm, pi);
+  else if (type == 2 || type == 4) FN(inner_stress)(d, g, rho, u, type, nrm, pi);
+  else FN(moment_stress)(d, g, rho, u, pi);
+}
+
+/* The regularisation of a local boundary cell, flat or an internal edge or corner
+ * (CombinedRLBdynamics::collide, src/dynamics/dynamics.h:505-516, before the mixed-in
+ * collision): rho, u and Pi from the boundary momenta, then f_i = f_i^eq(rho, u) +
+ * fromPiToFneq(i, Pi). */
+static void FN(local_regularize)(const lbo_desc* d, REAL rho, const REAL* u, int type, const int* nrm, REAL* g)
+{
+  const int q = d->q, dim = d->d;
+  REAL uSqr = 0;
+  for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+  REAL pi[6];
+  FN(boundary_stress)(d, g, rho, u, type, nrm, pi);
+  for (int i = 0; i < q; ++i) g[i] = FN(second_order)(d, i, rho, u, uSqr) + FN(fneq_of_pi)(d, i, pi);
+}
+
+/* RLB collision with the boundary momenta (collision::RLB, src/dynamics/collision.h:82-112):
+ * f_i = f_i^eq(rho, u) + (1 - omega) fromPiToFneq(i, Pi), Pi from the momenta's stress. */
+static REAL FN(rlb_with)(const lbo_desc* d, REAL omega, REAL rho, const REAL* u, int type, const int* nrm, REAL* g)
+{
+  const int q = d->q, dim = d->d;
+  REAL uSqr = 0;
+  for (int a = 0; a < dim; ++a) uSqr += u[a] * u[a];
+  REAL pi[6];
+  FN(boundary_stress)(d, g, rho, u, type, nrm, pi);
+  for (int i = 0; i < q; ++i)
+    g[i] = FN(second_order)(d, i, rho, u, uSqr) + ((REAL)1 - omega) * FN(fneq_of_pi)(d, i, pi);
+  return uSqr;
 }
 
 /* BGK collision with given rho, u: lbm::bgkCollision (src/dynamics/lbm.h:395-403). */
@@ -617,16 +648,15 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
         FN(fd_meta)(c, b, &type, nrm);
         for (int i = 0; i < q; ++i) g[i] = LOAD(f[i * n + x]);
         FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
-        if (c->fd_kind[b] >= 3 && type == 0) {
-          /* local boundary: regularised first, then the BGK collision with the same momenta */
-          FN(local_regularize)(d, rho, u, nrm, g);
-          FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
-        } else if (type == 2 || type == 4) {
-          /* internal edge / corner: CombinedRLBdynamics, regularised the same way */
-          FN(inner_regularize)(d, rho, u, type, nrm, g);
+        if ((c->fd_kind[b] >= 3 && type == 0) || type == 2 || type == 4) {
+          /* local flat cell, internal edge / corner: CombinedRLBdynamics, regularised first, then
+           * the mixed-in collision with the momenta of the rebuilt cell */
+          FN(local_regularize)(d, rho, u, type, nrm, g);
           FN(fd_momenta)(d, g, c->fd_kind[b], type, nrm, c->fd_value + 4 * b, &rho, u);
         }
-        cellUsq[x] = FN(bgk_with)(d, (REAL)c->omega, rho, u, g);
+        /* the mixed-in dynamics: RLB for kinds 5 and 6, BGK otherwise */
+        if (c->fd_kind[b] >= 5) cellUsq[x] = FN(rlb_with)(d, (REAL)c->omega, rho, u, type, nrm, g);
+        else cellUsq[x] = FN(bgk_with)(d, (REAL)c->omega, rho, u, g);
         cellRho[x] = rho;
         for (int i = 0; i < q; ++i) f[i * n + x] = STORE(g[i]);
       } else if (m == LBO_BOUNCE_BACK) {

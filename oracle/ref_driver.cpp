@@ -30,7 +30,7 @@
  *    lbref geo --mat FILE --n NX NY [NZ] [--periodic PX PY [PZ]] [--dyn ...] [--omega W] ...
  *          [--bouzidi M,...] [--lid M --ulid U] [--bounceback M,...] [--outside M,...]
  *          [--ivel M,... (--poiseuille UMAX | --uconst UX UY [UZ])] [--ivel-lid M] [--ipres M --rho R]
- *          [--bbvel M] [--local] [--bgk-mat M]
+ *          [--bbvel M] [--local] [--local-rlb] [--bgk-mat M]
  *          [--classify M] [--classify-only] [--force-mat M --force-every K] [--moments]
  *          [--no-pops] [--steps S] [--out PREFIX]
  *  The geo case reads the int32 materials of the core cells from FILE (x slowest, z fastest)
@@ -47,7 +47,8 @@
  *  --local sets boundary::LocalVelocity / LocalPressure with BGK as the mixed-in dynamics on the
  *  --ivel / --ivel-lid / --ipres materials instead (src/boundary/localVelocity3D.h:47-115,
  *  localPressure3D.h, localVelocity2D.h: CombinedRLBdynamics on flat faces, the interpolated
- *  boundary's edges and corners).
+ *  boundary's edges and corners); --local-rlb sets them with their default mixed-in dynamics,
+ *  RLBdynamics (boundary/localVelocity.h:44-49, localPressure.h:31-36).
  *  --bgk-mat M puts BGKdynamics on material M beside the --dyn dynamics of material 1.
  *  --classify M writes PREFIX.normals.bin (int32 {core cell, type, n0, n1, n2} per cell of
  *  material M, fluid 1, outside {0, --outside...}); --classify-only stops there.
@@ -147,6 +148,7 @@ struct Options {
   double poiseuille = -1.0, uconst[3] = {0, 0, 0}, rhoOut = 1.0;
   bool classifyOnly = false, moments = false, noPops = false;
   bool local = false;  // --local: LocalVelocity / LocalPressure (BGK mixin) instead of the interpolated ones
+  bool localRlb = false;  // --local-rlb: the same with their default RLB mixin
   int bgkMat = -1;     // --bgk-mat M: BGKdynamics on material M beside the --dyn dynamics on material 1
 };
 
@@ -238,6 +240,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--ivel-lid") o.ivelLidMat = std::atoi(next());
     else if (a == "--bbvel") o.bbvelMat = std::atoi(next());
     else if (a == "--local") o.local = true;
+    else if (a == "--local-rlb") o.local = o.localRlb = true;
     else if (a == "--bgk-mat") o.bgkMat = std::atoi(next());
     else if (a == "--ipres") o.ipresMat = std::atoi(next());
     else if (a == "--poiseuille") o.poiseuille = std::atof(next());
@@ -376,7 +379,10 @@ int runGeo(const Options& o) {
   std::vector<int> ivelAll = o.ivelMats;
   if (o.ivelLidMat >= 0) ivelAll.push_back(o.ivelLidMat);
   for (int m : ivelAll) {
-    if (o.local)
+    if (o.localRlb)
+      boundary::set<T, DESCRIPTOR, boundary::LocalVelocity<T,DESCRIPTOR>>(
+        lat, geo.getMaterialIndicator({m}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+    else if (o.local)
       boundary::set<T, DESCRIPTOR, boundary::LocalVelocity<T,DESCRIPTOR,BGKdynamics<T,DESCRIPTOR>>>(
         lat, geo.getMaterialIndicator({m}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
     else
@@ -385,7 +391,10 @@ int runGeo(const Options& o) {
   }
   auto isIvel = [&](int m) { return std::find(ivelAll.begin(), ivelAll.end(), m) != ivelAll.end(); };
   if (o.ipresMat >= 0) {
-    if (o.local)
+    if (o.localRlb)
+      boundary::set<T, DESCRIPTOR, boundary::LocalPressure<T,DESCRIPTOR>>(
+        lat, geo.getMaterialIndicator({o.ipresMat}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
+    else if (o.local)
       boundary::set<T, DESCRIPTOR, boundary::LocalPressure<T,DESCRIPTOR,BGKdynamics<T,DESCRIPTOR>>>(
         lat, geo.getMaterialIndicator({o.ipresMat}), geo.getMaterialIndicator({1}), geo.getMaterialIndicator(std::vector<int>(outside)));
     else

@@ -249,6 +249,22 @@ GEO = {
                                                                       *RND, "--steps", "60"]),
     "geo_step_d3q19_ivel_bgk_f32": ("d3q19_f32", (12, 11, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
                                                                 "--ivel-lid", "3", "--ulid", "0.05", "--steps", "60"]),
+    # LocalVelocity / LocalPressure with their default mixed-in dynamics, RLBdynamics: the flat
+    # cells, internal edges and corners regularised twice (CombinedRLBdynamics, then the RLB
+    # collision), the external edges and corners collided by RLB with the fixed-velocity momenta
+    "geo_cavity_d3q19_lrlb_bgk_f64": ("d3q19_f64_nocse", (9, 8, 10), ["--dyn", "bgk", "--omega", "1.4", "--ivel", "2",
+                                                                      "--ivel-lid", "3", "--ulid", "0.05",
+                                                                      "--local-rlb", *RND, "--steps", "60"]),
+    "geo_cavity_d2q9_lrlb_bgk_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
+                                                                  "--ivel-lid", "3", "--ulid", "0.1", "--local-rlb",
+                                                                  "--steps", "150"]),
+    "geo_step_d3q27_lrlb_trt_f64": ("d3q27_f64_nocse", (11, 10, 9), ["--dyn", "trt", "--omega", "1.6", "--magic",
+                                                                     "0.25", "--ivel", "2", "--ivel-lid", "3",
+                                                                     "--ulid", "0.05", "--local-rlb", "--steps", "80"]),
+    "geo_channel_d3q19_lrlb_f64": ("d3q19_f64_nocse", (20, 12, 11), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "3",
+                                                                     "--poiseuille", "0.05", "--ipres", "4", "--rho",
+                                                                     "0.99", "--bounceback", "2", "--bouzidi", "5",
+                                                                     "--local-rlb", *RND, "--steps", "60"]),
     # two fluid dynamics in one block: ForcedBGK on material 1 and BGK on material 6 (periodic)
     "geo_two_dyn_d3q19_fbgk_bgk_f64": ("d3q19_f64_nocse", (12, 10, 9), ["--dyn", "fbgk", "--omega", "1.3", "--force",
                                                                         "1e-4", "2e-5", "0", "--periodic", "1", "1",
@@ -261,9 +277,11 @@ GEO_STEP = {"geo_step_d2q9_ivel_bgk_f64": (slice(8, None), slice(None, 5)),
             "geo_step_d3q19_ivel_bgk_f64": (slice(7, None), slice(None, 5), slice(6, None)),
             "geo_step_d3q27_ivel_trt_f64": (slice(6, None), slice(None, 5), slice(5, None)),
             "geo_step_d3q19_lvel_bgk_f64": (slice(7, None), slice(None, 5), slice(6, None)),
-            "geo_step_d3q19_ivel_bgk_f32": (slice(7, None), slice(None, 5), slice(6, None))}
+            "geo_step_d3q19_ivel_bgk_f32": (slice(7, None), slice(None, 5), slice(6, None)),
+            "geo_step_d3q27_lrlb_trt_f64": (slice(6, None), slice(None, 5), slice(5, None))}
 GEO_SPHERE = {"geo_channel_d3q27_trt_f64": (8, 7, 7, 3), "geo_channel_d3q27_trt_f32": (8, 7, 7, 3),
-              "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5), "geo_channel_d3q19_lvel_lpres_f64": (6, 5, 6, 2.5)}
+              "geo_channel_d3q19_bgk_rnd_f64": (6, 5, 6, 2.5), "geo_channel_d3q19_lvel_lpres_f64": (6, 5, 6, 2.5),
+              "geo_channel_d3q19_lrlb_f64": (6, 5, 6, 2.5)}
 
 
 def geo_material(name: str) -> np.ndarray:

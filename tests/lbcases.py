@@ -163,7 +163,8 @@ def case_setup(fx: dict) -> dict:
         setup["cell_dyn"] = cd
         kinds = bc[:, 1].astype(np.int32)
         if a["local"]:
-            kinds = kinds + 2  # LocalVelocity / LocalPressure: kinds 3 and 4
+            # LocalVelocity / LocalPressure: kinds 3 and 4 (BGK mixin), 5 and 6 (RLB mixin)
+            kinds = kinds + (4 if a["rlb"] else 2)
         setup["fd"] = {"cells": bc[:, 0].astype(np.int64), "kinds": kinds,
                        "types": bc[:, 2].astype(np.int32), "normals": np.ascontiguousarray(bc[:, 3:6], np.int32),
                        "values": np.ascontiguousarray(fx["vals"][bc[:, 0]])}
@@ -190,7 +191,8 @@ def geo_args(meta: dict) -> dict:
     lid = value("--lid")
     return {"bouzidi": ints("--bouzidi"), "bounceback": ints("--bounceback"), "ivel": ints("--ivel"),
             "ivel_lid": ints("--ivel-lid"), "ipres": ints("--ipres"), "lid": int(lid) if lid else None,
-            "bbvel": ints("--bbvel"), "local": "--local" in args,
+            "bbvel": ints("--bbvel"), "local": "--local" in args or "--local-rlb" in args,
+            "rlb": "--local-rlb" in args,
             "bgk_mat": int(value("--bgk-mat")) if value("--bgk-mat") else None,
             "force_mat": ints("--force-mat")}
 

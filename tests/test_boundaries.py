@@ -149,7 +149,10 @@ def build_from_materials(fx, storage):
     if a["bbvel"]:
         cells = np.nonzero(np.isin(mat, a["bbvel"]))[0]
         lat.set_bounce_back_velocity(cells, fx["vals"][cells, 0], fx["vals"][cells, 1:4])
-    vel, pres = (lbx.FD_LOCAL_VELOCITY, lbx.FD_LOCAL_PRESSURE) if a["local"] else (lbx.FD_VELOCITY, lbx.FD_PRESSURE)
+    vel, pres = (lbx.FD_VELOCITY, lbx.FD_PRESSURE)
+    if a["local"]:
+        vel, pres = ((lbx.FD_LOCAL_VELOCITY_RLB, lbx.FD_LOCAL_PRESSURE_RLB) if a["rlb"]
+                     else (lbx.FD_LOCAL_VELOCITY, lbx.FD_LOCAL_PRESSURE))
     for m in a["ivel"] + a["ivel_lid"]:
         lat.set_interpolated_boundary(vel, mat, m, fx["vals"])
     for m in a["ipres"]:
