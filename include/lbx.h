@@ -158,6 +158,14 @@ int lbx_set_dynamics(lbx_lattice lattice, int32_t dynamics, const lbx_params* pa
  * classes (LBX_ERR_UNSUPPORTED). */
 int lbx_set_dynamics_class(lbx_lattice lattice, int32_t cls, const lbx_params* params);
 
+/* lbx_set_dynamics_class with a dynamics of its own for class `cls` (LBX_BGK ..
+ * LBX_SMAGORINSKY_FORCED_BGK; ConstRhoBGK returns LBX_ERR_UNSUPPORTED): a block whose
+ * materials carry dynamics of different kinds, e.g. TRTdynamics on one material beside
+ * BGKdynamics on another (dynamics::set per material, core/blockDynamicsMap.h:264-310).  The
+ * class's cells collide with that dynamics and these parameters; params = NULL removes the
+ * class. */
+int lbx_set_dynamics_class_kind(lbx_lattice lattice, int32_t cls, int32_t dynamics, const lbx_params* params);
+
 /* Per-cell dynamics ids for the core cells ([core cells], lbx_cell_dynamics); NULL resets
  * to "bulk everywhere" (defineDynamics over a material, core/blockLattice.hh:274-286). */
 int lbx_set_cell_dynamics(lbx_lattice lattice, const uint8_t* ids);

@@ -173,6 +173,7 @@ struct lbx_lattice_s {
   // class c is defined
   int classMask = 0;
   lbx_params classParams[3] = {};
+  int classDyn[3] = {0, 0, 0};  // a class's own dynamics (lbx_set_dynamics_class_kind), 0: the lattice's
   int blockX = 256, blockY = 1;
   int kernel = 2;
   int cellsPerThread = 1;
@@ -246,6 +247,7 @@ LaunchArgs args_of(const lbx_lattice_s* L) {
     a.classParam[c][1] = pc.magic;
     a.classParam[c][2] = pc.smagorinsky;
     for (int k = 0; k < 3; ++k) a.classParam[c][3 + k] = pc.force[k];
+    a.classDyn[c] = (L->classMask >> c & 1) ? L->classDyn[c] : 0;
   }
   return a;
 }
@@ -1062,10 +1064,21 @@ int lbx_set_dynamics_class(lbx_lattice L, int32_t cls, const lbx_params* params)
   if (L->dynamics == LBX_CONST_RHO_BGK)
     return fail(LBX_ERR_UNSUPPORTED, "ConstRhoBGK couples every cell to one average density; no classes");
   L->classParams[cls - 1] = *params;
+  L->classDyn[cls - 1] = 0;
   L->classMask |= 1 << (cls - 1);
   // the classes run on the one-cell-per-thread step kernel
   L->kernel = 1;
   L->cellsPerThread = 1;
+  return LBX_OK;
+}
+
+int lbx_set_dynamics_class_kind(lbx_lattice L, int32_t cls, int32_t dynamics, const lbx_params* params) {
+  if (!L) return fail(LBX_ERR_INVALID, "null lattice");
+  if (!params) return lbx_set_dynamics_class(L, cls, nullptr);
+  if (dynamics < LBX_BGK || dynamics > LBX_SMAGORINSKY_FORCED_BGK)
+    return fail(LBX_ERR_UNSUPPORTED, "a class's dynamics must be BGK, TRT, Smagorinsky-BGK or a forced one");
+  if (int rc = lbx_set_dynamics_class(L, cls, params)) return rc;
+  L->classDyn[cls - 1] = dynamics == L->dynamics ? 0 : dynamics;
   return LBX_OK;
 }
 

@@ -234,8 +234,23 @@ static __global__ void __launch_bounds__(kFinalizeThreads) k_finalize4(const dou
 // lattice has none.
 template <typename R> struct ClassParams {
   CollisionParams<R> p[3];
+  int dyn[3];  // the class's dynamics when it is not the lattice's (DYN_*), else 0
   int used;
 };
+
+// One collision of any bulk dynamics chosen at run time: the cells of a parameter class whose
+// dynamics differ in kind from the lattice's (BGK beside TRT, say).  Out of line: one copy per
+// descriptor and precision serves every kernel, and only those cells pay for the call.
+template <int Q, typename R>
+__device__ __noinline__ void collide_kind(int dyn, R (&f)[Q], const CollisionParams<R>& p, R& rho, R& usq) {
+  switch (dyn) {
+    case DYN_TRT: collide<Q, R, DYN_TRT>(f, p, rho, usq); break;
+    case DYN_SMAGORINSKY: collide<Q, R, DYN_SMAGORINSKY>(f, p, rho, usq); break;
+    case DYN_FORCED_BGK: collide<Q, R, DYN_FORCED_BGK>(f, p, rho, usq); break;
+    case DYN_FORCED_SMAGORINSKY: collide<Q, R, DYN_FORCED_SMAGORINSKY>(f, p, rho, usq); break;
+    default: collide<Q, R, DYN_BGK>(f, p, rho, usq); break;
+  }
+}
 // Class c's parameters by value selects (no indexing into the parameter space).
 template <typename R>
 __device__ __forceinline__ CollisionParams<R> class_params(const ClassParams<R>& cls, int c) {
@@ -276,8 +291,11 @@ __global__ void __launch_bounds__(256) k_collide_stream(S* __restrict__ pop, Geo
     }
     if (bulk_kind(kind)) {
       if (cls.used && kind >= kCellClassFirst) {
-        const CollisionParams<R> pc = class_params(cls, int(kind) - kCellClassFirst);
-        collide<Q, R, DYN>(f, pc, rho, usq);
+        const int c = int(kind) - kCellClassFirst;
+        const CollisionParams<R> pc = class_params(cls, c);
+        const int cd = c == 0 ? cls.dyn[0] : (c == 1 ? cls.dyn[1] : cls.dyn[2]);
+        if (cd == 0 || cd == DYN) collide<Q, R, DYN>(f, pc, rho, usq);
+        else collide_kind<Q, R>(cd, f, pc, rho, usq);
       } else {
         collide<Q, R, DYN>(f, p, rho, usq);
       }
@@ -2246,6 +2264,7 @@ struct LaunchArgs {
   const int32_t* bIdx;      // per padded cell: boundary-list entry (lbx_lattice_s::bIdx)
   int classes;              // parameter classes in use (then the step runs kernel 1)
   double classParam[3][6];  // per class: omega, magic, smagorinsky, force[3]
+  int classDyn[3];          // per class: its dynamics (DYN_*), 0 for the lattice's own
   double* statPart;     // block partials of the statistics (4 doubles per block)
   int64_t statCapacity; // blocks statPart can hold
   int blockX, blockY;
@@ -2452,6 +2471,7 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     if (a.stats && nblocks > a.statCapacity) return cudaErrorInvalidValue;
     ClassParams<R> cls;
     cls.used = a.classes;
+    for (int c = 0; c < 3; ++c) cls.dyn[c] = a.classDyn[c];
     for (int c = 0; c < 3; ++c) {
       cls.p[c] = p;
       cls.p[c].omega = R(a.classParam[c][0]);

@@ -120,6 +120,7 @@ def _load() -> C.CDLL:
         "lbx_set_dynamics": ([VP, I32, P(Params)], C.c_int),
         "lbx_set_cell_dynamics": ([VP, VP], C.c_int),
         "lbx_set_dynamics_class": ([VP, I32, P(Params)], C.c_int),
+        "lbx_set_dynamics_class_kind": ([VP, I32, I32, P(Params)], C.c_int),
         "lbx_set_bouzidi_links": ([VP, I64, VP, VP, VP], C.c_int),
         "lbx_set_bouzidi_from_materials": ([VP, VP, I32, I32, VP, VP], C.c_int),
         "lbx_build_bouzidi_links": ([I32, P(I32), P(I32), VP, I32, I32, VP, VP, I64, VP, VP, VP, P(I64)], C.c_int),
@@ -370,9 +371,12 @@ class BlockLattice:
         self.define_dynamics(self._dyn, **{key: value})
 
     def set_dynamics_class(self, cls: int, omega: float | None = None, magic: float | None = None,
-                           smagorinsky: float | None = None, force=None, remove: bool = False) -> None:
+                           smagorinsky: float | None = None, force=None, remove: bool = False,
+                           dynamics: str | None = None) -> None:
         """Parameters of class `cls` (1..3) of the bulk dynamics (lbx_set_dynamics_class): cells
-        marked CELL_BULK_CLASS_<cls> collide with them; unspecified values are the lattice's."""
+        marked CELL_BULK_CLASS_<cls> collide with them; unspecified values are the lattice's.
+        `dynamics` (a key of DYNAMICS) gives the class a dynamics of its own
+        (lbx_set_dynamics_class_kind)."""
         if remove:
             check(lib.lbx_set_dynamics_class(self._h, cls, None), "lbx_set_dynamics_class")
             return
@@ -386,6 +390,10 @@ class BlockLattice:
             p.smagorinsky = smagorinsky
         if force is not None:
             p.force = (C.c_double * 3)(*(list(force) + [0.0] * 3)[:3])
+        if dynamics is not None:
+            check(lib.lbx_set_dynamics_class_kind(self._h, cls, DYNAMICS[dynamics], C.byref(p)),
+                  "lbx_set_dynamics_class_kind")
+            return
         check(lib.lbx_set_dynamics_class(self._h, cls, C.byref(p)), "lbx_set_dynamics_class")
 
     def set_cell_dynamics(self, ids: np.ndarray | None) -> None:

@@ -82,6 +82,10 @@ typedef struct {
   /* {omega, magic, smagorinsky, force_x, force_y, force_z} of classes 1..3 (read for the
    * LBO_FLUID_CLASS_* cells) */
   const double* class_params;
+  /* Optional (NULL: the case's own dynamics for every class): the dynamics of classes 1..3
+   * (enum lbo_dynamics, -1: the case's own), e.g. TRTdynamics on one material beside
+   * BGKdynamics on another (dynamics::set per material, core/blockDynamicsMap.h:264-310) */
+  const int32_t* class_dynamics;
 } lbo_case;
 
 /* Run `steps` collide-and-stream steps in place.  stats (may be NULL) receives per step

@@ -630,6 +630,8 @@ static int FN(run)(const lbo_case* c, STORE_T* f, int64_t steps, double* stats)
         lbo_case cc = *c;
         if (m != LBO_FLUID) {
           const double* cp = c->class_params + 6 * (m - LBO_FLUID_CLASS_1);
+          if (c->class_dynamics && c->class_dynamics[m - LBO_FLUID_CLASS_1] >= 0)
+            cc.dynamics = c->class_dynamics[m - LBO_FLUID_CLASS_1];
           cc.omega = cp[0];
           cc.magic = cp[1];
           cc.smagorinsky = cp[2];

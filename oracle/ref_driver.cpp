@@ -30,7 +30,7 @@
  *    lbref geo --mat FILE --n NX NY [NZ] [--periodic PX PY [PZ]] [--dyn ...] [--omega W] ...
  *          [--bouzidi M,...] [--lid M --ulid U] [--bounceback M,...] [--outside M,...]
  *          [--ivel M,... (--poiseuille UMAX | --uconst UX UY [UZ])] [--ivel-lid M] [--ipres M --rho R]
- *          [--bbvel M] [--local] [--local-rlb] [--bgk-mat M]
+ *          [--bbvel M] [--local] [--local-rlb] [--bgk-mat M] [--trt-mat M]
  *          [--classify M] [--classify-only] [--force-mat M --force-every K] [--moments]
  *          [--no-pops] [--steps S] [--out PREFIX]
  *  The geo case reads the int32 materials of the core cells from FILE (x slowest, z fastest)
@@ -150,6 +150,7 @@ struct Options {
   bool local = false;  // --local: LocalVelocity / LocalPressure (BGK mixin) instead of the interpolated ones
   bool localRlb = false;  // --local-rlb: the same with their default RLB mixin
   int bgkMat = -1;     // --bgk-mat M: BGKdynamics on material M beside the --dyn dynamics on material 1
+  int trtMat = -1;     // --trt-mat M: TRTdynamics on material M beside the --dyn dynamics on material 1
 };
 
 std::vector<int> parseList(const char* s) {
@@ -242,6 +243,7 @@ Options parse(int argc, char** argv) {
     else if (a == "--local") o.local = true;
     else if (a == "--local-rlb") o.local = o.localRlb = true;
     else if (a == "--bgk-mat") o.bgkMat = std::atoi(next());
+    else if (a == "--trt-mat") o.trtMat = std::atoi(next());
     else if (a == "--ipres") o.ipresMat = std::atoi(next());
     else if (a == "--poiseuille") o.poiseuille = std::atof(next());
     else if (a == "--uconst") { for (int d = 0; d < D; ++d) o.uconst[d] = std::atof(next()); }
@@ -359,6 +361,7 @@ int runGeo(const Options& o) {
   // a second fluid dynamics on one material (a block with two dynamics, as an application sets
   // them per material with dynamics::set)
   if (o.bgkMat >= 0) lat.template defineDynamics<BGKdynamics<T,DESCRIPTOR>>(geo, o.bgkMat);
+  if (o.trtMat >= 0) lat.template defineDynamics<TRTdynamics<T,DESCRIPTOR>>(geo, o.trtMat);
 
   Nowhere<D> nowhere;
   if (o.lidMat >= 0) {
@@ -428,7 +431,7 @@ int runGeo(const Options& o) {
   }
 
   lat.template setParameter<descriptors::OMEGA>(T(o.omega));
-  if (o.dyn == "trt") lat.template setParameter<collision::TRT::MAGIC>(T(o.magic));
+  if (o.dyn == "trt" || o.trtMat >= 0) lat.template setParameter<collision::TRT::MAGIC>(T(o.magic));
   if (o.dyn == "smag" || o.dyn == "fsmag") lat.template setParameter<collision::LES::SMAGORINSKY>(T(o.cs));
 
   // imposed values: values[4 * c ...] = velocity (inlet) or {rho, 0, 0, 0} (outlet)
@@ -452,7 +455,8 @@ int runGeo(const Options& o) {
         cell.template setField<FORCE>(fv);
       }
 #endif
-      if (o.init == "random" && (mat[c] == 1 || isIvel(mat[c]) || mat[c] == o.ipresMat || mat[c] == o.bgkMat)) {
+      if (o.init == "random" && (mat[c] == 1 || isIvel(mat[c]) || mat[c] == o.ipresMat || mat[c] == o.bgkMat ||
+                                 mat[c] == o.trtMat)) {
         T rho = T(1.0 + o.amp * (unit(o.seed, c, 60) - 0.5));
         T u[D] = {};
         for (int d = 0; d < D; ++d) u[d] = T(o.u0 * (unit(o.seed, c, 61 + d) - 0.5));

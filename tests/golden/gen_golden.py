@@ -269,6 +269,14 @@ GEO = {
     "geo_two_dyn_d3q19_fbgk_bgk_f64": ("d3q19_f64_nocse", (12, 10, 9), ["--dyn", "fbgk", "--omega", "1.3", "--force",
                                                                         "1e-4", "2e-5", "0", "--periodic", "1", "1",
                                                                         "1", "--bgk-mat", "6", *RND, "--steps", "40"]),
+    # two fluid dynamics of different kinds in one block: BGK on material 1, TRT on material 6;
+    # and TRT on 1 with BGK on 6
+    "geo_two_dyn_d3q19_bgk_trt_f64": ("d3q19_f64_nocse", (12, 10, 9), ["--dyn", "bgk", "--omega", "1.3", "--magic",
+                                                                       "0.1", "--periodic", "1", "1", "1",
+                                                                       "--trt-mat", "6", *RND, "--steps", "40"]),
+    "geo_two_dyn_d2q9_trt_bgk_f64": ("d2q9_f64_nocse", (16, 14), ["--dyn", "trt", "--omega", "1.6", "--magic", "0.3",
+                                                                  "--periodic", "1", "1", "--bgk-mat", "6", *RND,
+                                                                  "--steps", "60"]),
     "geo_two_dyn_d2q9_fbgk_bgk_f64": ("d2q9_f64_nocse", (16, 14), ["--dyn", "fbgk", "--omega", "1.6", "--force",
                                                                    "1e-4", "-3e-5", "--periodic", "1", "1",
                                                                    "--bgk-mat", "6", *RND, "--steps", "60"]),

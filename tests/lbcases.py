@@ -149,11 +149,16 @@ def case_setup(fx: dict) -> dict:
         for m in a["bbvel"]:
             cd[mat == m] = 4
         if a["bgk_mat"] is not None:
-            # the second fluid dynamics: BGK beside ForcedBGK is the forced dynamics with a zero
-            # force, parameter class 1 (cell id 8)
+            # the second fluid dynamics, parameter class 1 (cell id 8): BGK beside ForcedBGK is the
+            # forced dynamics with a zero force; beside another kind it is BGK itself
             cd[mat == a["bgk_mat"]] = 8
             setup["classes"] = {1: {"omega": meta["omega"], "magic": meta["magic"], "cs": meta["cs"],
-                                    "force": [0.0, 0.0, 0.0]}}
+                                    "force": [0.0, 0.0, 0.0],
+                                    "dyn": None if meta["dyn"] in ("bgk", "fbgk") else "bgk"}}
+        if a["trt_mat"] is not None:
+            cd[mat == a["trt_mat"]] = 8
+            setup["classes"] = {1: {"omega": meta["omega"], "magic": meta["magic"], "cs": meta["cs"],
+                                    "force": [0.0, 0.0, 0.0], "dyn": None if meta["dyn"] == "trt" else "trt"}}
         if a["bbvel"]:
             cells = np.nonzero(np.isin(mat, a["bbvel"]))[0].astype(np.int64)
             setup["bbv"] = {"cells": cells, "rho": np.ascontiguousarray(fx["vals"][cells, 0]),
@@ -194,6 +199,7 @@ def geo_args(meta: dict) -> dict:
             "bbvel": ints("--bbvel"), "local": "--local" in args or "--local-rlb" in args,
             "rlb": "--local-rlb" in args,
             "bgk_mat": int(value("--bgk-mat")) if value("--bgk-mat") else None,
+            "trt_mat": int(value("--trt-mat")) if value("--trt-mat") else None,
             "force_mat": ints("--force-mat")}
 
 
@@ -215,7 +221,7 @@ class _Case(C.Structure):
                 ("link_wall", C.c_void_p), ("n_fd", C.c_int64), ("fd_cell", C.c_void_p),
                 ("fd_kind", C.c_void_p), ("fd_dir", C.c_void_p), ("fd_orient", C.c_void_p),
                 ("fd_value", C.c_void_p), ("fd_type", C.c_void_p), ("fd_normal", C.c_void_p),
-                ("bbv_value", C.c_void_p), ("class_params", C.c_void_p)]
+                ("bbv_value", C.c_void_p), ("class_params", C.c_void_p), ("class_dynamics", C.c_void_p)]
 
 
 _oracle = None
@@ -284,10 +290,14 @@ def run_oracle(setup: dict, f: np.ndarray, steps: int, dtype=np.float64, storage
         c.bbv_value = bv.ctypes.data
     if setup.get("classes"):
         cp = np.zeros((3, 6))
+        cdyn = np.full(3, -1, np.int32)
         for k, prm in setup["classes"].items():
             cp[k - 1] = [prm["omega"], prm["magic"], prm["cs"], *list(prm["force"])[:3]]
-        keep.append(cp)
+            if prm.get("dyn"):
+                cdyn[k - 1] = DYN_CODE[prm["dyn"]]
+        keep += [cp, cdyn]
         c.class_params = cp.ctypes.data
+        c.class_dynamics = cdyn.ctypes.data
     if setup["links"] is not None:
         cells, dirs, wall = (np.ascontiguousarray(a) for a in setup["links"])
         keep += [cells, dirs, wall]
@@ -346,9 +356,9 @@ def fluid_mask(fx: dict) -> np.ndarray:
         return np.isin(fx["mat"], (1, 3, 4))
     if fx["meta"]["case"] == "geo":
         m = fx["mat"] == 1
-        bgk = geo_args(fx["meta"])["bgk_mat"]
-        if bgk is not None:
-            m |= fx["mat"] == bgk
+        for second in (geo_args(fx["meta"])["bgk_mat"], geo_args(fx["meta"])["trt_mat"]):
+            if second is not None:
+                m |= fx["mat"] == second
         if "bclass" in fx:
             m[fx["bclass"][:, 0]] = True
         m[local_flat_cells(fx)] = False

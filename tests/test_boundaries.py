@@ -136,8 +136,12 @@ def build_from_materials(fx, storage):
     for m in a["bounceback"]:
         cd[mat == m] = 2
     if a["bgk_mat"] is not None:  # BGK beside ForcedBGK: the forced dynamics with force 0
-        lat.set_dynamics_class(1, force=(0.0, 0.0, 0.0))
+        other = None if meta["dyn"] in ("bgk", "fbgk") else "bgk"
+        lat.set_dynamics_class(1, force=(0.0, 0.0, 0.0), dynamics=other)
         cd[mat == a["bgk_mat"]] = lbx.CELL_BULK_CLASS_1
+    if a["trt_mat"] is not None:  # TRT beside another kind: a class of its own dynamics
+        lat.set_dynamics_class(1, dynamics=None if meta["dyn"] == "trt" else "trt")
+        cd[mat == a["trt_mat"]] = lbx.CELL_BULK_CLASS_1
     lat.set_cell_dynamics(cd)
     solid = list(a["bouzidi"]) + ([a["lid"]] if a["lid"] is not None else [])
     if solid:

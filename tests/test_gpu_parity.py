@@ -28,7 +28,8 @@ def make_lattice(setup: dict, storage: str) -> lbx.BlockLattice:
     lat.define_dynamics(L.GPU_DYN[setup["dyn"]], omega=setup["omega"], magic=setup["magic"],
                         smagorinsky=setup["cs"], force=setup["force"])
     for k, prm in (setup.get("classes") or {}).items():
-        lat.set_dynamics_class(k, omega=prm["omega"], magic=prm["magic"], smagorinsky=prm["cs"], force=prm["force"])
+        lat.set_dynamics_class(k, omega=prm["omega"], magic=prm["magic"], smagorinsky=prm["cs"], force=prm["force"],
+                               dynamics=L.GPU_DYN[prm["dyn"]] if prm.get("dyn") else None)
     if setup["cell_dyn"] is not None:
         # boundary cells (ids 3 and 4) are marked by their own setters below
         cd = setup["cell_dyn"]
