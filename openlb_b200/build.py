@@ -24,7 +24,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "lib" / "liblbx.so"
 INCLUDE = PKG.parent / "include"
 PLATFORM = PKG / "platform"
-HOST_EXAMPLES = {"cavity3d": PLATFORM / "cavity3d.cpp"}
+HOST_EXAMPLES = {"cavity3d": PLATFORM / "cavity3d.cpp", "cavity2d": PLATFORM / "cavity2d.cpp"}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

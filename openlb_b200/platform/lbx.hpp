@@ -55,6 +55,19 @@ struct SmagorinskyBGKdynamics { static constexpr int id = LBX_SMAGORINSKY_BGK; }
 struct ForcedBGKdynamics { static constexpr int id = LBX_FORCED_BGK; };
 struct SmagorinskyForcedBGKdynamics { static constexpr int id = LBX_SMAGORINSKY_FORCED_BGK; };
 struct ConstRhoBGKdynamics { static constexpr int id = LBX_CONST_RHO_BGK; };
+// cell kinds without a fluid dynamics (defineDynamics over a material)
+struct NoDynamics { static constexpr int id = -LBX_CELL_NONE - 1; };
+struct BounceBack { static constexpr int id = -LBX_CELL_BOUNCE_BACK - 1; };
+
+// boundary::set<...> kinds over a material (lbx_set_interpolated_boundary)
+enum class BoundaryKind : int32_t {
+  InterpolatedVelocity = LBX_FD_VELOCITY,
+  InterpolatedPressure = LBX_FD_PRESSURE,
+  LocalVelocityBGK = LBX_FD_LOCAL_VELOCITY,
+  LocalPressureBGK = LBX_FD_LOCAL_PRESSURE,
+  LocalVelocity = LBX_FD_LOCAL_VELOCITY_RLB,
+  LocalPressure = LBX_FD_LOCAL_PRESSURE_RLB,
+};
 
 // ---- parameters (descriptors::OMEGA, collision::TRT::MAGIC, collision::LES::SMAGORINSKY) ------
 struct OMEGA {};
@@ -105,7 +118,11 @@ class BlockLattice {
   }
   BlockLattice(const BlockLattice&) = delete;
   BlockLattice& operator=(const BlockLattice&) = delete;
-  BlockLattice(BlockLattice&& o) noexcept : h_(std::exchange(o.h_, nullptr)), core_(o.core_), dyn_(o.dyn_), params_(o.params_) {}
+  BlockLattice(BlockLattice&& o) noexcept
+      : h_(std::exchange(o.h_, nullptr)), core_(o.core_), dyn_(o.dyn_), params_(o.params_),
+        fluidDefined_(o.fluidDefined_), cellMap_(std::move(o.cellMap_)) {
+    for (int c = 0; c < 3; ++c) classDyn_[c] = o.classDyn_[c];
+  }
 
   lbx_lattice handle() const { return h_; }
   int64_t coreCells() const { return int64_t(core_[0]) * core_[1] * core_[2]; }
@@ -124,13 +141,62 @@ class BlockLattice {
     else if constexpr (std::is_same_v<PARAM, MAGIC>) params_.magic = v;
     else if constexpr (std::is_same_v<PARAM, SMAGORINSKY>) params_.smagorinsky = v;
     else static_assert(sizeof(PARAM) == 0, "unknown scalar parameter");
-    check(lbx_set_dynamics(h_, dyn_, &params_), "lbx_set_dynamics");
+    applyParameters();
   }
   template <typename PARAM>
   void setParameter(std::array<double, 3> v) {
     static_assert(std::is_same_v<PARAM, FORCE>, "only FORCE is a vector parameter");
     for (int a = 0; a < 3; ++a) params_.force[a] = v[a];
-    check(lbx_set_dynamics(h_, dyn_, &params_), "lbx_set_dynamics");
+    applyParameters();
+  }
+
+  // defineDynamics<DYNAMICS>(material, m) (SuperLattice::defineDynamics over a material
+  // indicator, core/superLattice.hh): the cells of material m get DYNAMICS.  The first fluid
+  // dynamics becomes the lattice's; another kind becomes a parameter class of its own
+  // (lbx_set_dynamics_class_kind, at most three); NoDynamics and BounceBack mark the cells.
+  // Parameters are shared by every dynamics, as the reference's setParameter sets them.
+  template <typename DYN>
+  void defineDynamics(const std::vector<int32_t>& material, int32_t m) {
+    if (int64_t(material.size()) != coreCells()) throw std::invalid_argument("material map must cover the core cells");
+    if (cellMap_.empty()) cellMap_.assign(size_t(coreCells()), uint8_t(LBX_CELL_NONE));
+    uint8_t id;
+    if constexpr (DYN::id < 0) {
+      id = uint8_t(-DYN::id - 1);
+    } else {
+      if (!fluidDefined_) {
+        dyn_ = DYN::id;
+        fluidDefined_ = true;
+        check(lbx_set_dynamics(h_, dyn_, &params_), "lbx_set_dynamics");
+      }
+      id = LBX_CELL_BULK;
+      if (DYN::id != dyn_) {
+        int cls = 0;
+        for (int c = 0; c < 3; ++c)
+          if (classDyn_[c] == DYN::id || (cls == 0 && classDyn_[c] == 0)) {
+            cls = c + 1;
+            if (classDyn_[c] == DYN::id) break;
+          }
+        if (cls == 0) throw std::domain_error("more than four fluid dynamics in one block");
+        classDyn_[cls - 1] = DYN::id;
+        check(lbx_set_dynamics_class_kind(h_, cls, DYN::id, &params_), "lbx_set_dynamics_class_kind");
+        id = uint8_t(LBX_CELL_BULK_CLASS_1 + cls - 1);
+      }
+    }
+    for (size_t c = 0; c < material.size(); ++c)
+      if (material[c] == m) cellMap_[c] = id;
+    check(lbx_set_cell_dynamics(h_, cellMap_.data()), "lbx_set_cell_dynamics");
+  }
+
+  // boundary::set<KIND>(lattice, geometry, m) with the default fluid (1) and outside (0)
+  // materials (boundary/setBoundary.h:112-121), then the values an application gives with
+  // setVelocity / defineRho: values[4 c ...] = velocity, or {rho, tangential velocity}, of core
+  // cell c (only the boundary cells' entries are read).
+  void setBoundary(BoundaryKind kind, const std::vector<int32_t>& material, int32_t m,
+                   const std::vector<double>& values) {
+    if (int64_t(material.size()) != coreCells() || int64_t(values.size()) != 4 * coreCells())
+      throw std::invalid_argument("material [cells] and values [4 * cells]");
+    check(lbx_set_interpolated_boundary(h_, int32_t(kind), material.data(), m, 0, nullptr, 0, nullptr, values.data()),
+          "lbx_set_interpolated_boundary");
   }
 
   void setCellDynamics(const std::vector<CellDynamics>& ids) {
@@ -238,10 +304,20 @@ class BlockLattice {
   }
 
  private:
+  void applyParameters() {
+    check(lbx_set_dynamics(h_, dyn_, &params_), "lbx_set_dynamics");
+    for (int c = 0; c < 3; ++c)
+      if (classDyn_[c] != 0)
+        check(lbx_set_dynamics_class_kind(h_, c + 1, classDyn_[c], &params_), "lbx_set_dynamics_class_kind");
+  }
+
   lbx_lattice h_ = nullptr;
   std::array<int, 3> core_;
   int dyn_ = LBX_BGK;
   lbx_params params_{};
+  bool fluidDefined_ = false;
+  int classDyn_[3] = {0, 0, 0};      // the dynamics of parameter classes 1..3 (0: unused)
+  std::vector<uint8_t> cellMap_;   // per core cell: lbx_cell_dynamics (defineDynamics over materials)
 };
 
 }  // namespace lbx

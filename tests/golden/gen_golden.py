@@ -171,6 +171,11 @@ GEO = {
     # the lid the top row including its corners
     "geo_cavity_d2q9_ivel_bgk_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
                                                                   "--ivel-lid", "3", "--ulid", "0.1", "--steps", "150"]),
+    # the same set-up from rest, as examples/laminar/cavity2d starts it (the C++ example
+    # openlb_b200/platform/cavity2d.cpp runs it through the C++ host layer)
+    "geo_cavity2d_d2q9_ivel_bgk_rest_f64": ("d2q9_f64_nocse", (34, 34), ["--dyn", "bgk", "--omega", "1.6", "--ivel",
+                                                                         "2", "--ivel-lid", "3", "--ulid", "0.1",
+                                                                         "--init", "rest", "--steps", "400"]),
     "geo_cavity_d2q9_ivel_bgk_f32": ("d2q9_f32", (14, 12), ["--dyn", "bgk", "--omega", "1.3", "--ivel", "2",
                                                             "--ivel-lid", "3", "--ulid", "0.1", "--steps", "150"]),
     "geo_cavity_d2q9_ivel_constrho_f64": ("d2q9_f64_nocse", (14, 12), ["--dyn", "constrho", "--omega", "1.3",

@@ -57,3 +57,35 @@ def test_example_equals_the_python_binding(storage, arg):
     assert got["max_u"] == st["max_u"]
     assert got["mass"] == mass
     assert 0 < got["max_u"] < 0.1
+
+
+EXE2 = Path(lbx.LIB_PATH).parent / "cavity2d"
+
+
+def test_cavity2d_example_is_built_and_fails_loudly_without_a_device():
+    assert EXE2.exists(), "run python -m openlb_b200.build"
+    if lbx.device_count() > 0:
+        pytest.skip("a device is present")
+    proc = subprocess.run([str(EXE2), "14", "12", "2"], capture_output=True, text=True, timeout=120)
+    assert proc.returncode == 1
+    assert "lbx_lattice_create" in proc.stderr
+
+
+@pytest.mark.gpu
+def test_cavity2d_example_matches_the_reference():
+    """cavity2d's set-up through the C++ layer -- defineDynamics<BGK> over material 1,
+    boundary::set<InterpolatedVelocity> over the walls (2) and the lid (3, corners included),
+    iniEquilibrium at rest, initialize() -- against the reference's own run of that set-up (the
+    fixture geo_cavity2d_d2q9_ivel_bgk_rest_f64: 34 x 34, omega 1.6, lid 0.1, 400 steps)."""
+    import lbcases as L
+    fx = L.load_fixture("geo_cavity2d_d2q9_ivel_bgk_rest_f64")
+    meta = fx["meta"]
+    proc = subprocess.run([str(EXE2), "34", "34", str(meta["steps"]), "f64", repr(meta["omega"]), repr(meta["ulid"])],
+                          capture_output=True, text=True, timeout=300)
+    assert proc.returncode == 0, proc.stderr
+    got = json.loads(proc.stdout.strip().splitlines()[-1])
+    ref = fx["stats"][-1]
+    assert got["cells"] == L.counted_cells(fx)
+    assert abs(got["average_rho"] - ref[0]) <= 1e-12 * abs(ref[0])
+    assert abs(got["average_energy"] - ref[1]) <= 1e-12 * abs(ref[1])
+    assert abs(got["max_u"] - ref[2]) <= 1e-12 * abs(ref[2])
