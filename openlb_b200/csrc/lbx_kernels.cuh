@@ -17,6 +17,7 @@
 // step is a single launch.
 #pragma once
 
+#include <atomic>
 #include <cstring>
 #include <type_traits>
 
@@ -2297,23 +2298,23 @@ inline int64_t fd_blocks(int64_t nFd) { return (nFd + 255) / 256; }
 
 // How far ahead in launch order the step kernel prefetches into L2: one wave of resident blocks
 // (the block that takes over a finishing block's SM).  `cache` belongs to one kernel: per device,
-// the block size it was computed for and the resident blocks.
+// the block size it was computed for (high 32 bits) and the resident blocks (low 32 bits) in one
+// atomic word, so host threads launching at once read a consistent pair.
 template <typename F>
-int l2_ahead_blocks(F kern, int threads, int (&cache)[64][2]) {
+int l2_ahead_blocks(F kern, int threads, std::atomic<uint64_t> (&cache)[64]) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-  int* c = cache[dev & 63];
-  if (c[0] != threads) {
-    int perSM = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, 0) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
-      cudaGetLastError();
-      return 0;
-    }
-    c[1] = perSM * sms;
-    c[0] = threads;
+  const uint64_t v = cache[dev & 63].load(std::memory_order_relaxed);
+  if (uint32_t(v >> 32) == uint32_t(threads)) return int(uint32_t(v));
+  int perSM = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, threads, 0) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
   }
-  return c[1];
+  const int blocks = perSM * sms;
+  cache[dev & 63].store((uint64_t(uint32_t(threads)) << 32) | uint32_t(blocks), std::memory_order_relaxed);
+  return blocks;
 }
 
 template <int Q, typename S>
@@ -2500,7 +2501,7 @@ cudaError_t launch_step_dyn(const LaunchArgs& a, cudaStream_t stream) {
     auto go = [&](auto kk, auto doubled, auto mapped) {
       auto kern =
           k_collide_stream_groups<Q, S, DYN, decltype(kk)::value, decltype(doubled)::value, decltype(mapped)::value>;
-      static int aheadCache[64][2] = {};  // one per instantiation of this lambda, i.e. per kernel
+      static std::atomic<uint64_t> aheadCache[64] = {};  // one per instantiation of this lambda, i.e. per kernel
       int ahead = 0;
       if constexpr (decltype(doubled)::value)
         if (a.kernel == 5) ahead = l2_ahead_blocks(kern, int(block.x * block.y), aheadCache);
