@@ -49,8 +49,9 @@ typedef enum { LBX_D2Q9 = 9, LBX_D3Q19 = 19, LBX_D3Q27 = 27 } lbx_descriptor;
  * collision in float registers; reductions are FP64 in every form. */
 typedef enum { LBX_F64 = 0, LBX_F32 = 1, LBX_F16DEV = 2, LBX_BF16DEV = 3 } lbx_storage;
 
-/* Bulk dynamics of a lattice (one per lattice; the per-cell map below selects it, plain
- * bounce-back or no dynamics per cell). */
+/* Bulk dynamics of a lattice (the lattice's own; the per-cell map below selects it, plain
+ * bounce-back, no dynamics or one of up to three parameter classes per cell, and a class may
+ * carry another of these dynamics, lbx_set_dynamics_class_kind). */
 typedef enum {
   LBX_BGK = 1,                   /* BGKdynamics            dynamics/dynamics.h:89-99 */
   LBX_TRT = 2,                   /* TRTdynamics            dynamics/dynamics.h:529-536 */
